@@ -1,0 +1,106 @@
+/* sdft_b200: B200-native generalized Davidson hot path of Sparse-DFT behind a C ABI.
+ *
+ * Plain pointers and sizes only. Complex arrays are interleaved (re, im)
+ * doubles; blocks are column-major with leading dimension = rows unless a
+ * leading dimension is passed. Every call returns an sdft_b200_status; the
+ * text of the last failure on the calling thread is read with
+ * sdft_b200_last_error. No exception crosses this boundary.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the Sparse-DFT source tree).
+ */
+#ifndef SDFT_B200_H
+#define SDFT_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SDFT_B200_API __attribute__((visibility("default")))
+#else
+#define SDFT_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SDFT_B200_OK = 0,
+  SDFT_B200_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  SDFT_B200_OVERFLOW = 2,         /* std::overflow_error */
+  SDFT_B200_RUNTIME_ERROR = 3,    /* std::runtime_error (numerical failure) */
+  SDFT_B200_CUDA_ERROR = 4,       /* runtime_error("CUDA: ...") / cuBLAS / cuSOLVER */
+  SDFT_B200_OUT_OF_MEMORY = 5,    /* std::bad_alloc */
+  SDFT_B200_NONFINITE = 6         /* runtime_error on a nonfinite operator result */
+} sdft_b200_status;
+
+enum { SDFT_B200_PRECISION_FP64 = 0, SDFT_B200_PRECISION_MIXED = 1 };
+enum { SDFT_B200_MEMORY_HOST = 0, SDFT_B200_MEMORY_DEVICE = 1 };
+enum { SDFT_B200_HAMILTONIAN = 0, SDFT_B200_OVERLAP = 1 };
+
+typedef struct sdft_b200_context sdft_b200_context;
+typedef struct sdft_b200_operator sdft_b200_operator;
+
+/* Copies the calling thread's last error message; returns its full length. */
+SDFT_B200_API size_t sdft_b200_last_error(char* buffer, size_t length);
+/* Library version string (static storage). */
+SDFT_B200_API const char* sdft_b200_version(void);
+
+/* One CUDA stream + library handles on `device`. `stream` may be NULL (a
+ * private non-blocking stream is created) or a cudaStream_t to share.
+ * Replaces: make_cuda_accelerator() / class Accelerator, src/compute_backend.hpp:64-91. */
+SDFT_B200_API sdft_b200_status sdft_b200_context_create(int device, void* stream, sdft_b200_context** out);
+SDFT_B200_API sdft_b200_status sdft_b200_context_destroy(sdft_b200_context* context);
+SDFT_B200_API sdft_b200_status sdft_b200_context_synchronize(sdft_b200_context* context);
+
+/* Plane-wave sphere 1/2|G+k|^2 <= cutoff_ev, sorted by (kinetic, h, k, l);
+ * reciprocal rows are b1, b2, b3. Call with capacity 0 to get *count first.
+ * Replaces: enumerate_g_vectors, src/pw_core.hpp:17-19 (src/pw_core.cpp:140-171). */
+SDFT_B200_API sdft_b200_status sdft_b200_enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
+                                               double hartree_to_ev, int32_t* hkl, double* cartesian,
+                                               double* kinetic_ev, size_t capacity, size_t* count);
+
+/* Device-resident H~ = T + V(r) + sum_a B_a^H D_a B_a and
+ * S~ = (1+regularization) I + sum_a B_a^H Q_a B_a.
+ * hkl: npw x 3 basis indices; kinetic_ev: 1/2|G+k|^2 in eV; potential: V(G)
+ * (Hartree) on potential_count keys; per atom a: projectors[a] rows of
+ * amplitudes (row-major np_a x npw), D_a and Q_a (row-major np_a x np_a).
+ * Replaces: PlaneWaveOperator::PlaneWaveOperator, src/plane_wave_operator.hpp:27-30. */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_create(sdft_b200_context* context, size_t npw, const int32_t* hkl,
+                                           const double* kinetic_ev, size_t potential_count,
+                                           const int32_t* potential_hkl, const double* potential, size_t atoms,
+                                           const uint64_t* projectors, const double* amplitudes, const double* d,
+                                           const double* q, double hartree_to_ev, double regularization,
+                                           sdft_b200_operator** out);
+SDFT_B200_API sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op);
+
+/* Grid shape, grid points and total projector rows.
+ * Replaces: PlaneWaveOperator::fft_grid_points, src/plane_wave_operator.hpp:38. */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t shape[3], size_t* grid_points,
+                                         size_t* projectors, size_t* npw);
+/* Sphere-to-grid index map (npw values), T (Hartree), H and S diagonals
+ * (npw each), V(r) (grid_points values); any pointer may be NULL.
+ * Replaces: the Impl members indices/kinetic/h_diagonal/s_diagonal/local_real,
+ * src/plane_wave_operator.cpp:33-34. */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_arrays(const sdft_b200_operator* op, uint64_t* indices, double* kinetic,
+                                           double* h_diagonal, double* s_diagonal, double* local_potential);
+
+/* y = H~ x or S~ x for `columns` columns (npw x columns). memory selects host
+ * or device pointers; host calls are synchronous.
+ * Replaces: HermitianOperator::apply_block_into, src/pw_core.hpp:116-117
+ * (Impl::apply_block_into, src/plane_wave_operator.cpp:218-306). */
+SDFT_B200_API sdft_b200_status sdft_b200_apply(sdft_b200_operator* op, int which, const double* x, size_t columns, double* y,
+                                 int precision, int memory);
+/* Joint (H~x, S~x) sharing one B x.
+ * Replaces: HermitianOperator::apply_pair_into, src/pw_core.hpp:122-124 (src/plane_wave_operator.cpp:307-374). */
+SDFT_B200_API sdft_b200_status sdft_b200_apply_pair(sdft_b200_operator* op, const double* x, size_t columns, double* hy,
+                                      double* sy, int precision, int memory);
+/* P = B x (projectors x columns).
+ * Replaces: HermitianOperator::project_into, src/pw_core.hpp:130-131 (src/plane_wave_operator.cpp:375-380). */
+SDFT_B200_API sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size_t columns, double* p,
+                                   int precision, int memory);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

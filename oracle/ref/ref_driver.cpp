@@ -1,0 +1,259 @@
+// C entry points over the reference's own C++ API, so that Python tests can
+// call the unmodified reference code (built with the shims beside this file)
+// as an oracle. Test infrastructure only: nothing in the product links this.
+//
+// Each function converts flat arrays into the reference's types and calls:
+//   enumerate_g_vectors                 src/pw_core.cpp:140-171
+//   PlaneWaveOperator ctor              src/plane_wave_operator.cpp:393-516
+//   hamiltonian()/overlap() callbacks   src/plane_wave_operator.cpp:672-719
+//   solve_generalized_hermitian_davidson src/pw_core.cpp:532-1437
+//   kinetic_preconditioner              src/pw_core.cpp:33-47
+//   save/load_solver_snapshot           src/plane_wave_operator.cpp:542-653
+//   plane_wave_density_fft              src/density_functionals.cpp:407-460
+//   pbe_unpolarized                     src/pbe_xc.cpp:116-140
+// Complex arrays are interleaved (re, im) doubles, column-major blocks.
+#include "plane_wave_operator.hpp"
+#include "pw_core.hpp"
+#include "compute_backend.hpp"
+#include "density_functionals.hpp"
+#include "pbe_xc.hpp"
+#include "env_cache.hpp"
+
+#include <algorithm>
+#include <complex>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+using C = std::complex<double>;
+
+void set_error(char* buffer, long length, const std::exception& e) {
+  if (!buffer || length <= 0) return;
+  std::string text = std::string(typeid(e).name()) + ": " + e.what();
+  const auto count = std::min<std::size_t>(text.size(), static_cast<std::size_t>(length - 1));
+  std::memcpy(buffer, text.data(), count);
+  buffer[count] = 0;
+}
+
+struct Handle {
+  std::unique_ptr<sdft::PlaneWaveOperator> op;
+};
+}  // namespace
+
+extern "C" {
+
+long ref_enumerate_g_vectors(const double* reciprocal, double cutoff_ev, const double* kpoint,
+                             double hartree_to_ev, int* hkl, double* cartesian,
+                             double* kinetic_ev, long capacity) {
+  std::array<sdft::Vec3, 3> recip{};
+  for (int a = 0; a < 3; ++a) recip[a] = {reciprocal[3 * a], reciprocal[3 * a + 1], reciprocal[3 * a + 2]};
+  const sdft::Vec3 k{kpoint[0], kpoint[1], kpoint[2]};
+  const auto g = sdft::enumerate_g_vectors(recip, cutoff_ev, k, hartree_to_ev);
+  if (hkl && static_cast<long>(g.size()) <= capacity) {
+    for (std::size_t i = 0; i < g.size(); ++i) {
+      hkl[3 * i] = g[i].h;
+      hkl[3 * i + 1] = g[i].k;
+      hkl[3 * i + 2] = g[i].l;
+      cartesian[3 * i] = g[i].cartesian.x;
+      cartesian[3 * i + 1] = g[i].cartesian.y;
+      cartesian[3 * i + 2] = g[i].cartesian.z;
+      kinetic_ev[i] = g[i].kinetic_ev;
+    }
+  }
+  return static_cast<long>(g.size());
+}
+
+void* ref_operator_create(long n, const int* hkl, const double* cartesian, const double* kinetic_ev,
+                          long nv, const int* v_hkl, const double* v_values, long atoms,
+                          const long* projectors, const double* amplitudes, const double* d,
+                          const double* q, double hartree_to_ev, double regularization,
+                          unsigned long long projector_identity, char* error, long error_length) {
+  try {
+    std::vector<sdft::GVector> basis(static_cast<std::size_t>(n));
+    for (long i = 0; i < n; ++i)
+      basis[i] = {hkl[3 * i], hkl[3 * i + 1], hkl[3 * i + 2],
+                  {cartesian[3 * i], cartesian[3 * i + 1], cartesian[3 * i + 2]}, kinetic_ev[i]};
+    sdft::FourierDensity potential;
+    for (long i = 0; i < nv; ++i)
+      potential[{v_hkl[3 * i], v_hkl[3 * i + 1], v_hkl[3 * i + 2]}] = C(v_values[2 * i], v_values[2 * i + 1]);
+    std::vector<sdft::ComplexPawOperator> paw;
+    std::size_t amp_offset = 0, block_offset = 0;
+    for (long a = 0; a < atoms; ++a) {
+      sdft::ComplexPawOperator p;
+      p.projectors = static_cast<std::size_t>(projectors[a]);
+      const std::size_t np = p.projectors;
+      p.amplitudes.resize(np * n);
+      for (std::size_t i = 0; i < np * static_cast<std::size_t>(n); ++i)
+        p.amplitudes[i] = C(amplitudes[2 * (amp_offset + i)], amplitudes[2 * (amp_offset + i) + 1]);
+      p.d.resize(np * np);
+      p.q.resize(np * np);
+      for (std::size_t i = 0; i < np * np; ++i) {
+        p.d[i] = C(d[2 * (block_offset + i)], d[2 * (block_offset + i) + 1]);
+        p.q[i] = C(q[2 * (block_offset + i)], q[2 * (block_offset + i) + 1]);
+      }
+      amp_offset += np * n;
+      block_offset += np * np;
+      paw.push_back(std::move(p));
+    }
+    auto handle = std::make_unique<Handle>();
+    handle->op = std::make_unique<sdft::PlaneWaveOperator>(basis, potential, std::move(paw), hartree_to_ev,
+                                                           regularization, projector_identity);
+    return handle.release();
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return nullptr;
+  }
+}
+
+void ref_operator_destroy(void* handle) { delete static_cast<Handle*>(handle); }
+
+long ref_operator_grid(void* handle) { return static_cast<long>(static_cast<Handle*>(handle)->op->fft_grid_points()); }
+
+int ref_apply(void* handle, int overlap, const double* x, long columns, double* y, int exact,
+              char* error, long error_length) {
+  try {
+    auto* h = static_cast<Handle*>(handle);
+    auto op = overlap ? h->op->overlap() : h->op->hamiltonian();
+    op.apply_block_into(reinterpret_cast<const C*>(x), static_cast<std::size_t>(columns),
+                        reinterpret_cast<C*>(y), exact != 0);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+int ref_apply_pair(void* handle, const double* x, long columns, double* hy, double* sy, int exact,
+                   char* error, long error_length) {
+  try {
+    auto* h = static_cast<Handle*>(handle);
+    auto op = h->op->hamiltonian();
+    op.apply_pair_into(reinterpret_cast<const C*>(x), static_cast<std::size_t>(columns),
+                       reinterpret_cast<C*>(hy), reinterpret_cast<C*>(sy), exact != 0);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+int ref_project(void* handle, const double* x, long columns, double* p, char* error, long error_length) {
+  try {
+    auto op = static_cast<Handle*>(handle)->op->hamiltonian();
+    op.project_into(reinterpret_cast<const C*>(x), static_cast<std::size_t>(columns), reinterpret_cast<C*>(p), true);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+long ref_projector_rows(void* handle) {
+  return static_cast<long>(static_cast<Handle*>(handle)->op->hamiltonian().projector_rows);
+}
+
+int ref_davidson(void* handle, long roots, long max_iterations, double tolerance, const double* initial,
+                 double* eigenvalues, double* vectors, double* residuals, int* converged,
+                 long* iterations, char* error, long error_length) {
+  try {
+    auto* h = static_cast<Handle*>(handle);
+    auto ham = h->op->hamiltonian();
+    auto ovl = h->op->overlap();
+    std::vector<C> warm;
+    if (initial) warm.assign(reinterpret_cast<const C*>(initial), reinterpret_cast<const C*>(initial) + roots * ham.dimension);
+    const auto result = sdft::solve_generalized_hermitian_davidson(ham, ovl, static_cast<std::size_t>(roots),
+                                                                   static_cast<std::size_t>(max_iterations), tolerance, warm);
+    std::copy(result.eigenvalues.begin(), result.eigenvalues.end(), eigenvalues);
+    std::copy(result.residual_norms.begin(), result.residual_norms.end(), residuals);
+    std::memcpy(vectors, result.eigenvectors.data(), result.eigenvectors.size() * sizeof(C));
+    *converged = result.converged ? 1 : 0;
+    *iterations = static_cast<long>(result.iterations);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+double ref_kinetic_preconditioner(double kinetic, double wavefunction_kinetic) {
+  return sdft::kinetic_preconditioner(kinetic, wavefunction_kinetic);
+}
+
+int ref_save_snapshot(void* handle, const char* path, long roots, long iterations, double tolerance,
+                      const double* initial, long initial_count, char* error, long error_length) {
+  try {
+    std::vector<C> warm;
+    if (initial && initial_count)
+      warm.assign(reinterpret_cast<const C*>(initial), reinterpret_cast<const C*>(initial) + initial_count);
+    static_cast<Handle*>(handle)->op->save_solver_snapshot(path, static_cast<std::size_t>(roots),
+                                                           static_cast<std::size_t>(iterations), tolerance, warm);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+void* ref_load_snapshot(const char* path, long* roots, long* iterations, double* tolerance,
+                        char* error, long error_length) {
+  try {
+    std::size_t r = 0, it = 0;
+    std::vector<C> initial;
+    auto handle = std::make_unique<Handle>();
+    handle->op = sdft::PlaneWaveOperator::load_solver_snapshot(path, r, it, *tolerance, initial);
+    *roots = static_cast<long>(r);
+    *iterations = static_cast<long>(it);
+    return handle.release();
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return nullptr;
+  }
+}
+
+// Band density on the support keys (h,k,l); output interleaved complex per key.
+int ref_plane_wave_density_fft(long n, const int* hkl, long bands, const double* coefficients,
+                               const double* occupations, double volume, long support_count,
+                               const int* support_hkl, double* density, char* error, long error_length) {
+  try {
+    std::vector<std::tuple<int, int, int>> g(static_cast<std::size_t>(n));
+    for (long i = 0; i < n; ++i) g[i] = {hkl[3 * i], hkl[3 * i + 1], hkl[3 * i + 2]};
+    std::vector<C> coeff(reinterpret_cast<const C*>(coefficients), reinterpret_cast<const C*>(coefficients) + n * bands);
+    std::vector<double> occ(occupations, occupations + bands);
+    sdft::FourierDensity support;
+    for (long i = 0; i < support_count; ++i) support[{support_hkl[3 * i], support_hkl[3 * i + 1], support_hkl[3 * i + 2]}] = C(0, 0);
+    const auto result = sdft::plane_wave_density_fft(g, coeff, occ, volume, support);
+    for (long i = 0; i < support_count; ++i) {
+      const auto found = result.find({support_hkl[3 * i], support_hkl[3 * i + 1], support_hkl[3 * i + 2]});
+      const C v = found == result.end() ? C(0, 0) : found->second;
+      density[2 * i] = v.real();
+      density[2 * i + 1] = v.imag();
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+// Per point: energy_density, energy_per_particle, exchange_energy_density,
+// correlation_energy_density, exchange_potential, correlation_potential,
+// gradient_squared_coefficient.
+void ref_pbe_unpolarized(long count, const double* density, const double* gradient, double* out) {
+  for (long i = 0; i < count; ++i) {
+    const auto p = sdft::pbe_unpolarized(density[i], gradient[i]);
+    double* o = out + 7 * i;
+    o[0] = p.energy_density;
+    o[1] = p.energy_per_particle;
+    o[2] = p.exchange_energy_density;
+    o[3] = p.correlation_energy_density;
+    o[4] = p.exchange_potential;
+    o[5] = p.correlation_potential;
+    o[6] = p.gradient_squared_coefficient;
+  }
+}
+
+void ref_refresh_environment() { sdft::refresh_environment_cache(); }
+}

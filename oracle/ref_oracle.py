@@ -1,0 +1,205 @@
+"""ctypes access to the reference's own CPU implementation (oracle/_ref/libsdft_ref.so).
+
+TEST INFRASTRUCTURE ONLY. This module is the checker: only tests/, the smoke
+check in __graft_entry__ and bench.py's CPU-baseline leg may import it. The
+library is the reference's unmodified src/*.cpp compiled by oracle/ref/Makefile
+against this project's FFTW3-API shim and the OpenBLAS found in the image.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIBRARY = HERE / "_ref" / "libsdft_ref.so"
+REPLAY = HERE / "_ref" / "sdft_solver_replay"
+
+_dbl = ctypes.POINTER(ctypes.c_double)
+_int = ctypes.POINTER(ctypes.c_int)
+_long = ctypes.POINTER(ctypes.c_long)
+
+
+def available() -> bool:
+    return LIBRARY.exists()
+
+
+def _ptr(array, kind=_dbl):
+    return array.ctypes.data_as(kind)
+
+
+class ReferenceLibrary:
+    def __init__(self, path: pathlib.Path = LIBRARY):
+        if not path.exists():
+            raise FileNotFoundError(f"reference oracle library not built: {path} (make -C oracle/ref)")
+        os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        self.lib = ctypes.CDLL(str(path))
+        L = self.lib
+        L.ref_enumerate_g_vectors.restype = ctypes.c_long
+        L.ref_enumerate_g_vectors.argtypes = [_dbl, ctypes.c_double, _dbl, ctypes.c_double, _int, _dbl, _dbl,
+                                              ctypes.c_long]
+        L.ref_operator_create.restype = ctypes.c_void_p
+        L.ref_operator_create.argtypes = [ctypes.c_long, _int, _dbl, _dbl, ctypes.c_long, _int, _dbl,
+                                          ctypes.c_long, _long, _dbl, _dbl, _dbl, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_ulonglong, ctypes.c_char_p, ctypes.c_long]
+        L.ref_operator_destroy.argtypes = [ctypes.c_void_p]
+        L.ref_operator_grid.restype = ctypes.c_long
+        L.ref_operator_grid.argtypes = [ctypes.c_void_p]
+        L.ref_apply.restype = ctypes.c_int
+        L.ref_apply.argtypes = [ctypes.c_void_p, ctypes.c_int, _dbl, ctypes.c_long, _dbl, ctypes.c_int,
+                                ctypes.c_char_p, ctypes.c_long]
+        L.ref_apply_pair.restype = ctypes.c_int
+        L.ref_apply_pair.argtypes = [ctypes.c_void_p, _dbl, ctypes.c_long, _dbl, _dbl, ctypes.c_int,
+                                     ctypes.c_char_p, ctypes.c_long]
+        L.ref_project.restype = ctypes.c_int
+        L.ref_project.argtypes = [ctypes.c_void_p, _dbl, ctypes.c_long, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_projector_rows.restype = ctypes.c_long
+        L.ref_projector_rows.argtypes = [ctypes.c_void_p]
+        L.ref_davidson.restype = ctypes.c_int
+        L.ref_davidson.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl, _dbl,
+                                   _dbl, _int, _long, ctypes.c_char_p, ctypes.c_long]
+        L.ref_kinetic_preconditioner.restype = ctypes.c_double
+        L.ref_kinetic_preconditioner.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.ref_save_snapshot.restype = ctypes.c_int
+        L.ref_save_snapshot.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_long, ctypes.c_long,
+                                        ctypes.c_double, _dbl, ctypes.c_long, ctypes.c_char_p, ctypes.c_long]
+        L.ref_load_snapshot.restype = ctypes.c_void_p
+        L.ref_load_snapshot.argtypes = [ctypes.c_char_p, _long, _long, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_plane_wave_density_fft.restype = ctypes.c_int
+        L.ref_plane_wave_density_fft.argtypes = [ctypes.c_long, _int, ctypes.c_long, _dbl, _dbl, ctypes.c_double,
+                                                 ctypes.c_long, _int, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_pbe_unpolarized.restype = None
+        L.ref_pbe_unpolarized.argtypes = [ctypes.c_long, _dbl, _dbl, _dbl]
+        L.ref_refresh_environment.restype = None
+
+    # -- basis ---------------------------------------------------------------
+    def enumerate_g_vectors(self, reciprocal, cutoff_ev, kpoint=(0.0, 0.0, 0.0), hartree_to_ev=27.211386245988):
+        recip = np.ascontiguousarray(reciprocal, dtype=np.float64).reshape(9)
+        k = np.ascontiguousarray(kpoint, dtype=np.float64)
+        dummy_i = np.zeros(3, dtype=np.int32)
+        dummy_d = np.zeros(3)
+        n = self.lib.ref_enumerate_g_vectors(_ptr(recip), cutoff_ev, _ptr(k), hartree_to_ev, _ptr(dummy_i, _int),
+                                             _ptr(dummy_d), _ptr(dummy_d), 0)
+        hkl = np.zeros((n, 3), dtype=np.int32)
+        cart = np.zeros((n, 3))
+        kin = np.zeros(n)
+        self.lib.ref_enumerate_g_vectors(_ptr(recip), cutoff_ev, _ptr(k), hartree_to_ev, _ptr(hkl, _int),
+                                         _ptr(cart), _ptr(kin), n)
+        return hkl, cart, kin
+
+    def kinetic_preconditioner(self, kinetic, wavefunction_kinetic):
+        return self.lib.ref_kinetic_preconditioner(kinetic, wavefunction_kinetic)
+
+    def pbe(self, density, gradient):
+        n = np.ascontiguousarray(density, dtype=np.float64)
+        g = np.ascontiguousarray(gradient, dtype=np.float64)
+        out = np.zeros((n.size, 7))
+        self.lib.ref_pbe_unpolarized(n.size, _ptr(n), _ptr(g), _ptr(out))
+        return out
+
+    def density(self, hkl, coefficients, occupations, volume, support_hkl):
+        hkl = np.ascontiguousarray(hkl, dtype=np.int32)
+        coeff = np.ascontiguousarray(coefficients, dtype=np.complex128)  # (bands, n) band-major
+        occ = np.ascontiguousarray(occupations, dtype=np.float64)
+        sup = np.ascontiguousarray(support_hkl, dtype=np.int32)
+        out = np.zeros(sup.shape[0], dtype=np.complex128)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.ref_plane_wave_density_fft(hkl.shape[0], _ptr(hkl, _int), occ.size,
+                                                 coeff.view(np.float64).ctypes.data_as(_dbl), _ptr(occ), volume,
+                                                 sup.shape[0], _ptr(sup, _int), out.view(np.float64).ctypes.data_as(_dbl),
+                                                 err, 512)
+        if rc:
+            raise RuntimeError(err.value.decode())
+        return out
+
+
+class ReferenceOperator:
+    """The reference's PlaneWaveOperator built from synthetic OperatorInputs."""
+
+    def __init__(self, lib: ReferenceLibrary, inputs=None, handle=None, projector_identity: int = 0):
+        self.lib = lib
+        if handle is not None:
+            self.handle = handle
+            return
+        x = inputs
+        hkl = np.ascontiguousarray(x.hkl, dtype=np.int32)
+        cart = np.ascontiguousarray(x.cartesian, dtype=np.float64)
+        kin = np.ascontiguousarray(x.kinetic_ev, dtype=np.float64)
+        vh = np.ascontiguousarray(x.v_hkl, dtype=np.int32)
+        vv = np.ascontiguousarray(x.v_values, dtype=np.complex128)
+        proj = np.ascontiguousarray(x.projectors, dtype=np.int64)
+        amp = np.ascontiguousarray(x.amplitudes, dtype=np.complex128)
+        d = np.ascontiguousarray(x.d, dtype=np.complex128)
+        q = np.ascontiguousarray(x.q, dtype=np.complex128)
+        self._keep = (hkl, cart, kin, vh, vv, proj, amp, d, q)
+        err = ctypes.create_string_buffer(1024)
+        self.handle = lib.lib.ref_operator_create(
+            hkl.shape[0], _ptr(hkl, _int), _ptr(cart), _ptr(kin), vh.shape[0], _ptr(vh, _int),
+            vv.view(np.float64).ctypes.data_as(_dbl), proj.size, _ptr(proj, _long),
+            amp.view(np.float64).ctypes.data_as(_dbl), d.view(np.float64).ctypes.data_as(_dbl),
+            q.view(np.float64).ctypes.data_as(_dbl), x.hartree_to_ev, x.regularization, projector_identity, err, 1024)
+        if not self.handle:
+            raise ValueError(err.value.decode())
+        self.n = hkl.shape[0]
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.lib.lib.ref_operator_destroy(self.handle)
+            self.handle = None
+
+    @property
+    def grid_points(self) -> int:
+        return self.lib.lib.ref_operator_grid(self.handle)
+
+    def _call(self, fn, *args):
+        err = ctypes.create_string_buffer(1024)
+        rc = fn(*args, err, 1024)
+        if rc:
+            raise RuntimeError(err.value.decode())
+
+    def apply(self, x, overlap=False, exact=True):
+        """x: (n, cols) complex128 -> H~x or S~x, column-major blocks."""
+        xf = np.asfortranarray(x, dtype=np.complex128)
+        cols = xf.shape[1]
+        y = np.zeros_like(xf, order="F")
+        self._call(self.lib.lib.ref_apply, self.handle, int(overlap), xf.ctypes.data_as(_dbl), cols,
+                   y.ctypes.data_as(_dbl), int(exact))
+        return y
+
+    def apply_pair(self, x, exact=True):
+        xf = np.asfortranarray(x, dtype=np.complex128)
+        cols = xf.shape[1]
+        hy = np.zeros_like(xf, order="F")
+        sy = np.zeros_like(xf, order="F")
+        self._call(self.lib.lib.ref_apply_pair, self.handle, xf.ctypes.data_as(_dbl), cols, hy.ctypes.data_as(_dbl),
+                   sy.ctypes.data_as(_dbl), int(exact))
+        return hy, sy
+
+    def project(self, x):
+        xf = np.asfortranarray(x, dtype=np.complex128)
+        rows = self.lib.lib.ref_projector_rows(self.handle)
+        p = np.zeros((rows, xf.shape[1]), dtype=np.complex128, order="F")
+        self._call(self.lib.lib.ref_project, self.handle, xf.ctypes.data_as(_dbl), xf.shape[1], p.ctypes.data_as(_dbl))
+        return p
+
+    def davidson(self, roots, max_iterations=256, tolerance=1e-12, initial=None):
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        vec = np.zeros((roots, self.n), dtype=np.complex128)  # band-major
+        conv = ctypes.c_int(0)
+        iters = ctypes.c_long(0)
+        init = None
+        if initial is not None:
+            init = np.ascontiguousarray(initial, dtype=np.complex128)
+        self._call(self.lib.lib.ref_davidson, self.handle, roots, max_iterations, tolerance,
+                   init.ctypes.data_as(_dbl) if init is not None else None, _ptr(eig), vec.ctypes.data_as(_dbl),
+                   _ptr(res), ctypes.byref(conv), ctypes.byref(iters))
+        return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),
+                "iterations": int(iters.value)}
+
+    def save_snapshot(self, path, roots, iterations, tolerance, initial=None):
+        init = np.ascontiguousarray(initial if initial is not None else np.zeros(0), dtype=np.complex128)
+        self._call(self.lib.lib.ref_save_snapshot, self.handle, str(path).encode(), roots, iterations, tolerance,
+                   init.ctypes.data_as(_dbl), init.size)

@@ -1,0 +1,170 @@
+"""CPU restatement (numpy) of the reference's hot-path arithmetic.
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA library. Only tests/, the
+smoke check in __graft_entry__ and bench.py's CPU-baseline leg may import it;
+the product never does. It is pinned against the reference itself (the
+unmodified C++ built into oracle/_ref by oracle/ref/Makefile) by
+tests/test_oracle_pins.py, and against committed fixtures in tests/golden/.
+
+Each function cites the reference lines it restates (paths relative to the
+Sparse-DFT source tree).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+HARTREE_TO_EV = 27.211386245988
+
+
+def fast_fft_length(minimum: int) -> int:
+    """Smallest 2/3/5/7-smooth n >= minimum (src/fft_planning.hpp:16-23)."""
+    n = minimum
+    while True:
+        r = n
+        for p in (2, 3, 5, 7):
+            while r % p == 0:
+                r //= p
+        if r == 1:
+            return n
+        n += 1
+
+
+def grid_shape(hkl: np.ndarray, v_hkl: np.ndarray, minimal: bool = False):
+    """Alias-free FFT grid of the operator (src/plane_wave_operator.cpp:400-457)."""
+    low = hkl.min(axis=0)
+    high = hkl.max(axis=0)
+    width = high - low
+    retained = np.all(np.abs(v_hkl) <= width[None, :], axis=1)
+    radius = np.abs(v_hkl[retained]).max(axis=0) if retained.any() else np.zeros(3, dtype=int)
+    shape = []
+    for a in range(3):
+        minimum = max(3, 2 * max(int(radius[a]), int(width[a])) + 1)
+        shape.append(minimum if minimal else fast_fft_length(minimum))
+    return tuple(shape), retained
+
+
+def index_map(hkl: np.ndarray, shape) -> np.ndarray:
+    """Row-major wrapped grid index ((h mod n0)*n1 + k mod n1)*n2 + l mod n2 (src/plane_wave_operator.cpp:94-97)."""
+    n0, n1, n2 = shape
+    h = np.mod(hkl[:, 0], n0).astype(np.int64)
+    k = np.mod(hkl[:, 1], n1).astype(np.int64)
+    l = np.mod(hkl[:, 2], n2).astype(np.int64)
+    return ((h * n1 + k) * n2 + l).astype(np.uint64)
+
+
+def backward_fft(grid: np.ndarray) -> np.ndarray:
+    """Unnormalised sum_G c_G exp(+iG.r), FFTW_BACKWARD convention."""
+    return np.fft.ifftn(grid) * grid.size
+
+
+def forward_fft(grid: np.ndarray) -> np.ndarray:
+    """Unnormalised sum_r f(r) exp(-iG.r), FFTW_FORWARD convention."""
+    return np.fft.fftn(grid)
+
+
+def kinetic_preconditioner(kinetic: float, wavefunction_kinetic: float) -> float:
+    """Bounded rational preconditioner (src/pw_core.cpp:33-47)."""
+    if not (math.isfinite(kinetic) and kinetic >= 0 and math.isfinite(wavefunction_kinetic) and wavefunction_kinetic >= 0):
+        raise ValueError("kinetic preconditioner requires nonnegative Hartree energies")
+    scale = 1.5 * max(wavefunction_kinetic, 2.0 / 27.211386245988)
+    x = kinetic / scale
+    if x > 1.0:
+        inv = 1.0 / x
+        p = inv * (8.0 + inv * (12.0 + inv * (18.0 + 27.0 * inv)))
+        return (2.0 / scale) * p / (p + 16.0)
+    p = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x))
+    return (2.0 / scale) * p / (p + 16.0 * x * x * x * x)
+
+
+class Operator:
+    """H~ and S~ of the reference's PlaneWaveOperator (src/plane_wave_operator.cpp:218-374, 393-516)."""
+
+    def __init__(self, x, minimal: bool = False):
+        self.n = x.hkl.shape[0]
+        self.shape, retained = grid_shape(x.hkl, x.v_hkl, minimal)
+        self.count = int(np.prod(self.shape))
+        grid = np.zeros(self.shape, dtype=np.complex128)
+        keys = x.v_hkl[retained]
+        vals = x.v_values[retained]
+        grid[np.mod(keys[:, 0], self.shape[0]), np.mod(keys[:, 1], self.shape[1]),
+             np.mod(keys[:, 2], self.shape[2])] = vals
+        real = backward_fft(grid)
+        if np.any(np.abs(real.imag) > 1e-9 * np.maximum(1.0, np.abs(real.real))):
+            raise RuntimeError("complex real-space local potential")
+        self.local_real = real.real.reshape(-1).copy()
+        self.indices = index_map(x.hkl, self.shape)
+        self.kinetic = x.kinetic_ev / x.hartree_to_ev
+        self.regularization = x.regularization
+        self.b = np.asarray(x.amplitudes, dtype=np.complex128)  # (np, n)
+        self.atom_offsets = np.concatenate([[0], np.cumsum(x.projectors)]).astype(int)
+        self.d = [0.5 * (m + m.conj().T) for m in x.d]
+        self.q = [0.5 * (m + m.conj().T) for m in x.q]
+        zero = np.all(x.v_hkl == 0, axis=1)
+        v0 = float(x.v_values[zero][0].real) if zero.any() else 0.0
+        self.h_diagonal = self.kinetic + v0
+        self.s_diagonal = np.full(self.n, 1.0 + self.regularization)
+        for a, (lo, hi) in enumerate(zip(self.atom_offsets[:-1], self.atom_offsets[1:])):
+            b = self.b[lo:hi]
+            self.h_diagonal = self.h_diagonal + np.real(np.sum(b.conj() * (self.d[a] @ b), axis=0))
+            self.s_diagonal = self.s_diagonal + np.real(np.sum(b.conj() * (self.q[a] @ b), axis=0))
+
+    def local(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, dtype=np.complex128).reshape(self.n, -1, order="F")
+        out = np.empty_like(x)
+        flat_index = self.indices.astype(np.int64)
+        for c in range(x.shape[1]):
+            grid = np.zeros(self.count, dtype=np.complex128)
+            grid[flat_index] = x[:, c]
+            field = backward_fft(grid.reshape(self.shape)) * self.local_real.reshape(self.shape)
+            back = forward_fft(field).reshape(-1)
+            out[:, c] = self.kinetic * x[:, c] + back[flat_index] / float(self.count)
+        return out
+
+    def _onsite(self, p: np.ndarray, blocks) -> np.ndarray:
+        out = np.zeros_like(p)
+        for a, (lo, hi) in enumerate(zip(self.atom_offsets[:-1], self.atom_offsets[1:])):
+            out[lo:hi] = blocks[a] @ p[lo:hi]
+        return out
+
+    def project(self, x):
+        return self.b @ np.asarray(x, dtype=np.complex128).reshape(self.n, -1, order="F")
+
+    def apply_h(self, x):
+        x = np.asarray(x, dtype=np.complex128).reshape(self.n, -1, order="F")
+        y = self.local(x)
+        if self.b.shape[0]:
+            y = y + self.b.conj().T @ self._onsite(self.b @ x, self.d)
+        return y
+
+    def apply_s(self, x):
+        x = np.asarray(x, dtype=np.complex128).reshape(self.n, -1, order="F")
+        y = (1.0 + self.regularization) * x
+        if self.b.shape[0]:
+            y = y + self.b.conj().T @ self._onsite(self.b @ x, self.q)
+        return y
+
+    def dense(self):
+        """Dense H~ and S~ (small cases only), column by column."""
+        eye = np.eye(self.n, dtype=np.complex128)
+        return self.apply_h(eye), self.apply_s(eye)
+
+
+def generalized_eigenvalues(h: np.ndarray, s: np.ndarray, roots: int) -> np.ndarray:
+    """Lowest roots of H v = e S v by Cholesky reduction (dense oracle, small n)."""
+    hh = 0.5 * (h + h.conj().T)
+    ss = 0.5 * (s + s.conj().T)
+    lower = np.linalg.cholesky(ss)
+    inv = np.linalg.inv(lower)
+    a = inv @ hh @ inv.conj().T
+    return np.linalg.eigvalsh(0.5 * (a + a.conj().T))[:roots]
+
+
+def certified_residuals(op: Operator, eigenvalues: np.ndarray, vectors: np.ndarray):
+    """Fresh FP64 ||H x - e S x|| and |x^H S x - 1| per root (src/solver_replay_cli.cpp:30-45)."""
+    hx = op.apply_h(vectors)
+    sx = op.apply_s(vectors)
+    res = np.linalg.norm(hx - sx * eigenvalues[None, :], axis=0)
+    metric = np.real(np.sum(vectors.conj() * sx, axis=0))
+    return res, np.abs(metric - 1.0)

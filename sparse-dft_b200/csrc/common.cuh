@@ -1,0 +1,69 @@
+// Shared device/host utilities for the sm_100a plane-wave PAW library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace sdft_b200 {
+
+// Errors carry the reference's exception classes across the C ABI as codes.
+struct InvalidArgument : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct Overflow : std::overflow_error {
+  using std::overflow_error::overflow_error;
+};
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct NonFinite : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+inline void check_cuda(cudaError_t code, const char* what) {
+  if (code != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(code));
+}
+#define SDFT_CUDA(call) ::sdft_b200::check_cuda((call), #call)
+#define SDFT_LAUNCH(what) ::sdft_b200::check_cuda(cudaGetLastError(), what)
+
+// Interleaved complex in precision T (float2/double2 layout).
+template <typename T>
+struct alignas(2 * sizeof(T)) Cx {
+  T re, im;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ Cx<T> cx(T re, T im) {
+  return Cx<T>{re, im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ Cx<T> operator+(Cx<T> a, Cx<T> b) {
+  return {a.re + b.re, a.im + b.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ Cx<T> operator-(Cx<T> a, Cx<T> b) {
+  return {a.re - b.re, a.im - b.im};
+}
+template <typename T>
+__host__ __device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx<T> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+__host__ __device__ __forceinline__ Cx<T> cscale(Cx<T> a, T s) {
+  return {a.re * s, a.im * s};
+}
+
+template <typename To, typename From>
+__host__ __device__ __forceinline__ Cx<To> cconvert(Cx<From> a) {
+  return {static_cast<To>(a.re), static_cast<To>(a.im)};
+}
+
+constexpr int kWarp = 32;
+constexpr int kSmCount = 148;  // B200: 2 dies x 74 SMs
+
+inline std::size_t ceil_div(std::size_t a, std::size_t b) { return (a + b - 1) / b; }
+
+}  // namespace sdft_b200

@@ -1,0 +1,153 @@
+// Mixed-radix (2, 3, 4, 5, 7) line FFT on shared memory, one warp per line.
+//
+// Stockham autosort formulation (each stage reads x[j + r*n/R], applies the
+// twiddle W^(r*(j mod Ns)*n/(Ns*R)), a radix-R DFT, and writes to
+// (j/Ns)*Ns*R + (j mod Ns) + r*Ns), executed in place: every lane first loads
+// all inputs of its butterflies into registers, the warp synchronises, then
+// the lane writes its outputs. Lines may be strided in shared memory, so the
+// same routine serves rows, columns and pencils of a staged tile.
+//
+// Sign convention (the reference's FFTW calls): forward X_k = sum x_j
+// exp(-2 pi i jk/n), backward uses +i, both unnormalised. Twiddles come from a
+// table w[m] = exp(-2 pi i m/n) evaluated on the host in long double.
+#pragma once
+#include "common.cuh"
+
+namespace sdft_b200 {
+
+constexpr int kMaxStages = 12;
+constexpr int kMaxLine = 512;
+
+struct LinePlan {
+  int n = 1;
+  int stages = 0;
+  int radix[kMaxStages] = {};
+};
+
+// Host: factor n into supported radices (4 first, then 2, 3, 5, 7).
+LinePlan make_line_plan(int n);
+bool fft_length_supported(int n);
+// Smallest 2/3/5/7-smooth length >= minimum (the reference's fast_fft_length,
+// src/fft_planning.hpp:16-23).
+int fast_fft_length(int minimum);
+
+template <typename T, bool INV>
+__device__ __forceinline__ Cx<T> twiddle(const Cx<T>* tw, int index) {
+  Cx<T> w = tw[index];
+  if (INV) w.im = -w.im;
+  return w;
+}
+
+// (a) * (+/- i)
+template <typename T, bool INV>
+__device__ __forceinline__ Cx<T> rotate_quarter(Cx<T> a) {
+  // forward: multiply by -i -> (im, -re); backward: by +i -> (-im, re)
+  return INV ? Cx<T>{-a.im, a.re} : Cx<T>{a.im, -a.re};
+}
+
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void radix_dft(Cx<T>* v, const Cx<T>* tw, int unit) {
+  if constexpr (R == 2) {
+    const Cx<T> a = v[0], b = v[1];
+    v[0] = a + b;
+    v[1] = a - b;
+  } else if constexpr (R == 4) {
+    const Cx<T> a = v[0] + v[2], c = v[0] - v[2], d = v[1] + v[3];
+    const Cx<T> e = rotate_quarter<T, INV>(v[1] - v[3]);
+    v[0] = a + d;
+    v[2] = a - d;
+    v[1] = c + e;
+    v[3] = c - e;
+  } else {
+    // Odd R: pair r with R-r. omega^q = tw[q*unit] (forward sign).
+    constexpr int H = (R - 1) / 2;
+    Cx<T> a[H], b[H];
+#pragma unroll
+    for (int r = 1; r <= H; ++r) {
+      a[r - 1] = v[r] + v[R - r];
+      b[r - 1] = v[r] - v[R - r];
+    }
+    Cx<T> y[R];
+    Cx<T> sum = v[0];
+#pragma unroll
+    for (int r = 0; r < H; ++r) sum = sum + a[r];
+    y[0] = sum;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      T cre = v[0].re, cim = v[0].im, sre = 0, sim = 0;
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const Cx<T> w = tw[((r * q) % R) * unit];  // cos, -sin (forward)
+        cre += a[r - 1].re * w.re;
+        cim += a[r - 1].im * w.re;
+        // i * S * b with S = w.im (forward) or -w.im (backward)
+        const T s = INV ? -w.im : w.im;
+        sre -= b[r - 1].im * s;
+        sim += b[r - 1].re * s;
+      }
+      y[q] = Cx<T>{cre + sre, cim + sim};
+      y[R - q] = Cx<T>{cre - sre, cim - sim};
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = y[q];
+  }
+}
+
+template <typename T, int R, int NMAX, bool INV>
+__device__ __forceinline__ void line_stage(Cx<T>* line, int stride, int n, int ns, const Cx<T>* tw, int lane) {
+  constexpr int MAXB = (NMAX / R + kWarp - 1) / kWarp;
+  const int m = n / R;
+  const int twstride = n / (ns * R);
+  const int unit = n / R;
+  Cx<T> v[MAXB][R];
+#pragma unroll
+  for (int b = 0; b < MAXB; ++b) {
+    const int j = lane + b * kWarp;
+    if (j < m) {
+      const int k = j % ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        Cx<T> x = line[(j + r * m) * stride];
+        if (r > 0 && k > 0) x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
+        v[b][r] = x;
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < MAXB; ++b) {
+    const int j = lane + b * kWarp;
+    if (j < m) {
+      radix_dft<T, R, INV>(v[b], tw, unit);
+      const int k = j % ns;
+      const int base = (j / ns) * ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) line[(base + r * ns) * stride] = v[b][r];
+    }
+  }
+  __syncwarp();
+}
+
+// One warp transforms one line of plan.n elements at line[e*stride].
+template <typename T, int NMAX, bool INV>
+__device__ void fft_line(Cx<T>* line, int stride, const LinePlan& plan, const Cx<T>* tw, int lane) {
+  int ns = 1;
+  for (int s = 0; s < plan.stages; ++s) {
+    const int r = plan.radix[s];
+    switch (r) {
+      case 2: line_stage<T, 2, NMAX, INV>(line, stride, plan.n, ns, tw, lane); break;
+      case 3: line_stage<T, 3, NMAX, INV>(line, stride, plan.n, ns, tw, lane); break;
+      case 4: line_stage<T, 4, NMAX, INV>(line, stride, plan.n, ns, tw, lane); break;
+      case 5: line_stage<T, 5, NMAX, INV>(line, stride, plan.n, ns, tw, lane); break;
+      case 7: line_stage<T, 7, NMAX, INV>(line, stride, plan.n, ns, tw, lane); break;
+      default: break;  // rejected on the host
+    }
+    ns *= r;
+  }
+}
+
+// Host-side twiddle tables, w[m] = exp(-2 pi i m / n), one per (n, precision).
+template <typename T>
+const Cx<T>* device_twiddles(int n);
+
+}  // namespace sdft_b200

@@ -1,0 +1,47 @@
+// Complex GEMMs for the PAW projector chain and the Davidson subspace work.
+#pragma once
+#include <cublas_v2.h>
+
+#include "common.cuh"
+
+namespace sdft_b200 {
+
+enum class Op { N, C };  // C = conjugate transpose (the reference's MatrixOp::Adjoint)
+
+// Grow-only device scratch owned by a context.
+struct Scratch {
+  void* ptr = nullptr;
+  std::size_t bytes = 0;
+  void* reserve(std::size_t need);
+  void release();
+  ~Scratch() { release(); }
+};
+
+// C(m x n, ldc) = op(A) B (+ C if add), all complex FP64 column-major,
+// FP64 arithmetic through cuBLAS ZGEMM (plain library GEMM).
+void zgemm(cublasHandle_t handle, Op aop, Op bop, int m, int n, int k, const Cx<double>* a, long long lda,
+           const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add);
+
+// Mixed search GEMM: FP64 storage in/out, products accumulated in FP32 by
+// the hand-written split-K kernel. aop applies to A; B is always normal.
+// `a32` may point to an FP32 copy of A (same layout, ld lda) or be null.
+void gemm_mixed(Op aop, int m, int n, int k, const Cx<double>* a, const Cx<float>* a32, long long lda,
+                const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, Scratch& workspace,
+                cudaStream_t stream);
+
+// Per-atom block-diagonal product out[off_a + i, c] = sum_j M_a(i,j) P[off_a + j, c]
+// with error-free FP64 products and compensated sums (TwoSum + FMA), the
+// reference's compensated_paw_product order (src/paw_compensated_product.hpp:41-56).
+// blocks: column-major per atom, block a at storage[a]; offsets[a] = first row.
+void block_product(int atoms, const int* offsets, const long long* storage, int max_block, const Cx<double>* blocks,
+                   const Cx<double>* p, long long ldp, int columns, Cx<double>* out, long long ldo,
+                   cudaStream_t stream);
+
+// y = alpha * x (columns of length n, leading dims ldx/ldy).
+void scale_copy(const Cx<double>* x, long long ldx, Cx<double>* y, long long ldy, int n, int columns, double alpha,
+                cudaStream_t stream);
+
+// FP64 -> FP32 copy of n complex values.
+void demote(const Cx<double>* src, Cx<float>* dst, std::size_t n, cudaStream_t stream);
+
+}  // namespace sdft_b200

@@ -1,0 +1,379 @@
+// Fused local Hamiltonian (the reference's FFT loop, src/plane_wave_operator.cpp:237-257,
+// and the CUDA scatter/cuFFT/multiply/cuFFT/gather chain, src/compute_cuda.cu:141-177)
+// as three hand-written passes over a pruned slab:
+//
+//   plane_in   (one CTA per active grid row i0 and column): scatter the sphere
+//              points of that plane into shared memory, backward FFT along
+//              i2 on the active i1 rows, backward FFT along i1 on every i2
+//              column, store the plane to the slab.
+//   pencil     (one CTA per 32 (i1,i2) lines and column): load the active i0
+//              entries, zero-pad to n0, backward FFT along i0, multiply by
+//              V(r), forward FFT, store back only the active i0 entries.
+//   plane_out  (per active i0 and column): forward FFT along i1 and i2, gather
+//              the sphere points, y = T x + value/N.
+//
+// Rows i0 outside the sphere's span never reach HBM: the slab holds
+// slots*n1*n2 complex values per column instead of n0*n1*n2.
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <set>
+
+#include "local_hamiltonian.cuh"
+
+namespace sdft_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPencilLines = 32;
+
+template <typename T>
+struct LocalArgs {
+  int n0, n1, n2, n2p, slots, krows;
+  long long n12;
+  const int* slot_row;
+  const int* point_offset;
+  const int* point_g;
+  const int* point_smem;
+  const int* krow;
+  LinePlan p0, p1, p2;
+  const Cx<T>* tw0;
+  const Cx<T>* tw1;
+  const Cx<T>* tw2;
+};
+
+template <typename T, int NMAX>
+__global__ void __launch_bounds__(kThreads, 2) plane_in_kernel(const Cx<double>* __restrict__ x, long long ldx,
+                                                            LocalArgs<T> a, Cx<T>* __restrict__ slab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tw2 = tw1 + a.n1;
+  Cx<T>* plane = tw2 + a.n2;
+  const int s = blockIdx.x, c = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  for (int i = tid; i < a.n1; i += blockDim.x) tw1[i] = a.tw1[i];
+  for (int i = tid; i < a.n2; i += blockDim.x) tw2[i] = a.tw2[i];
+  const int plane_elems = a.n1 * a.n2p;
+  for (int i = tid; i < plane_elems; i += blockDim.x) plane[i] = Cx<T>{0, 0};
+  __syncthreads();
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  const int p_end = a.point_offset[s + 1];
+  for (int p = a.point_offset[s] + tid; p < p_end; p += blockDim.x)
+    plane[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
+  __syncthreads();
+  for (int r = warp; r < a.krows; r += warps) fft_line<T, NMAX, true>(plane + a.krow[r] * a.n2p, 1, a.p2, tw2, lane);
+  __syncthreads();
+  for (int l = warp; l < a.n2; l += warps) fft_line<T, NMAX, true>(plane + l, a.n2p, a.p1, tw1, lane);
+  __syncthreads();
+  Cx<T>* out = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
+  for (int i = tid; i < a.n12; i += blockDim.x) {
+    const int i1 = i / a.n2, i2 = i - i1 * a.n2;
+    out[i] = plane[i1 * a.n2p + i2];
+  }
+}
+
+template <typename T, int NMAX>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 2) pencil_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
+                                                          const T* __restrict__ potential) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TL = kPencilLines, STRIDE = TL + 1;
+  Cx<T>* tw0 = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tile = tw0 + a.n0;
+  const long long kl0 = static_cast<long long>(blockIdx.x) * TL;
+  const int c = blockIdx.y;
+  const int lines = static_cast<int>(min(static_cast<long long>(TL), a.n12 - kl0));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  for (int i = tid; i < a.n0; i += blockDim.x) tw0[i] = a.tw0[i];
+  for (int i = tid; i < a.n0 * STRIDE; i += blockDim.x) tile[i] = Cx<T>{0, 0};
+  __syncthreads();
+  Cx<T>* base = slab + static_cast<long long>(c) * a.slots * a.n12 + kl0;
+  for (int idx = tid; idx < a.slots * TL; idx += blockDim.x) {
+    const int s = idx / TL, t = idx - s * TL;
+    if (t < lines) tile[a.slot_row[s] * STRIDE + t] = base[static_cast<long long>(s) * a.n12 + t];
+  }
+  __syncthreads();
+  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, true>(tile + t, STRIDE, a.p0, tw0, lane);
+  __syncthreads();
+  for (int idx = tid; idx < a.n0 * TL; idx += blockDim.x) {
+    const int i = idx / TL, t = idx - i * TL;
+    if (t < lines) {
+      const T v = potential[static_cast<long long>(i) * a.n12 + kl0 + t];
+      tile[i * STRIDE + t] = cscale(tile[i * STRIDE + t], v);
+    }
+  }
+  __syncthreads();
+  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, false>(tile + t, STRIDE, a.p0, tw0, lane);
+  __syncthreads();
+  for (int idx = tid; idx < a.slots * TL; idx += blockDim.x) {
+    const int s = idx / TL, t = idx - s * TL;
+    if (t < lines) base[static_cast<long long>(s) * a.n12 + t] = tile[a.slot_row[s] * STRIDE + t];
+  }
+}
+
+template <typename T, int NMAX>
+__global__ void __launch_bounds__(kThreads, 2) plane_out_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
+                                                             const Cx<double>* __restrict__ x, long long ldx,
+                                                             const double* __restrict__ kinetic, double count,
+                                                             Cx<double>* __restrict__ y, long long ldy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tw2 = tw1 + a.n1;
+  Cx<T>* plane = tw2 + a.n2;
+  const int s = blockIdx.x, c = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  for (int i = tid; i < a.n1; i += blockDim.x) tw1[i] = a.tw1[i];
+  for (int i = tid; i < a.n2; i += blockDim.x) tw2[i] = a.tw2[i];
+  const Cx<T>* in = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
+  for (int i = tid; i < a.n12; i += blockDim.x) {
+    const int i1 = i / a.n2, i2 = i - i1 * a.n2;
+    plane[i1 * a.n2p + i2] = in[i];
+  }
+  __syncthreads();
+  for (int l = warp; l < a.n2; l += warps) fft_line<T, NMAX, false>(plane + l, a.n2p, a.p1, tw1, lane);
+  __syncthreads();
+  for (int r = warp; r < a.krows; r += warps) fft_line<T, NMAX, false>(plane + a.krow[r] * a.n2p, 1, a.p2, tw2, lane);
+  __syncthreads();
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
+  const int p_end = a.point_offset[s + 1];
+  for (int p = a.point_offset[s] + tid; p < p_end; p += blockDim.x) {
+    const int g = a.point_g[p];
+    const Cx<double> v = cconvert<double>(plane[a.point_smem[p]]);
+    const Cx<double> in_g = xc[g];
+    const double t = kinetic[g];
+    yc[g] = Cx<double>{t * in_g.re + v.re / count, t * in_g.im + v.im / count};
+  }
+}
+
+// Lines along a strided axis: element e of line i at base + e*stride + i.
+template <typename T, int NMAX, bool INV, int TL>
+__global__ void __launch_bounds__(kThreads, 2) fft_strided_kernel(Cx<T>* __restrict__ data, int n, long long stride,
+                                                               long long inner, long long outer_stride, LinePlan p,
+                                                               const Cx<T>* __restrict__ tw_global) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int STRIDE = TL + 1;
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tile = tw + n;
+  const long long i0 = static_cast<long long>(blockIdx.x) * TL;
+  const int lines = static_cast<int>(min(static_cast<long long>(TL), inner - i0));
+  Cx<T>* base = data + static_cast<long long>(blockIdx.y) * outer_stride + i0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  for (int i = tid; i < n; i += blockDim.x) tw[i] = tw_global[i];
+  for (int idx = tid; idx < n * TL; idx += blockDim.x) {
+    const int e = idx / TL, t = idx - e * TL;
+    if (t < lines) tile[e * STRIDE + t] = base[e * stride + t];
+  }
+  __syncthreads();
+  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, INV>(tile + t, STRIDE, p, tw, lane);
+  __syncthreads();
+  for (int idx = tid; idx < n * TL; idx += blockDim.x) {
+    const int e = idx / TL, t = idx - e * TL;
+    if (t < lines) base[e * stride + t] = tile[e * STRIDE + t];
+  }
+}
+
+// Contiguous rows of length n (the innermost axis).
+template <typename T, int NMAX, bool INV, int TR>
+__global__ void __launch_bounds__(kThreads, 2) fft_rows_kernel(Cx<T>* __restrict__ data, int n, int np, long long rows,
+                                                            LinePlan p, const Cx<T>* __restrict__ tw_global) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tile = tw + n;
+  const long long r0 = static_cast<long long>(blockIdx.x) * TR;
+  const int count = static_cast<int>(min(static_cast<long long>(TR), rows - r0));
+  Cx<T>* base = data + r0 * n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  for (int i = tid; i < n; i += blockDim.x) tw[i] = tw_global[i];
+  for (int idx = tid; idx < count * n; idx += blockDim.x) {
+    const int r = idx / n, e = idx - r * n;
+    tile[r * np + e] = base[idx];
+  }
+  __syncthreads();
+  for (int r = warp; r < count; r += warps) fft_line<T, NMAX, INV>(tile + r * np, 1, p, tw, lane);
+  __syncthreads();
+  for (int idx = tid; idx < count * n; idx += blockDim.x) {
+    const int r = idx / n, e = idx - r * n;
+    base[idx] = tile[r * np + e];
+  }
+}
+
+template <typename Kernel>
+void allow_smem(Kernel kernel, std::size_t bytes) {
+  if (bytes > 227 * 1024) throw InvalidArgument("FFT tile does not fit in shared memory");
+  SDFT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+}
+
+template <typename T>
+LocalArgs<T> make_args(const SpherePlan& plan) {
+  LocalArgs<T> a{};
+  a.n0 = plan.n[0];
+  a.n1 = plan.n[1];
+  a.n2 = plan.n[2];
+  a.n2p = plan.n2p;
+  a.slots = plan.slots;
+  a.krows = plan.krows;
+  a.n12 = static_cast<long long>(plan.n[1]) * plan.n[2];
+  a.slot_row = plan.slot_row;
+  a.point_offset = plan.point_offset;
+  a.point_g = plan.point_g;
+  a.point_smem = plan.point_smem;
+  a.krow = plan.krow;
+  a.p0 = plan.line[0];
+  a.p1 = plan.line[1];
+  a.p2 = plan.line[2];
+  a.tw0 = device_twiddles<T>(plan.n[0]);
+  a.tw1 = device_twiddles<T>(plan.n[1]);
+  a.tw2 = device_twiddles<T>(plan.n[2]);
+  return a;
+}
+
+template <typename T, int NMAX>
+void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns,
+                            const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
+                            cudaStream_t stream) {
+  const LocalArgs<T> a = make_args<T>(plan);
+  const std::size_t plane_smem = sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + static_cast<std::size_t>(plan.n[1]) * plan.n2p);
+  const std::size_t pencil_smem = sizeof(Cx<T>) * (plan.n[0] + static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
+  allow_smem(plane_in_kernel<T, NMAX>, plane_smem);
+  allow_smem(pencil_kernel<T, NMAX>, pencil_smem);
+  allow_smem(plane_out_kernel<T, NMAX>, plane_smem);
+  const dim3 planes(plan.slots, columns);
+  plane_in_kernel<T, NMAX><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
+  SDFT_LAUNCH("plane_in_kernel");
+  const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
+  pencil_kernel<T, NMAX><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+  SDFT_LAUNCH("pencil_kernel");
+  plane_out_kernel<T, NMAX><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
+                                                                      static_cast<double>(plan.count), y, ldy);
+  SDFT_LAUNCH("plane_out_kernel");
+}
+
+template <typename T, int NMAX, bool INV>
+void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
+  const long long n12 = static_cast<long long>(n[1]) * n[2];
+  const long long count = n12 * n[0];
+  constexpr int TL = NMAX <= 128 ? 16 : 8;
+  // axis 2: contiguous rows
+  {
+    const LinePlan p = make_line_plan(n[2]);
+    const int np = n[2] | 1;
+    constexpr int TR = TL;
+    const std::size_t smem = sizeof(Cx<T>) * (n[2] + static_cast<std::size_t>(TR) * np);
+    allow_smem(fft_rows_kernel<T, NMAX, INV, TR>, smem);
+    const long long rows = count / n[2] * batch;
+    fft_rows_kernel<T, NMAX, INV, TR><<<static_cast<unsigned>(ceil_div(rows, TR)), kThreads, smem, stream>>>(
+        grid, n[2], np, rows, p, device_twiddles<T>(n[2]));
+    SDFT_LAUNCH("fft_rows_kernel");
+  }
+  // axis 1: stride n2, n0*batch outer blocks
+  {
+    const LinePlan p = make_line_plan(n[1]);
+    const std::size_t smem = sizeof(Cx<T>) * (n[1] + static_cast<std::size_t>(n[1]) * (TL + 1));
+    allow_smem(fft_strided_kernel<T, NMAX, INV, TL>, smem);
+    const dim3 blocks(static_cast<unsigned>(ceil_div(n[2], TL)), static_cast<unsigned>(n[0] * batch));
+    fft_strided_kernel<T, NMAX, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[1], n[2], n[2], n12, p,
+                                                                            device_twiddles<T>(n[1]));
+    SDFT_LAUNCH("fft_strided_kernel axis1");
+  }
+  // axis 0: stride n1*n2
+  {
+    const LinePlan p = make_line_plan(n[0]);
+    const std::size_t smem = sizeof(Cx<T>) * (n[0] + static_cast<std::size_t>(n[0]) * (TL + 1));
+    allow_smem(fft_strided_kernel<T, NMAX, INV, TL>, smem);
+    const dim3 blocks(static_cast<unsigned>(ceil_div(n12, TL)), static_cast<unsigned>(batch));
+    fft_strided_kernel<T, NMAX, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[0], n12, n12, count, p,
+                                                                            device_twiddles<T>(n[0]));
+    SDFT_LAUNCH("fft_strided_kernel axis0");
+  }
+}
+
+}  // namespace
+
+void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& indices) {
+  release();
+  for (int a = 0; a < 3; ++a) {
+    if (shape[a] < 1 || !fft_length_supported(shape[a]))
+      throw InvalidArgument("grid axis length must be a 2/3/5/7-smooth integer in [1,512]");
+    n[a] = shape[a];
+    line[a] = make_line_plan(shape[a]);
+  }
+  count = static_cast<std::size_t>(n[0]) * n[1] * n[2];
+  if (indices.empty() || indices.size() > static_cast<std::size_t>(std::numeric_limits<int>::max()))
+    throw InvalidArgument("plane-wave index map size out of range");
+  npw = static_cast<int>(indices.size());
+  n2p = n[2] | 1;
+  const std::size_t n12 = static_cast<std::size_t>(n[1]) * n[2];
+  std::vector<int> slot_of_row(n[0], -1);
+  std::set<int> rows0, rows1;
+  for (auto idx : indices) {
+    if (idx >= count) throw InvalidArgument("plane-wave index outside the FFT grid");
+    rows0.insert(static_cast<int>(idx / n12));
+    rows1.insert(static_cast<int>((idx / n[2]) % n[1]));
+  }
+  std::vector<int> h_slot_row(rows0.begin(), rows0.end());
+  slots = static_cast<int>(h_slot_row.size());
+  for (int s = 0; s < slots; ++s) slot_of_row[h_slot_row[s]] = s;
+  std::vector<int> h_krow(rows1.begin(), rows1.end());
+  krows = static_cast<int>(h_krow.size());
+  std::vector<int> h_offset(slots + 1, 0);
+  for (auto idx : indices) ++h_offset[slot_of_row[idx / n12] + 1];
+  for (int s = 0; s < slots; ++s) h_offset[s + 1] += h_offset[s];
+  std::vector<int> fill(h_offset.begin(), h_offset.end() - 1);
+  std::vector<int> h_g(npw), h_smem(npw);
+  for (int g = 0; g < npw; ++g) {
+    const auto idx = indices[g];
+    const int s = slot_of_row[idx / n12];
+    const int i1 = static_cast<int>((idx / n[2]) % n[1]);
+    const int i2 = static_cast<int>(idx % n[2]);
+    const int p = fill[s]++;
+    h_g[p] = g;
+    h_smem[p] = i1 * n2p + i2;
+  }
+  auto upload = [](int*& dst, const std::vector<int>& src) {
+    SDFT_CUDA(cudaMalloc(&dst, sizeof(int) * std::max<std::size_t>(1, src.size())));
+    SDFT_CUDA(cudaMemcpy(dst, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice));
+  };
+  upload(slot_row, h_slot_row);
+  upload(point_offset, h_offset);
+  upload(point_g, h_g);
+  upload(point_smem, h_smem);
+  upload(krow, h_krow);
+}
+
+void SpherePlan::release() {
+  for (int** p : {&slot_row, &point_offset, &point_g, &point_smem, &krow}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+}
+
+template <typename T>
+void local_hamiltonian(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns, const T* potential,
+                       const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab, cudaStream_t stream) {
+  if (columns <= 0) return;
+  const int nmax = std::max({plan.n[0], plan.n[1], plan.n[2]});
+  if (nmax > 128) throw InvalidArgument("operator FFT grid axes above 128 points are not supported");
+  local_hamiltonian_impl<T, 128>(plan, x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
+}
+
+template <typename T>
+void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream) {
+  const int nmax = std::max({n[0], n[1], n[2]});
+  if (nmax <= 128) {
+    if (backward) fft3d_impl<T, 128, true>(grid, n, batch, stream);
+    else fft3d_impl<T, 128, false>(grid, n, batch, stream);
+  } else {
+    if (backward) fft3d_impl<T, 512, true>(grid, n, batch, stream);
+    else fft3d_impl<T, 512, false>(grid, n, batch, stream);
+  }
+}
+
+template void local_hamiltonian<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,
+                                       const double*, Cx<double>*, long long, Cx<float>*, cudaStream_t);
+template void local_hamiltonian<double>(const SpherePlan&, const Cx<double>*, long long, int, const double*,
+                                        const double*, Cx<double>*, long long, Cx<double>*, cudaStream_t);
+template void fft3d<float>(Cx<float>*, const int[3], int, bool, cudaStream_t);
+template void fft3d<double>(Cx<double>*, const int[3], int, bool, cudaStream_t);
+
+}  // namespace sdft_b200

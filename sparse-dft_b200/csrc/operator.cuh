@@ -1,0 +1,113 @@
+// Device-resident plane-wave PAW operator and its execution context.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "gemm.cuh"
+#include "local_hamiltonian.cuh"
+
+namespace sdft_b200 {
+
+enum class Precision : int { FP64 = 0, Mixed = 1 };
+
+// One CUDA stream with its library handles and grow-only scratch. A context is
+// used by one host thread at a time (the reference keeps one Accelerator per
+// host thread, src/compute_backend.cpp:62-73).
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  Scratch slab32, slab64, gemm_work, staging_in, staging_out, staging_aux, projections, onsite;
+  explicit Context(int device, cudaStream_t stream);
+  ~Context();
+  Context(const Context&) = delete;
+  Context& operator=(const Context&) = delete;
+  void synchronize() const;
+};
+
+struct GVectorList {
+  std::vector<int> hkl;         // 3 per vector
+  std::vector<double> cartesian;
+  std::vector<double> kinetic_ev;
+};
+
+// Plane-wave sphere enumeration, same arithmetic/order as src/pw_core.cpp:140-171.
+GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
+                                double hartree_to_ev);
+
+struct OperatorInput {
+  std::size_t npw = 0;
+  const int* hkl = nullptr;          // npw x 3
+  const double* kinetic_ev = nullptr;
+  std::size_t potential_count = 0;
+  const int* potential_hkl = nullptr;  // x3
+  const double* potential = nullptr;   // interleaved complex
+  std::size_t atoms = 0;
+  const std::uint64_t* projectors = nullptr;  // per atom
+  const double* amplitudes = nullptr;  // per atom row-major np_a x npw, interleaved complex
+  const double* d = nullptr;           // per atom row-major np_a x np_a
+  const double* q = nullptr;
+  double hartree_to_ev = 27.211386245988;
+  double regularization = 1e-12;
+};
+
+class DeviceOperator {
+ public:
+  DeviceOperator(Context& ctx, const OperatorInput& input);
+  ~DeviceOperator();
+  DeviceOperator(const DeviceOperator&) = delete;
+  DeviceOperator& operator=(const DeviceOperator&) = delete;
+
+  Context& context() const { return ctx_; }
+  int npw() const { return npw_; }
+  int projectors() const { return np_; }
+  int atoms() const { return atoms_; }
+  const SpherePlan& plan() const { return plan_; }
+  double regularization() const { return regularization_; }
+  const std::vector<double>& kinetic() const { return h_kinetic_; }
+  const std::vector<double>& h_diagonal() const { return h_diag_; }
+  const std::vector<double>& s_diagonal() const { return s_diag_; }
+  const std::vector<std::uint64_t>& indices() const { return h_indices_; }
+  const std::vector<double>& local_real() const { return h_local_real_; }
+  const double* device_kinetic() const { return kinetic_; }
+
+  // Device-pointer applies on ctx.stream; x, y are npw x columns (ld npw).
+  void apply_hamiltonian(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
+  void apply_overlap(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
+  void apply_pair(const Cx<double>* x, int columns, Cx<double>* hy, Cx<double>* sy, Precision precision);
+  // P = B x (np x columns, ld np)
+  void project(const Cx<double>* x, int columns, Cx<double>* p, Precision precision);
+
+  std::size_t device_bytes() const;
+
+ private:
+  void local_part(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
+  void paw_add(const Cx<double>* p, int columns, bool overlap, Cx<double>* y, Precision precision);
+  void backproject(const Cx<double>* dp, int columns, Cx<double>* y, Precision precision);
+
+  Context& ctx_;
+  int npw_ = 0, np_ = 0, atoms_ = 0, max_block_ = 0;
+  double regularization_ = 0;
+  SpherePlan plan_;
+  std::vector<double> h_kinetic_, h_diag_, h_local_real_;
+  std::vector<double> s_diag_;
+  std::vector<std::uint64_t> h_indices_;
+  double* kinetic_ = nullptr;
+  double* v64_ = nullptr;
+  float* v32_ = nullptr;
+  Cx<double>* b_ = nullptr;      // np x npw column-major (ld np)
+  Cx<float>* b32_ = nullptr;
+  Cx<double>* d_ = nullptr;      // per-atom column-major blocks
+  Cx<double>* q_ = nullptr;
+  int* block_offsets_ = nullptr;         // [atoms+1]
+  long long* block_storage_ = nullptr;   // [atoms]
+};
+
+}  // namespace sdft_b200

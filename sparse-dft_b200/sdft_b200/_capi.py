@@ -1,0 +1,98 @@
+"""ctypes binding of the C ABI in include/sdft_b200.h (libsdft_b200.so, built in-tree).
+
+There is no Python or CPU implementation behind this module: if the shared
+library is missing, importing the bindings raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import re
+
+LIBRARY = pathlib.Path(__file__).resolve().parent / "_lib" / "libsdft_b200.so"
+HEADER = pathlib.Path(__file__).resolve().parents[2] / "include" / "sdft_b200.h"
+
+OK, INVALID_ARGUMENT, OVERFLOW, RUNTIME_ERROR, CUDA_ERROR, OUT_OF_MEMORY, NONFINITE = range(7)
+FP64, MIXED = 0, 1
+HOST, DEVICE = 0, 1
+HAMILTONIAN, OVERLAP = 0, 1
+
+
+class SdftError(RuntimeError):
+    """A non-OK status from the library; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[status {status}] {message}")
+        self.status = status
+
+
+class InvalidArgument(SdftError, ValueError):
+    pass
+
+
+class OverflowFailure(SdftError, OverflowError):
+    pass
+
+
+_ERRORS = {INVALID_ARGUMENT: InvalidArgument, OVERFLOW: OverflowFailure}
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise ImportError(f"libsdft_b200.so is not built ({LIBRARY}); run __graft_entry__.build() or "
+                              "make -C sparse-dft_b200")
+        _lib = ctypes.CDLL(str(LIBRARY))
+        _declare(_lib)
+    return _lib
+
+
+def declared_symbols() -> list[str]:
+    """Every function the public header declares."""
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"SDFT_B200_API\s+[\w\s\*]*?\b(sdft_b200_\w+)\s*\(", text)))
+
+
+P = ctypes.c_void_p
+D = ctypes.POINTER(ctypes.c_double)
+I32 = ctypes.POINTER(ctypes.c_int32)
+U64 = ctypes.POINTER(ctypes.c_uint64)
+SZ = ctypes.c_size_t
+SZP = ctypes.POINTER(ctypes.c_size_t)
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    def fn(name, args, res=ctypes.c_int):
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+
+    fn("sdft_b200_last_error", [ctypes.c_char_p, SZ], SZ)
+    fn("sdft_b200_version", [], ctypes.c_char_p)
+    fn("sdft_b200_context_create", [ctypes.c_int, P, ctypes.POINTER(P)])
+    fn("sdft_b200_context_destroy", [P])
+    fn("sdft_b200_context_synchronize", [P])
+    fn("sdft_b200_enumerate_g_vectors", [D, ctypes.c_double, D, ctypes.c_double, I32, D, D, SZ, SZP])
+    fn("sdft_b200_operator_create", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,
+                                     ctypes.POINTER(P)])
+    fn("sdft_b200_operator_destroy", [P])
+    fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP])
+    fn("sdft_b200_operator_arrays", [P, U64, D, D, D, D])
+    fn("sdft_b200_apply", [P, ctypes.c_int, P, SZ, P, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_apply_pair", [P, P, SZ, P, P, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_project", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
+
+
+def last_error() -> str:
+    lib = library()
+    buf = ctypes.create_string_buffer(4096)
+    lib.sdft_b200_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise _ERRORS.get(status, SdftError)(status, last_error())

@@ -1,0 +1,174 @@
+"""Host-side mirror of the reference's PlaneWaveOperator / HermitianOperator interface.
+
+Thin wrappers over the C ABI: every numerical call runs the CUDA library.
+Arrays may be numpy (host memory, synchronous) or torch CUDA tensors (device
+memory, asynchronous on the context's stream).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+
+_PREC = {"fp64": C.FP64, "mixed": C.MIXED, C.FP64: C.FP64, C.MIXED: C.MIXED}
+
+
+def _precision(value) -> int:
+    try:
+        return _PREC[value]
+    except KeyError:
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {value!r}") from None
+
+
+def _dptr(array):
+    return array.ctypes.data_as(C.D)
+
+
+class Context:
+    """A CUDA stream plus library handles on one device (the reference's per-thread Accelerator)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self._lib = C.library()
+        handle = ctypes.c_void_p()
+        C.check(self._lib.sdft_b200_context_create(device, ctypes.c_void_p(stream or 0), ctypes.byref(handle)))
+        self.handle = handle
+        self.device = device
+
+    def synchronize(self) -> None:
+        C.check(self._lib.sdft_b200_context_synchronize(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.sdft_b200_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def enumerate_g_vectors(reciprocal, cutoff_ev: float, kpoint=(0.0, 0.0, 0.0), hartree_to_ev: float = 27.211386245988):
+    """Plane-wave basis (hkl int32 (n,3), cartesian (n,3), kinetic_ev (n,)) from the library's host code."""
+    lib = C.library()
+    recip = np.ascontiguousarray(reciprocal, dtype=np.float64).reshape(9)
+    k = np.ascontiguousarray(kpoint, dtype=np.float64)
+    count = ctypes.c_size_t()
+    C.check(lib.sdft_b200_enumerate_g_vectors(_dptr(recip), cutoff_ev, _dptr(k), hartree_to_ev, None, None, None, 0,
+                                              ctypes.byref(count)))
+    n = count.value
+    hkl = np.zeros((n, 3), dtype=np.int32)
+    cart = np.zeros((n, 3))
+    kin = np.zeros(n)
+    C.check(lib.sdft_b200_enumerate_g_vectors(_dptr(recip), cutoff_ev, _dptr(k), hartree_to_ev,
+                                              hkl.ctypes.data_as(C.I32), _dptr(cart), _dptr(kin), n,
+                                              ctypes.byref(count)))
+    return hkl, cart, kin
+
+
+class PlaneWaveOperator:
+    """Device-resident H~ and S~ built from the reference's constructor arguments."""
+
+    def __init__(self, context: Context, inputs):
+        self.context = context
+        self._lib = C.library()
+        x = inputs
+        hkl = np.ascontiguousarray(x.hkl, dtype=np.int32)
+        kin = np.ascontiguousarray(x.kinetic_ev, dtype=np.float64)
+        vh = np.ascontiguousarray(x.v_hkl, dtype=np.int32)
+        vv = np.ascontiguousarray(x.v_values, dtype=np.complex128)
+        proj = np.ascontiguousarray(x.projectors, dtype=np.uint64)
+        amp = np.ascontiguousarray(x.amplitudes, dtype=np.complex128)
+        d = np.ascontiguousarray(x.d, dtype=np.complex128)
+        q = np.ascontiguousarray(x.q, dtype=np.complex128)
+        handle = ctypes.c_void_p()
+        C.check(self._lib.sdft_b200_operator_create(
+            context.handle, hkl.shape[0], hkl.ctypes.data_as(C.I32), _dptr(kin), vh.shape[0],
+            vh.ctypes.data_as(C.I32), vv.ctypes.data_as(C.D), proj.size, proj.ctypes.data_as(C.U64),
+            amp.ctypes.data_as(C.D), d.ctypes.data_as(C.D), q.ctypes.data_as(C.D), x.hartree_to_ev, x.regularization,
+            ctypes.byref(handle)))
+        self.handle = handle
+        shape = np.zeros(3, dtype=np.int32)
+        grid = ctypes.c_size_t()
+        nproj = ctypes.c_size_t()
+        npw = ctypes.c_size_t()
+        C.check(self._lib.sdft_b200_operator_info(handle, shape.ctypes.data_as(C.I32), ctypes.byref(grid),
+                                                  ctypes.byref(nproj), ctypes.byref(npw)))
+        self.shape = tuple(int(v) for v in shape)
+        self.grid_points = grid.value
+        self.projectors = nproj.value
+        self.npw = npw.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.sdft_b200_operator_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def arrays(self) -> dict:
+        n, count = self.npw, self.grid_points
+        out = {"indices": np.zeros(n, dtype=np.uint64), "kinetic": np.zeros(n), "h_diagonal": np.zeros(n),
+               "s_diagonal": np.zeros(n), "local_potential": np.zeros(count)}
+        C.check(self._lib.sdft_b200_operator_arrays(self.handle, out["indices"].ctypes.data_as(C.U64),
+                                                    _dptr(out["kinetic"]), _dptr(out["h_diagonal"]),
+                                                    _dptr(out["s_diagonal"]), _dptr(out["local_potential"])))
+        return out
+
+    # -- applications --------------------------------------------------------
+    def _block(self, x):
+        """(pointer, columns, memory, keepalive) for a (npw, cols) block."""
+        if hasattr(x, "data_ptr") and getattr(x, "is_cuda", False):
+            if x.dtype.__repr__() != "torch.complex128" or x.dim() != 2 or x.shape[0] != self.npw:
+                raise ValueError("device blocks must be complex128 tensors of shape (npw, columns)")
+            if not (x.stride(0) == 1 and x.stride(1) == self.npw):
+                raise ValueError("device blocks must be column-major with leading dimension npw")
+            return ctypes.c_void_p(x.data_ptr()), int(x.shape[1]), C.DEVICE, x
+        arr = np.asfortranarray(x, dtype=np.complex128)
+        if arr.ndim == 1:
+            arr = arr.reshape(-1, 1, order="F")
+        if arr.shape[0] != self.npw:
+            raise ValueError("input rows must equal the plane-wave count")
+        return ctypes.c_void_p(arr.ctypes.data), int(arr.shape[1]), C.HOST, arr
+
+    @staticmethod
+    def _like(x, rows=None):
+        if hasattr(x, "data_ptr") and getattr(x, "is_cuda", False):
+            import torch
+            r = rows if rows is not None else x.shape[0]
+            return torch.empty((x.shape[1], r), dtype=x.dtype, device=x.device).T
+        arr = np.asfortranarray(x, dtype=np.complex128)
+        if arr.ndim == 1:
+            arr = arr.reshape(-1, 1, order="F")
+        r = rows if rows is not None else arr.shape[0]
+        return np.zeros((r, arr.shape[1]), dtype=np.complex128, order="F")
+
+    def apply(self, x, overlap: bool = False, precision="fp64", out=None):
+        ptr, cols, mem, keep = self._block(x)
+        y = self._like(keep) if out is None else out
+        yptr = ctypes.c_void_p(y.data_ptr() if mem == C.DEVICE else y.ctypes.data)
+        C.check(self._lib.sdft_b200_apply(self.handle, C.OVERLAP if overlap else C.HAMILTONIAN, ptr, cols, yptr,
+                                          _precision(precision), mem))
+        return y
+
+    def apply_pair(self, x, precision="fp64"):
+        ptr, cols, mem, keep = self._block(x)
+        hy, sy = self._like(keep), self._like(keep)
+        hp = ctypes.c_void_p(hy.data_ptr() if mem == C.DEVICE else hy.ctypes.data)
+        sp = ctypes.c_void_p(sy.data_ptr() if mem == C.DEVICE else sy.ctypes.data)
+        C.check(self._lib.sdft_b200_apply_pair(self.handle, ptr, cols, hp, sp, _precision(precision), mem))
+        return hy, sy
+
+    def project(self, x, precision="fp64"):
+        ptr, cols, mem, keep = self._block(x)
+        p = self._like(keep, rows=self.projectors)
+        pp = ctypes.c_void_p(p.data_ptr() if mem == C.DEVICE else p.ctypes.data)
+        C.check(self._lib.sdft_b200_project(self.handle, ptr, cols, pp, _precision(precision), mem))
+        return p

@@ -1,0 +1,310 @@
+"""Seeded synthetic operator inputs for the generalized Davidson hot path.
+
+Every workload the benchmarks and tests use is built here from a fixed seed:
+no dataset or pseudopotential file is read. The construction:
+
+* cubic cell a*I (bohr); Si diamond sites (fcc + (1/4,1/4,1/4)), GaAs
+  zincblende (Ga on fcc, As on the +(1/4,1/4,1/4) sites), replicated for
+  supercells;
+* plane-wave basis from ``enumerate_g_vectors`` (kinetic sort, then h,k,l),
+  the same rule as the reference (src/pw_core.cpp:140-171);
+* V_loc(G) = sum_a exp(-iG.tau_a) depth_a (2 pi w^2)^{3/2}/Omega exp(-|G|^2 w^2/2)
+  (a real-space Gaussian well of depth ``depth_a`` Hartree and width w = 1 bohr
+  per atom) plus seeded complex noise of standard deviation ``noise`` Hartree
+  per Fourier component on 1/2|G|^2 <= noise_cut*Ecut, paired so that
+  V(-G) = conj V(G) and V(0) is real;
+* 8 projectors per atom: l=0 with sigma in {0.8, 1.2} and l=1 (3 real m) with
+  sigma in {0.8, 1.2}; the Fourier transform of r^l exp(-r^2/(2 sigma^2)) Y_lm:
+  B_p(G+k) = Omega^{-1/2} (-i)^l (2 pi)^{3/2} sigma^{2l+3} |G+k|^l
+             exp(-|G+k|^2 sigma^2/2) Y_lm(G+k) exp(-i (G+k).tau);
+  Y_lm are the real harmonics without Condon-Shortley phase used by the
+  reference (src/paw_compensation.cpp:122-148);
+* D_a: real symmetric 8x8, entries U(-0.5, 0.5) Hartree;
+* Q_a: real symmetric 8x8, entries U(-0.5, 0.5), all atoms scaled by the
+  largest s in (0, 1] with lambda_min(S) >= 0.3, S evaluated on the
+  projector span exactly as the reference's overlap() signature check does
+  (src/plane_wave_operator.cpp:702-717).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Sequence
+
+import numpy as np
+
+HARTREE_TO_EV = 27.211386245988
+TWO_PI = 6.283185307179586476925286766559
+
+
+@dataclasses.dataclass
+class OperatorInputs:
+    """Arrays that define one H~ / S~ pencil, in the reference's conventions."""
+
+    name: str
+    lattice: np.ndarray          # (3,3) rows are lattice vectors, bohr
+    reciprocal: np.ndarray       # (3,3) rows are reciprocal vectors, 1/bohr
+    volume: float
+    positions: np.ndarray        # (atoms,3) fractional
+    species: np.ndarray          # (atoms,) int
+    kpoint: np.ndarray           # (3,) fractional
+    ecut_ha: float
+    hkl: np.ndarray              # (n,3) int32, basis order
+    cartesian: np.ndarray        # (n,3) G (without k), 1/bohr
+    kinetic_ev: np.ndarray       # (n,) 1/2|G+k|^2 in eV
+    v_hkl: np.ndarray            # (nv,3) int32 potential keys
+    v_values: np.ndarray         # (nv,) complex128 Hartree
+    projectors: np.ndarray       # (atoms,) int64
+    amplitudes: np.ndarray       # (sum np, n) complex128, row-major per atom
+    d: np.ndarray                # (atoms, np, np) complex128
+    q: np.ndarray                # (atoms, np, np) complex128
+    roots: int
+    tolerance: float = 1e-12
+    max_iterations: int = 256
+    regularization: float = 1e-12
+    hartree_to_ev: float = HARTREE_TO_EV
+    q_scale: float = 1.0
+
+    @property
+    def npw(self) -> int:
+        return int(self.hkl.shape[0])
+
+    @property
+    def total_projectors(self) -> int:
+        return int(self.projectors.sum())
+
+
+def _cross(a, b):
+    return np.array([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
+
+
+def _dot(a, b):
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+
+def enumerate_g_vectors(reciprocal: np.ndarray, cutoff_ev: float, kpoint: Sequence[float] = (0.0, 0.0, 0.0),
+                        hartree_to_ev: float = HARTREE_TO_EV):
+    """Plane-wave sphere 1/2|G+k|^2 <= cutoff, sorted by (kinetic, h, k, l).
+
+    Same arithmetic, operation order and ordering as the reference's
+    enumerate_g_vectors (src/pw_core.cpp:140-171), so the integer order is
+    bit-identical. Returns (hkl int32 (n,3), cartesian (n,3), kinetic_ev (n,)).
+    """
+    b0, b1, b2 = (np.asarray(reciprocal[i], dtype=np.float64) for i in range(3))
+    if not (cutoff_ev > 0 and math.isfinite(cutoff_ev)):
+        raise ValueError("plane-wave cutoff must be finite and positive")
+    gmax = math.sqrt(2.0 * cutoff_ev / hartree_to_ev)
+    det = float(_dot(b0, _cross(b1, b2)))
+    if abs(det) < 1e-12 or not math.isfinite(det):
+        raise ValueError("reciprocal lattice is singular")
+    d0 = _cross(b1, b2) * (1.0 / det)
+    d1 = _cross(b2, b0) * (1.0 / det)
+    d2 = _cross(b0, b1) * (1.0 / det)
+    kx, ky, kz = (float(v) for v in kpoint)
+    hmax = int(math.ceil(gmax * math.sqrt(float(_dot(d0, d0))) + abs(kx))) + 1
+    kmax = int(math.ceil(gmax * math.sqrt(float(_dot(d1, d1))) + abs(ky))) + 1
+    lmax = int(math.ceil(gmax * math.sqrt(float(_dot(d2, d2))) + abs(kz))) + 1
+    shift = (b0 * kx + b1 * ky) + b2 * kz
+    h, k, l = np.meshgrid(np.arange(-hmax, hmax + 1), np.arange(-kmax, kmax + 1), np.arange(-lmax, lmax + 1),
+                          indexing="ij")
+    h = h.ravel().astype(np.float64)
+    k = k.ravel().astype(np.float64)
+    l = l.ravel().astype(np.float64)
+    # g = (b0*h + b1*k) + b2*l, component-wise, as add(add(scale,scale),scale)
+    gx = (b0[0] * h + b1[0] * k) + b2[0] * l
+    gy = (b0[1] * h + b1[1] * k) + b2[1] * l
+    gz = (b0[2] * h + b1[2] * k) + b2[2] * l
+    sx, sy, sz = gx + shift[0], gy + shift[1], gz + shift[2]
+    g2 = (sx * sx + sy * sy) + sz * sz
+    keep = 0.5 * g2 <= cutoff_ev / hartree_to_ev + 1e-12
+    kinetic = (0.5 * g2[keep]) * hartree_to_ev
+    hi, ki, li = h[keep].astype(np.int32), k[keep].astype(np.int32), l[keep].astype(np.int32)
+    order = np.lexsort((li, ki, hi, kinetic))
+    hkl = np.stack([hi[order], ki[order], li[order]], axis=1).astype(np.int32)
+    cart = np.stack([gx[keep][order], gy[keep][order], gz[keep][order]], axis=1)
+    return hkl, cart, kinetic[order]
+
+
+def real_harmonic(l: int, m: int, q: np.ndarray) -> np.ndarray:
+    """Real spherical harmonics Y_lm(q/|q|), no Condon-Shortley phase.
+
+    Restates the associated-Legendre recurrence of the reference's
+    paw_real_spherical_harmonic (src/paw_compensation.cpp:122-148), vectorised
+    over rows of q. Y_00 = 1/sqrt(4 pi) at q = 0, higher l give 0 there.
+    """
+    q = np.asarray(q, dtype=np.float64)
+    radius = np.sqrt(q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1] + q[:, 2] * q[:, 2])
+    small = radius < 1e-14
+    safe = np.where(small, 1.0, radius)
+    z = np.clip(q[:, 2] / safe, -1.0, 1.0)
+    s = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    order = abs(m)
+    pmm = np.ones_like(z)
+    for kk in range(1, order + 1):
+        pmm = pmm * ((2.0 * kk - 1.0) * s)
+    value = pmm
+    if l > order:
+        previous = pmm
+        value = (2.0 * order + 1.0) * z * pmm
+        for degree in range(order + 2, l + 1):
+            nxt = ((2.0 * degree - 1.0) * z * value - (degree + order - 1.0) * previous) / (degree - order)
+            previous, value = value, nxt
+    factor = math.sqrt((2.0 * l + 1.0) / (4.0 * math.pi) *
+                       math.exp(math.lgamma(l - order + 1.0) - math.lgamma(l + order + 1.0)))
+    if order:
+        factor *= math.sqrt(2.0)
+    angle = order * np.arctan2(q[:, 1], q[:, 0])
+    result = factor * value * (np.sin(angle) if m < 0 else np.cos(angle))
+    return np.where(small, (1.0 / math.sqrt(4.0 * math.pi)) if l == 0 else 0.0, result)
+
+
+DIAMOND_FCC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]], dtype=np.float64)
+
+
+def zincblende_sites(reps: int):
+    """Fractional positions and species (0 = fcc site, 1 = +1/4 site) of a reps^3 supercell."""
+    base = []
+    for sub, offset in ((0, 0.0), (1, 0.25)):
+        for site in DIAMOND_FCC:
+            base.append((sub, site + offset))
+    positions, species = [], []
+    for i in range(reps):
+        for j in range(reps):
+            for k in range(reps):
+                for sub, site in base:
+                    positions.append((site + np.array([i, j, k], dtype=np.float64)) / reps)
+                    species.append(sub)
+    return np.array(positions), np.array(species, dtype=np.int64)
+
+
+def _potential_keys(reciprocal: np.ndarray, cut_ha: float):
+    """All integer G with 1/2|G|^2 <= cut_ha, lexicographic (h,k,l) order."""
+    hkl, cart, _ = enumerate_g_vectors(reciprocal, cut_ha * HARTREE_TO_EV)
+    order = np.lexsort((hkl[:, 2], hkl[:, 1], hkl[:, 0]))
+    return hkl[order], cart[order]
+
+
+def local_potential(lattice, reciprocal, positions, depths, ecut_ha, noise, noise_cut, width, rng):
+    volume = abs(float(np.linalg.det(lattice)))
+    hkl, cart = _potential_keys(reciprocal, noise_cut * ecut_ha)
+    tau = positions @ lattice                      # cartesian atom positions
+    g2 = np.einsum("ij,ij->i", cart, cart)
+    shape = (2.0 * math.pi * width * width) ** 1.5 / volume * np.exp(-0.5 * g2 * width * width)
+    phase = np.exp(-1j * (cart @ tau.T))           # (nv, atoms)
+    values = shape * (phase @ np.asarray(depths, dtype=np.float64))
+    # Hermitian noise: draw on the positive half, mirror to -G.
+    positive = (hkl[:, 0] > 0) | ((hkl[:, 0] == 0) & ((hkl[:, 1] > 0) | ((hkl[:, 1] == 0) & (hkl[:, 2] > 0))))
+    zero = (hkl[:, 0] == 0) & (hkl[:, 1] == 0) & (hkl[:, 2] == 0)
+    draws = rng.standard_normal((hkl.shape[0], 2))
+    noise_values = noise * (draws[:, 0] + 1j * draws[:, 1]) / math.sqrt(2.0)
+    noise_values[zero] = noise * draws[zero, 0]
+    values = values + np.where(positive | zero, noise_values, 0.0)
+    index = {tuple(key): i for i, key in enumerate(hkl.tolist())}
+    negative = np.nonzero(~(positive | zero))[0]
+    partner = np.array([index[(-hkl[i, 0], -hkl[i, 1], -hkl[i, 2])] for i in negative], dtype=np.int64)
+    values[negative] = np.conj(values[partner])
+    values[zero] = values[zero].real
+    return hkl.astype(np.int32), values.astype(np.complex128)
+
+
+def projector_amplitudes(cartesian, kcart, positions, lattice, volume):
+    """(atoms*8, n) complex128 row-major: 2 s-type then 2 x 3 p-type per atom."""
+    q = cartesian + kcart[None, :]
+    qn = np.sqrt(np.einsum("ij,ij->i", q, q))
+    tau = positions @ lattice
+    rows = []
+    channels = [(0, 0, 0.8), (0, 0, 1.2)] + [(1, m, s) for s in (0.8, 1.2) for m in (-1, 0, 1)]
+    ylm = {(l, m): real_harmonic(l, m, q) for l, m, _ in channels}
+    for a in range(tau.shape[0]):
+        structure = np.exp(-1j * (q @ tau[a]))
+        for l, m, sigma in channels:
+            radial = (2.0 * math.pi) ** 1.5 * sigma ** (2 * l + 3) * qn ** l * np.exp(-0.5 * qn * qn * sigma * sigma)
+            rows.append(((-1j) ** l) / math.sqrt(volume) * radial * ylm[(l, m)] * structure)
+    return np.ascontiguousarray(np.array(rows, dtype=np.complex128))
+
+
+def _block_diag(blocks: np.ndarray) -> np.ndarray:
+    atoms, p, _ = blocks.shape
+    out = np.zeros((atoms * p, atoms * p), dtype=blocks.dtype)
+    for a in range(atoms):
+        out[a * p:(a + 1) * p, a * p:(a + 1) * p] = blocks[a]
+    return out
+
+
+def overlap_minimum(amplitudes: np.ndarray, q_blocks: np.ndarray, regularization: float) -> float:
+    """lambda_min of S~ on the projector span, as src/plane_wave_operator.cpp:702-717 evaluates it."""
+    gram = amplitudes @ amplitudes.conj().T
+    w, v = np.linalg.eigh(0.5 * (gram + gram.conj().T))
+    root = (v * np.sqrt(np.maximum(w, 0.0))) @ v.conj().T
+    qfull = _block_diag(q_blocks)
+    small = (1.0 + regularization) * np.eye(gram.shape[0]) + root @ qfull @ root
+    lam = np.linalg.eigvalsh(0.5 * (small + small.conj().T))
+    return float(min(1.0 + regularization, lam.min()))
+
+
+def _scale_q(amplitudes, q_raw, regularization, floor=0.3):
+    if overlap_minimum(amplitudes, q_raw, regularization) >= floor:
+        return 1.0
+    lo, hi = 0.0, 1.0
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        if overlap_minimum(amplitudes, mid * q_raw, regularization) >= floor:
+            lo = mid
+        else:
+            hi = mid
+    return lo
+
+
+def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, depths=(-2.0, -2.0),
+                   kpoint=(0.0, 0.0, 0.0), seed: int = 2026, noise: float = 0.05, noise_cut: float = 4.0,
+                   width: float = 1.0, tolerance: float = 1e-12, max_iterations: int = 256,
+                   regularization: float = 1e-12) -> OperatorInputs:
+    """One synthetic H~/S~ pencil on an a*reps cubic zincblende/diamond supercell."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cell = a * reps
+    lattice = np.eye(3) * cell
+    reciprocal = np.eye(3) * (TWO_PI / cell)
+    volume = cell ** 3
+    positions, species = zincblende_sites(reps)
+    atom_depths = np.array([depths[s] for s in species], dtype=np.float64)
+    hkl, cart, kinetic = enumerate_g_vectors(reciprocal, ecut_ha * HARTREE_TO_EV, kpoint)
+    v_hkl, v_values = local_potential(lattice, reciprocal, positions, atom_depths, ecut_ha, noise, noise_cut,
+                                      width, rng)
+    kcart = np.asarray(kpoint, dtype=np.float64) @ reciprocal
+    amplitudes = projector_amplitudes(cart, kcart, positions, lattice, volume)
+    atoms = positions.shape[0]
+    d = rng.uniform(-0.5, 0.5, size=(atoms, 8, 8))
+    d = 0.5 * (d + np.transpose(d, (0, 2, 1)))
+    q_raw = rng.uniform(-0.5, 0.5, size=(atoms, 8, 8))
+    q_raw = 0.5 * (q_raw + np.transpose(q_raw, (0, 2, 1)))
+    scale = _scale_q(amplitudes, q_raw.astype(np.complex128), regularization)
+    return OperatorInputs(name=name, lattice=lattice, reciprocal=reciprocal, volume=volume, positions=positions,
+                          species=species, kpoint=np.asarray(kpoint, dtype=np.float64), ecut_ha=ecut_ha, hkl=hkl,
+                          cartesian=cart, kinetic_ev=kinetic, v_hkl=v_hkl, v_values=v_values,
+                          projectors=np.full(atoms, 8, dtype=np.int64), amplitudes=amplitudes,
+                          d=d.astype(np.complex128), q=(scale * q_raw).astype(np.complex128), roots=roots,
+                          tolerance=tolerance, max_iterations=max_iterations, regularization=regularization,
+                          q_scale=scale)
+
+
+def si8(seed: int = 2026, **kw) -> OperatorInputs:
+    """Diamond-cubic Si8, a = 10.26 bohr, Gamma, Ecut 15 Ha, 16 bands."""
+    return build_operator("si8", 10.26, 1, 15.0, 16, seed=seed, **kw)
+
+
+def si64(seed: int = 2026, **kw) -> OperatorInputs:
+    """Si64 supercell, a = 20.52 bohr (2x2x2 of 10.26), Gamma, Ecut 15 Ha, 160 bands, 512 projectors."""
+    return build_operator("si64", 10.26, 2, 15.0, 160, seed=seed, **kw)
+
+
+def gaas_kpoint(index: int, seed: int = 2026, **kw) -> OperatorInputs:
+    """GaAs 2x2x2 zincblende (a = 21.36), Ecut 18 Ha, 192 bands, k of a 3x3x3 Monkhorst-Pack mesh."""
+    i, j, k = index // 9, (index // 3) % 3, index % 3
+    kpoint = tuple((2 * v - 2) / 6.0 for v in (i, j, k))  # ((2n - q - 1)/2q) for q = 3, n = 1..3
+    return build_operator(f"gaas_k{index}", 10.68, 2, 18.0, 192, depths=(-2.2, -1.8), kpoint=kpoint, seed=seed,
+                          **kw)
+
+
+def tiny(seed: int = 7, ecut_ha: float = 4.0, roots: int = 6, a: float = 7.0, **kw) -> OperatorInputs:
+    """A small diamond cell for fast parity tests (a few hundred plane waves)."""
+    return build_operator("tiny", a, 1, ecut_ha, roots, seed=seed, **kw)

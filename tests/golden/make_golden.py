@@ -1,0 +1,113 @@
+"""Generates tests/golden/*.npz from the reference's own CPU implementation.
+
+Run in a container that has the reference built into oracle/_ref:
+
+    make -C oracle/ref && python tests/golden/make_golden.py [--si64]
+
+Inputs are the seeded synthetic pencils of sdft_b200.synthetic (regenerated
+from their seeds by the tests, so only reference OUTPUTS are stored). Values
+come from the unmodified reference: the PWO3 solver snapshot it writes
+(src/plane_wave_operator.cpp:542-569) for its internal arrays, its
+apply_block_into / apply_pair_into callbacks for H~x, S~x, and
+solve_generalized_hermitian_davidson for eigenpairs.
+"""
+from __future__ import annotations
+
+import argparse
+import pathlib
+import struct
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "sparse-dft_b200"))
+
+from sdft_b200 import synthetic  # noqa: E402
+from oracle import ref_oracle  # noqa: E402
+
+HERE = pathlib.Path(__file__).resolve().parent
+
+
+def read_pwo3(path):
+    """Parse a PWO3 snapshot (little-endian; layout of src/plane_wave_operator.cpp:553-567)."""
+    raw = pathlib.Path(path).read_bytes()
+    if raw[:8] != b"SDFTPWO3":
+        raise ValueError("not a PWO3 snapshot")
+    n, count, s0, s1, s2, nproj, roots, iters, ninit = struct.unpack_from("<9Q", raw, 8)
+    reg, tol = struct.unpack_from("<2d", raw, 80)
+    off = 96
+    (atoms,) = struct.unpack_from("<Q", raw, off)
+    off += 8
+    channels = np.frombuffer(raw, dtype="<u8", count=atoms, offset=off)
+    off += 8 * atoms
+    out = {"shape": (s0, s1, s2), "count": count, "regularization": reg, "tolerance": tol, "roots": roots,
+           "iterations": iters, "channels": channels.copy()}
+    out["indices"] = np.frombuffer(raw, dtype="<u8", count=n, offset=off).copy()
+    off += 8 * n
+    for name, length in (("kinetic", n), ("h_diagonal", n), ("s_diagonal", n), ("local_real", count)):
+        out[name] = np.frombuffer(raw, dtype="<f8", count=length, offset=off).copy()
+        off += 8 * length
+    out["all_b"] = np.frombuffer(raw, dtype="<c16", count=nproj * n, offset=off).reshape((nproj, n), order="F").copy()
+    off += 16 * nproj * n
+    d, q = [], []
+    for c in channels:
+        c = int(c)
+        d.append(np.frombuffer(raw, dtype="<c16", count=c * c, offset=off).reshape((c, c), order="F").copy())
+        off += 16 * c * c
+        q.append(np.frombuffer(raw, dtype="<c16", count=c * c, offset=off).reshape((c, c), order="F").copy())
+        off += 16 * c * c
+    out["d"], out["q"] = d, q
+    out["initial"] = np.frombuffer(raw, dtype="<c16", count=ninit, offset=off).copy()
+    return out
+
+
+def probe_block(npw: int, columns: int, seed: int) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.asfortranarray(rng.standard_normal((npw, columns)) + 1j * rng.standard_normal((npw, columns)))
+
+
+def operator_fixture(lib, inputs, name, columns=4, seed=11, solve=True):
+    op = ref_oracle.ReferenceOperator(lib, inputs)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = pathlib.Path(tmp) / "op.pwop"
+        op.save_snapshot(path, inputs.roots, inputs.max_iterations, inputs.tolerance)
+        snap = read_pwo3(path)
+    x = probe_block(inputs.npw, columns, seed)
+    hx = op.apply(x, overlap=False, exact=True)
+    sx = op.apply(x, overlap=True, exact=True)
+    fields = dict(shape=np.array(snap["shape"]), indices=snap["indices"], kinetic=snap["kinetic"],
+                  h_diagonal=snap["h_diagonal"], s_diagonal=snap["s_diagonal"], local_real=snap["local_real"],
+                  hkl=inputs.hkl, kinetic_ev=inputs.kinetic_ev, probe_seed=np.array(seed), hx=hx, sx=sx)
+    if solve:
+        t = time.time()
+        result = op.davidson(inputs.roots, inputs.max_iterations, inputs.tolerance)
+        fields.update(eigenvalues=result["eigenvalues"], residuals=result["residuals"],
+                      converged=np.array(result["converged"]), iterations=np.array(result["iterations"]),
+                      seconds=np.array(time.time() - t))
+    np.savez_compressed(HERE / f"{name}.npz", **fields)
+    print(name, "npw", inputs.npw, "grid", snap["shape"], {k: v for k, v in fields.items() if k in ("iterations",)})
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
+    args = parser.parse_args()
+    lib = ref_oracle.ReferenceLibrary()
+    operator_fixture(lib, synthetic.tiny(), "tiny")
+    operator_fixture(lib, synthetic.si8(), "si8", solve=True)
+    if args.si64:
+        inputs = synthetic.si64()
+        op = ref_oracle.ReferenceOperator(lib, inputs)
+        t = time.time()
+        result = op.davidson(inputs.roots, inputs.max_iterations, inputs.tolerance)
+        np.savez_compressed(HERE / "si64_solution.npz", eigenvalues=result["eigenvalues"],
+                            residuals=result["residuals"], converged=np.array(result["converged"]),
+                            iterations=np.array(result["iterations"]), seconds=np.array(time.time() - t))
+
+
+if __name__ == "__main__":
+    main()

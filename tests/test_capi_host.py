@@ -1,0 +1,69 @@
+"""C ABI checks that need no GPU: the library loads, exports its header, host logic is exact."""
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from sdft_b200 import _capi as C
+from sdft_b200 import operator as sop
+from sdft_b200 import synthetic
+
+
+def test_library_loads():
+    assert C.LIBRARY.exists(), "libsdft_b200.so must be built in-tree"
+    lib = C.library()
+    assert b"sm_100a" in lib.sdft_b200_version()
+
+
+def test_every_declared_symbol_is_exported():
+    declared = C.declared_symbols()
+    assert len(declared) >= 13
+    exported = subprocess.run(["nm", "-D", "--defined-only", str(C.LIBRARY)], capture_output=True, text=True,
+                              check=True).stdout
+    names = {line.split()[-1] for line in exported.splitlines() if line.strip()}
+    missing = [s for s in declared if s not in names]
+    assert not missing, missing
+    lib = C.library()
+    for s in declared:
+        assert hasattr(lib, s)
+
+
+def test_library_is_sm100a_only():
+    out = subprocess.run(["cuobjdump", "--list-elf", str(C.LIBRARY)], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+@pytest.mark.parametrize("factory", [synthetic.tiny, synthetic.si8])
+def test_enumeration_bit_exact(golden, factory):
+    x = factory()
+    hkl, cart, kin = sop.enumerate_g_vectors(x.reciprocal, x.ecut_ha * synthetic.HARTREE_TO_EV)
+    g = golden(x.name)
+    assert np.array_equal(hkl, g["hkl"]) and np.array_equal(kin, g["kinetic_ev"])
+    assert np.array_equal(cart, x.cartesian)
+
+
+def test_enumeration_kpoint_and_errors():
+    x = synthetic.tiny()
+    for k in ((1 / 3, 0.0, -1 / 3), (0.25, 0.5, 0.0)):
+        a = sop.enumerate_g_vectors(x.reciprocal, 4.0 * synthetic.HARTREE_TO_EV, k)
+        b = synthetic.enumerate_g_vectors(x.reciprocal, 4.0 * synthetic.HARTREE_TO_EV, k)
+        assert all(np.array_equal(u, v) for u, v in zip(a, b))
+    with pytest.raises(C.InvalidArgument):
+        sop.enumerate_g_vectors(x.reciprocal, -1.0)
+    with pytest.raises(C.InvalidArgument):
+        sop.enumerate_g_vectors(np.zeros((3, 3)), 10.0)
+    assert "cutoff" in C.last_error() or "singular" in C.last_error()
+
+
+def test_context_without_gpu_reports_cuda_error():
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    lib = C.library()
+    handle = ctypes.c_void_p()
+    status = lib.sdft_b200_context_create(0, None, ctypes.byref(handle))
+    assert status == C.CUDA_ERROR
+    assert "CUDA" in C.last_error()
