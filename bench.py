@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark: certified eigenpairs/s of the generalized Davidson solve on one B200.
+
+Workload: the Si64-shaped Gamma-point pencil (a = 20.52 bohr, 64 atoms, Ecut 15 Ha,
+NPW 23847, FFT grid 70^3, 512 projectors, 160 bands, tolerance 1e-12 Ha, cold
+start), seeded synthetic inputs. One step = one full Davidson solve of that
+pencil in the mixed-precision form (FP32 FFT/V_loc, FP32-accumulated search
+GEMMs, FP64 Rayleigh-Ritz, refresh and certification), inputs resident in HBM.
+The FP64 plain form is timed on the same GPU beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs N independent replicas (one per rank, launched by torchrun); the
+solve itself does not shard. --impl reference times the reference's own CPU
+implementation (oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "sparse-dft_b200"))
+
+METRIC = "certified eigenpairs/s at <=1e-12 Ha, mixed vs FP64 on 1 B200; p50/p99 solve ms"
+UNIT = "certified eigenpairs/s"
+TOLERANCE = 1e-12
+WORKLOAD = "si64_gamma_davidson"
+
+
+def config(args, extra=None):
+    cfg = {"workload": WORKLOAD, "cell": "Si64 diamond 2x2x2, a=20.52 bohr", "npw": 23847, "fft_grid": [70, 70, 70],
+           "projectors": 512, "bands": 160, "ecut_ha": 15.0, "tolerance_ha": TOLERANCE, "start": "cold",
+           "l2": "inputs larger than L2 (basis + images 1.5 GB, slab 220 MB per 160-column apply)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def load_inputs():
+    """Synthetic Si64 pencil; cached as .npz in the temp dir (seeded, deterministic)."""
+    import numpy as np
+    from sdft_b200 import synthetic
+    cache = pathlib.Path(tempfile.gettempdir()) / "sdft_b200_si64_seed2026.npz"
+    if cache.exists():
+        data = dict(np.load(cache))
+        return synthetic.OperatorInputs(
+            name="si64", lattice=data["lattice"], reciprocal=data["reciprocal"], volume=float(data["volume"]),
+            positions=data["positions"], species=data["species"], kpoint=data["kpoint"], ecut_ha=15.0,
+            hkl=data["hkl"], cartesian=data["cartesian"], kinetic_ev=data["kinetic_ev"], v_hkl=data["v_hkl"],
+            v_values=data["v_values"], projectors=data["projectors"], amplitudes=data["amplitudes"], d=data["d"],
+            q=data["q"], roots=160, q_scale=float(data["q_scale"]))
+    x = synthetic.si64()
+    try:
+        np.savez(cache, lattice=x.lattice, reciprocal=x.reciprocal, volume=x.volume, positions=x.positions,
+                 species=x.species, kpoint=x.kpoint, hkl=x.hkl, cartesian=x.cartesian, kinetic_ev=x.kinetic_ev,
+                 v_hkl=x.v_hkl, v_values=x.v_values, projectors=x.projectors, amplitudes=x.amplitudes, d=x.d,
+                 q=x.q, q_scale=x.q_scale)
+    except OSError:
+        pass
+    return x
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.path = pathlib.Path(tempfile.mkstemp(prefix="sdft_clocks_", suffix=".csv")[1])
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        loaded = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit() and float(r[3] or 0) > 200.0] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def distributed():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_cpu_sample(inputs, iterations: int):
+    """The reference's own Davidson (oracle/_ref) for `iterations` iterations on the host cores."""
+    from oracle import ref_oracle
+    lib = ref_oracle.ReferenceLibrary()
+    op = ref_oracle.ReferenceOperator(lib, inputs)
+    t0 = time.perf_counter()
+    result = op.davidson(inputs.roots, iterations, TOLERANCE)
+    seconds = time.perf_counter() - t0
+    return seconds, result
+
+
+def cpu_full_solve_iterations() -> int:
+    """Iterations the reference needs for this pencil (recorded with its solution in tests/golden)."""
+    import numpy as np
+    return int(np.load(ROOT / "tests" / "golden" / "si64_solution.npz")["iterations"])
+
+
+def run_reference(args):
+    world, rank, _ = distributed()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    inputs = load_inputs()
+    full_iterations = cpu_full_solve_iterations()
+    sample_iterations = 2
+    for _ in range(args.warmup):
+        pass  # the reference has no device state to warm; its setup is outside the timed region
+    times = []
+    for _ in range(args.steps):
+        seconds, _ = reference_cpu_sample(inputs, sample_iterations)
+        times.append(seconds)
+    per_iteration = statistics.median(times) / sample_iterations
+    solve = per_iteration * full_iterations
+    value = inputs.roots / solve
+    sample = (f"reference Davidson (oracle/_ref, unmodified src/ + FFTW-API shim) for {sample_iterations} iterations "
+              f"per step, extrapolated to the {full_iterations} iterations the reference needs for this pencil")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": config(args, {"parallelism": "cpu", "threads": threads}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "extrapolated_solve_ms": solve * 1e3}), flush=True)
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    world, rank, local = distributed()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(local)
+    from sdft_b200 import _capi as C
+    from sdft_b200.operator import Context, PlaneWaveOperator
+
+    inputs = load_inputs()
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream.cuda_stream)
+    op = PlaneWaveOperator(ctx, inputs)
+    roots = inputs.roots
+    lib = C.library()
+
+    def solve(precision):
+        return op.davidson(roots, 256, TOLERANCE, precision=precision, vectors=False)
+
+    def certified(result):
+        return int(np.sum(result["residuals"] <= TOLERANCE))
+
+    for _ in range(max(args.warmup, 0)):
+        solve("mixed")
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = lib.sdft_b200_kernel_launches()
+    step_ms, pairs, iters, stats = [], 0, [], None
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start_all = torch.cuda.Event(enable_timing=True)
+        end_all = torch.cuda.Event(enable_timing=True)
+        start_all.record(stream)
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            result = solve("mixed")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            pairs += certified(result)
+            iters.append(result["iterations"])
+            stats = result["stats"]
+        end_all.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.sdft_b200_kernel_launches() - launches0
+    barrier(world)
+    total_ms = max_over_ranks(start_all.elapsed_time(end_all), world)
+    value = pairs * world / (total_ms / 1e3)
+
+    # FP64 plain form on the same GPU (after the timed region).
+    fp64_ms, fp64_pairs = [], 0
+    for _ in range(max(1, min(args.steps, 2))):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r64 = solve("fp64")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms.append(e0.elapsed_time(e1))
+        fp64_pairs += certified(r64)
+    fp64_value = fp64_pairs / (sum(fp64_ms) / 1e3)
+
+    # Roofline of the fused local H~psi (FP32 slab FFT) on a 160-column block.
+    roofline = fused_local_roofline(op, inputs, stream)
+
+    # End to end through the public API with host buffers: operator upload from
+    # host arrays, solve, eigenvectors read back, every step.
+    e2e = end_to_end(ctx, inputs, stream, steps=max(1, min(args.steps, 2)))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(inputs)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (mixed search, FP64 certificate)",
+            "data": "synthetic (seeded)",
+            "config": config(args, {"parallelism": f"replicas{world}", "precision": "mixed"}),
+            "p50_solve_ms": statistics.median(step_ms), "p99_solve_ms": float(np.percentile(step_ms, 99)),
+            "iterations": iters, "certified_pairs_per_solve": pairs / args.steps,
+            "fp64_plain": {"value": fp64_value, "unit": UNIT, "p50_solve_ms": statistics.median(fp64_ms),
+                           "certified_pairs_per_solve": fp64_pairs / len(fp64_ms)},
+            "mixed_over_fp64": statistics.median(fp64_ms) / statistics.median(step_ms),
+            "solver_stats": stats, "clocks": clocks.summary(), "gpu_launches": int(launches),
+            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    op.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def fused_local_roofline(op, inputs, stream):
+    import torch
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    cols = inputs.roots
+    x = torch.randn(cols, op.npw, dtype=torch.complex128, device="cuda").T
+    y = torch.empty((cols, op.npw), dtype=torch.complex128, device="cuda").T
+    for _ in range(3):
+        op.local_apply(x, y, precision="mixed")
+    torch.cuda.synchronize()
+    reps = 20
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        op.local_apply(x, y, precision="mixed")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    n0, n1, n2 = op.shape
+    slots = op.active_rows
+    # algorithmic bytes per column: FP64 psi in + T psi re-read + FP64 out, plus
+    # one FP32 slab write+read between plane and pencil passes, each direction.
+    per_column = 3 * 16 * op.npw + 2 * (2 * 8 * slots * n1 * n2)
+    algorithmic = per_column * cols + 4 * n0 * n1 * n2
+    achieved = algorithmic / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "fused local H~psi (plane_in + pencil + plane_out), FP32, 160 columns",
+            "ms_per_launch": ms, "algorithmic_bytes": algorithmic,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+
+def end_to_end(ctx, inputs, stream, steps):
+    import numpy as np
+    import torch
+    from sdft_b200.operator import PlaneWaveOperator
+    h2d = (inputs.amplitudes.nbytes + inputs.v_values.nbytes + inputs.v_hkl.nbytes + inputs.hkl.nbytes +
+           inputs.kinetic_ev.nbytes + inputs.d.nbytes + inputs.q.nbytes)
+    d2h = inputs.roots * inputs.npw * 16 + 2 * inputs.roots * 8
+    pairs, seconds = 0, 0.0
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        op = PlaneWaveOperator(ctx, inputs)
+        result = op.davidson(inputs.roots, 256, TOLERANCE, precision="mixed", vectors=True)
+        torch.cuda.synchronize()
+        seconds += time.perf_counter() - t0
+        pairs += int(np.sum(result["residuals"] <= TOLERANCE))
+        op.close()
+    return {"value": pairs / seconds, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "path": "sdft_b200_operator_create (host arrays) + sdft_b200_davidson (host eigenvectors)"}
+
+
+def cpu_baseline(inputs):
+    from oracle import ref_oracle
+    if not ref_oracle.available():
+        return None
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    iterations = 2
+    seconds, _ = reference_cpu_sample(inputs, iterations)
+    full = cpu_full_solve_iterations()
+    solve = seconds / iterations * full
+    return {"value": inputs.roots / solve, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference Davidson for {iterations} iterations on the host cores "
+                      f"({seconds:.1f} s), extrapolated to its {full}-iteration solve of this pencil"}
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

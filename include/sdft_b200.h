@@ -45,6 +45,10 @@ typedef struct sdft_b200_operator sdft_b200_operator;
 SDFT_B200_API size_t sdft_b200_last_error(char* buffer, size_t length);
 /* Library version string (static storage). */
 SDFT_B200_API const char* sdft_b200_version(void);
+/* Number of this library's own CUDA kernels launched by the process so far
+ * (cuBLAS/cuSOLVER launches are not counted). No reference counterpart: it
+ * backs the benchmark's launch accounting. */
+SDFT_B200_API unsigned long long sdft_b200_kernel_launches(void);
 
 /* One CUDA stream + library handles on `device`. `stream` may be NULL (a
  * private non-blocking stream is created) or a cudaStream_t to share.
@@ -74,10 +78,11 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_create(sdft_b200_context* cont
                                            sdft_b200_operator** out);
 SDFT_B200_API sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op);
 
-/* Grid shape, grid points and total projector rows.
+/* Grid shape, grid points, total projector rows, plane waves, and the number
+ * of grid rows i0 that hold sphere points (the rows the fused FFT keeps).
  * Replaces: PlaneWaveOperator::fft_grid_points, src/plane_wave_operator.hpp:38. */
 SDFT_B200_API sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t shape[3], size_t* grid_points,
-                                         size_t* projectors, size_t* npw);
+                                         size_t* projectors, size_t* npw, size_t* active_rows);
 /* Sphere-to-grid index map (npw values), T (Hartree), H and S diagonals
  * (npw each), V(r) (grid_points values); any pointer may be NULL.
  * Replaces: the Impl members indices/kinetic/h_diagonal/s_diagonal/local_real,
@@ -91,6 +96,12 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_arrays(const sdft_b200_operato
  * (Impl::apply_block_into, src/plane_wave_operator.cpp:218-306). */
 SDFT_B200_API sdft_b200_status sdft_b200_apply(sdft_b200_operator* op, int which, const double* x, size_t columns, double* y,
                                  int precision, int memory);
+/* Local part only, y = T x + (1/N) FFT_fwd(V(r) FFT_bwd(x))[idx], on the
+ * operator's resident grid maps and V(r). MIXED runs the FFTs and V(r) in FP32.
+ * Replaces: Accelerator::local_hamiltonian / accelerated_local_hamiltonian,
+ * src/compute_backend.hpp:42-45,81-83 (CPU loop src/plane_wave_operator.cpp:237-257). */
+SDFT_B200_API sdft_b200_status sdft_b200_apply_local(sdft_b200_operator* op, const double* x, size_t columns, double* y,
+                                                     int precision, int memory);
 /* Joint (H~x, S~x) sharing one B x.
  * Replaces: HermitianOperator::apply_pair_into, src/pw_core.hpp:122-124 (src/plane_wave_operator.cpp:307-374). */
 SDFT_B200_API sdft_b200_status sdft_b200_apply_pair(sdft_b200_operator* op, const double* x, size_t columns, double* hy,
@@ -99,6 +110,43 @@ SDFT_B200_API sdft_b200_status sdft_b200_apply_pair(sdft_b200_operator* op, cons
  * Replaces: HermitianOperator::project_into, src/pw_core.hpp:130-131 (src/plane_wave_operator.cpp:375-380). */
 SDFT_B200_API sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size_t columns, double* p,
                                    int precision, int memory);
+
+/* Davidson controls. precision selects the search arithmetic (MIXED: FP32
+ * FFT/V_loc and FP32-accumulated projector and subspace products; FP64: the
+ * plain form throughout); Rayleigh-Ritz, the FP64 refresh and the final
+ * certificate are FP64 on the device in both. subspace_factor in [4,16]
+ * (capacity = min(npw, max(factor*roots, 64)); 0 selects 8). handoff: search
+ * residual below which the basis is re-applied in FP64 (0 selects 1e-8). */
+typedef struct {
+  size_t roots;
+  size_t max_iterations;
+  double tolerance;
+  int precision;
+  int subspace_factor;
+  double handoff;
+} sdft_b200_davidson_options;
+
+typedef struct {
+  size_t iterations;
+  int converged;
+  double max_residual;
+  double seconds;
+  double rayleigh_ritz_seconds;
+  size_t h_columns_search, h_columns_fp64, s_columns_search, s_columns_fp64;
+  int rayleigh_ritz_calls, restarts, fp64_refreshes, certifications, handoff_iteration, block_rank_fallbacks;
+} sdft_b200_davidson_stats;
+
+/* Lowest `roots` eigenpairs of H~ x = e S~ x. initial: band-major roots x npw
+ * warm vectors or NULL; eigenvectors: band-major roots x npw output (may be
+ * NULL); residuals: fresh FP64 ||H~x - e S~x|| per root. memory applies to
+ * initial/eigenvectors (eigenvalues, residuals and stats are host memory).
+ * A solve that exhausts max_iterations returns OK with stats->converged = 0
+ * and its fresh residuals, as the reference does.
+ * Replaces: solve_generalized_hermitian_davidson(const HermitianOperator&, const HermitianOperator&,
+ * size_t, size_t, double, const std::vector<std::complex<double>>&), src/pw_core.hpp:184-188. */
+SDFT_B200_API sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                                  const double* initial, double* eigenvalues, double* eigenvectors,
+                                                  double* residuals, sdft_b200_davidson_stats* stats, int memory);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/sdft_b200.h"
+#include "davidson.cuh"
 #include "operator.cuh"
 
 struct sdft_b200_context {
@@ -12,6 +13,7 @@ struct sdft_b200_context {
 };
 struct sdft_b200_operator {
   std::unique_ptr<sdft_b200::DeviceOperator> impl;
+  std::unique_ptr<sdft_b200::DavidsonSolver> solver;  // workspace reused across solves
 };
 
 namespace {
@@ -102,6 +104,8 @@ size_t sdft_b200_last_error(char* buffer, size_t length) {
 
 const char* sdft_b200_version(void) { return "sdft_b200 0.1 sm_100a"; }
 
+unsigned long long sdft_b200_kernel_launches(void) { return sdft_b200::launch_count(); }
+
 sdft_b200_status sdft_b200_context_create(int device, void* stream, sdft_b200_context** out) {
   return guarded([&] {
     require(out != nullptr, "null context output");
@@ -172,7 +176,7 @@ sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op) {
 }
 
 sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t shape[3], size_t* grid_points,
-                                         size_t* projectors, size_t* npw) {
+                                         size_t* projectors, size_t* npw, size_t* active_rows) {
   return guarded([&] {
     require(op != nullptr, "null operator");
     const auto& plan = op->impl->plan();
@@ -181,6 +185,25 @@ sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t s
     if (grid_points) *grid_points = plan.count;
     if (projectors) *projectors = static_cast<size_t>(op->impl->projectors());
     if (npw) *npw = static_cast<size_t>(op->impl->npw());
+    if (active_rows) *active_rows = static_cast<size_t>(plan.slots);
+  });
+}
+
+sdft_b200_status sdft_b200_apply_local(sdft_b200_operator* op, const double* x, size_t columns, double* y,
+                                       int precision, int memory) {
+  return guarded([&] {
+    require(op && x && y && columns && x != y, "invalid direct plane-wave input/output buffers");
+    require(columns <= static_cast<size_t>(INT32_MAX), "too many columns");
+    auto& o = *op->impl;
+    auto& ctx = o.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    const std::size_t n = static_cast<std::size_t>(o.npw()) * columns;
+    Staged stage(ctx, memory);
+    const auto* dx = stage.in(x, n, ctx.staging_in);
+    auto* dy = stage.out(y, n, ctx.staging_out);
+    o.apply_local(dx, static_cast<int>(columns), dy, precision_of(precision));
+    stage.back(y, dy, n);
+    stage.finish();
   });
 }
 
@@ -256,6 +279,65 @@ sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size
     o.project(dx, static_cast<int>(columns), dp, precision_of(precision));
     stage.back(p, dp, m);
     stage.finish();
+  });
+}
+
+sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                   const double* initial, double* eigenvalues, double* eigenvectors,
+                                   double* residuals, sdft_b200_davidson_stats* stats, int memory) {
+  return guarded([&] {
+    require(op && options && eigenvalues && residuals, "invalid matrix-free Davidson problem");
+    require(memory == SDFT_B200_MEMORY_HOST || memory == SDFT_B200_MEMORY_DEVICE, "memory must be host or device");
+    auto& o = *op->impl;
+    auto& ctx = o.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid matrix-free Davidson problem");
+    require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid matrix-free Davidson problem");
+    sdft_b200::DavidsonOptions d;
+    d.roots = static_cast<int>(options->roots);
+    d.max_iterations = static_cast<int>(options->max_iterations);
+    d.tolerance = options->tolerance;
+    d.precision = precision_of(options->precision);
+    d.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
+    d.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    const std::size_t block = static_cast<std::size_t>(o.npw()) * d.roots;
+    const Cx<double>* warm = nullptr;
+    if (initial) {
+      Staged stage(ctx, memory);
+      warm = stage.in(initial, block, ctx.staging_in);
+    }
+    if (!op->solver) op->solver = std::make_unique<sdft_b200::DavidsonSolver>(o);
+    auto& solver = *op->solver;
+    solver.solve(d, warm);
+    const auto& values = solver.eigenvalues();
+    const auto& res = solver.residuals();
+    std::copy(values.begin(), values.end(), eigenvalues);
+    std::copy(res.begin(), res.end(), residuals);
+    if (eigenvectors) {
+      // column-major npw x roots on the device is band-major roots x npw
+      SDFT_CUDA(cudaMemcpyAsync(eigenvectors, solver.vectors(), sizeof(Cx<double>) * block,
+                                memory == SDFT_B200_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                ctx.stream));
+      ctx.synchronize();
+    }
+    if (stats) {
+      const auto& st = solver.stats();
+      stats->iterations = static_cast<size_t>(st.iterations);
+      stats->converged = st.converged ? 1 : 0;
+      stats->max_residual = st.max_residual;
+      stats->seconds = st.seconds;
+      stats->rayleigh_ritz_seconds = st.rr_seconds;
+      stats->h_columns_search = static_cast<size_t>(st.h_columns_search);
+      stats->h_columns_fp64 = static_cast<size_t>(st.h_columns_fp64);
+      stats->s_columns_search = static_cast<size_t>(st.s_columns_search);
+      stats->s_columns_fp64 = static_cast<size_t>(st.s_columns_fp64);
+      stats->rayleigh_ritz_calls = st.rayleigh_ritz;
+      stats->restarts = st.restarts;
+      stats->fp64_refreshes = st.fp64_refreshes;
+      stats->certifications = st.certifications;
+      stats->handoff_iteration = st.handoff_iteration;
+      stats->block_rank_fallbacks = st.block_rank_fallbacks;
+    }
   });
 }
 

@@ -26,8 +26,11 @@ struct NonFinite : std::runtime_error {
 inline void check_cuda(cudaError_t code, const char* what) {
   if (code != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(code));
 }
+// Counts this library's own kernel launches (library GEMMs/eigensolvers excluded).
+void count_launch();
+unsigned long long launch_count();
 #define SDFT_CUDA(call) ::sdft_b200::check_cuda((call), #call)
-#define SDFT_LAUNCH(what) ::sdft_b200::check_cuda(cudaGetLastError(), what)
+#define SDFT_LAUNCH(what) (::sdft_b200::count_launch(), ::sdft_b200::check_cuda(cudaGetLastError(), what))
 
 // Interleaved complex in precision T (float2/double2 layout).
 template <typename T>

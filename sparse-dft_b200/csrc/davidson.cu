@@ -1,0 +1,423 @@
+// Device-resident generalized block Davidson (restates the control flow of the
+// reference's solve_generalized_hermitian_davidson, src/pw_core.cpp:532-1437,
+// with its default flags: joint H/S, block CGS2 in the S metric, incremental
+// Galerkin slabs, kinetic preconditioner, thick restart to 2*roots, FP64
+// refresh when the approximate search converges, fresh FP64 certification).
+//
+// Every NPW-long array (basis, H/S images, Ritz block, residuals) stays in HBM
+// for the whole solve; the host sees only per-column scalars (residual norms,
+// Ritz values) to take the same branch decisions as the reference.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cmath>
+#include <numeric>
+#include <string>
+
+#include "davidson.cuh"
+#include "dense.cuh"
+
+namespace sdft_b200 {
+
+namespace {
+void check_solver(cusolverStatus_t status, const char* what) {
+  if (status != CUSOLVER_STATUS_SUCCESS)
+    throw CudaError(std::string("cuSOLVER error ") + std::to_string(static_cast<int>(status)) + " in " + what);
+}
+double now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+template <typename T>
+T* as(Scratch& s, std::size_t count) {
+  return static_cast<T*>(s.reserve(sizeof(T) * std::max<std::size_t>(count, 1)));
+}
+}  // namespace
+
+std::vector<double> DavidsonSolver::download(const double* device, int count) {
+  std::vector<double> host(std::max(count, 0));
+  if (count > 0) {
+    SDFT_CUDA(cudaMemcpyAsync(host.data(), device, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                              op_.context().stream));
+    op_.context().synchronize();
+  }
+  return host;
+}
+
+void DavidsonSolver::gemm(Op aop, int m, int n, int k, const Cx<double>* a, long long lda, const Cx<double>* b,
+                          long long ldb, Cx<double>* c, long long ldc, bool add, double alpha, bool exact) {
+  auto& ctx = op_.context();
+  if (exact) zgemm(ctx.blas, aop, Op::N, m, n, k, a, lda, b, ldb, c, ldc, add, alpha);
+  else gemm_mixed(aop, m, n, k, a, nullptr, lda, b, ldb, c, ldc, add, ctx.gemm_work, ctx.stream, alpha);
+}
+
+void DavidsonSolver::apply_h(const Cx<double>* x, int cols, Cx<double>* y, bool exact) {
+  op_.apply_hamiltonian(x, cols, y, exact ? Precision::FP64 : Precision::Mixed);
+  (exact ? stats_.h_columns_fp64 : stats_.h_columns_search) += cols;
+}
+
+void DavidsonSolver::apply_s(const Cx<double>* x, int cols, Cx<double>* y, bool exact) {
+  op_.apply_overlap(x, cols, y, exact ? Precision::FP64 : Precision::Mixed);
+  (exact ? stats_.s_columns_fp64 : stats_.s_columns_search) += cols;
+}
+
+void DavidsonSolver::apply_pair(const Cx<double>* x, int cols, Cx<double>* hy, Cx<double>* sy, bool exact) {
+  op_.apply_pair(x, cols, hy, sy, exact ? Precision::FP64 : Precision::Mixed);
+  (exact ? stats_.h_columns_fp64 : stats_.h_columns_search) += cols;
+  (exact ? stats_.s_columns_fp64 : stats_.s_columns_search) += cols;
+}
+
+// One direction at a time (src/pw_core.cpp:796-853): CGS2 in the S metric with
+// FP64 operators, reject norm^2 < 1e-24.
+bool DavidsonSolver::append_single(const Cx<double>* source) {
+  if (size_ >= capacity_) return false;
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  Cx<double>* v = as<Cx<double>>(original_, static_cast<std::size_t>(n_) * kmax_);
+  Cx<double>* sv = as<Cx<double>>(metric_, static_cast<std::size_t>(n_) * kmax_);
+  Cx<double>* proj = as<Cx<double>>(projections_, static_cast<std::size_t>(capacity_) * kmax_);
+  if (source != v) copy_block(source, n_, v, n_, n_, 1, st);
+  column_norms(v, n_, n_, 1, dsmall_, st);
+  const double norm = download(dsmall_, 1)[0];
+  if (!std::isfinite(norm)) throw std::runtime_error("nonfinite Davidson direction");
+  if (norm == 0) return false;
+  unit_columns(v, n_, n_, 1, dsmall_, st);
+  for (int pass = 0; pass < 2 && size_; ++pass) {
+    apply_s(v, 1, sv, true);
+    gemm(Op::C, size_, 1, n_, v_, n_, sv, n_, proj, size_, false, 1.0, true);
+    gemm(Op::N, n_, 1, size_, v_, n_, proj, size_, v, n_, true, -1.0, true);
+  }
+  apply_s(v, 1, sv, true);
+  metric_norms(v, sv, n_, n_, 1, dsmall_, st);
+  const double norm2 = download(dsmall_, 1)[0];
+  if (!std::isfinite(norm2) || norm2 < -1e-10) throw std::runtime_error("Davidson encountered non-positive overlap direction");
+  if (norm2 < 1e-24) return false;
+  scale_columns(v, n_, n_, 1, dsmall_, true, st);
+  scale_columns(sv, n_, n_, 1, dsmall_, true, st);
+  copy_block(v, n_, v_ + static_cast<long long>(size_) * n_, n_, n_, 1, st);
+  copy_block(sv, n_, sv_ + static_cast<long long>(size_) * n_, n_, n_, 1, st);
+  ++size_;
+  return true;
+}
+
+// Block CGS2 in the S metric (src/pw_core.cpp:871-1013). `vectors` is an
+// n x k workspace block that this call may overwrite.
+bool DavidsonSolver::append_block(Cx<double>* vectors, int k) {
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  const int before = size_;
+  k = std::min(k, capacity_ - size_);
+  if (k <= 0) return false;
+  auto serial = [&]() {
+    for (int j = 0; j < k; ++j) append_single(vectors + static_cast<long long>(j) * n_);
+    return size_ > before;
+  };
+  if (k == 1) return serial();
+  const bool exact = exact_mode_;
+  column_norms(vectors, n_, n_, k, dsmall_, st);
+  const auto norms = download(dsmall_, k);
+  for (double v : norms)
+    if (!(v > 0) || !std::isfinite(v)) return serial();
+  unit_columns(vectors, n_, n_, k, dsmall_, st);
+  Cx<double>* original = as<Cx<double>>(original_, static_cast<std::size_t>(n_) * kmax_);
+  Cx<double>* metric = as<Cx<double>>(metric_, static_cast<std::size_t>(n_) * kmax_);
+  Cx<double>* proj = as<Cx<double>>(projections_, static_cast<std::size_t>(capacity_) * kmax_);
+  copy_block(vectors, n_, original, n_, n_, k, st);
+  apply_s(vectors, k, metric, exact);
+  for (int pass = 0; size_ && pass < 2; ++pass) {
+    gemm(Op::C, size_, k, n_, v_, n_, metric, n_, proj, size_, false, 1.0, exact);
+    gemm(Op::N, n_, k, size_, v_, n_, proj, size_, vectors, n_, true, -1.0, exact);
+    apply_s(vectors, k, metric, exact);
+  }
+  // Gram matrix, metric eigendecomposition and normalisation U diag(1/sqrt(l)).
+  Cx<double>* gram = as<Cx<double>>(gram_, static_cast<std::size_t>(kmax_) * kmax_ * 2);
+  Cx<double>* herm = gram + static_cast<std::size_t>(kmax_) * kmax_;
+  gemm(Op::C, k, k, n_, vectors, n_, metric, n_, gram, k, false, 1.0, exact);
+  hermitian_part(gram, k, herm, k, k, st);
+  double* lam = as<double>(small_, static_cast<std::size_t>(kmax_) * 2);
+  int lwork = 0;
+  check_solver(cusolverDnZheevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k,
+                                           reinterpret_cast<cuDoubleComplex*>(herm), k, lam, &lwork),
+               "zheevd_bufferSize");
+  auto* work = as<cuDoubleComplex>(rr_work_, static_cast<std::size_t>(lwork));
+  int* info = as<int>(info_, 4);
+  check_solver(cusolverDnZheevd(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, k,
+                                reinterpret_cast<cuDoubleComplex*>(herm), k, lam, work, lwork, info),
+               "zheevd");
+  int host_info = 0;
+  SDFT_CUDA(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  const auto eig = download(lam, k);
+  if (host_info) throw std::runtime_error("block Davidson metric decomposition failed");
+  const double smallest = *std::min_element(eig.begin(), eig.end());
+  const double largest = *std::max_element(eig.begin(), eig.end());
+  if (smallest < -1e-10) throw std::runtime_error("block Davidson encountered non-positive overlap");
+  if (!(largest > 0) || smallest < 1e-10 * largest) {
+    ++stats_.block_rank_fallbacks;
+    copy_block(original, n_, vectors, n_, n_, k, st);
+    return serial();
+  }
+  scale_columns(herm, k, k, k, lam, true, st);  // U diag(1/sqrt(lambda))
+  gemm(Op::N, n_, k, k, vectors, n_, herm, k, v_ + static_cast<long long>(size_) * n_, n_, false, 1.0, exact);
+  gemm(Op::N, n_, k, k, metric, n_, herm, k, sv_ + static_cast<long long>(size_) * n_, n_, false, 1.0, exact);
+  size_ += k;
+  return true;
+}
+
+// Galerkin slabs for the new columns (src/pw_core.cpp:771-785).
+void DavidsonSolver::update_projected(const Cx<double>* applied, Cx<double>* cached) {
+  const int first = incremental_ ? projected_size_ : 0;
+  if (first == size_) return;
+  const int columns = size_ - first;
+  gemm(Op::C, size_, columns, n_, v_, n_, applied + static_cast<long long>(first) * n_, n_,
+       cached + static_cast<long long>(first) * capacity_, capacity_, false, 1.0, exact_mode_);
+  if (first)
+    gemm(Op::C, columns, first, n_, v_ + static_cast<long long>(first) * n_, n_, applied, n_, cached + first,
+         capacity_, false, 1.0, exact_mode_);
+}
+
+// Generalized Hermitian eigensolve of the projected pencil in FP64 on the
+// device (the reference calls LAPACK zhegvd, src/pw_core.cpp:104-121).
+void DavidsonSolver::rayleigh_ritz() {
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  const double t0 = now();
+  const int m = size_;
+  auto* a = as<Cx<double>>(rr_a_, static_cast<std::size_t>(capacity_) * capacity_);
+  auto* b = as<Cx<double>>(rr_b_, static_cast<std::size_t>(capacity_) * capacity_);
+  hermitian_part(ch_, capacity_, a, m, m, st);
+  hermitian_part(cs_, capacity_, b, m, m, st);
+  int lwork = 0;
+  check_solver(cusolverDnZhegvd_bufferSize(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                           CUBLAS_FILL_MODE_LOWER, m, reinterpret_cast<cuDoubleComplex*>(a), m,
+                                           reinterpret_cast<cuDoubleComplex*>(b), m, w_, &lwork),
+               "zhegvd_bufferSize");
+  auto* work = as<cuDoubleComplex>(rr_work_, static_cast<std::size_t>(lwork));
+  int* info = as<int>(info_, 4);
+  check_solver(cusolverDnZhegvd(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m,
+                                reinterpret_cast<cuDoubleComplex*>(a), m, reinterpret_cast<cuDoubleComplex*>(b), m, w_,
+                                work, lwork, info),
+               "zhegvd");
+  int host_info = 0;
+  SDFT_CUDA(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  values_ = download(w_, std::min(m, roots_));
+  if (host_info) throw std::runtime_error("Davidson Rayleigh-Ritz failed: info=" + std::to_string(host_info));
+  ++stats_.rayleigh_ritz;
+  stats_.rr_seconds += now() - t0;
+}
+
+// Fresh FP64 certificate of the Ritz block (src/pw_core.cpp:1125-1149).
+void DavidsonSolver::certify() {
+  const cudaStream_t st = op_.context().stream;
+  ++stats_.certifications;
+  apply_s(x_, roots_, sx_, true);
+  metric_norms(x_, sx_, n_, n_, roots_, dsmall_, st);
+  const auto metric = download(dsmall_, roots_);
+  for (double m : metric)
+    if (!std::isfinite(m) || !(m > 0)) throw std::runtime_error("invalid Davidson Ritz S norm");
+  scale_columns(x_, n_, n_, roots_, dsmall_, true, st);
+  apply_pair(x_, roots_, hx_, sx_, true);
+  double* values = dsmall_ + roots_;
+  double* metrics = dsmall_ + 2 * roots_;
+  double* norms = dsmall_ + 3 * roots_;
+  rayleigh_certificate(x_, hx_, sx_, n_, n_, roots_, values, metrics, r_, norms, st);
+  values_ = download(values, roots_);
+  residual_norms_ = download(norms, roots_);
+  SDFT_CUDA(cudaMemcpyAsync(w_, values, sizeof(double) * roots_, cudaMemcpyDeviceToDevice, st));
+}
+
+void DavidsonSolver::refresh_images() {
+  apply_pair(v_, size_, hv_, sv_, true);
+  computed_h_ = size_;
+  projected_size_ = 0;
+}
+
+void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) {
+  auto& ctx = op_.context();
+  SDFT_CUDA(cudaSetDevice(ctx.device));
+  const cudaStream_t st = ctx.stream;
+  const double start = now();
+  const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
+  stats_ = DavidsonStats{};
+  n_ = op_.npw();
+  roots_ = o.roots;
+  if (roots_ < 1 || roots_ > n_ || o.max_iterations < 1 || !std::isfinite(o.tolerance) || o.tolerance <= 0)
+    throw InvalidArgument("invalid matrix-free Davidson problem");
+  if (o.subspace_factor < 4 || o.subspace_factor > 16)
+    throw InvalidArgument("SDFT_DAVIDSON_SUBSPACE_FACTOR must be in [4,16]");
+  for (std::size_t i = 0; i < op_.s_diagonal().size(); ++i)
+    if (!std::isfinite(op_.h_diagonal()[i]) || !std::isfinite(op_.s_diagonal()[i]) || op_.s_diagonal()[i] <= 0)
+      throw InvalidArgument("invalid Davidson operator diagonal");
+  tolerance_ = o.tolerance;
+  capacity_ = std::min(n_, std::max(o.subspace_factor * roots_, 64));
+  const bool warm = initial != nullptr && 2 * roots_ < n_;
+  const int guard_count = std::min(n_, 2 * roots_);
+  kmax_ = std::min(capacity_, std::max(3 * roots_, 2));
+  exact_mode_ = o.precision == Precision::FP64;
+  incremental_ = o.tolerance >= 1e-12;
+  strict_projection_ = false;
+  size_ = computed_h_ = projected_size_ = 0;
+  residual_history_.clear();
+  const std::size_t nc = static_cast<std::size_t>(n_) * capacity_;
+  v_ = as<Cx<double>>(basis_, nc);
+  hv_ = as<Cx<double>>(hbasis_, nc);
+  sv_ = as<Cx<double>>(sbasis_, nc);
+  ch_ = as<Cx<double>>(cached_h_, static_cast<std::size_t>(capacity_) * capacity_);
+  cs_ = as<Cx<double>>(cached_s_, static_cast<std::size_t>(capacity_) * capacity_);
+  w_ = as<double>(rr_w_, capacity_);
+  x_ = as<Cx<double>>(xs_, static_cast<std::size_t>(n_) * roots_);
+  sx_ = as<Cx<double>>(sxs_, static_cast<std::size_t>(n_) * roots_);
+  hx_ = as<Cx<double>>(hxs_, static_cast<std::size_t>(n_) * roots_);
+  r_ = as<Cx<double>>(res_, static_cast<std::size_t>(n_) * roots_);
+  dsmall_ = as<double>(order_, static_cast<std::size_t>(std::max(capacity_, 4 * roots_)) * 4);
+  Cx<double>* block = as<Cx<double>>(block_, static_cast<std::size_t>(n_) * kmax_);
+  int* dselect = as<int>(select_, static_cast<std::size_t>(std::max(n_, roots_)));
+
+  // Seeds (src/pw_core.cpp:1016-1112): warm vectors (perturbed) + 2*roots
+  // canonical guards on the lowest H/S diagonal ratios, each with full support.
+  std::vector<int> order(n_);
+  std::iota(order.begin(), order.end(), 0);
+  const auto& hd = op_.h_diagonal();
+  const auto& sd = op_.s_diagonal();
+  std::stable_sort(order.begin(), order.end(), [&](int i, int j) { return hd[i] / sd[i] < hd[j] / sd[j]; });
+  int seeds = 0;
+  unsigned long long draw = 0;
+  if (warm) {
+    copy_block(initial, n_, block, n_, n_, roots_, st);
+    seeds = roots_;
+  }
+  {
+    const int guards = std::min(guard_count, kmax_ - seeds);
+    SDFT_CUDA(cudaMemcpyAsync(dselect, order.data(), sizeof(int) * guards, cudaMemcpyHostToDevice, st));
+    broad_seed_block(n_, guards, draw, dselect, block + static_cast<long long>(seeds) * n_, n_, st);
+    draw += 2ULL * n_ * guards;
+    seeds += guards;
+  }
+  append_block(block, seeds);
+
+  values_.assign(roots_, 0.0);
+  residual_norms_.assign(roots_, 0.0);
+  bool certified = false;
+  int iteration = 0;
+  for (; iteration < o.max_iterations; ++iteration) {
+    // flush_h (src/pw_core.cpp:786-795)
+    if (computed_h_ < size_) {
+      apply_h(v_ + static_cast<long long>(computed_h_) * n_, size_ - computed_h_,
+              hv_ + static_cast<long long>(computed_h_) * n_, exact_mode_);
+      computed_h_ = size_;
+    }
+    update_projected(hv_, ch_);
+    update_projected(sv_, cs_);
+    projected_size_ = size_;
+    rayleigh_ritz();
+    const Cx<double>* rotation = static_cast<const Cx<double>*>(rr_a_.ptr);  // size x size, ld size
+    // Ritz block, its S image and search residual (src/pw_core.cpp:1178-1181)
+    gemm(Op::N, n_, roots_, size_, v_, n_, rotation, size_, x_, n_, false, 1.0, exact_mode_);
+    gemm(Op::N, n_, roots_, size_, sv_, n_, rotation, size_, sx_, n_, false, 1.0, exact_mode_);
+    gemm(Op::N, n_, roots_, size_, hv_, n_, rotation, size_, r_, n_, false, 1.0, exact_mode_);
+    search_residual(r_, sx_, n_, n_, roots_, w_, r_, st);
+    column_norms(r_, n_, n_, roots_, dsmall_, st);
+    residual_norms_ = download(dsmall_, roots_);
+    stats_.iterations = iteration + 1;
+    double max_res = *std::max_element(residual_norms_.begin(), residual_norms_.end());
+    bool converged = std::all_of(residual_norms_.begin(), residual_norms_.end(),
+                                 [&](double r) { return r <= tolerance_; });
+    residual_history_.push_back(max_res);
+    if (trace)
+      std::fprintf(stderr, "sdft_b200 davidson iteration=%d size=%d mode=%s max_search_residual=%.3e\n", iteration,
+                   size_, exact_mode_ ? "fp64" : "mixed", max_res);
+    // Approximate search hands over to FP64 (src/pw_core.cpp:1184-1196). FP32
+    // arithmetic cannot reach 1e-8, so a stalled search hands over as well.
+    if (!exact_mode_) {
+      bool stalled = false;
+      const std::size_t h = residual_history_.size();
+      if (h >= 6 && max_res < 1e-3) {
+        const double recent = std::min({residual_history_[h - 1], residual_history_[h - 2], residual_history_[h - 3]});
+        const double earlier = *std::min_element(residual_history_.begin(), residual_history_.end() - 3);
+        stalled = recent > 0.5 * earlier;
+      }
+      if (max_res < o.handoff || stalled || iteration + 1 == o.max_iterations) {
+        exact_mode_ = true;
+        ++stats_.fp64_refreshes;
+        stats_.handoff_iteration = iteration;
+        refresh_images();
+        continue;
+      }
+    }
+    bool fresh = false;
+    if (exact_mode_ && max_res <= 8 * tolerance_) {
+      certify();
+      fresh = true;
+      converged = std::all_of(residual_norms_.begin(), residual_norms_.end(), [&](double r) { return r <= tolerance_; });
+      max_res = *std::max_element(residual_norms_.begin(), residual_norms_.end());
+    }
+    if (converged && !fresh) {
+      certify();
+      fresh = true;
+      converged = std::all_of(residual_norms_.begin(), residual_norms_.end(), [&](double r) { return r <= tolerance_; });
+      max_res = *std::max_element(residual_norms_.begin(), residual_norms_.end());
+      if (!converged && !exact_mode_) {
+        exact_mode_ = true;
+        ++stats_.fp64_refreshes;
+        refresh_images();
+        continue;
+      }
+    }
+    // Rebuild the whole projected pencil at the FP64 floor (src/pw_core.cpp:1247-1267).
+    if (exact_mode_ && !converged && tolerance_ <= 1e-12 && !strict_projection_ && max_res <= 1e-10) {
+      if (!fresh) {
+        certify();
+        fresh = true;
+        converged = std::all_of(residual_norms_.begin(), residual_norms_.end(), [&](double r) { return r <= tolerance_; });
+      }
+      if (!converged) {
+        refresh_images();
+        incremental_ = false;
+        strict_projection_ = true;
+        continue;
+      }
+    }
+    if (converged) {
+      certified = fresh;
+      if (certified) break;
+    }
+    // Thick restart (src/pw_core.cpp:1357-1383).
+    if (size_ + roots_ > capacity_) {
+      const int keep = std::min(size_, 2 * roots_);
+      gemm(Op::N, n_, keep, size_, v_, n_, rotation, size_, block, n_, false, 1.0, exact_mode_);
+      size_ = computed_h_ = projected_size_ = 0;
+      ++stats_.restarts;
+      append_block(block, keep);
+    }
+    // Preconditioned corrections for unconverged roots (src/pw_core.cpp:1384-1401).
+    const int previous = size_;
+    std::vector<int> selected;
+    for (int r = 0; r < roots_ && size_ + static_cast<int>(selected.size()) < capacity_; ++r)
+      if (residual_norms_[r] > 0.5 * tolerance_) selected.push_back(r);
+    if (!selected.empty()) {
+      Cx<double>* corrections = static_cast<Cx<double>*>(res_.ptr);  // precondition in place into r_
+      kinetic_precondition(r_, x_, n_, n_, roots_, op_.device_kinetic(), corrections, n_, st);
+      SDFT_CUDA(cudaMemcpyAsync(dselect, selected.data(), sizeof(int) * selected.size(), cudaMemcpyHostToDevice, st));
+      gather_columns(corrections, n_, n_, dselect, static_cast<int>(selected.size()), block, n_, st);
+      append_block(block, static_cast<int>(selected.size()));
+    }
+    if (size_ == previous) {
+      bool added = false;
+      for (int j = 0; j < n_ && !added; ++j) {
+        zero_block(block, n_, n_, 1, st);
+        const Cx<double> one{1.0, 0.0};
+        SDFT_CUDA(cudaMemcpyAsync(block + order[j], &one, sizeof(one), cudaMemcpyHostToDevice, st));
+        added = append_single(block);
+      }
+      if (!added) break;
+    }
+  }
+  if (!certified) certify();
+  stats_.converged = std::all_of(residual_norms_.begin(), residual_norms_.end(), [&](double r) { return r <= tolerance_; });
+  stats_.max_residual = *std::max_element(residual_norms_.begin(), residual_norms_.end());
+  ctx.synchronize();
+  stats_.seconds = now() - start;
+}
+
+}  // namespace sdft_b200

@@ -1,0 +1,77 @@
+// Device-resident generalized block Davidson in the S~ metric.
+#pragma once
+#include <vector>
+
+#include "operator.cuh"
+
+namespace sdft_b200 {
+
+struct DavidsonOptions {
+  int roots = 0;
+  int max_iterations = 256;
+  double tolerance = 1e-10;
+  Precision precision = Precision::FP64;  // search precision; certification is always FP64
+  int subspace_factor = 8;                // capacity = min(n, max(factor*roots, 64)), in [4,16]
+  double handoff = 1e-8;                  // search residual that hands the basis to FP64
+};
+
+struct DavidsonStats {
+  int iterations = 0;
+  bool converged = false;
+  double max_residual = 0.0;
+  long long h_columns_search = 0, h_columns_fp64 = 0, s_columns_search = 0, s_columns_fp64 = 0;
+  int rayleigh_ritz = 0, restarts = 0, fp64_refreshes = 0, certifications = 0, handoff_iteration = -1;
+  int block_rank_fallbacks = 0;
+  double seconds = 0.0, rr_seconds = 0.0;
+};
+
+class DavidsonSolver {
+ public:
+  explicit DavidsonSolver(DeviceOperator& op) : op_(op) {}
+  // initial: device n x roots (column-major) warm vectors, or null for a cold start.
+  void solve(const DavidsonOptions& options, const Cx<double>* initial);
+
+  const std::vector<double>& eigenvalues() const { return values_; }
+  const std::vector<double>& residuals() const { return residual_norms_; }
+  const Cx<double>* vectors() const { return x_; }  // n x roots, S-normalised, on the device
+  const DavidsonStats& stats() const { return stats_; }
+
+ private:
+  Precision mode() const { return exact_mode_ ? Precision::FP64 : Precision::Mixed; }
+  void gemm(Op aop, int m, int n, int k, const Cx<double>* a, long long lda, const Cx<double>* b, long long ldb,
+            Cx<double>* c, long long ldc, bool add, double alpha, bool exact);
+  void apply_h(const Cx<double>* x, int cols, Cx<double>* y, bool exact);
+  void apply_s(const Cx<double>* x, int cols, Cx<double>* y, bool exact);
+  void apply_pair(const Cx<double>* x, int cols, Cx<double>* hy, Cx<double>* sy, bool exact);
+  bool append_block(Cx<double>* vectors, int k);
+  bool append_single(const Cx<double>* v);
+  void update_projected(const Cx<double>* applied, Cx<double>* cached);
+  void rayleigh_ritz();
+  void certify();
+  void refresh_images();
+  std::vector<double> download(const double* device, int count);
+
+  DeviceOperator& op_;
+  DavidsonStats stats_;
+  int n_ = 0, roots_ = 0, capacity_ = 0, kmax_ = 0;
+  int size_ = 0, computed_h_ = 0, projected_size_ = 0;
+  bool exact_mode_ = true, incremental_ = true, strict_projection_ = false;
+  double tolerance_ = 1e-10;
+  Scratch basis_, hbasis_, sbasis_, cached_h_, cached_s_, rr_a_, rr_b_, rr_w_, rr_work_, info_;
+  Scratch xs_, sxs_, hxs_, res_, block_, metric_, original_, projections_, gram_, small_, order_, select_;
+  Cx<double>* v_ = nullptr;
+  Cx<double>* hv_ = nullptr;
+  Cx<double>* sv_ = nullptr;
+  Cx<double>* ch_ = nullptr;
+  Cx<double>* cs_ = nullptr;
+  Cx<double>* x_ = nullptr;
+  Cx<double>* sx_ = nullptr;
+  Cx<double>* hx_ = nullptr;
+  Cx<double>* r_ = nullptr;
+  double* w_ = nullptr;       // RR eigenvalues (device)
+  double* dsmall_ = nullptr;  // per-column device scalars (norms, metric, values)
+  std::vector<double> values_, residual_norms_;
+  std::vector<double> residual_history_;
+};
+
+}  // namespace sdft_b200

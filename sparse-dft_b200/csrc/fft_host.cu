@@ -8,7 +8,15 @@
 #include <tuple>
 #include <vector>
 
+#include <atomic>
+
 namespace sdft_b200 {
+
+namespace {
+std::atomic<unsigned long long> launches{0};
+}
+void count_launch() { launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return launches.load(std::memory_order_relaxed); }
 
 LinePlan make_line_plan(int n) {
   if (n < 1 || n > kMaxLine) throw InvalidArgument("FFT length out of the supported range [1, 512]");

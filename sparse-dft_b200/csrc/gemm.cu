@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kGemmThreads) cgemm_simt_kernel(int m, int n, 
 }
 
 __global__ void reduce_partials_kernel(int m, int n, int splits, const Cx<float>* __restrict__ partial,
-                                       Cx<double>* __restrict__ c, long long ldc, bool add) {
+                                       Cx<double>* __restrict__ c, long long ldc, bool add, double alpha) {
   const long long total = static_cast<long long>(m) * n;
   for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
        idx += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -125,6 +125,8 @@ __global__ void reduce_partials_kernel(int m, int n, int splits, const Cx<float>
     }
     const long long i = idx % m, j = idx / m;
     Cx<double>& out = c[i + j * ldc];
+    re *= alpha;
+    im *= alpha;
     if (add) {
       re += out.re;
       im += out.im;
@@ -197,9 +199,9 @@ unsigned grid_for(long long total, int threads) {
 }  // namespace
 
 void zgemm(cublasHandle_t handle, Op aop, Op bop, int m, int n, int k, const Cx<double>* a, long long lda,
-           const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add) {
+           const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, double alpha) {
   if (m <= 0 || n <= 0 || k <= 0) return;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  const cuDoubleComplex one = make_cuDoubleComplex(alpha, 0.0);
   const cuDoubleComplex beta = make_cuDoubleComplex(add ? 1.0 : 0.0, 0.0);
   check_blas(cublasZgemm(handle, aop == Op::N ? CUBLAS_OP_N : CUBLAS_OP_C, bop == Op::N ? CUBLAS_OP_N : CUBLAS_OP_C,
                          m, n, k, &one, reinterpret_cast<const cuDoubleComplex*>(a), static_cast<int>(lda),
@@ -210,7 +212,7 @@ void zgemm(cublasHandle_t handle, Op aop, Op bop, int m, int n, int k, const Cx<
 
 void gemm_mixed(Op aop, int m, int n, int k, const Cx<double>* a, const Cx<float>* a32, long long lda,
                 const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, Scratch& workspace,
-                cudaStream_t stream) {
+                cudaStream_t stream, double alpha) {
   if (m <= 0 || n <= 0 || k <= 0) return;
   const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n, BN));
   int splits = static_cast<int>(std::min<long long>(std::max<long long>(1, (2 * 148 + tiles - 1) / tiles),
@@ -230,7 +232,7 @@ void gemm_mixed(Op aop, int m, int n, int k, const Cx<double>* a, const Cx<float
   }
   SDFT_LAUNCH("cgemm_simt_kernel");
   const long long total = static_cast<long long>(m) * n;
-  reduce_partials_kernel<<<grid_for(total, 256), 256, 0, stream>>>(m, n, splits, partial, c, ldc, add);
+  reduce_partials_kernel<<<grid_for(total, 256), 256, 0, stream>>>(m, n, splits, partial, c, ldc, add, alpha);
   SDFT_LAUNCH("reduce_partials_kernel");
 }
 

@@ -82,6 +82,10 @@ class DeviceOperator {
   void apply_hamiltonian(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
   void apply_overlap(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
   void apply_pair(const Cx<double>* x, int columns, Cx<double>* hy, Cx<double>* sy, Precision precision);
+  // Local part only: y = T x + V(r) term.
+  void apply_local(const Cx<double>* x, int columns, Cx<double>* y, Precision precision) {
+    local_part(x, columns, y, precision);
+  }
   // P = B x (np x columns, ld np)
   void project(const Cx<double>* x, int columns, Cx<double>* p, Precision precision);
 

@@ -64,6 +64,24 @@ SZ = ctypes.c_size_t
 SZP = ctypes.POINTER(ctypes.c_size_t)
 
 
+class DavidsonOptions(ctypes.Structure):
+    _fields_ = [("roots", ctypes.c_size_t), ("max_iterations", ctypes.c_size_t), ("tolerance", ctypes.c_double),
+                ("precision", ctypes.c_int), ("subspace_factor", ctypes.c_int), ("handoff", ctypes.c_double)]
+
+
+class DavidsonStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_size_t), ("converged", ctypes.c_int), ("max_residual", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("rayleigh_ritz_seconds", ctypes.c_double),
+                ("h_columns_search", ctypes.c_size_t), ("h_columns_fp64", ctypes.c_size_t),
+                ("s_columns_search", ctypes.c_size_t), ("s_columns_fp64", ctypes.c_size_t),
+                ("rayleigh_ritz_calls", ctypes.c_int), ("restarts", ctypes.c_int), ("fp64_refreshes", ctypes.c_int),
+                ("certifications", ctypes.c_int), ("handoff_iteration", ctypes.c_int),
+                ("block_rank_fallbacks", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def _declare(lib: ctypes.CDLL) -> None:
     def fn(name, args, res=ctypes.c_int):
         f = getattr(lib, name)
@@ -72,6 +90,7 @@ def _declare(lib: ctypes.CDLL) -> None:
 
     fn("sdft_b200_last_error", [ctypes.c_char_p, SZ], SZ)
     fn("sdft_b200_version", [], ctypes.c_char_p)
+    fn("sdft_b200_kernel_launches", [], ctypes.c_ulonglong)
     fn("sdft_b200_context_create", [ctypes.c_int, P, ctypes.POINTER(P)])
     fn("sdft_b200_context_destroy", [P])
     fn("sdft_b200_context_synchronize", [P])
@@ -79,11 +98,14 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_operator_create", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,
                                      ctypes.POINTER(P)])
     fn("sdft_b200_operator_destroy", [P])
-    fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP])
+    fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
+    fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_operator_arrays", [P, U64, D, D, D, D])
     fn("sdft_b200_apply", [P, ctypes.c_int, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_pair", [P, P, SZ, P, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_project", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_davidson", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
+                              ctypes.c_int])
 
 
 def last_error() -> str:

@@ -13,6 +13,7 @@ import numpy as np
 from . import _capi as C
 
 _PREC = {"fp64": C.FP64, "mixed": C.MIXED, C.FP64: C.FP64, C.MIXED: C.MIXED}
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 
 def _precision(value) -> int:
@@ -30,9 +31,12 @@ class Context:
     """A CUDA stream plus library handles on one device (the reference's per-thread Accelerator)."""
 
     def __init__(self, device: int = 0, stream: int | None = None):
+        """stream: None for a private stream, or a cudaStream_t handle to share
+        (0, torch's default stream, is passed on as cudaStreamLegacy)."""
         self._lib = C.library()
         handle = ctypes.c_void_p()
-        C.check(self._lib.sdft_b200_context_create(device, ctypes.c_void_p(stream or 0), ctypes.byref(handle)))
+        raw = None if stream is None else (stream if stream != 0 else CUDA_STREAM_LEGACY)
+        C.check(self._lib.sdft_b200_context_create(device, ctypes.c_void_p(raw), ctypes.byref(handle)))
         self.handle = handle
         self.device = device
 
@@ -95,12 +99,14 @@ class PlaneWaveOperator:
         grid = ctypes.c_size_t()
         nproj = ctypes.c_size_t()
         npw = ctypes.c_size_t()
+        rows = ctypes.c_size_t()
         C.check(self._lib.sdft_b200_operator_info(handle, shape.ctypes.data_as(C.I32), ctypes.byref(grid),
-                                                  ctypes.byref(nproj), ctypes.byref(npw)))
+                                                  ctypes.byref(nproj), ctypes.byref(npw), ctypes.byref(rows)))
         self.shape = tuple(int(v) for v in shape)
         self.grid_points = grid.value
         self.projectors = nproj.value
         self.npw = npw.value
+        self.active_rows = rows.value
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -158,6 +164,14 @@ class PlaneWaveOperator:
                                           _precision(precision), mem))
         return y
 
+    def local_apply(self, x, out=None, precision="fp64"):
+        """T x + V(r) term only (the reference's Accelerator::local_hamiltonian)."""
+        ptr, cols, mem, keep = self._block(x)
+        y = self._like(keep) if out is None else out
+        yptr = ctypes.c_void_p(y.data_ptr() if mem == C.DEVICE else y.ctypes.data)
+        C.check(self._lib.sdft_b200_apply_local(self.handle, ptr, cols, yptr, _precision(precision), mem))
+        return y
+
     def apply_pair(self, x, precision="fp64"):
         ptr, cols, mem, keep = self._block(x)
         hy, sy = self._like(keep), self._like(keep)
@@ -172,3 +186,29 @@ class PlaneWaveOperator:
         pp = ctypes.c_void_p(p.data_ptr() if mem == C.DEVICE else p.ctypes.data)
         C.check(self._lib.sdft_b200_project(self.handle, ptr, cols, pp, _precision(precision), mem))
         return p
+
+    # -- eigensolver ---------------------------------------------------------
+    def davidson(self, roots: int, max_iterations: int = 256, tolerance: float = 1e-10, precision="fp64",
+                 initial=None, subspace_factor: int = 8, handoff: float = 1e-8, vectors: bool = True):
+        """Lowest eigenpairs of H~x = e S~x (the reference's solve_generalized_hermitian_davidson).
+
+        Returns a dict with eigenvalues, residuals (fresh FP64), eigenvectors
+        (band-major roots x npw, or None), converged, iterations and stats.
+        """
+        opts = C.DavidsonOptions(roots=roots, max_iterations=max_iterations, tolerance=tolerance,
+                                 precision=_precision(precision), subspace_factor=subspace_factor, handoff=handoff)
+        stats = C.DavidsonStats()
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        init_ptr = None
+        keep = None
+        if initial is not None:
+            keep = np.ascontiguousarray(initial, dtype=np.complex128).reshape(roots, self.npw)
+            init_ptr = ctypes.c_void_p(keep.ctypes.data)
+        vec = np.zeros((roots, self.npw), dtype=np.complex128) if vectors else None
+        vec_ptr = ctypes.c_void_p(vec.ctypes.data) if vec is not None else None
+        C.check(self._lib.sdft_b200_davidson(self.handle, ctypes.byref(opts), init_ptr, _dptr(eig), vec_ptr,
+                                             _dptr(res), ctypes.byref(stats), C.HOST))
+        info = stats.as_dict()
+        return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
+                "iterations": int(info["iterations"]), "stats": info}
