@@ -204,7 +204,8 @@ def run_b200(args):
     from sdft_b200.operator import Context, PlaneWaveOperator
 
     inputs = load_inputs()
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # library kernels and the CUDA events share this stream
+    torch.cuda.set_stream(stream)
     ctx = Context(local, stream.cuda_stream)
     op = PlaneWaveOperator(ctx, inputs)
     roots = inputs.roots

@@ -111,6 +111,19 @@ SDFT_B200_API sdft_b200_status sdft_b200_apply_pair(sdft_b200_operator* op, cons
 SDFT_B200_API sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size_t columns, double* p,
                                    int precision, int memory);
 
+enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
+
+/* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with
+ * explicit leading dimensions. FP64: FP64 arithmetic (cuBLAS ZGEMM). MIXED:
+ * BF16 split products on the tcgen05 tensor cores with FP32 accumulation
+ * (op(B) must be NORMAL). memory applies to a, b and c.
+ * Replaces: complex_gemm(MatrixOp, MatrixOp, m, n, k, a, lda, b, ldb, c, ldc, exact, add),
+ * src/compute_backend.hpp:23-26 (exact=true -> FP64, exact=false -> MIXED). */
+SDFT_B200_API sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int bop, size_t m,
+                                                      size_t n, size_t k, const double* a, size_t lda,
+                                                      const double* b, size_t ldb, double* c, size_t ldc,
+                                                      int precision, int add, int memory);
+
 /* Davidson controls. precision selects the search arithmetic (MIXED: FP32
  * FFT/V_loc and FP32-accumulated projector and subspace products; FP64: the
  * plain form throughout); Rayleigh-Ritz, the FP64 refresh and the final

@@ -1,5 +1,6 @@
 // extern "C" boundary (include/sdft_b200.h): converts exceptions into status
 // codes and a thread-local message, and host pointers into staged device copies.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -279,6 +280,46 @@ sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size
     o.project(dx, static_cast<int>(columns), dp, precision_of(precision));
     stage.back(p, dp, m);
     stage.finish();
+  });
+}
+
+sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int bop, size_t m, size_t n, size_t k,
+                                        const double* a, size_t lda, const double* b, size_t ldb, double* c,
+                                        size_t ldc, int precision, int add, int memory) {
+  return guarded([&] {
+    require(context && a && b && c && m && n && k, "invalid complex GEMM shape/leading dimension");
+    require((aop == SDFT_B200_OP_NORMAL || aop == SDFT_B200_OP_ADJOINT) &&
+                (bop == SDFT_B200_OP_NORMAL || bop == SDFT_B200_OP_ADJOINT),
+            "invalid complex GEMM operation");
+    const std::size_t ar = aop == SDFT_B200_OP_NORMAL ? m : k, ac = aop == SDFT_B200_OP_NORMAL ? k : m;
+    const std::size_t br = bop == SDFT_B200_OP_NORMAL ? k : n, bc = bop == SDFT_B200_OP_NORMAL ? n : k;
+    require(lda >= ar && ldb >= br && ldc >= m, "invalid complex GEMM shape/leading dimension");
+    if (std::max({m, n, k, lda, ldb, ldc}) > static_cast<size_t>(INT32_MAX))
+      throw std::overflow_error("BLAS dimension overflow");
+    const Precision p = precision_of(precision);
+    require(p == Precision::FP64 || bop == SDFT_B200_OP_NORMAL, "mixed complex GEMM needs a normal right operand");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    Staged stage(ctx, memory);
+    const auto* da = stage.in(a, lda * (ac - 1) + ar, ctx.staging_in);
+    const auto* db = stage.in(b, ldb * (bc - 1) + br, ctx.staging_aux);
+    const std::size_t csize = ldc * (n - 1) + m;
+    Cx<double>* dc = stage.out(c, csize, ctx.staging_out);
+    if (memory == SDFT_B200_MEMORY_HOST && add)
+      SDFT_CUDA(cudaMemcpyAsync(dc, c, sizeof(Cx<double>) * csize, cudaMemcpyHostToDevice, ctx.stream));
+    const sdft_b200::Op ao = aop == SDFT_B200_OP_NORMAL ? sdft_b200::Op::N : sdft_b200::Op::C;
+    const sdft_b200::Op bo = bop == SDFT_B200_OP_NORMAL ? sdft_b200::Op::N : sdft_b200::Op::C;
+    if (p == Precision::FP64)
+      sdft_b200::zgemm(ctx.blas, ao, bo, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), da,
+                       static_cast<long long>(lda), db, static_cast<long long>(ldb), dc, static_cast<long long>(ldc),
+                       add != 0);
+    else
+      sdft_b200::gemm_tc(ao, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), da,
+                         static_cast<long long>(lda), nullptr, db, static_cast<long long>(ldb), dc,
+                         static_cast<long long>(ldc), add != 0, 1.0, sdft_b200::search_split(), ctx.tc, ctx.stream);
+    stage.back(c, dc, csize);
+    ctx.synchronize();
+    if (sdft_b200::umma_error_flag_read_and_clear()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
   });
 }
 

@@ -19,6 +19,7 @@
 
 #include "davidson.cuh"
 #include "dense.cuh"
+#include "umma_gemm.cuh"
 
 namespace sdft_b200 {
 
@@ -42,6 +43,7 @@ std::vector<double> DavidsonSolver::download(const double* device, int count) {
     SDFT_CUDA(cudaMemcpyAsync(host.data(), device, sizeof(double) * count, cudaMemcpyDeviceToHost,
                               op_.context().stream));
     op_.context().synchronize();
+    if (umma_error_flag_read_and_clear()) throw CudaError("tensor-core GEMM wait limit exceeded");
   }
   return host;
 }
@@ -50,7 +52,7 @@ void DavidsonSolver::gemm(Op aop, int m, int n, int k, const Cx<double>* a, long
                           long long ldb, Cx<double>* c, long long ldc, bool add, double alpha, bool exact) {
   auto& ctx = op_.context();
   if (exact) zgemm(ctx.blas, aop, Op::N, m, n, k, a, lda, b, ldb, c, ldc, add, alpha);
-  else gemm_mixed(aop, m, n, k, a, nullptr, lda, b, ldb, c, ldc, add, ctx.gemm_work, ctx.stream, alpha);
+  else gemm_tc(aop, m, n, k, a, lda, nullptr, b, ldb, c, ldc, add, alpha, search_split(), ctx.tc, ctx.stream);
 }
 
 void DavidsonSolver::apply_h(const Cx<double>* x, int cols, Cx<double>* y, bool exact) {

@@ -67,14 +67,14 @@ __device__ __forceinline__ void radix_dft(Cx<T>* v, const Cx<T>* tw, int unit) {
       a[r - 1] = v[r] + v[R - r];
       b[r - 1] = v[r] - v[R - r];
     }
-    Cx<T> y[R];
-    Cx<T> sum = v[0];
+    const Cx<T> x0 = v[0];
+    Cx<T> sum = x0;
 #pragma unroll
     for (int r = 0; r < H; ++r) sum = sum + a[r];
-    y[0] = sum;
+    v[0] = sum;
 #pragma unroll
     for (int q = 1; q <= H; ++q) {
-      T cre = v[0].re, cim = v[0].im, sre = 0, sim = 0;
+      T cre = x0.re, cim = x0.im, sre = 0, sim = 0;
 #pragma unroll
       for (int r = 1; r <= H; ++r) {
         const Cx<T> w = tw[((r * q) % R) * unit];  // cos, -sin (forward)
@@ -85,11 +85,9 @@ __device__ __forceinline__ void radix_dft(Cx<T>* v, const Cx<T>* tw, int unit) {
         sre -= b[r - 1].im * s;
         sim += b[r - 1].re * s;
       }
-      y[q] = Cx<T>{cre + sre, cim + sim};
-      y[R - q] = Cx<T>{cre - sre, cim - sim};
+      v[q] = Cx<T>{cre + sre, cim + sim};
+      v[R - q] = Cx<T>{cre - sre, cim - sim};
     }
-#pragma unroll
-    for (int q = 0; q < R; ++q) v[q] = y[q];
   }
 }
 
@@ -144,6 +142,131 @@ __device__ void fft_line(Cx<T>* line, int stride, const LinePlan& plan, const Cx
     }
     ns *= r;
   }
+}
+
+// Whole-CTA batched variant (blockDim.x == 256): lanes map to lines (32 per
+// batch) and the 8 warps split each stage's butterflies, so index arithmetic
+// and twiddle loads are warp-uniform and every lane works on its own line.
+// Line t's element e lives at base[line_offset(t) * line_stride + e * elem_stride],
+// line_offset(t) = rows ? rows[t] : t. Contains __syncthreads: call uniformly.
+constexpr int kFftThreads = 256;
+constexpr int kFftWarps = kFftThreads / kWarp;
+
+template <typename T, int R, int NMAX, bool INV>
+__device__ __forceinline__ void cta_stage(Cx<T>* line, int es, int n, int ns, const Cx<T>* tw, int warp,
+                                          bool active) {
+  constexpr int MAXB = ((NMAX + R - 1) / R + kFftWarps - 1) / kFftWarps;
+  const int m = n / R;
+  const int twstride = n / (ns * R);
+  const int unit = n / R;
+  Cx<T> v[MAXB][R];
+#pragma unroll
+  for (int b = 0; b < MAXB; ++b) {
+    const int j = warp + b * kFftWarps;
+    if (j < m && active) {
+      const int k = j % ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        Cx<T> x = line[(j + r * m) * es];
+        if (r > 0 && k > 0) x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
+        v[b][r] = x;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < MAXB; ++b) {
+    const int j = warp + b * kFftWarps;
+    if (j < m && active) {
+      radix_dft<T, R, INV>(v[b], tw, unit);
+      const int k = j % ns;
+      const int base = (j / ns) * ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) line[(base + r * ns) * es] = v[b][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T, int NMAX, bool INV>
+__device__ void fft_lines(Cx<T>* base, int count, int line_stride, int elem_stride, const int* rows,
+                          const LinePlan& plan, const Cx<T>* tw) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int b0 = 0; b0 < count; b0 += kWarp) {
+    const int t = b0 + lane;
+    const bool active = t < count;
+    const int offset = active ? (rows ? rows[t] : t) : 0;
+    Cx<T>* line = base + offset * line_stride;
+    int ns = 1;
+    for (int s = 0; s < plan.stages; ++s) {
+      const int r = plan.radix[s];
+      switch (r) {
+        case 2: cta_stage<T, 2, NMAX, INV>(line, elem_stride, plan.n, ns, tw, warp, active); break;
+        case 3: cta_stage<T, 3, NMAX, INV>(line, elem_stride, plan.n, ns, tw, warp, active); break;
+        case 4: cta_stage<T, 4, NMAX, INV>(line, elem_stride, plan.n, ns, tw, warp, active); break;
+        case 5: cta_stage<T, 5, NMAX, INV>(line, elem_stride, plan.n, ns, tw, warp, active); break;
+        case 7: cta_stage<T, 7, NMAX, INV>(line, elem_stride, plan.n, ns, tw, warp, active); break;
+        default: break;
+      }
+      ns *= r;
+    }
+  }
+}
+
+// Out-of-place (ping-pong) batched variant: every stage reads one buffer and
+// writes the other, so only one butterfly is live per thread and any line
+// length works. Lanes map to lines, warps split butterflies, one
+// __syncthreads per stage. Returns the buffer that holds the result.
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void pp_butterflies(const Cx<T>* src_line, Cx<T>* dst_line, int es, int n, int ns,
+                                               const Cx<T>* tw, int warp) {
+  const int m = n / R, twstride = n / (ns * R), unit = n / R;
+  for (int j = warp; j < m; j += kFftWarps) {
+    const int k = j % ns;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      Cx<T> x = src_line[(j + r * m) * es];
+      if (r > 0 && k > 0) x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
+      v[r] = x;
+    }
+    radix_dft<T, R, INV>(v, tw, unit);
+    const int base = (j / ns) * ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst_line[(base + r * ns) * es] = v[r];
+  }
+}
+
+template <typename T, bool INV>
+__device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
+                               const int* rows, const LinePlan& plan, const Cx<T>* tw) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int ns = 1;
+  for (int s = 0; s < plan.stages; ++s) {
+    const int r = plan.radix[s];
+    for (int b0 = 0; b0 < count; b0 += kWarp) {
+      const int t = b0 + lane;
+      if (t < count) {
+        const int offset = (rows ? rows[t] : t) * line_stride;
+        const Cx<T>* in = src + offset;
+        Cx<T>* out = dst + offset;
+        switch (r) {
+          case 2: pp_butterflies<T, 2, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
+          case 3: pp_butterflies<T, 3, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
+          case 4: pp_butterflies<T, 4, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
+          case 5: pp_butterflies<T, 5, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
+          case 7: pp_butterflies<T, 7, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
+          default: break;
+        }
+      }
+    }
+    __syncthreads();
+    Cx<T>* swap = src;
+    src = dst;
+    dst = swap;
+    ns *= r;
+  }
+  return src;
 }
 
 // Host-side twiddle tables, w[m] = exp(-2 pi i m / n), one per (n, precision).

@@ -27,114 +27,6 @@ void check_blas(cublasStatus_t status, const char* what) {
     throw CudaError(std::string("cuBLAS error ") + std::to_string(static_cast<int>(status)) + " in " + what);
 }
 
-constexpr int BM = 64, BN = 64, BK = 16, kGemmThreads = 256;
-
-// Split-K SIMT complex GEMM, FP32 accumulation. Partial sums go to
-// partial[split][col][row] (ld m); the reduction kernel adds them in fixed
-// split order so the result is deterministic.
-template <Op AOP, typename TA>
-__global__ void __launch_bounds__(kGemmThreads) cgemm_simt_kernel(int m, int n, int k, int k_per_split,
-                                                                  const Cx<TA>* __restrict__ a, long long lda,
-                                                                  const Cx<double>* __restrict__ b, long long ldb,
-                                                                  Cx<float>* __restrict__ partial) {
-  __shared__ float Ar[BK][BM], Ai[BK][BM], Br[BK][BN], Bi[BK][BN];
-  const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
-  const int tile_m = blockIdx.x * BM, tile_n = blockIdx.y * BN, split = blockIdx.z;
-  const int k_begin = split * k_per_split;
-  const int k_end = min(k, k_begin + k_per_split);
-  float cr[4][4] = {}, ci[4][4] = {};
-  for (int k0 = k_begin; k0 < k_end; k0 += BK) {
-#pragma unroll
-    for (int r = 0; r < (BM * BK) / kGemmThreads; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      int i, kk;
-      if (AOP == Op::N) {
-        i = idx % BM;
-        kk = idx / BM;
-      } else {
-        kk = idx % BK;
-        i = idx / BK;
-      }
-      const int gi = tile_m + i, gk = k0 + kk;
-      float re = 0.f, im = 0.f;
-      if (gi < m && gk < k_end) {
-        const Cx<TA> v = AOP == Op::N ? a[gi + static_cast<long long>(gk) * lda]
-                                      : a[gk + static_cast<long long>(gi) * lda];
-        re = static_cast<float>(v.re);
-        im = AOP == Op::N ? static_cast<float>(v.im) : -static_cast<float>(v.im);
-      }
-      Ar[kk][i] = re;
-      Ai[kk][i] = im;
-    }
-#pragma unroll
-    for (int r = 0; r < (BN * BK) / kGemmThreads; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      const int kk = idx % BK, j = idx / BK;
-      const int gj = tile_n + j, gk = k0 + kk;
-      float re = 0.f, im = 0.f;
-      if (gj < n && gk < k_end) {
-        const Cx<double> v = b[gk + static_cast<long long>(gj) * ldb];
-        re = static_cast<float>(v.re);
-        im = static_cast<float>(v.im);
-      }
-      Br[kk][j] = re;
-      Bi[kk][j] = im;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      float ar[4], ai[4], br[4], bi[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        ar[q] = Ar[kk][tx + 16 * q];
-        ai[q] = Ai[kk][tx + 16 * q];
-        br[q] = Br[kk][ty + 16 * q];
-        bi[q] = Bi[kk][ty + 16 * q];
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          cr[p][q] += ar[p] * br[q] - ai[p] * bi[q];
-          ci[p][q] += ar[p] * bi[q] + ai[p] * br[q];
-        }
-    }
-    __syncthreads();
-  }
-  Cx<float>* out = partial + static_cast<long long>(split) * m * n;
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int gi = tile_m + tx + 16 * p, gj = tile_n + ty + 16 * q;
-      if (gi < m && gj < n) out[gi + static_cast<long long>(gj) * m] = Cx<float>{cr[p][q], ci[p][q]};
-    }
-}
-
-__global__ void reduce_partials_kernel(int m, int n, int splits, const Cx<float>* __restrict__ partial,
-                                       Cx<double>* __restrict__ c, long long ldc, bool add, double alpha) {
-  const long long total = static_cast<long long>(m) * n;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    double re = 0.0, im = 0.0;
-    for (int s = 0; s < splits; ++s) {
-      const Cx<float> v = partial[s * total + idx];
-      re += v.re;
-      im += v.im;
-    }
-    const long long i = idx % m, j = idx / m;
-    Cx<double>& out = c[i + j * ldc];
-    re *= alpha;
-    im *= alpha;
-    if (add) {
-      re += out.re;
-      im += out.im;
-    }
-    out = Cx<double>{re, im};
-  }
-}
-
 struct CompensatedSum {
   double sum = 0.0, correction = 0.0;
   __device__ __forceinline__ void add(double value) {
@@ -208,32 +100,6 @@ void zgemm(cublasHandle_t handle, Op aop, Op bop, int m, int n, int k, const Cx<
                          reinterpret_cast<const cuDoubleComplex*>(b), static_cast<int>(ldb), &beta,
                          reinterpret_cast<cuDoubleComplex*>(c), static_cast<int>(ldc)),
              "cublasZgemm");
-}
-
-void gemm_mixed(Op aop, int m, int n, int k, const Cx<double>* a, const Cx<float>* a32, long long lda,
-                const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, Scratch& workspace,
-                cudaStream_t stream, double alpha) {
-  if (m <= 0 || n <= 0 || k <= 0) return;
-  const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n, BN));
-  int splits = static_cast<int>(std::min<long long>(std::max<long long>(1, (2 * 148 + tiles - 1) / tiles),
-                                                    std::max(1, k / 512)));
-  splits = std::min(splits, 64);
-  const int k_per_split = static_cast<int>(ceil_div(ceil_div(k, splits), BK) * BK);
-  splits = static_cast<int>(ceil_div(k, k_per_split));
-  auto* partial = static_cast<Cx<float>*>(
-      workspace.reserve(sizeof(Cx<float>) * static_cast<std::size_t>(m) * n * splits));
-  const dim3 grid(static_cast<unsigned>(ceil_div(m, BM)), static_cast<unsigned>(ceil_div(n, BN)), splits);
-  if (aop == Op::N) {
-    if (a32) cgemm_simt_kernel<Op::N, float><<<grid, kGemmThreads, 0, stream>>>(m, n, k, k_per_split, a32, lda, b, ldb, partial);
-    else cgemm_simt_kernel<Op::N, double><<<grid, kGemmThreads, 0, stream>>>(m, n, k, k_per_split, a, lda, b, ldb, partial);
-  } else {
-    if (a32) cgemm_simt_kernel<Op::C, float><<<grid, kGemmThreads, 0, stream>>>(m, n, k, k_per_split, a32, lda, b, ldb, partial);
-    else cgemm_simt_kernel<Op::C, double><<<grid, kGemmThreads, 0, stream>>>(m, n, k, k_per_split, a, lda, b, ldb, partial);
-  }
-  SDFT_LAUNCH("cgemm_simt_kernel");
-  const long long total = static_cast<long long>(m) * n;
-  reduce_partials_kernel<<<grid_for(total, 256), 256, 0, stream>>>(m, n, splits, partial, c, ldc, add, alpha);
-  SDFT_LAUNCH("reduce_partials_kernel");
 }
 
 void block_product(int atoms, const int* offsets, const long long* storage, int max_block, const Cx<double>* blocks,

@@ -22,13 +22,6 @@ struct Scratch {
 void zgemm(cublasHandle_t handle, Op aop, Op bop, int m, int n, int k, const Cx<double>* a, long long lda,
            const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, double alpha = 1.0);
 
-// Mixed search GEMM: FP64 storage in/out, products accumulated in FP32 by
-// the hand-written split-K kernel. aop applies to A; B is always normal.
-// `a32` may point to an FP32 copy of A (same layout, ld lda) or be null.
-void gemm_mixed(Op aop, int m, int n, int k, const Cx<double>* a, const Cx<float>* a32, long long lda,
-                const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, Scratch& workspace,
-                cudaStream_t stream, double alpha = 1.0);
-
 // Per-atom block-diagonal product out[off_a + i, c] = sum_j M_a(i,j) P[off_a + j, c]
 // with error-free FP64 products and compensated sums (TwoSum + FMA), the
 // reference's compensated_paw_product order (src/paw_compensated_product.hpp:41-56).

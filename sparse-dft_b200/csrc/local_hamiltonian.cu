@@ -43,103 +43,105 @@ struct LocalArgs {
   const Cx<T>* tw2;
 };
 
-template <typename T, int NMAX>
-__global__ void __launch_bounds__(kThreads, 2) plane_in_kernel(const Cx<double>* __restrict__ x, long long ldx,
+template <typename T>
+__global__ void __launch_bounds__(kThreads) plane_in_kernel(const Cx<double>* __restrict__ x, long long ldx,
                                                             LocalArgs<T> a, Cx<T>* __restrict__ slab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(smem_raw);
   Cx<T>* tw2 = tw1 + a.n1;
-  Cx<T>* plane = tw2 + a.n2;
+  const int plane_elems = a.n1 * a.n2p;
+  Cx<T>* plane_a = tw2 + a.n2;
+  Cx<T>* plane_b = plane_a + plane_elems;
   const int s = blockIdx.x, c = blockIdx.y;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int i = tid; i < a.n1; i += blockDim.x) tw1[i] = a.tw1[i];
   for (int i = tid; i < a.n2; i += blockDim.x) tw2[i] = a.tw2[i];
-  const int plane_elems = a.n1 * a.n2p;
-  for (int i = tid; i < plane_elems; i += blockDim.x) plane[i] = Cx<T>{0, 0};
+  for (int i = tid; i < 2 * plane_elems; i += blockDim.x) plane_a[i] = Cx<T>{0, 0};
   __syncthreads();
   const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
   const int p_end = a.point_offset[s + 1];
   for (int p = a.point_offset[s] + tid; p < p_end; p += blockDim.x)
-    plane[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
+    plane_a[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
   __syncthreads();
-  for (int r = warp; r < a.krows; r += warps) fft_line<T, NMAX, true>(plane + a.krow[r] * a.n2p, 1, a.p2, tw2, lane);
-  __syncthreads();
-  for (int l = warp; l < a.n2; l += warps) fft_line<T, NMAX, true>(plane + l, a.n2p, a.p1, tw1, lane);
-  __syncthreads();
+  // i2 along the active i1 rows, then i1 along every i2 column (rows outside
+  // the active set stay zero in both buffers).
+  Cx<T>* rows_done = fft_lines_pp<T, true>(plane_a, plane_b, a.krows, a.n2p, 1, a.krow, a.p2, tw2);
+  Cx<T>* other = rows_done == plane_a ? plane_b : plane_a;
+  Cx<T>* done = fft_lines_pp<T, true>(rows_done, other, a.n2, 1, a.n2p, nullptr, a.p1, tw1);
   Cx<T>* out = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
   for (int i = tid; i < a.n12; i += blockDim.x) {
     const int i1 = i / a.n2, i2 = i - i1 * a.n2;
-    out[i] = plane[i1 * a.n2p + i2];
+    out[i] = done[i1 * a.n2p + i2];
   }
 }
 
-template <typename T, int NMAX>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 2) pencil_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pencil_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                           const T* __restrict__ potential) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int TL = kPencilLines, STRIDE = TL + 1;
   Cx<T>* tw0 = reinterpret_cast<Cx<T>*>(smem_raw);
-  Cx<T>* tile = tw0 + a.n0;
+  Cx<T>* tile_a = tw0 + a.n0;
+  Cx<T>* tile_b = tile_a + a.n0 * STRIDE;
   const long long kl0 = static_cast<long long>(blockIdx.x) * TL;
   const int c = blockIdx.y;
   const int lines = static_cast<int>(min(static_cast<long long>(TL), a.n12 - kl0));
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int i = tid; i < a.n0; i += blockDim.x) tw0[i] = a.tw0[i];
-  for (int i = tid; i < a.n0 * STRIDE; i += blockDim.x) tile[i] = Cx<T>{0, 0};
+  for (int i = tid; i < a.n0 * STRIDE; i += blockDim.x) tile_a[i] = Cx<T>{0, 0};
   __syncthreads();
   Cx<T>* base = slab + static_cast<long long>(c) * a.slots * a.n12 + kl0;
   for (int idx = tid; idx < a.slots * TL; idx += blockDim.x) {
     const int s = idx / TL, t = idx - s * TL;
-    if (t < lines) tile[a.slot_row[s] * STRIDE + t] = base[static_cast<long long>(s) * a.n12 + t];
+    if (t < lines) tile_a[a.slot_row[s] * STRIDE + t] = base[static_cast<long long>(s) * a.n12 + t];
   }
   __syncthreads();
-  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, true>(tile + t, STRIDE, a.p0, tw0, lane);
-  __syncthreads();
+  Cx<T>* field = fft_lines_pp<T, true>(tile_a, tile_b, lines, 1, STRIDE, nullptr, a.p0, tw0);
   for (int idx = tid; idx < a.n0 * TL; idx += blockDim.x) {
     const int i = idx / TL, t = idx - i * TL;
     if (t < lines) {
       const T v = potential[static_cast<long long>(i) * a.n12 + kl0 + t];
-      tile[i * STRIDE + t] = cscale(tile[i * STRIDE + t], v);
+      field[i * STRIDE + t] = cscale(field[i * STRIDE + t], v);
     }
   }
   __syncthreads();
-  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, false>(tile + t, STRIDE, a.p0, tw0, lane);
-  __syncthreads();
+  Cx<T>* back = fft_lines_pp<T, false>(field, field == tile_a ? tile_b : tile_a, lines, 1, STRIDE, nullptr, a.p0, tw0);
   for (int idx = tid; idx < a.slots * TL; idx += blockDim.x) {
     const int s = idx / TL, t = idx - s * TL;
-    if (t < lines) base[static_cast<long long>(s) * a.n12 + t] = tile[a.slot_row[s] * STRIDE + t];
+    if (t < lines) base[static_cast<long long>(s) * a.n12 + t] = back[a.slot_row[s] * STRIDE + t];
   }
 }
 
-template <typename T, int NMAX>
-__global__ void __launch_bounds__(kThreads, 2) plane_out_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
+template <typename T>
+__global__ void __launch_bounds__(kThreads) plane_out_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                              const Cx<double>* __restrict__ x, long long ldx,
                                                              const double* __restrict__ kinetic, double count,
                                                              Cx<double>* __restrict__ y, long long ldy) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw1 = reinterpret_cast<Cx<T>*>(smem_raw);
   Cx<T>* tw2 = tw1 + a.n1;
-  Cx<T>* plane = tw2 + a.n2;
+  const int plane_elems = a.n1 * a.n2p;
+  Cx<T>* plane_a = tw2 + a.n2;
+  Cx<T>* plane_b = plane_a + plane_elems;
   const int s = blockIdx.x, c = blockIdx.y;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int i = tid; i < a.n1; i += blockDim.x) tw1[i] = a.tw1[i];
   for (int i = tid; i < a.n2; i += blockDim.x) tw2[i] = a.tw2[i];
   const Cx<T>* in = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
   for (int i = tid; i < a.n12; i += blockDim.x) {
     const int i1 = i / a.n2, i2 = i - i1 * a.n2;
-    plane[i1 * a.n2p + i2] = in[i];
+    plane_a[i1 * a.n2p + i2] = in[i];
   }
   __syncthreads();
-  for (int l = warp; l < a.n2; l += warps) fft_line<T, NMAX, false>(plane + l, a.n2p, a.p1, tw1, lane);
-  __syncthreads();
-  for (int r = warp; r < a.krows; r += warps) fft_line<T, NMAX, false>(plane + a.krow[r] * a.n2p, 1, a.p2, tw2, lane);
-  __syncthreads();
+  Cx<T>* cols_done = fft_lines_pp<T, false>(plane_a, plane_b, a.n2, 1, a.n2p, nullptr, a.p1, tw1);
+  Cx<T>* done = fft_lines_pp<T, false>(cols_done, cols_done == plane_a ? plane_b : plane_a, a.krows, a.n2p, 1,
+                                       a.krow, a.p2, tw2);
   const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
   Cx<double>* yc = y + static_cast<long long>(c) * ldy;
   const int p_end = a.point_offset[s + 1];
   for (int p = a.point_offset[s] + tid; p < p_end; p += blockDim.x) {
     const int g = a.point_g[p];
-    const Cx<double> v = cconvert<double>(plane[a.point_smem[p]]);
+    const Cx<double> v = cconvert<double>(done[a.point_smem[p]]);
     const Cx<double> in_g = xc[g];
     const double t = kinetic[g];
     yc[g] = Cx<double>{t * in_g.re + v.re / count, t * in_g.im + v.im / count};
@@ -147,54 +149,54 @@ __global__ void __launch_bounds__(kThreads, 2) plane_out_kernel(const Cx<T>* __r
 }
 
 // Lines along a strided axis: element e of line i at base + e*stride + i.
-template <typename T, int NMAX, bool INV, int TL>
-__global__ void __launch_bounds__(kThreads, 2) fft_strided_kernel(Cx<T>* __restrict__ data, int n, long long stride,
+template <typename T, bool INV, int TL>
+__global__ void __launch_bounds__(kThreads) fft_strided_kernel(Cx<T>* __restrict__ data, int n, long long stride,
                                                                long long inner, long long outer_stride, LinePlan p,
                                                                const Cx<T>* __restrict__ tw_global) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int STRIDE = TL + 1;
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
-  Cx<T>* tile = tw + n;
+  Cx<T>* tile_a = tw + n;
+  Cx<T>* tile_b = tile_a + n * STRIDE;
   const long long i0 = static_cast<long long>(blockIdx.x) * TL;
   const int lines = static_cast<int>(min(static_cast<long long>(TL), inner - i0));
   Cx<T>* base = data + static_cast<long long>(blockIdx.y) * outer_stride + i0;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int i = tid; i < n; i += blockDim.x) tw[i] = tw_global[i];
   for (int idx = tid; idx < n * TL; idx += blockDim.x) {
     const int e = idx / TL, t = idx - e * TL;
-    if (t < lines) tile[e * STRIDE + t] = base[e * stride + t];
+    if (t < lines) tile_a[e * STRIDE + t] = base[e * stride + t];
   }
   __syncthreads();
-  for (int t = warp; t < lines; t += warps) fft_line<T, NMAX, INV>(tile + t, STRIDE, p, tw, lane);
-  __syncthreads();
+  const Cx<T>* done = fft_lines_pp<T, INV>(tile_a, tile_b, lines, 1, STRIDE, nullptr, p, tw);
   for (int idx = tid; idx < n * TL; idx += blockDim.x) {
     const int e = idx / TL, t = idx - e * TL;
-    if (t < lines) base[e * stride + t] = tile[e * STRIDE + t];
+    if (t < lines) base[e * stride + t] = done[e * STRIDE + t];
   }
 }
 
 // Contiguous rows of length n (the innermost axis).
-template <typename T, int NMAX, bool INV, int TR>
-__global__ void __launch_bounds__(kThreads, 2) fft_rows_kernel(Cx<T>* __restrict__ data, int n, int np, long long rows,
+template <typename T, bool INV, int TR>
+__global__ void __launch_bounds__(kThreads) fft_rows_kernel(Cx<T>* __restrict__ data, int n, int np, long long rows,
                                                             LinePlan p, const Cx<T>* __restrict__ tw_global) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
-  Cx<T>* tile = tw + n;
+  Cx<T>* tile_a = tw + n;
+  Cx<T>* tile_b = tile_a + TR * np;
   const long long r0 = static_cast<long long>(blockIdx.x) * TR;
   const int count = static_cast<int>(min(static_cast<long long>(TR), rows - r0));
   Cx<T>* base = data + r0 * n;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   for (int i = tid; i < n; i += blockDim.x) tw[i] = tw_global[i];
   for (int idx = tid; idx < count * n; idx += blockDim.x) {
     const int r = idx / n, e = idx - r * n;
-    tile[r * np + e] = base[idx];
+    tile_a[r * np + e] = base[idx];
   }
   __syncthreads();
-  for (int r = warp; r < count; r += warps) fft_line<T, NMAX, INV>(tile + r * np, 1, p, tw, lane);
-  __syncthreads();
+  const Cx<T>* done = fft_lines_pp<T, INV>(tile_a, tile_b, count, np, 1, nullptr, p, tw);
   for (int idx = tid; idx < count * n; idx += blockDim.x) {
     const int r = idx / n, e = idx - r * n;
-    base[idx] = tile[r * np + e];
+    base[idx] = done[r * np + e];
   }
 }
 
@@ -228,61 +230,63 @@ LocalArgs<T> make_args(const SpherePlan& plan) {
   return a;
 }
 
-template <typename T, int NMAX>
+template <typename T>
 void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns,
                             const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
                             cudaStream_t stream) {
   const LocalArgs<T> a = make_args<T>(plan);
-  const std::size_t plane_smem = sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + static_cast<std::size_t>(plan.n[1]) * plan.n2p);
-  const std::size_t pencil_smem = sizeof(Cx<T>) * (plan.n[0] + static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
-  allow_smem(plane_in_kernel<T, NMAX>, plane_smem);
-  allow_smem(pencil_kernel<T, NMAX>, pencil_smem);
-  allow_smem(plane_out_kernel<T, NMAX>, plane_smem);
+  const std::size_t plane_smem =
+      sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + 2 * static_cast<std::size_t>(plan.n[1]) * plan.n2p);
+  const std::size_t pencil_smem =
+      sizeof(Cx<T>) * (plan.n[0] + 2 * static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
+  allow_smem(plane_in_kernel<T>, plane_smem);
+  allow_smem(pencil_kernel<T>, pencil_smem);
+  allow_smem(plane_out_kernel<T>, plane_smem);
   const dim3 planes(plan.slots, columns);
-  plane_in_kernel<T, NMAX><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
+  plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
   SDFT_LAUNCH("plane_in_kernel");
   const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
-  pencil_kernel<T, NMAX><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+  pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
   SDFT_LAUNCH("pencil_kernel");
-  plane_out_kernel<T, NMAX><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
-                                                                      static_cast<double>(plan.count), y, ldy);
+  plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
+                                                                static_cast<double>(plan.count), y, ldy);
   SDFT_LAUNCH("plane_out_kernel");
 }
 
-template <typename T, int NMAX, bool INV>
+template <typename T, bool INV>
 void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
   const long long n12 = static_cast<long long>(n[1]) * n[2];
   const long long count = n12 * n[0];
-  constexpr int TL = NMAX <= 128 ? 16 : 8;
+  constexpr int TL = 32;
   // axis 2: contiguous rows
   {
     const LinePlan p = make_line_plan(n[2]);
     const int np = n[2] | 1;
     constexpr int TR = TL;
-    const std::size_t smem = sizeof(Cx<T>) * (n[2] + static_cast<std::size_t>(TR) * np);
-    allow_smem(fft_rows_kernel<T, NMAX, INV, TR>, smem);
+    const std::size_t smem = sizeof(Cx<T>) * (n[2] + 2 * static_cast<std::size_t>(TR) * np);
+    allow_smem(fft_rows_kernel<T, INV, TR>, smem);
     const long long rows = count / n[2] * batch;
-    fft_rows_kernel<T, NMAX, INV, TR><<<static_cast<unsigned>(ceil_div(rows, TR)), kThreads, smem, stream>>>(
+    fft_rows_kernel<T, INV, TR><<<static_cast<unsigned>(ceil_div(rows, TR)), kThreads, smem, stream>>>(
         grid, n[2], np, rows, p, device_twiddles<T>(n[2]));
     SDFT_LAUNCH("fft_rows_kernel");
   }
   // axis 1: stride n2, n0*batch outer blocks
   {
     const LinePlan p = make_line_plan(n[1]);
-    const std::size_t smem = sizeof(Cx<T>) * (n[1] + static_cast<std::size_t>(n[1]) * (TL + 1));
-    allow_smem(fft_strided_kernel<T, NMAX, INV, TL>, smem);
+    const std::size_t smem = sizeof(Cx<T>) * (n[1] + 2 * static_cast<std::size_t>(n[1]) * (TL + 1));
+    allow_smem(fft_strided_kernel<T, INV, TL>, smem);
     const dim3 blocks(static_cast<unsigned>(ceil_div(n[2], TL)), static_cast<unsigned>(n[0] * batch));
-    fft_strided_kernel<T, NMAX, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[1], n[2], n[2], n12, p,
+    fft_strided_kernel<T, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[1], n[2], n[2], n12, p,
                                                                             device_twiddles<T>(n[1]));
     SDFT_LAUNCH("fft_strided_kernel axis1");
   }
   // axis 0: stride n1*n2
   {
     const LinePlan p = make_line_plan(n[0]);
-    const std::size_t smem = sizeof(Cx<T>) * (n[0] + static_cast<std::size_t>(n[0]) * (TL + 1));
-    allow_smem(fft_strided_kernel<T, NMAX, INV, TL>, smem);
+    const std::size_t smem = sizeof(Cx<T>) * (n[0] + 2 * static_cast<std::size_t>(n[0]) * (TL + 1));
+    allow_smem(fft_strided_kernel<T, INV, TL>, smem);
     const dim3 blocks(static_cast<unsigned>(ceil_div(n12, TL)), static_cast<unsigned>(batch));
-    fft_strided_kernel<T, NMAX, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[0], n12, n12, count, p,
+    fft_strided_kernel<T, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[0], n12, n12, count, p,
                                                                             device_twiddles<T>(n[0]));
     SDFT_LAUNCH("fft_strided_kernel axis0");
   }
@@ -354,19 +358,16 @@ void local_hamiltonian(const SpherePlan& plan, const Cx<double>* x, long long ld
   if (columns <= 0) return;
   const int nmax = std::max({plan.n[0], plan.n[1], plan.n[2]});
   if (nmax > 128) throw InvalidArgument("operator FFT grid axes above 128 points are not supported");
-  local_hamiltonian_impl<T, 128>(plan, x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
+  (void)nmax;
+  local_hamiltonian_impl<T>(plan, x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
 }
 
 template <typename T>
 void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream) {
   const int nmax = std::max({n[0], n[1], n[2]});
-  if (nmax <= 128) {
-    if (backward) fft3d_impl<T, 128, true>(grid, n, batch, stream);
-    else fft3d_impl<T, 128, false>(grid, n, batch, stream);
-  } else {
-    if (backward) fft3d_impl<T, 512, true>(grid, n, batch, stream);
-    else fft3d_impl<T, 512, false>(grid, n, batch, stream);
-  }
+  if (nmax > kMaxLine) throw InvalidArgument("3D FFT axes above 512 points are not supported");
+  if (backward) fft3d_impl<T, true>(grid, n, batch, stream);
+  else fft3d_impl<T, false>(grid, n, batch, stream);
 }
 
 template void local_hamiltonian<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,

@@ -62,7 +62,8 @@ Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
 Context::~Context() {
   if (solver) cusolverDnDestroy(solver);
   if (blas) cublasDestroy(blas);
-  for (Scratch* s : {&slab32, &slab64, &gemm_work, &staging_in, &staging_out, &staging_aux, &projections, &onsite})
+  for (Scratch* s : {&slab32, &slab64, &staging_in, &staging_out, &staging_aux, &projections, &onsite, &tc.a, &tc.b,
+                     &tc.partial})
     s->release();
   if (owns_stream && stream) cudaStreamDestroy(stream);
 }
@@ -320,8 +321,9 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
   upload(v32_, v32);
   if (np_) {
     upload(b_, all_b);
-    SDFT_CUDA(cudaMalloc(&b32_, sizeof(Cx<float>) * all_b.size()));
-    demote(b_, b32_, all_b.size(), ctx.stream);
+    const Split split = search_split();
+    pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
+    pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
     upload(d_, d_blocks);
     upload(q_, q_blocks);
     upload(block_offsets_, offsets);
@@ -332,15 +334,18 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
 
 DeviceOperator::~DeviceOperator() {
   plan_.release();
+  release(b_packed_);
+  release(bh_packed_);
   for (void* p : {static_cast<void*>(kinetic_), static_cast<void*>(v64_), static_cast<void*>(v32_),
-                  static_cast<void*>(b_), static_cast<void*>(b32_), static_cast<void*>(d_), static_cast<void*>(q_),
+                  static_cast<void*>(b_), static_cast<void*>(d_), static_cast<void*>(q_),
                   static_cast<void*>(block_offsets_), static_cast<void*>(block_storage_)})
     if (p) cudaFree(p);
 }
 
 std::size_t DeviceOperator::device_bytes() const {
   std::size_t bytes = plan_.count * (sizeof(double) + sizeof(float)) + npw_ * (sizeof(double) + 2 * sizeof(int));
-  bytes += static_cast<std::size_t>(np_) * npw_ * (sizeof(Cx<double>) + sizeof(Cx<float>));
+  bytes += static_cast<std::size_t>(np_) * npw_ * sizeof(Cx<double>);
+  bytes += sizeof(std::uint16_t) * static_cast<std::size_t>(b_packed_.ld * b_packed_.rows + bh_packed_.ld * bh_packed_.rows);
   return bytes;
 }
 
@@ -359,14 +364,16 @@ void DeviceOperator::project(const Cx<double>* x, int columns, Cx<double>* p, Pr
   if (precision == Precision::FP64)
     zgemm(ctx_.blas, Op::N, Op::N, np_, columns, npw_, b_, np_, x, npw_, p, np_, false);
   else
-    gemm_mixed(Op::N, np_, columns, npw_, b_, b32_, np_, x, npw_, p, np_, false, ctx_.gemm_work, ctx_.stream);
+    gemm_tc(Op::N, np_, columns, npw_, b_, np_, &b_packed_, x, npw_, p, np_, false, 1.0, b_packed_.split, ctx_.tc,
+            ctx_.stream);
 }
 
 void DeviceOperator::backproject(const Cx<double>* dp, int columns, Cx<double>* y, Precision precision) {
   if (precision == Precision::FP64)
     zgemm(ctx_.blas, Op::C, Op::N, npw_, columns, np_, b_, np_, dp, np_, y, npw_, true);
   else
-    gemm_mixed(Op::C, npw_, columns, np_, b_, b32_, np_, dp, np_, y, npw_, true, ctx_.gemm_work, ctx_.stream);
+    gemm_tc(Op::C, npw_, columns, np_, b_, np_, &bh_packed_, dp, np_, y, npw_, true, 1.0, bh_packed_.split, ctx_.tc,
+            ctx_.stream);
 }
 
 void DeviceOperator::paw_add(const Cx<double>* p, int columns, bool overlap, Cx<double>* y, Precision precision) {

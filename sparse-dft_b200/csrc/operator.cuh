@@ -10,6 +10,7 @@
 
 #include "gemm.cuh"
 #include "local_hamiltonian.cuh"
+#include "umma_gemm.cuh"
 
 namespace sdft_b200 {
 
@@ -24,7 +25,8 @@ struct Context {
   bool owns_stream = false;
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
-  Scratch slab32, slab64, gemm_work, staging_in, staging_out, staging_aux, projections, onsite;
+  Scratch slab32, slab64, staging_in, staging_out, staging_aux, projections, onsite;
+  TensorCoreWorkspace tc;
   explicit Context(int device, cudaStream_t stream);
   ~Context();
   Context(const Context&) = delete;
@@ -107,7 +109,8 @@ class DeviceOperator {
   double* v64_ = nullptr;
   float* v32_ = nullptr;
   Cx<double>* b_ = nullptr;      // np x npw column-major (ld np)
-  Cx<float>* b32_ = nullptr;
+  PackedA b_packed_;             // B (np x npw) for P = B x on the tensor cores
+  PackedA bh_packed_;            // B^H (npw x np) for y += B^H P
   Cx<double>* d_ = nullptr;      // per-atom column-major blocks
   Cx<double>* q_ = nullptr;
   int* block_offsets_ = nullptr;         // [atoms+1]

@@ -1,0 +1,553 @@
+// tcgen05 / TMEM / TMA BF16 GEMM for the mixed-precision complex products.
+//
+// One CTA computes a 128 x BN FP32 tile of Ahat Bhat^T over a range of 64-wide
+// K blocks (split-K across CTAs). Warp 0 lane 0 streams A and B tiles with TMA
+// (128-byte swizzle, no multicast) into a STAGES-deep shared-memory ring;
+// warp 1 lane 0 issues tcgen05.mma (M=128, N=BN, K=16 per instruction) into a
+// tensor-memory accumulator and releases ring slots with tcgen05.commit; then
+// all four warps drain the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32w..32w+31) and write either FP32 split-K partials or the final FP64
+// complex result. Every mbarrier wait is bounded; a wait that runs out sets a
+// device error word and the CTA winds down (the host turns it into an error).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+
+#include "umma_gemm.cuh"
+
+namespace sdft_b200 {
+
+namespace {
+
+constexpr int BM = 128, BK = 64, kThreads = 128;
+constexpr unsigned long long kWaitLimitNs = 2000000000ULL;  // 2 s per wait
+
+__device__ unsigned int g_umma_error = 0;
+
+__device__ __forceinline__ std::uint32_t smem_u32(const void* p) {
+  return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(std::uint64_t* bar, std::uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(std::uint64_t* bar, std::uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, std::uint32_t parity) {
+  std::uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false (and the error word set) when the phase does not
+// complete within the limit or another thread already gave up.
+__device__ bool mbar_wait(std::uint64_t* bar, std::uint32_t parity) {
+  const unsigned long long start = globaltimer();
+  for (std::uint32_t spin = 0;; ++spin) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((spin & 255u) == 255u) {
+      if (*reinterpret_cast<volatile unsigned int*>(&g_umma_error) != 0u) return false;
+      if (globaltimer() - start > kWaitLimitNs) {
+        atomicExch(&g_umma_error, 1u);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, std::uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<std::uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void umma_bf16(std::uint32_t d_tmem, std::uint64_t adesc, std::uint64_t bdesc,
+                                          std::uint32_t idesc, std::uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+          d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(std::uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzle shared-memory matrix descriptor (rows of 128 B,
+// 8-row atoms 1024 B apart): start>>4, LBO 1, SBO 64 (x16 B), version 1, SWIZZLE_128B.
+__device__ __forceinline__ std::uint64_t smem_desc(std::uint32_t addr) {
+  return (static_cast<std::uint64_t>((addr >> 4) & 0x3FFFu)) | (1ULL << 16) | (64ULL << 32) | (1ULL << 46) |
+         (2ULL << 61);
+}
+
+template <int BN>
+__host__ __device__ constexpr std::uint32_t instr_desc() {
+  // D=F32 (bits 4-5 = 1), A=B=BF16 (bits 7-9 = 1, 10-12 = 1), K-major both, N>>3 at 17, M>>4 at 24.
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<std::uint32_t>(BN >> 3) << 17) |
+         (static_cast<std::uint32_t>(BM >> 4) << 24);
+}
+
+template <int BN>
+__host__ __device__ constexpr int stages() {
+  return BN >= 256 ? 4 : 6;
+}
+
+struct EpilogueArgs {
+  int m, n2;                   // rows, real columns (2 x complex columns)
+  Cx<float>* partial;          // split-K output [split][n2/2][m] or null
+  Cx<double>* c;               // direct output (when partial is null)
+  long long ldc;
+  double alpha;
+  int add;
+};
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     int k_blocks_total, int k_blocks_per_split, EpilogueArgs ep) {
+  constexpr int S = stages<BN>();
+  constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE = A_BYTES + B_BYTES;
+  constexpr std::uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<std::uintptr_t>(smem_raw) + 1023) & ~static_cast<std::uintptr_t>(1023));
+  std::uint64_t* full = reinterpret_cast<std::uint64_t*>(smem + S * STAGE);
+  std::uint64_t* empty = full + S;
+  std::uint64_t* accum = empty + S;
+  std::uint32_t* tmem_holder = reinterpret_cast<std::uint32_t*>(accum + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tile_m = blockIdx.x * BM, tile_n = blockIdx.y * BN;
+  const int kb0 = blockIdx.z * k_blocks_per_split;
+  const int nkb = max(0, min(k_blocks_total, kb0 + k_blocks_per_split) - kb0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const std::uint32_t tmem = *tmem_holder;
+
+  int issued = 0;
+  if (warp == 0 && lane == 0) {
+    // TMA producer
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % S;
+      if (i >= S && !mbar_wait(&empty[s], ((i / S) - 1) & 1)) break;
+      mbar_arrive_expect_tx(&full[s], STAGE);
+      const int kc = (kb0 + i) * BK;
+      tma_load_2d(smem + s * STAGE, &map_a, kc, tile_m, &full[s]);
+      tma_load_2d(smem + s * STAGE + A_BYTES, &map_b, kc, tile_n, &full[s]);
+      issued = i + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // tcgen05.mma issuer
+    constexpr std::uint32_t idesc = instr_desc<BN>();
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % S;
+      if (!mbar_wait(&full[s], (i / S) & 1)) break;
+      tc_fence_after();
+      const std::uint32_t a_addr = smem_u32(smem + s * STAGE), b_addr = a_addr + A_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk)
+        umma_bf16(tmem, smem_desc(a_addr + kk * 32), smem_desc(b_addr + kk * 32), idesc, (i | kk) != 0);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(accum);
+  }
+  __syncwarp();
+  // Epilogue: warp w reads TMEM lanes 32w..32w+31 (tile rows).
+  const bool have = __all_sync(0xffffffffu, nkb > 0 && mbar_wait(accum, 0));
+  tc_fence_after();
+  const int row = tile_m + warp * 32 + lane;
+  const int n_complex_total = ep.n2 / 2;
+  for (int c0 = 0; c0 < BN; c0 += 16) {
+    std::uint32_t r[16];
+    if (have) {
+      const std::uint32_t taddr = tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c0);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    } else {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) r[q] = 0u;
+    }
+    if (row < ep.m) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = (tile_n + c0) / 2 + q;
+        if (j >= n_complex_total) break;
+        const float re = __uint_as_float(r[2 * q]), im = __uint_as_float(r[2 * q + 1]);
+        if (ep.partial) {
+          ep.partial[(static_cast<long long>(blockIdx.z) * n_complex_total + j) * ep.m + row] = Cx<float>{re, im};
+        } else {
+          Cx<double>& out = ep.c[row + static_cast<long long>(j) * ep.ldc];
+          double vr = ep.alpha * static_cast<double>(re), vi = ep.alpha * static_cast<double>(im);
+          if (ep.add) {
+            vr += out.re;
+            vi += out.im;
+          }
+          out = Cx<double>{vr, vi};
+        }
+      }
+    }
+  }
+  // Wind-down: drain TMA copies still in flight on the error path, free TMEM.
+  if (warp == 0 && lane == 0 && *reinterpret_cast<volatile unsigned int*>(&g_umma_error) != 0u) {
+    for (int i = max(0, issued - S); i < issued; ++i) mbar_wait(&full[i % S], (i / S) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+__global__ void reduce_splits_kernel(int m, int n, int splits, const Cx<float>* __restrict__ partial,
+                                     Cx<double>* __restrict__ c, long long ldc, bool add, double alpha) {
+  const long long total = static_cast<long long>(m) * n;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      const Cx<float> v = partial[s * total + idx];
+      re += v.re;
+      im += v.im;
+    }
+    const long long i = idx % m, j = idx / m;
+    Cx<double>& out = c[i + j * ldc];
+    re *= alpha;
+    im *= alpha;
+    if (add) {
+      re += out.re;
+      im += out.im;
+    }
+    out = Cx<double>{re, im};
+  }
+}
+
+// ---- packing (FP64 complex -> BF16 split terms) ---------------------------
+
+// Split-term index of product p on the A and B side: BF16x3 pairs (0,0) (0,1)
+// (1,0); BF16x6 adds (0,2) (1,1) (2,0).
+__host__ __device__ constexpr int term_a(int p) { return p == 2 || p == 4 ? 1 : p == 5 ? 2 : 0; }
+__host__ __device__ constexpr int term_b(int p) { return p == 1 || p == 4 ? 1 : p == 3 ? 2 : 0; }
+
+__device__ __forceinline__ void split3(double x, std::uint16_t t[3]) {
+  const __nv_bfloat16 h0 = __double2bfloat16(x);
+  const double r1 = x - static_cast<double>(__bfloat162float(h0));
+  const __nv_bfloat16 h1 = __double2bfloat16(r1);
+  const double r2 = r1 - static_cast<double>(__bfloat162float(h1));
+  const __nv_bfloat16 h2 = __double2bfloat16(r2);
+  t[0] = __bfloat16_as_ushort(h0);
+  t[1] = __bfloat16_as_ushort(h1);
+  t[2] = __bfloat16_as_ushort(h2);
+}
+
+// Writes the 2P A-side entries of one complex value.
+template <int P>
+__device__ __forceinline__ void write_a(std::uint16_t* dst, Cx<double> v) {
+  std::uint16_t re[3], im[3];
+  split3(v.re, re);
+  split3(v.im, im);
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    dst[2 * p] = re[term_a(p)];
+    dst[2 * p + 1] = im[term_a(p)];
+  }
+}
+
+template <int P, bool CONJ_T>
+__global__ void pack_a_direct_kernel(const Cx<double>* __restrict__ src, long long lds, int rows, int k,
+                                     std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
+  // CONJ_T: A[i,k] = conj(src[k + i*lds]) (k contiguous in the source).
+  const long long total = static_cast<long long>(rows) * k;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long i = idx / k, kk = idx % k;
+    Cx<double> v = src[kk + i * lds];
+    if (CONJ_T) v.im = -v.im;
+    write_a<P>(out + i * ldo + kk * 2 * P, v);
+  }
+  // zero padding [2Pk, kexp) of every row
+  const long long pad = kexp - 2LL * P * k;
+  const long long ptotal = static_cast<long long>(rows) * pad;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < ptotal;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long i = idx / pad, q = idx % pad;
+    out[i * ldo + 2LL * P * k + q] = 0;
+  }
+}
+
+// A[i,k] = src[i + k*lds] (rows contiguous): 32x32 shared-memory transpose.
+template <int P>
+__global__ void pack_a_transpose_kernel(const Cx<double>* __restrict__ src, long long lds, int rows, int k,
+                                        std::uint16_t* __restrict__ out, long long ldo, long long out_k_offset) {
+  __shared__ Cx<double> tile[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + tx, kk = k0 + r;
+    tile[r][tx] = (i < rows && kk < k) ? src[i + static_cast<long long>(kk) * lds] : Cx<double>{0, 0};
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, kk = k0 + tx;
+    if (i < rows && kk < k) write_a<P>(out + static_cast<long long>(i) * ldo + (out_k_offset + kk) * 2 * P, tile[tx][r]);
+  }
+}
+
+template <int P>
+__global__ void zero_pad_kernel(std::uint16_t* __restrict__ out, long long ldo, int rows, long long from, long long to) {
+  const long long pad = to - from;
+  const long long total = static_cast<long long>(rows) * pad;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x)
+    out[(idx / pad) * ldo + from + idx % pad] = 0;
+}
+
+template <int P>
+__global__ void pack_b_kernel(const Cx<double>* __restrict__ src, long long ldb, int k, int n,
+                              std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
+  const long long total = static_cast<long long>(n) * k;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long j = idx / k, kk = idx % k;
+    const Cx<double> v = src[kk + j * ldb];
+    std::uint16_t re[3], im[3];
+    split3(v.re, re);
+    split3(v.im, im);
+    std::uint16_t* row0 = out + (2 * j) * ldo + kk * 2 * P;
+    std::uint16_t* row1 = row0 + ldo;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const int t = term_b(p);
+      row0[2 * p] = re[t];
+      row0[2 * p + 1] = im[t] ^ 0x8000u;  // -Im (sign flip is exact)
+      row1[2 * p] = im[t];
+      row1[2 * p + 1] = re[t];
+    }
+  }
+  const long long pad = kexp - 2LL * P * k;
+  const long long ptotal = 2LL * n * pad;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < ptotal;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x)
+    out[(idx / pad) * ldo + 2LL * P * k + idx % pad] = 0;
+}
+
+unsigned grid_for(long long total) {
+  return static_cast<unsigned>(std::min<long long>(std::max<long long>(1, (total + 255) / 256), 148LL * 16));
+}
+
+// ---- tensor maps -----------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult status;
+    SDFT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &status));
+    if (status != cudaDriverEntryPointSuccess || !ptr) throw CudaError("cuTensorMapEncodeTiled is unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  });
+  return fn;
+}
+
+CUtensorMap kmajor_map(const std::uint16_t* base, long long rows, long long kexp, long long ld, int box_rows) {
+  if (reinterpret_cast<std::uintptr_t>(base) % 16 != 0 || (ld * 2) % 16 != 0)
+    throw InvalidArgument("BF16 operand base and row stride must be 16-byte aligned");
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(kexp), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * 2)};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t element_strides[2] = {1, 1};
+  const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<std::uint16_t*>(base), dims,
+                                 strides, box, element_strides, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed: " + std::to_string(static_cast<int>(r)));
+  return map;
+}
+
+template <int BN>
+void launch(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n2,
+            long long kexp, const EpilogueArgs& ep_in, int splits, int k_blocks, int kpb, cudaStream_t stream) {
+  constexpr int S = stages<BN>();
+  const std::size_t smem = static_cast<std::size_t>(S) * (BM * BK * 2 + BN * BK * 2) + 1024 + 256;
+  SDFT_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+  const CUtensorMap map_a = kmajor_map(a, m, kexp, lda, BM);
+  const CUtensorMap map_b = kmajor_map(b, n2, kexp, ldb, BN);
+  const dim3 grid(static_cast<unsigned>(ceil_div(m, BM)), static_cast<unsigned>(ceil_div(n2, BN)), splits);
+  umma_gemm_kernel<BN><<<grid, kThreads, smem, stream>>>(map_a, map_b, k_blocks, kpb, ep_in);
+  SDFT_LAUNCH("umma_gemm_kernel");
+}
+
+}  // namespace
+
+bool umma_available() {
+  int device = 0, major = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess) return false;
+  return major == 10;
+}
+
+void pack_a(Op aop, const Cx<double>* src, long long lds, int rows, int k, Split split, std::uint16_t* out,
+            long long ldo, cudaStream_t stream) {
+  const long long kexp = expanded_k(k, split);
+  if (aop == Op::C) {
+    const long long total = static_cast<long long>(rows) * std::max<long long>(k, kexp - 2LL * split_terms(split) * k);
+    if (split == Split::BF16x3)
+      pack_a_direct_kernel<3, true><<<grid_for(total), 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
+    else
+      pack_a_direct_kernel<6, true><<<grid_for(total), 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
+    SDFT_LAUNCH("pack_a_direct_kernel");
+    return;
+  }
+  const dim3 grid(static_cast<unsigned>(ceil_div(rows, 32)), static_cast<unsigned>(ceil_div(k, 32)));
+  if (split == Split::BF16x3)
+    pack_a_transpose_kernel<3><<<grid, dim3(32, 8), 0, stream>>>(src, lds, rows, k, out, ldo, 0);
+  else
+    pack_a_transpose_kernel<6><<<grid, dim3(32, 8), 0, stream>>>(src, lds, rows, k, out, ldo, 0);
+  SDFT_LAUNCH("pack_a_transpose_kernel");
+  const long long from = 2LL * split_terms(split) * k;
+  if (kexp > from) {
+    zero_pad_kernel<3><<<grid_for(static_cast<long long>(rows) * (kexp - from)), 256, 0, stream>>>(out, ldo, rows,
+                                                                                                  from, kexp);
+    SDFT_LAUNCH("zero_pad_kernel");
+  }
+}
+
+void pack_a_columns(const Cx<double>* src, long long lds, int rows, int first, int count, Split split,
+                    std::uint16_t* out, long long ldo, cudaStream_t stream) {
+  if (count <= 0) return;
+  const dim3 grid(static_cast<unsigned>(ceil_div(rows, 32)), static_cast<unsigned>(ceil_div(count, 32)));
+  const Cx<double>* s = src + static_cast<long long>(first) * lds;
+  if (split == Split::BF16x3)
+    pack_a_transpose_kernel<3><<<grid, dim3(32, 8), 0, stream>>>(s, lds, rows, count, out, ldo, first);
+  else
+    pack_a_transpose_kernel<6><<<grid, dim3(32, 8), 0, stream>>>(s, lds, rows, count, out, ldo, first);
+  SDFT_LAUNCH("pack_a_transpose_kernel");
+}
+
+void pack_b(const Cx<double>* src, long long ldb, int k, int n, Split split, std::uint16_t* out, long long ldo,
+            cudaStream_t stream) {
+  const long long kexp = expanded_k(k, split);
+  const long long total = static_cast<long long>(n) * std::max<long long>(k, 2 * (kexp - 2LL * split_terms(split) * k));
+  if (split == Split::BF16x3) pack_b_kernel<3><<<grid_for(total), 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
+  else pack_b_kernel<6><<<grid_for(total), 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
+  SDFT_LAUNCH("pack_b_kernel");
+}
+
+void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n,
+                       long long kexp, Cx<double>* c, long long ldc, bool add, double alpha, Scratch& workspace,
+                       cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || kexp <= 0) return;
+  if (kexp % BK != 0) throw InvalidArgument("expanded K must be a multiple of 64");
+  const int n2 = 2 * n;
+  const int k_blocks = static_cast<int>(kexp / BK);
+  const bool wide = n2 > 128;
+  const int bn = wide ? 256 : 128;
+  const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n2, bn));
+  int splits = static_cast<int>(std::min<long long>(std::max<long long>(1, (2 * 148 + tiles - 1) / tiles),
+                                                    std::max(1, k_blocks / 8)));
+  splits = std::min(splits, 128);
+  const int kpb = static_cast<int>(ceil_div(k_blocks, splits));
+  splits = static_cast<int>(ceil_div(k_blocks, kpb));
+  EpilogueArgs ep{m, n2, nullptr, c, ldc, alpha, add ? 1 : 0};
+  if (splits > 1)
+    ep.partial = static_cast<Cx<float>*>(workspace.reserve(sizeof(Cx<float>) * static_cast<std::size_t>(m) * n * splits));
+  if (wide) launch<256>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
+  else launch<128>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
+  if (splits > 1) {
+    reduce_splits_kernel<<<grid_for(static_cast<long long>(m) * n), 256, 0, stream>>>(m, n, splits, ep.partial, c, ldc,
+                                                                                     add, alpha);
+    SDFT_LAUNCH("reduce_splits_kernel");
+  }
+}
+
+Split search_split() {
+  static const Split split = [] {
+    const char* v = std::getenv("SDFT_B200_SPLIT");
+    if (!v || std::string(v) == "x6") return Split::BF16x6;
+    if (std::string(v) == "x3") return Split::BF16x3;
+    throw InvalidArgument("SDFT_B200_SPLIT must be x3 or x6");
+  }();
+  return split;
+}
+
+void pack_persistent(Op aop, const Cx<double>* a, long long lda, int rows, int k, Split split, PackedA& out,
+                     cudaStream_t stream) {
+  release(out);
+  out.ld = expanded_k(k, split);
+  out.rows = rows;
+  out.k = k;
+  out.split = split;
+  SDFT_CUDA(cudaMalloc(&out.data, sizeof(std::uint16_t) * static_cast<std::size_t>(out.ld) * rows));
+  pack_a(aop, a, lda, rows, k, split, out.data, out.ld, stream);
+}
+
+void release(PackedA& packed) {
+  if (packed.data) cudaFree(packed.data);
+  packed = PackedA{};
+}
+
+void gemm_tc(Op aop, int m, int n, int k, const Cx<double>* a, long long lda, const PackedA* packed,
+             const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, double alpha, Split split,
+             TensorCoreWorkspace& ws, cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || k <= 0) return;
+  const long long kexp = expanded_k(k, split);
+  const std::uint16_t* pa;
+  long long lda_p;
+  if (packed) {
+    if (packed->rows != m || packed->k != k || packed->split != split) throw InvalidArgument("packed operand shape mismatch");
+    pa = packed->data;
+    lda_p = packed->ld;
+  } else {
+    auto* buf = static_cast<std::uint16_t*>(ws.a.reserve(sizeof(std::uint16_t) * static_cast<std::size_t>(kexp) * m));
+    pack_a(aop, a, lda, m, k, split, buf, kexp, stream);
+    pa = buf;
+    lda_p = kexp;
+  }
+  auto* pb = static_cast<std::uint16_t*>(ws.b.reserve(sizeof(std::uint16_t) * static_cast<std::size_t>(kexp) * 2 * n));
+  pack_b(b, ldb, k, n, split, pb, kexp, stream);
+  umma_complex_gemm(pa, lda_p, pb, kexp, m, n, kexp, c, ldc, add, alpha, ws.partial, stream);
+}
+
+unsigned int umma_error_flag_read_and_clear() {
+  unsigned int value = 0, zero = 0;
+  SDFT_CUDA(cudaMemcpyFromSymbol(&value, g_umma_error, sizeof(value)));
+  if (value) SDFT_CUDA(cudaMemcpyToSymbol(g_umma_error, &zero, sizeof(zero)));
+  return value;
+}
+
+}  // namespace sdft_b200

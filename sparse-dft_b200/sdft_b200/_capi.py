@@ -100,6 +100,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_operator_destroy", [P])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_complex_gemm", [P, ctypes.c_int, ctypes.c_int, SZ, SZ, SZ, P, SZ, P, SZ, P, SZ, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_operator_arrays", [P, U64, D, D, D, D])
     fn("sdft_b200_apply", [P, ctypes.c_int, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_pair", [P, P, SZ, P, P, ctypes.c_int, ctypes.c_int])

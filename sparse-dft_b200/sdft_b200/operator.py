@@ -212,3 +212,25 @@ class PlaneWaveOperator:
         info = stats.as_dict()
         return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
                 "iterations": int(info["iterations"]), "stats": info}
+
+
+def complex_gemm(context: Context, a, b, adjoint_a: bool = False, precision="fp64", c=None):
+    """C = op(A) B (+ c when given), the reference's complex_gemm (host arrays).
+
+    precision 'fp64' is exact FP64; 'mixed' runs BF16 split products on the
+    tensor cores with FP32 accumulation.
+    """
+    lib = C.library()
+    a = np.asfortranarray(a, dtype=np.complex128)
+    b = np.asfortranarray(b, dtype=np.complex128)
+    m = a.shape[1] if adjoint_a else a.shape[0]
+    k = a.shape[0] if adjoint_a else a.shape[1]
+    if b.shape[0] != k:
+        raise ValueError("inner dimensions differ")
+    n = b.shape[1]
+    add = c is not None
+    out = np.asfortranarray(c, dtype=np.complex128).copy(order="F") if add else np.zeros((m, n), np.complex128, order="F")
+    C.check(lib.sdft_b200_complex_gemm(context.handle, 1 if adjoint_a else 0, 0, m, n, k, ctypes.c_void_p(a.ctypes.data),
+                                       a.shape[0], ctypes.c_void_p(b.ctypes.data), b.shape[0],
+                                       ctypes.c_void_p(out.ctypes.data), m, _precision(precision), int(add), C.HOST))
+    return out
