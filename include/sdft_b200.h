@@ -111,6 +111,30 @@ SDFT_B200_API sdft_b200_status sdft_b200_apply_pair(sdft_b200_operator* op, cons
 SDFT_B200_API sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size_t columns, double* p,
                                    int precision, int memory);
 
+/* Accelerator-style local part on caller arrays (no resident operator):
+ * output = kinetic o input + (1/N) FFT_fwd(potential . FFT_bwd(scatter(input)))[indices]
+ * for `columns` columns of npw values; potential holds the real V(r) on the
+ * shape[0] x shape[1] x shape[2] grid (row-major). A nonzero operator_identity
+ * promises immutable shape/indices/potential for that identity, so the device
+ * copies are reused; zero re-uploads them. kinetic and input are per call.
+ * Replaces: Accelerator::local_hamiltonian, src/compute_backend.hpp:81-83
+ * (accelerated_local_hamiltonian, src/compute_backend.hpp:42-45). */
+SDFT_B200_API sdft_b200_status sdft_b200_local_hamiltonian(sdft_b200_context* context, const int32_t shape[3],
+                                                           const uint64_t* indices, size_t npw, const double* kinetic,
+                                                           const double* potential, const double* input,
+                                                           size_t columns, double* output, int precision,
+                                                           uint64_t operator_identity);
+/* PAW chain on caller arrays: h = B^H (D (B x)), s = B^H (Q (B x)) with B the
+ * projectors x npw column-major matrix and D, Q dense projectors x projectors.
+ * A nonzero projector_identity keeps B resident (and its tensor-core packing);
+ * a nonzero identity keeps D and Q resident. Host pointers, synchronous.
+ * Replaces: Accelerator::paw_pair, src/compute_backend.hpp:87-88
+ * (accelerated_paw_pair, src/compute_backend.hpp:48-50). */
+SDFT_B200_API sdft_b200_status sdft_b200_paw_pair(sdft_b200_context* context, uint64_t identity, size_t npw,
+                                                  size_t projectors, size_t columns, const double* b, const double* d,
+                                                  const double* q, const double* input, double* h, double* s,
+                                                  int precision, uint64_t projector_identity);
+
 enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
 
 /* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with

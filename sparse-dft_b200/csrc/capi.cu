@@ -283,6 +283,33 @@ sdft_b200_status sdft_b200_project(sdft_b200_operator* op, const double* x, size
   });
 }
 
+sdft_b200_status sdft_b200_local_hamiltonian(sdft_b200_context* context, const int32_t shape[3],
+                                             const uint64_t* indices, size_t npw, const double* kinetic,
+                                             const double* potential, const double* input, size_t columns,
+                                             double* output, int precision, uint64_t operator_identity) {
+  return guarded([&] {
+    require(context && shape, "invalid accelerated FFT dimensions");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    const int s[3] = {shape[0], shape[1], shape[2]};
+    sdft_b200::accelerator_local_hamiltonian(ctx, s, indices, npw, kinetic, potential, input, columns, output,
+                                             precision_of(precision), operator_identity);
+  });
+}
+
+sdft_b200_status sdft_b200_paw_pair(sdft_b200_context* context, uint64_t identity, size_t npw, size_t projectors,
+                                    size_t columns, const double* b, const double* d, const double* q,
+                                    const double* input, double* h, double* s, int precision,
+                                    uint64_t projector_identity) {
+  return guarded([&] {
+    require(context != nullptr, "invalid CUDA PAW chain shape");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    sdft_b200::accelerator_paw_pair(ctx, identity, npw, projectors, columns, b, d, q, input, h, s,
+                                    precision_of(precision), projector_identity ? projector_identity : identity);
+  });
+}
+
 sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int bop, size_t m, size_t n, size_t k,
                                         const double* a, size_t lda, const double* b, size_t ldb, double* c,
                                         size_t ldc, int precision, int add, int memory) {

@@ -237,28 +237,54 @@ __device__ __forceinline__ void pp_butterflies(const Cx<T>* src_line, Cx<T>* dst
   }
 }
 
+// One butterfly (line offset `offset`, index j) of a ping-pong stage.
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void pp_butterfly(const Cx<T>* src, Cx<T>* dst, int offset, int j, int es, int n, int ns,
+                                             const Cx<T>* tw) {
+  const int m = n / R, twstride = n / (ns * R), unit = n / R;
+  const int k = j % ns;
+  const Cx<T>* in = src + offset;
+  Cx<T> v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    Cx<T> x = in[(j + r * m) * es];
+    if (r > 0 && k > 0) x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
+    v[r] = x;
+  }
+  radix_dft<T, R, INV>(v, tw, unit);
+  const int base = (j / ns) * ns * R + k;
+  Cx<T>* out = dst + offset;
+#pragma unroll
+  for (int r = 0; r < R; ++r) out[(base + r * ns) * es] = v[r];
+}
+
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void pp_stage_flat(const Cx<T>* src, Cx<T>* dst, int count, int line_stride, int es,
+                                              const int* rows, int n, int ns, const Cx<T>* tw) {
+  // Work items (line, butterfly) with lines fastest: consecutive threads hit
+  // consecutive lines at the same butterfly, so all lanes stay busy.
+  const int m = n / R;
+  const int items = count * m;
+  for (int item = threadIdx.x; item < items; item += blockDim.x) {
+    const int j = item / count, t = item - j * count;
+    const int offset = (rows ? rows[t] : t) * line_stride;
+    pp_butterfly<T, R, INV>(src, dst, offset, j, es, n, ns, tw);
+  }
+}
+
 template <typename T, bool INV>
 __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
                                const int* rows, const LinePlan& plan, const Cx<T>* tw) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int ns = 1;
   for (int s = 0; s < plan.stages; ++s) {
     const int r = plan.radix[s];
-    for (int b0 = 0; b0 < count; b0 += kWarp) {
-      const int t = b0 + lane;
-      if (t < count) {
-        const int offset = (rows ? rows[t] : t) * line_stride;
-        const Cx<T>* in = src + offset;
-        Cx<T>* out = dst + offset;
-        switch (r) {
-          case 2: pp_butterflies<T, 2, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
-          case 3: pp_butterflies<T, 3, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
-          case 4: pp_butterflies<T, 4, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
-          case 5: pp_butterflies<T, 5, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
-          case 7: pp_butterflies<T, 7, INV>(in, out, elem_stride, plan.n, ns, tw, warp); break;
-          default: break;
-        }
-      }
+    switch (r) {
+      case 2: pp_stage_flat<T, 2, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 3: pp_stage_flat<T, 3, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 4: pp_stage_flat<T, 4, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 5: pp_stage_flat<T, 5, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 7: pp_stage_flat<T, 7, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      default: break;
     }
     __syncthreads();
     Cx<T>* swap = src;

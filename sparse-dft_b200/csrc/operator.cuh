@@ -16,6 +16,24 @@ namespace sdft_b200 {
 
 enum class Precision : int { FP64 = 0, Mixed = 1 };
 
+// Device copies kept across Accelerator-style calls, keyed by the caller's
+// immutable identity tokens (src/compute_backend.hpp:32-41).
+struct AcceleratorCache {
+  std::uint64_t local_identity = 0;
+  int shape[3] = {0, 0, 0};
+  SpherePlan plan;
+  Scratch v64, v32, kinetic;
+  std::uint64_t projector_identity = 0, onsite_identity = 0;
+  int npw = 0, projectors = 0;
+  Scratch b, d, q;
+  PackedA b_packed, bh_packed;
+  ~AcceleratorCache() {
+    plan.release();
+    release(b_packed);
+    release(bh_packed);
+  }
+};
+
 // One CUDA stream with its library handles and grow-only scratch. A context is
 // used by one host thread at a time (the reference keeps one Accelerator per
 // host thread, src/compute_backend.cpp:62-73).
@@ -27,12 +45,21 @@ struct Context {
   cusolverDnHandle_t solver = nullptr;
   Scratch slab32, slab64, staging_in, staging_out, staging_aux, projections, onsite;
   TensorCoreWorkspace tc;
+  AcceleratorCache accel;
   explicit Context(int device, cudaStream_t stream);
   ~Context();
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
   void synchronize() const;
 };
+
+// Accelerator-style calls on caller host arrays (accelerator.cu).
+void accelerator_local_hamiltonian(Context& ctx, const int shape[3], const std::uint64_t* indices, std::size_t npw,
+                                   const double* kinetic, const double* potential, const double* input,
+                                   std::size_t columns, double* output, Precision precision, std::uint64_t identity);
+void accelerator_paw_pair(Context& ctx, std::uint64_t identity, std::size_t npw, std::size_t np,
+                          std::size_t columns, const double* b, const double* d, const double* q, const double* input,
+                          double* h, double* s, Precision precision, std::uint64_t projector_identity);
 
 struct GVectorList {
   std::vector<int> hkl;         // 3 per vector
