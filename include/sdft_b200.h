@@ -135,6 +135,16 @@ SDFT_B200_API sdft_b200_status sdft_b200_paw_pair(sdft_b200_context* context, ui
                                                   const double* q, const double* input, double* h, double* s,
                                                   int precision, uint64_t projector_identity);
 
+/* Spin-unpolarised PBE per point in FP64: for density n > 0 and gradient
+ * magnitude |grad n| >= 0, out[7*i ..] = energy density, energy per particle,
+ * exchange energy density, correlation energy density, exchange potential,
+ * correlation potential, 2 dE/d|grad n|^2 coefficient (the PbeXcPoint fields).
+ * Invalid points give INVALID_ARGUMENT, nonfinite results NONFINITE.
+ * Replaces: Accelerator::pbe_points / accelerated_pbe_points,
+ * src/compute_backend.hpp:46-47,84-86 (pbe_unpolarized, src/pbe_xc.cpp:116-140). */
+SDFT_B200_API sdft_b200_status sdft_b200_pbe_points(sdft_b200_context* context, const double* density,
+                                                    const double* gradient, size_t count, double* out, int memory);
+
 enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
 
 /* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with

@@ -168,3 +168,118 @@ def certified_residuals(op: Operator, eigenvalues: np.ndarray, vectors: np.ndarr
     res = np.linalg.norm(hx - sx * eigenvalues[None, :], axis=0)
     metric = np.real(np.sum(vectors.conj() * sx, axis=0))
     return res, np.abs(metric - 1.0)
+
+
+# --- PBE exchange-correlation (src/pbe_xc.cpp) -------------------------------
+
+_PBE_GAMMA = 0.031090690869654895
+_PBE_BETA = 0.06672455060314922
+_PBE_MU = 0.2195149727645171
+_PBE_KAPPA = 0.804
+
+
+class _Dual:
+    """Forward-mode value with d/dn and d/d|grad n|^2 over numpy arrays (src/pbe_xc.cpp:18-60)."""
+
+    __slots__ = ("v", "dn", "dg")
+
+    def __init__(self, v, dn, dg):
+        self.v, self.dn, self.dg = v, dn, dg
+
+    @staticmethod
+    def lift(x):
+        return x if isinstance(x, _Dual) else _Dual(x, 0.0, 0.0)
+
+    def __add__(self, o):
+        o = _Dual.lift(o)
+        return _Dual(self.v + o.v, self.dn + o.dn, self.dg + o.dg)
+
+    __radd__ = __add__
+
+    def __sub__(self, o):
+        o = _Dual.lift(o)
+        return _Dual(self.v - o.v, self.dn - o.dn, self.dg - o.dg)
+
+    def __rsub__(self, o):
+        return _Dual.lift(o) - self
+
+    def __neg__(self):
+        return _Dual(-self.v, -self.dn, -self.dg)
+
+    def __mul__(self, o):
+        if not isinstance(o, _Dual):
+            return _Dual(self.v * o, self.dn * o, self.dg * o)
+        return _Dual(self.v * o.v, self.dn * o.v + self.v * o.dn, self.dg * o.v + self.v * o.dg)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        if not isinstance(o, _Dual):
+            return self * (1.0 / o)
+        inv = 1.0 / o.v
+        inv2 = inv * inv
+        return _Dual(self.v * inv, (self.dn * o.v - self.v * o.dn) * inv2, (self.dg * o.v - self.v * o.dg) * inv2)
+
+    def __rtruediv__(self, o):
+        return _Dual.lift(o) / self
+
+    def pow(self, p):
+        value = np.sqrt(self.v) if p == 0.5 else np.power(self.v, p)
+        d = p * value / self.v
+        return _Dual(value, d * self.dn, d * self.dg)
+
+    def log1p(self):
+        return _Dual(np.log1p(self.v), self.dn / (1.0 + self.v), self.dg / (1.0 + self.v))
+
+    def expm1(self):
+        value = np.expm1(self.v)
+        return _Dual(value, (1.0 + value) * self.dn, (1.0 + value) * self.dg)
+
+
+def _pw92(rs: _Dual) -> _Dual:
+    """PW92 unpolarised correlation energy per particle (src/pbe_xc.cpp:62-72)."""
+    a, alpha1, b1, b2, b3, b4 = 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294
+    root = rs.pow(0.5)
+    poly = b1 * root + b2 * rs + b3 * rs * root + b4 * rs * rs
+    return -2.0 * a * (1.0 + alpha1 * rs) * (1.0 / (2.0 * a * poly)).log1p()
+
+
+def pbe_unpolarized(density, gradient_magnitude) -> np.ndarray:
+    """(count, 7) PbeXcPoint rows (src/pbe_xc.cpp:74-140): energy density, energy per
+    particle, exchange and correlation energy densities, their d/dn potentials and the
+    |grad n|^2 coefficient with the cancellation-free sigma response."""
+    nv = np.asarray(density, dtype=np.float64).ravel()
+    gv = np.asarray(gradient_magnitude, dtype=np.float64).ravel()
+    if (not np.all(nv > 0.0)) or (not np.all(np.isfinite(nv))) or np.any(gv < 0.0) or not np.all(np.isfinite(gv)):
+        raise ValueError("PBE density must be positive and gradient finite")
+    zero = np.zeros_like(nv)
+    n = _Dual(nv, np.ones_like(nv), zero)
+    g2 = _Dual(gv * gv, zero, np.ones_like(nv))
+    pi = math.pi
+    root_n = n.pow(1.0 / 3.0)
+    rs = np.cbrt(3.0 / (4.0 * pi)) / root_n
+    kf = np.cbrt(3.0 * pi * pi) * root_n
+    eps_x = (-0.75 * np.cbrt(3.0 / pi)) * root_n
+    s2 = g2 / (4.0 * kf * kf * n * n)
+    fx = (1.0 + _PBE_KAPPA) - _PBE_KAPPA / (1.0 + (_PBE_MU / _PBE_KAPPA) * s2)
+    exchange = n * eps_x * fx
+    eps_c = _pw92(rs)
+    ks2 = 4.0 * kf / pi
+    t2 = g2 / (4.0 * ks2 * n * n)
+    em1 = (-eps_c / _PBE_GAMMA).expm1()
+    a = (_PBE_BETA / _PBE_GAMMA) / em1
+    at2 = a * t2
+    t4a2 = at2 * at2
+    h = _PBE_GAMMA * ((_PBE_BETA / _PBE_GAMMA) * t2 * (1.0 + at2) / (1.0 + at2 + t4a2)).log1p()
+    correlation = n * (eps_c + h)
+    u = (_PBE_MU / _PBE_KAPPA) * s2.v
+    x = at2.v
+    den = 1.0 + x + x * x
+    bt = (_PBE_BETA / _PBE_GAMMA) * t2.v * (1.0 + x)
+    with np.errstate(all="ignore"):
+        far = (1.0 + 2.0 * x) / (den * (den + bt)) - 1.0 / ((1.0 + u) * (1.0 + u))
+        near = u * (2.0 + u) / ((1.0 + u) * (1.0 + u)) - (x * x * (3.0 + x * (2.0 + x)) + bt * den) / (den * (den + bt))
+    difference = np.where((u > 0.25) | (x > 0.25), far, near)
+    total = exchange.v + correlation.v
+    return np.stack([total, total / nv, exchange.v, correlation.v, exchange.dn, correlation.dn,
+                     _PBE_BETA / (2.0 * ks2.v * nv) * difference], axis=1)

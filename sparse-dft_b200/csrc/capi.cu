@@ -310,6 +310,27 @@ sdft_b200_status sdft_b200_paw_pair(sdft_b200_context* context, uint64_t identit
   });
 }
 
+sdft_b200_status sdft_b200_pbe_points(sdft_b200_context* context, const double* density, const double* gradient,
+                                      size_t count, double* out, int memory) {
+  return guarded([&] {
+    require(context && density && gradient && out && count, "invalid GPU PBE dimensions");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      sdft_b200::pbe_points(ctx, density, gradient, count, out);
+      return;
+    }
+    require(memory == SDFT_B200_MEMORY_HOST, "memory must be host or device");
+    auto* din = static_cast<double*>(ctx.staging_in.reserve(sizeof(double) * 2 * count));
+    auto* dout = static_cast<double*>(ctx.staging_out.reserve(sizeof(double) * 7 * count));
+    SDFT_CUDA(cudaMemcpyAsync(din, density, sizeof(double) * count, cudaMemcpyHostToDevice, ctx.stream));
+    SDFT_CUDA(cudaMemcpyAsync(din + count, gradient, sizeof(double) * count, cudaMemcpyHostToDevice, ctx.stream));
+    sdft_b200::pbe_points(ctx, din, din + count, count, dout);
+    SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * 7 * count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
 sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int bop, size_t m, size_t n, size_t k,
                                         const double* a, size_t lda, const double* b, size_t ldb, double* c,
                                         size_t ldc, int precision, int add, int memory) {

@@ -61,6 +61,9 @@ void accelerator_paw_pair(Context& ctx, std::uint64_t identity, std::size_t npw,
                           std::size_t columns, const double* b, const double* d, const double* q, const double* input,
                           double* h, double* s, Precision precision, std::uint64_t projector_identity);
 
+// PBE per point on device arrays (pbe.cu): out holds 7 values per point.
+void pbe_points(Context& ctx, const double* density, const double* gradient, std::size_t count, double* out);
+
 struct GVectorList {
   std::vector<int> hkl;         // 3 per vector
   std::vector<double> cartesian;

@@ -75,6 +75,12 @@ class B200Accelerator final : public Accelerator {
                                       reinterpret_cast<double*>(output), precision_, operator_identity));
   }
 
+  void pbe_points(const double* density, const double* gradient, std::size_t count, PbeXcPoint* output) override {
+    static_assert(sizeof(PbeXcPoint) == 7 * sizeof(double), "PbeXcPoint is seven doubles");
+    check(sdft_b200_pbe_points(context_, density, gradient, count, reinterpret_cast<double*>(output),
+                               SDFT_B200_MEMORY_HOST));
+  }
+
   bool paw_pair(std::uint64_t identity, std::size_t npw, std::size_t projectors, std::size_t columns,
                 const Complex64* b, const Complex64* d, const Complex64* q, const Complex64* input, Complex64* h,
                 Complex64* s, std::uint64_t projector_identity) override {

@@ -92,6 +92,22 @@ def operator_fixture(lib, inputs, name, columns=4, seed=11, solve=True):
     print(name, "npw", inputs.npw, "grid", snap["shape"], {k: v for k, v in fields.items() if k in ("iterations",)})
 
 
+def pbe_sampling(count: int = 131072):
+    """The density/gradient sweep of the reference's tests/native/pbe_backend_smoke.cpp:15-16."""
+    i = np.arange(count, dtype=np.float64)
+    n = np.exp(-23.025850929940457 + 27.630 * np.mod(i, 10007) / 10006.0)
+    g = np.where(np.mod(i, 7) == 0, 10.0 ** (-9.0 + 11.0 * np.mod(i, 31) / 30.0), n * np.mod(i, 101) / 3.0)
+    return n, g
+
+
+def pbe_fixture(lib, stride: int = 16):
+    """Reference PBE points (src/pbe_xc.cpp:119) on every stride-th point of the sweep."""
+    n, g = pbe_sampling()
+    n, g = n[::stride].copy(), g[::stride].copy()
+    np.savez_compressed(HERE / "pbe.npz", density=n, gradient=g, points=lib.pbe(n, g))
+    print("pbe", n.size, "points")
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
@@ -99,6 +115,7 @@ def main():
     lib = ref_oracle.ReferenceLibrary()
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
+    pbe_fixture(lib)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

@@ -87,3 +87,19 @@ def test_kpoint_enumeration_bit_exact(reference):
         hkl, cart, kin = synthetic.enumerate_g_vectors(x.reciprocal, 4.0 * synthetic.HARTREE_TO_EV, k)
         rh, rc, rk = reference.enumerate_g_vectors(x.reciprocal, 4.0 * synthetic.HARTREE_TO_EV, k)
         assert np.array_equal(hkl, rh) and np.array_equal(kin, rk) and np.array_equal(cart, rc)
+
+
+def test_pbe_restatement_matches_golden(golden):
+    g = golden("pbe")
+    points = sdft_oracle.pbe_unpolarized(g["density"], g["gradient"])
+    scaled = np.abs(points - g["points"]) / np.maximum(1.0, np.abs(g["points"]))
+    assert scaled.max() < 1e-14
+
+
+def test_pbe_restatement_matches_live_reference(reference):
+    rng = np.random.Generator(np.random.PCG64(5))
+    n = 10.0 ** rng.uniform(-10, 1.5, 4096)
+    g = n * rng.uniform(0, 40, 4096)
+    ref = reference.pbe(n, g)
+    scaled = np.abs(sdft_oracle.pbe_unpolarized(n, g) - ref) / np.maximum(1.0, np.abs(ref))
+    assert scaled.max() < 1e-14

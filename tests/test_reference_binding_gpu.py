@@ -47,3 +47,10 @@ def test_reference_plane_wave_operator_smoke_runs_on_b200(tmp_path):
                "SDFT_GPU_PAW_CHAIN": "1", "SDFT_GPU_MIN_WORK": "0"}, tmp_path)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "plane_wave_operator PASS" in out.stdout
+
+
+def test_reference_pbe_backend_smoke_runs_on_b200(tmp_path):
+    out = run("pbe_backend_smoke", [], {"SDFT_COMPUTE_BACKEND": "cuda", "SDFT_GPU_PBE": "1"}, tmp_path)
+    report = json.loads(out.stdout.strip().splitlines()[-1])
+    assert report["accelerated"], report
+    assert out.returncode == 0 and report["passed"], out.stdout + out.stderr
