@@ -145,6 +145,23 @@ SDFT_B200_API sdft_b200_status sdft_b200_paw_pair(sdft_b200_context* context, ui
 SDFT_B200_API sdft_b200_status sdft_b200_pbe_points(sdft_b200_context* context, const double* density,
                                                     const double* gradient, size_t count, double* out, int memory);
 
+/* Band density on a Fourier support, FP64:
+ * out[j] = (1/N) FFT_fwd( sum_b occupations[b]/volume |FFT_bwd(scatter psi_b)|^2 )[support_j]
+ * psi: `bands` x npw complex (interleaved re, im), band-major (band b at
+ * psi + 2*b*npw); hkl: npw keys (h,k,l) of the plane waves; support: `count`
+ * keys; out: `count` complex values in support order. The density grid is the
+ * reference's alias-free rule max(3, 2m+1) per axis, rounded up to a
+ * 2/3/5/7-smooth length (its SDFT_FAST_DENSITY_GRID=1 option). hkl, support
+ * and occupations are host arrays; psi and out follow `memory`.
+ * Occupations outside [0,2] or nonfinite, nonfinite coefficients of occupied
+ * bands, empty inputs and duplicate plane-wave keys give INVALID_ARGUMENT.
+ * Replaces: plane_wave_density_fft, src/density_functionals.hpp:15-19
+ * (src/density_functionals.cpp:407-460). */
+SDFT_B200_API sdft_b200_status sdft_b200_band_density(sdft_b200_context* context, const int32_t* hkl, size_t npw,
+                                                      const double* psi, const double* occupations, size_t bands,
+                                                      double volume, const int32_t* support, size_t count,
+                                                      double* out, int memory);
+
 enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
 
 /* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with

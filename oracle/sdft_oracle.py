@@ -283,3 +283,44 @@ def pbe_unpolarized(density, gradient_magnitude) -> np.ndarray:
     total = exchange.v + correlation.v
     return np.stack([total, total / nv, exchange.v, correlation.v, exchange.dn, correlation.dn,
                      _PBE_BETA / (2.0 * ks2.v * nv) * difference], axis=1)
+
+
+# --- Band density (src/density_functionals.cpp:407-460) -----------------------
+
+def density_grid_shape(hkl, support, fast: bool = False):
+    """Alias-free density grid max(3, 2m+1) per axis, m = max(max|support|, max_g - min_g)
+    with min/max seeded at 0 (src/density_functionals.cpp:415-428); `fast` rounds each axis
+    up to a 2/3/5/7-smooth length (SDFT_FAST_DENSITY_GRID=1, :355-365)."""
+    hkl = np.asarray(hkl).reshape(-1, 3)
+    support = np.asarray(support).reshape(-1, 3)
+    m = np.abs(support).max(axis=0)
+    span = np.maximum(hkl.max(axis=0), 0) - np.minimum(hkl.min(axis=0), 0)
+    n = [max(3, 2 * int(max(a, b)) + 1) for a, b in zip(m, span)]
+    return tuple(fast_fft_length(v) for v in n) if fast else tuple(n)
+
+
+def plane_wave_density(hkl, coefficients, occupations, volume, support, fast: bool = False) -> np.ndarray:
+    """n(G) at the support keys: (1/N) FFT_fwd(sum_b f_b/volume |FFT_bwd(scatter psi_b)|^2)
+    (src/density_functionals.cpp:407-460 with :71-77 and :269-284). coefficients: (bands, npw)."""
+    hkl = np.asarray(hkl).reshape(-1, 3)
+    support = np.asarray(support).reshape(-1, 3)
+    coefficients = np.asarray(coefficients, dtype=np.complex128).reshape(len(occupations), hkl.shape[0])
+    if hkl.size == 0 or support.size == 0 or not np.isfinite(volume) or volume <= 0:
+        raise ValueError("invalid plane-wave FFT density dimensions")
+    shape = density_grid_shape(hkl, support, fast)
+    flat = index_map(hkl, shape)
+    count = int(np.prod(shape))
+    density = np.zeros(count)
+    for band, f in enumerate(occupations):
+        if not np.isfinite(f) or f < 0 or f > 2:
+            raise ValueError("invalid FFT spin-summed occupation")
+        if f == 0:
+            continue
+        if not np.all(np.isfinite(coefficients[band].view(np.float64))):
+            raise ValueError("nonfinite wavefunction coefficient")
+        grid = np.zeros(count, dtype=np.complex128)
+        grid[flat] = coefficients[band]
+        field = backward_fft(grid.reshape(shape)).ravel()
+        density += f / volume * (field.real * field.real + field.imag * field.imag)
+    transformed = forward_fft(density.reshape(shape).astype(np.complex128)).ravel()
+    return transformed[index_map(support, shape)] / count

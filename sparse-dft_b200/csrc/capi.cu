@@ -7,6 +7,7 @@
 
 #include "../../include/sdft_b200.h"
 #include "davidson.cuh"
+#include "band_density.cuh"
 #include "operator.cuh"
 
 struct sdft_b200_context {
@@ -327,6 +328,30 @@ sdft_b200_status sdft_b200_pbe_points(sdft_b200_context* context, const double* 
     SDFT_CUDA(cudaMemcpyAsync(din + count, gradient, sizeof(double) * count, cudaMemcpyHostToDevice, ctx.stream));
     sdft_b200::pbe_points(ctx, din, din + count, count, dout);
     SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * 7 * count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
+sdft_b200_status sdft_b200_band_density(sdft_b200_context* context, const int32_t* hkl, size_t npw,
+                                        const double* psi, const double* occupations, size_t bands, double volume,
+                                        const int32_t* support, size_t count, double* out, int memory) {
+  return guarded([&] {
+    require(context && hkl && psi && occupations && support && out && npw && bands && count,
+            "invalid plane-wave FFT density dimensions");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    using C = sdft_b200::Cx<double>;
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      sdft_b200::band_density(ctx, hkl, npw, reinterpret_cast<const C*>(psi), occupations, bands, volume, support,
+                              count, reinterpret_cast<C*>(out));
+      return;
+    }
+    require(memory == SDFT_B200_MEMORY_HOST, "memory must be host or device");
+    auto* din = static_cast<C*>(ctx.staging_in.reserve(sizeof(C) * npw * bands));
+    auto* dout = static_cast<C*>(ctx.staging_out.reserve(sizeof(C) * count));
+    SDFT_CUDA(cudaMemcpyAsync(din, psi, sizeof(C) * npw * bands, cudaMemcpyHostToDevice, ctx.stream));
+    sdft_b200::band_density(ctx, hkl, npw, din, occupations, bands, volume, support, count, dout);
+    SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * count, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.synchronize();
   });
 }

@@ -253,20 +253,18 @@ void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long lo
   SDFT_LAUNCH("plane_out_kernel");
 }
 
-template <typename T, bool INV>
-void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
+template <typename T, bool INV, int TL>
+void fft3d_tiles(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
   const long long n12 = static_cast<long long>(n[1]) * n[2];
   const long long count = n12 * n[0];
-  constexpr int TL = 32;
   // axis 2: contiguous rows
   {
     const LinePlan p = make_line_plan(n[2]);
     const int np = n[2] | 1;
-    constexpr int TR = TL;
-    const std::size_t smem = sizeof(Cx<T>) * (n[2] + 2 * static_cast<std::size_t>(TR) * np);
-    allow_smem(fft_rows_kernel<T, INV, TR>, smem);
+    const std::size_t smem = sizeof(Cx<T>) * (n[2] + 2 * static_cast<std::size_t>(TL) * np);
+    allow_smem(fft_rows_kernel<T, INV, TL>, smem);
     const long long rows = count / n[2] * batch;
-    fft_rows_kernel<T, INV, TR><<<static_cast<unsigned>(ceil_div(rows, TR)), kThreads, smem, stream>>>(
+    fft_rows_kernel<T, INV, TL><<<static_cast<unsigned>(ceil_div(rows, TL)), kThreads, smem, stream>>>(
         grid, n[2], np, rows, p, device_twiddles<T>(n[2]));
     SDFT_LAUNCH("fft_rows_kernel");
   }
@@ -290,6 +288,16 @@ void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
                                                                             device_twiddles<T>(n[0]));
     SDFT_LAUNCH("fft_strided_kernel axis0");
   }
+}
+
+// Tile width: 32 lines when the widest axis fits in shared memory, else 16 or 8.
+template <typename T, bool INV>
+void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
+  const std::size_t nmax = std::max({n[0], n[1], n[2]});
+  auto fits = [&](std::size_t tl) { return sizeof(Cx<T>) * (nmax + 2 * nmax * (tl + 1)) <= 227 * 1024; };
+  if (fits(32)) fft3d_tiles<T, INV, 32>(grid, n, batch, stream);
+  else if (fits(16)) fft3d_tiles<T, INV, 16>(grid, n, batch, stream);
+  else fft3d_tiles<T, INV, 8>(grid, n, batch, stream);
 }
 
 }  // namespace
@@ -324,7 +332,8 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
   for (auto idx : indices) ++h_offset[slot_of_row[idx / n12] + 1];
   for (int s = 0; s < slots; ++s) h_offset[s + 1] += h_offset[s];
   std::vector<int> fill(h_offset.begin(), h_offset.end() - 1);
-  std::vector<int> h_g(npw), h_smem(npw);
+  std::vector<int> h_g(npw), h_smem(npw), h_compact(npw), kpos(n[1], -1);
+  for (int k = 0; k < krows; ++k) kpos[h_krow[k]] = k;
   for (int g = 0; g < npw; ++g) {
     const auto idx = indices[g];
     const int s = slot_of_row[idx / n12];
@@ -333,6 +342,7 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
     const int p = fill[s]++;
     h_g[p] = g;
     h_smem[p] = i1 * n2p + i2;
+    h_compact[p] = kpos[i1] * n[2] + i2;
   }
   auto upload = [](int*& dst, const std::vector<int>& src) {
     SDFT_CUDA(cudaMalloc(&dst, sizeof(int) * std::max<std::size_t>(1, src.size())));
@@ -342,11 +352,12 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
   upload(point_offset, h_offset);
   upload(point_g, h_g);
   upload(point_smem, h_smem);
+  upload(point_compact, h_compact);
   upload(krow, h_krow);
 }
 
 void SpherePlan::release() {
-  for (int** p : {&slot_row, &point_offset, &point_g, &point_smem, &krow}) {
+  for (int** p : {&slot_row, &point_offset, &point_g, &point_smem, &point_compact, &krow}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }

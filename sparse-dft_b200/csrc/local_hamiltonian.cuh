@@ -22,6 +22,7 @@ struct SpherePlan {
   int* point_offset = nullptr;  // [slots+1]
   int* point_g = nullptr;       // [npw] plane-wave index, grouped by slot
   int* point_smem = nullptr;    // [npw] i1*n2p + i2
+  int* point_compact = nullptr; // [npw] k*n2 + i2, k = position of i1 in krow
   int* krow = nullptr;          // [krows]
   LinePlan line[3];
 

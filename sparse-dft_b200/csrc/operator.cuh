@@ -34,6 +34,16 @@ struct AcceleratorCache {
   }
 };
 
+// Density-side device state: the sphere plan of the last band-density call
+// (reused while the density grid and the plane-wave keys repeat) and its slabs.
+struct DensityCache {
+  int shape[3] = {0, 0, 0};
+  std::vector<std::uint64_t> indices;
+  SpherePlan plan;
+  Scratch rows, planes, grid, meta;
+  ~DensityCache() { plan.release(); }
+};
+
 // One CUDA stream with its library handles and grow-only scratch. A context is
 // used by one host thread at a time (the reference keeps one Accelerator per
 // host thread, src/compute_backend.cpp:62-73).
@@ -46,6 +56,7 @@ struct Context {
   Scratch slab32, slab64, staging_in, staging_out, staging_aux, projections, onsite;
   TensorCoreWorkspace tc;
   AcceleratorCache accel;
+  DensityCache density;
   explicit Context(int device, cudaStream_t stream);
   ~Context();
   Context(const Context&) = delete;

@@ -26,7 +26,6 @@ struct Dual {
   double v, dn, dg;  // value, d/dn, d/d(|grad n|^2)
 };
 __device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.dn + b.dn, a.dg + b.dg}; }
-__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.dn - b.dn, a.dg - b.dg}; }
 __device__ __forceinline__ Dual operator-(Dual a) { return {-a.v, -a.dn, -a.dg}; }
 __device__ __forceinline__ Dual operator*(Dual a, Dual b) {
   return {a.v * b.v, a.dn * b.v + a.v * b.dn, a.dg * b.v + a.v * b.dg};
@@ -35,7 +34,6 @@ __device__ __forceinline__ Dual operator/(Dual a, Dual b) {
   const double inv = 1.0 / b.v, inv2 = inv * inv;
   return {a.v * inv, (a.dn * b.v - a.v * b.dn) * inv2, (a.dg * b.v - a.v * b.dg) * inv2};
 }
-__device__ __forceinline__ Dual operator+(Dual a, double b) { return {a.v + b, a.dn, a.dg}; }
 __device__ __forceinline__ Dual operator+(double a, Dual b) { return {a + b.v, b.dn, b.dg}; }
 __device__ __forceinline__ Dual operator-(double a, Dual b) { return {a - b.v, -b.dn, -b.dg}; }
 __device__ __forceinline__ Dual operator*(Dual a, double b) { return {a.v * b, a.dn * b, a.dg * b}; }

@@ -308,3 +308,18 @@ def gaas_kpoint(index: int, seed: int = 2026, **kw) -> OperatorInputs:
 def tiny(seed: int = 7, ecut_ha: float = 4.0, roots: int = 6, a: float = 7.0, **kw) -> OperatorInputs:
     """A small diamond cell for fast parity tests (a few hundred plane waves)."""
     return build_operator("tiny", a, 1, ecut_ha, roots, seed=seed, **kw)
+
+
+def density_support(inputs: OperatorInputs, factor: float) -> np.ndarray:
+    """Density Fourier support {1/2 |G|^2 <= factor * Ecut} of the cell, (m, 3) int32 keys."""
+    hkl, _, _ = enumerate_g_vectors(inputs.reciprocal, factor * inputs.ecut_ha * inputs.hartree_to_ev)
+    return np.ascontiguousarray(hkl, dtype=np.int32)
+
+
+def band_coefficients(inputs: OperatorInputs, bands: int, seed: int = 31) -> np.ndarray:
+    """Seeded normalised band-major plane-wave coefficients, (bands, npw) complex128,
+    with a kinetic decay so that the bands look like smooth valence states."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    decay = np.exp(-0.5 * inputs.kinetic_ev / inputs.hartree_to_ev)
+    c = (rng.standard_normal((bands, inputs.npw)) + 1j * rng.standard_normal((bands, inputs.npw))) * decay
+    return c / np.linalg.norm(c, axis=1, keepdims=True)

@@ -108,6 +108,25 @@ def pbe_fixture(lib, stride: int = 16):
     print("pbe", n.size, "points")
 
 
+def density_occupations(bands: int) -> np.ndarray:
+    """Mostly f = 2, one fractional and one empty band (the empty one is skipped)."""
+    occ = np.full(bands, 2.0)
+    occ[3] = 1.25
+    occ[bands // 2 - 1] = 0.0
+    return occ
+
+
+def density_fixture(lib, inputs, name, factor, bands):
+    """Reference plane_wave_density_fft (src/density_functionals.cpp:407) on seeded bands."""
+    support = synthetic.density_support(inputs, factor)
+    coefficients = synthetic.band_coefficients(inputs, bands)
+    occ = density_occupations(bands)
+    density = lib.density(inputs.hkl, coefficients, occ, inputs.volume, support)
+    np.savez_compressed(HERE / f"density_{name}.npz", support=support, occupations=occ, factor=np.array(factor),
+                        bands=np.array(bands), density=density)
+    print("density", name, "support", support.shape[0])
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
@@ -116,6 +135,8 @@ def main():
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
     pbe_fixture(lib)
+    density_fixture(lib, synthetic.tiny(), "tiny", 4.0, 6)
+    density_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

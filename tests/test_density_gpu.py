@@ -69,3 +69,115 @@ def test_pbe_rejects_empty(context):
     from sdft_b200 import _capi, density
     with pytest.raises(_capi.InvalidArgument, match="invalid GPU PBE dimensions"):
         density.pbe_points(context, np.zeros(0), np.zeros(0))
+
+
+# --- band density (src/density_functionals.cpp:407-460) ------------------------
+
+DENSITY_REL = 1e-12  # FP64 FFTs on a different (smooth) grid: rounding only
+
+
+def _occupations(bands):
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent / "golden"))
+    from make_golden import density_occupations
+    return density_occupations(bands)
+
+
+@pytest.mark.parametrize("name,factory", [("tiny", "tiny"), ("si8", "si8")])
+def test_band_density_matches_reference_fixture(context, golden, name, factory):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    g = golden(f"density_{name}")
+    x = getattr(synthetic, factory)()
+    coefficients = synthetic.band_coefficients(x, int(g["bands"]))
+    out = density.band_density(context, x.hkl, coefficients, g["occupations"], x.volume, g["support"])
+    assert relative_error(out, g["density"]) < DENSITY_REL
+
+
+@pytest.mark.parametrize("factor,bands", [(4.0, 32), (8.0, 8), (16.0, 4)])
+def test_band_density_si64_matches_oracle(context, factor, bands):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    x = synthetic.si64()
+    support = synthetic.density_support(x, factor)
+    coefficients = synthetic.band_coefficients(x, bands)
+    occ = _occupations(bands)
+    out = density.band_density(context, x.hkl, coefficients, occ, x.volume, support)
+    expected = sdft_oracle.plane_wave_density(x.hkl, coefficients, occ, x.volume, support, fast=True)
+    assert relative_error(out, expected) < DENSITY_REL
+
+
+def test_band_density_config_size_properties(context):
+    """128 bands at f = 16 (density grid 144^3): the G = 0 coefficient equals
+    sum_b f_b/Omega for normalised bands (Parseval), n(-G) = conj n(G), and the
+    device-memory path returns the host path's values."""
+    import torch
+    from sdft_b200 import density, synthetic
+    x = synthetic.si64()
+    support = synthetic.density_support(x, 16.0)
+    coefficients = synthetic.band_coefficients(x, 128)
+    occ = np.full(128, 2.0)
+    out = density.band_density(context, x.hkl, coefficients, occ, x.volume, support)
+    zero = int(np.flatnonzero(np.all(support == 0, axis=1))[0])
+    assert abs(out[zero] - occ.sum() / x.volume) < 1e-13 * occ.sum() / x.volume
+    position = {tuple(k): i for i, k in enumerate(support.tolist())}
+    mirror = np.array([position[(-h, -k, -l)] for h, k, l in support.tolist()])
+    assert np.max(np.abs(out[mirror] - np.conj(out))) < 1e-15 * np.max(np.abs(out)) * 1e3
+    device = density.band_density(context, x.hkl, torch.from_numpy(coefficients).cuda(), occ, x.volume, support)
+    assert np.array_equal(device.cpu().numpy(), out)
+
+
+def test_band_density_chunked_bands_match_single_pass(context, monkeypatch):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    x = synthetic.si8()
+    support = synthetic.density_support(x, 4.0)
+    coefficients = synthetic.band_coefficients(x, 16)
+    occ = _occupations(16)
+    whole = density.band_density(context, x.hkl, coefficients, occ, x.volume, support)
+    monkeypatch.setenv("SDFT_B200_DENSITY_SLAB_BYTES", str(3 * 1024 * 1024))  # a few bands per chunk
+    chunked = density.band_density(context, x.hkl, coefficients, occ, x.volume, support)
+    assert relative_error(chunked, whole) < 1e-14
+
+
+def test_band_density_is_linear_in_occupations(context):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    x = synthetic.tiny()
+    support = synthetic.density_support(x, 4.0)
+    c = synthetic.band_coefficients(x, 3)
+    parts = [density.band_density(context, x.hkl, c, np.eye(3)[b] * 2.0, x.volume, support) for b in range(3)]
+    occ = np.array([0.5, 2.0, 1.0])
+    both = density.band_density(context, x.hkl, c, occ, x.volume, support)
+    assert relative_error(both, sum(o / 2.0 * p for o, p in zip(occ, parts))) < 1e-13
+
+
+def test_band_density_edge_cases(context):
+    from sdft_b200 import _capi, density, synthetic
+    x = synthetic.tiny()
+    support = synthetic.density_support(x, 4.0)
+    c = synthetic.band_coefficients(x, 3)
+    # All bands empty: zero density, no transform of any band.
+    assert not np.any(density.band_density(context, x.hkl, c, np.zeros(3), x.volume, support))
+    # A nonfinite coefficient in an empty band is skipped, as in the reference.
+    bad = c.copy()
+    bad[1, 5] = np.nan
+    ok = density.band_density(context, x.hkl, bad, np.array([2.0, 0.0, 2.0]), x.volume, support)
+    assert np.all(np.isfinite(ok))
+    with pytest.raises(_capi.InvalidArgument, match="nonfinite wavefunction coefficient"):
+        density.band_density(context, x.hkl, bad, np.array([2.0, 1.0, 2.0]), x.volume, support)
+    for occ in ([2.0, 2.5, 0.0], [2.0, -0.1, 0.0], [np.nan, 1.0, 1.0]):
+        with pytest.raises(_capi.InvalidArgument, match="invalid FFT spin-summed occupation"):
+            density.band_density(context, x.hkl, c, np.array(occ), x.volume, support)
+    for volume in (0.0, -1.0, np.inf):
+        with pytest.raises(_capi.InvalidArgument, match="invalid plane-wave FFT density dimensions"):
+            density.band_density(context, x.hkl, c, np.ones(3), volume, support)
+    with pytest.raises(_capi.InvalidArgument):
+        density.band_density(context, x.hkl, c, np.ones(3), x.volume, np.zeros((0, 3), dtype=np.int32))
+    dup = x.hkl.copy()
+    dup[1] = dup[0]
+    with pytest.raises(_capi.InvalidArgument, match="duplicate plane-wave key"):
+        density.band_density(context, dup, c, np.ones(3), x.volume, support)
+    # The context stays usable after every rejected call.
+    again = density.band_density(context, x.hkl, c, np.ones(3), x.volume, support)
+    assert np.all(np.isfinite(again))

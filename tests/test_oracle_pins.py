@@ -103,3 +103,23 @@ def test_pbe_restatement_matches_live_reference(reference):
     ref = reference.pbe(n, g)
     scaled = np.abs(sdft_oracle.pbe_unpolarized(n, g) - ref) / np.maximum(1.0, np.abs(ref))
     assert scaled.max() < 1e-14
+
+
+@pytest.mark.parametrize("name,factory", [("tiny", synthetic.tiny), ("si8", synthetic.si8)])
+def test_band_density_restatement_matches_golden(golden, name, factory):
+    g = golden(f"density_{name}")
+    x = factory()
+    coefficients = synthetic.band_coefficients(x, int(g["bands"]))
+    for fast in (False, True):
+        out = sdft_oracle.plane_wave_density(x.hkl, coefficients, g["occupations"], x.volume, g["support"], fast)
+        assert relative_error(out, g["density"]) < 1e-13
+
+
+def test_band_density_grid_rule_matches_reference_cases():
+    x = synthetic.si8()
+    # Span 16 of the Si8 basis dominates a small support: 2*16+1 = 33, rounded to 35.
+    assert sdft_oracle.density_grid_shape(x.hkl, synthetic.density_support(x, 2.0)) == (33, 33, 33)
+    assert sdft_oracle.density_grid_shape(x.hkl, synthetic.density_support(x, 2.0), fast=True) == (35, 35, 35)
+    # min/max are seeded at 0: a basis on one side of the origin still counts from 0.
+    hkl = np.array([[2, 3, 4], [5, 3, 4]])
+    assert sdft_oracle.density_grid_shape(hkl, np.array([[0, 0, 0]])) == (11, 7, 9)
