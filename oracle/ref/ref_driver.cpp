@@ -11,6 +11,9 @@
 //   save/load_solver_snapshot           src/plane_wave_operator.cpp:542-653
 //   plane_wave_density_fft              src/density_functionals.cpp:407-460
 //   pbe_unpolarized                     src/pbe_xc.cpp:116-140
+//   onsite_density_from_amplitudes      src/onsite_density.hpp:10-36
+//   paw_lm_moments_from_density         src/paw_augmentation.cpp:490-525
+//   PawCompensationOperator ctor/density_sum src/paw_compensation.cpp:185-342,465-524
 // Complex arrays are interleaved (re, im) doubles, column-major blocks.
 #include "plane_wave_operator.hpp"
 #include "pw_core.hpp"
@@ -18,6 +21,9 @@
 #include "density_functionals.hpp"
 #include "pbe_xc.hpp"
 #include "env_cache.hpp"
+#include "onsite_density.hpp"
+#include "paw_augmentation.hpp"
+#include "paw_compensation.hpp"
 
 #include <algorithm>
 #include <complex>
@@ -256,4 +262,102 @@ void ref_pbe_unpolarized(long count, const double* density, const double* gradie
 }
 
 void ref_refresh_environment() { sdft::refresh_environment_cache(); }
+
+// rho_ij (row-major rows x rows) of one atom from amplitudes (rows x bands, column stride `stride`).
+int ref_onsite_density(long rows, long bands, const double* amplitudes, long stride, const double* occupations,
+                       double* out, char* error, long error_length) {
+  try {
+    const auto rho = sdft::onsite_density_from_amplitudes(
+        static_cast<std::size_t>(rows), static_cast<std::size_t>(bands), reinterpret_cast<const C*>(amplitudes),
+        static_cast<std::size_t>(stride), occupations);
+    std::memcpy(out, rho.data(), sizeof(C) * rho.size());
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+}
+
+namespace {
+sdft::PawAugmentationData augmentation(long channels, const int* channel_l, int max_l, long radial,
+                                       const double* radial_grid, const double* aug_moment,
+                                       const double* compensation_r2) {
+  sdft::PawAugmentationData a;
+  a.channel_l.assign(channel_l, channel_l + channels);
+  a.max_l = max_l;
+  a.radial_grid.assign(radial_grid, radial_grid + radial);
+  a.rmax = a.radial_grid.back();
+  a.rdep = a.radial_grid.back();
+  a.aug_moment.assign(aug_moment, aug_moment + channels * channels * (max_l + 1));
+  a.overlap_correction.assign(static_cast<std::size_t>(channels * channels), 0.0);
+  for (long i = 0; i < channels; ++i)
+    for (long j = 0; j < channels; ++j)
+      if (channel_l[i] == channel_l[j]) a.overlap_correction[i * channels + j] = a.moment(i, j, 0);
+  for (int l = 0; l <= max_l; ++l)
+    a.compensation_r2.emplace_back(compensation_r2 + l * radial, compensation_r2 + (l + 1) * radial);
+  a.compensation_q.assign(max_l + 1, {0.0, 0.0});
+  a.compensation_amplitudes.assign(max_l + 1, {0.0, 0.0});
+  return a;
+}
+}  // namespace
+
+extern "C" {
+
+// (L,M) moments transform [lm][i*dim+j]: paw_lm_moments_from_density of each unit matrix.
+int ref_lm_transform(long channels, const int* channel_l, int max_l, long radial, const double* radial_grid,
+                     const double* aug_moment, const double* compensation_r2, double* out, char* error,
+                     long error_length) {
+  try {
+    const auto a = augmentation(channels, channel_l, max_l, radial, radial_grid, aug_moment, compensation_r2);
+    std::size_t dim = 0;
+    for (int l : a.channel_l) dim += 2 * l + 1;
+    const std::size_t entries = dim * dim, lms = (max_l + 1) * (max_l + 1);
+    std::vector<C> unit(entries);
+    auto* o = reinterpret_cast<C*>(out);
+    for (std::size_t e = 0; e < entries; ++e) {
+      unit[e] = 1.0;
+      const auto m = sdft::paw_lm_moments_from_density(a, unit, dim);
+      unit[e] = 0.0;
+      for (std::size_t lm = 0; lm < lms; ++lm) o[lm * entries + e] = m[lm];
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+// Compensation charge on `count` reciprocal keys for `atoms` atoms sharing one
+// geometry; onsite: atoms x dim^2 complex row-major; out: count complex.
+int ref_compensation_density(const double* lattice, long atoms, const double* fractional, long count,
+                             const int* keys, long channels, const int* channel_l, int max_l, long radial,
+                             const double* radial_grid, const double* aug_moment, const double* compensation_r2,
+                             const double* onsite, double* out, char* error, long error_length) {
+  try {
+    const auto a = augmentation(channels, channel_l, max_l, radial, radial_grid, aug_moment, compensation_r2);
+    std::array<sdft::Vec3, 3> cell{};
+    for (int r = 0; r < 3; ++r) cell[r] = {lattice[3 * r], lattice[3 * r + 1], lattice[3 * r + 2]};
+    std::vector<std::tuple<int, int, int>> support(static_cast<std::size_t>(count));
+    for (long i = 0; i < count; ++i) support[i] = {keys[3 * i], keys[3 * i + 1], keys[3 * i + 2]};
+    std::size_t dim = 0;
+    for (int l : a.channel_l) dim += 2 * l + 1;
+    std::vector<sdft::PawCompensationOperator> ops;
+    ops.reserve(static_cast<std::size_t>(atoms));
+    std::vector<std::vector<C>> rho(static_cast<std::size_t>(atoms));
+    for (long i = 0; i < atoms; ++i) {
+      const sdft::Vec3 f{fractional[3 * i], fractional[3 * i + 1], fractional[3 * i + 2]};
+      ops.emplace_back(a, cell, f, support, sdft::AtomicUnitConvention::Codata, i ? &ops.front() : nullptr);
+      const auto* p = reinterpret_cast<const C*>(onsite) + i * dim * dim;
+      rho[i].assign(p, p + dim * dim);
+    }
+    const auto charge = sdft::PawCompensationOperator::density_sum(ops, rho);
+    auto* o = reinterpret_cast<C*>(out);
+    for (long i = 0; i < count; ++i) o[i] = charge.at(support[i]);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
 }

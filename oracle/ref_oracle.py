@@ -73,6 +73,16 @@ class ReferenceLibrary:
         L.ref_pbe_unpolarized.restype = None
         L.ref_pbe_unpolarized.argtypes = [ctypes.c_long, _dbl, _dbl, _dbl]
         L.ref_refresh_environment.restype = None
+        L.ref_onsite_density.restype = ctypes.c_int
+        L.ref_onsite_density.argtypes = [ctypes.c_long, ctypes.c_long, _dbl, ctypes.c_long, _dbl, _dbl,
+                                         ctypes.c_char_p, ctypes.c_long]
+        L.ref_lm_transform.restype = ctypes.c_int
+        L.ref_lm_transform.argtypes = [ctypes.c_long, _int, ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, _dbl,
+                                       ctypes.c_char_p, ctypes.c_long]
+        L.ref_compensation_density.restype = ctypes.c_int
+        L.ref_compensation_density.argtypes = [_dbl, ctypes.c_long, _dbl, ctypes.c_long, _int, ctypes.c_long, _int,
+                                               ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, _dbl, _dbl,
+                                               ctypes.c_char_p, ctypes.c_long]
 
     # -- basis ---------------------------------------------------------------
     def enumerate_g_vectors(self, reciprocal, cutoff_ev, kpoint=(0.0, 0.0, 0.0), hartree_to_ev=27.211386245988):
@@ -97,6 +107,56 @@ class ReferenceLibrary:
         g = np.ascontiguousarray(gradient, dtype=np.float64)
         out = np.zeros((n.size, 7))
         self.lib.ref_pbe_unpolarized(n.size, _ptr(n), _ptr(g), _ptr(out))
+        return out
+
+    @staticmethod
+    def _check(rc, err):
+        if rc:
+            raise RuntimeError(err.value.decode())
+
+    def onsite_density(self, amplitudes, occupations):
+        """rho_ij of one atom from amplitudes (rows, bands) (src/onsite_density.hpp:13)."""
+        p = np.asfortranarray(amplitudes, dtype=np.complex128)
+        occ = np.ascontiguousarray(occupations, dtype=np.float64)
+        out = np.zeros((p.shape[0], p.shape[0]), dtype=np.complex128)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.ref_onsite_density(p.shape[0], p.shape[1], p.ravel(order="F").view(np.float64).ctypes.data_as(_dbl),
+                                         p.shape[0], _ptr(occ), out.view(np.float64).ctypes.data_as(_dbl), err, 512)
+        self._check(rc, err)
+        return out
+
+    @staticmethod
+    def _augmentation(aug):
+        return (np.ascontiguousarray(aug["channel_l"], dtype=np.int32), int(aug["max_l"]),
+                np.ascontiguousarray(aug["radial_grid"], dtype=np.float64),
+                np.ascontiguousarray(aug["aug_moment"], dtype=np.float64),
+                np.ascontiguousarray(aug["compensation_r2"], dtype=np.float64))
+
+    def lm_transform(self, aug):
+        """[lm, i*dim+j] moments of unit occupations (src/paw_augmentation.cpp:490; src/paw_compensation.cpp:228-236)."""
+        ch, max_l, r, mom, r2 = self._augmentation(aug)
+        dim = int(np.sum(2 * ch + 1))
+        out = np.zeros(((max_l + 1) ** 2, dim * dim), dtype=np.complex128)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.ref_lm_transform(ch.size, _ptr(ch, _int), max_l, r.size, _ptr(r), _ptr(mom), _ptr(r2),
+                                       out.view(np.float64).ctypes.data_as(_dbl), err, 512)
+        self._check(rc, err)
+        return out
+
+    def compensation_density(self, lattice, fractional, keys, aug, onsite):
+        """PawCompensationOperator::density_sum over atoms sharing one geometry (src/paw_compensation.cpp:465)."""
+        ch, max_l, r, mom, r2 = self._augmentation(aug)
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        frac = np.ascontiguousarray(fractional, dtype=np.float64).reshape(-1, 3)
+        k = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+        rho = np.ascontiguousarray(onsite, dtype=np.complex128)
+        out = np.zeros(k.shape[0], dtype=np.complex128)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.ref_compensation_density(_ptr(lat), frac.shape[0], _ptr(frac), k.shape[0], _ptr(k, _int),
+                                               ch.size, _ptr(ch, _int), max_l, r.size, _ptr(r), _ptr(mom), _ptr(r2),
+                                               rho.view(np.float64).ctypes.data_as(_dbl),
+                                               out.view(np.float64).ctypes.data_as(_dbl), err, 512)
+        self._check(rc, err)
         return out
 
     def density(self, hkl, coefficients, occupations, volume, support_hkl):

@@ -87,6 +87,20 @@ struct Staged {
     if (memory == SDFT_B200_MEMORY_DEVICE) return;
     SDFT_CUDA(cudaMemcpyAsync(host, dev, sizeof(Cx<double>) * complex_count, cudaMemcpyDeviceToHost, ctx.stream));
   }
+  // rows x cols block with leading dimension ld: only the block's own
+  // entries are copied, so entries rows..ld-1 of each host column stay untouched.
+  void matrix_in(Cx<double>* dev, const double* host, std::size_t rows, std::size_t cols, std::size_t ld) {
+    if (memory == SDFT_B200_MEMORY_DEVICE) return;
+    const std::size_t pitch = sizeof(Cx<double>) * ld;
+    SDFT_CUDA(cudaMemcpy2DAsync(dev, pitch, host, pitch, sizeof(Cx<double>) * rows, cols, cudaMemcpyHostToDevice,
+                                ctx.stream));
+  }
+  void matrix_back(double* host, const Cx<double>* dev, std::size_t rows, std::size_t cols, std::size_t ld) {
+    if (memory == SDFT_B200_MEMORY_DEVICE) return;
+    const std::size_t pitch = sizeof(Cx<double>) * ld;
+    SDFT_CUDA(cudaMemcpy2DAsync(host, pitch, dev, pitch, sizeof(Cx<double>) * rows, cols, cudaMemcpyDeviceToHost,
+                                ctx.stream));
+  }
   void finish() {
     if (memory == SDFT_B200_MEMORY_HOST) ctx.synchronize();
   }
@@ -378,8 +392,7 @@ sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int
     const auto* db = stage.in(b, ldb * (bc - 1) + br, ctx.staging_aux);
     const std::size_t csize = ldc * (n - 1) + m;
     Cx<double>* dc = stage.out(c, csize, ctx.staging_out);
-    if (memory == SDFT_B200_MEMORY_HOST && add)
-      SDFT_CUDA(cudaMemcpyAsync(dc, c, sizeof(Cx<double>) * csize, cudaMemcpyHostToDevice, ctx.stream));
+    if (add) stage.matrix_in(dc, c, m, n, ldc);
     const sdft_b200::Op ao = aop == SDFT_B200_OP_NORMAL ? sdft_b200::Op::N : sdft_b200::Op::C;
     const sdft_b200::Op bo = bop == SDFT_B200_OP_NORMAL ? sdft_b200::Op::N : sdft_b200::Op::C;
     if (p == Precision::FP64)
@@ -390,7 +403,7 @@ sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int
       sdft_b200::gemm_tc(ao, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), da,
                          static_cast<long long>(lda), nullptr, db, static_cast<long long>(ldb), dc,
                          static_cast<long long>(ldc), add != 0, 1.0, sdft_b200::search_split(), ctx.tc, ctx.stream);
-    stage.back(c, dc, csize);
+    stage.matrix_back(c, dc, m, n, ldc);
     ctx.synchronize();
     if (sdft_b200::umma_error_flag_read_and_clear()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
   });

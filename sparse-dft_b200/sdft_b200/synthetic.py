@@ -323,3 +323,35 @@ def band_coefficients(inputs: OperatorInputs, bands: int, seed: int = 31) -> np.
     decay = np.exp(-0.5 * inputs.kinetic_ev / inputs.hartree_to_ev)
     c = (rng.standard_normal((bands, inputs.npw)) + 1j * rng.standard_normal((bands, inputs.npw))) * decay
     return c / np.linalg.norm(c, axis=1, keepdims=True)
+
+
+def augmentation(channel_l=(0, 0, 1, 1), max_l: int = 2, radial: int = 401, r0: float = 1e-4, rmax: float = 1.6,
+                 width: float = 0.45, seed: int = 41) -> dict:
+    """Synthetic one-centre augmentation data in the reference's PawAugmentationData
+    layout (radial arrays in Angstrom): a logarithmic radial mesh, Gaussian compensation
+    shapes g_L(r) r^2 ~ r^L exp(-r^2/width^2) r^2 with unit continuous L-moment, and
+    seeded aug_moment(i, j, L) symmetric in (i, j) on the Gaunt-allowed L."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    channel_l = np.asarray(channel_l, dtype=np.int32)
+    n = channel_l.size
+    step = math.log(rmax / r0) / (radial - 1)
+    r = r0 * np.exp(step * np.arange(radial))
+    r2 = np.zeros((max_l + 1, radial))
+    for L in range(max_l + 1):
+        norm = 0.5 * math.gamma(L + 1.5) * width ** (2 * L + 3)
+        r2[L] = r ** L * np.exp(-(r / width) ** 2) * r * r / norm
+    moment = np.zeros((n, n, max_l + 1))
+    for i in range(n):
+        for j in range(i, n):
+            lo, hi = abs(int(channel_l[i] - channel_l[j])), min(max_l, int(channel_l[i] + channel_l[j]))
+            for L in range(lo, hi + 1, 2):
+                moment[i, j, L] = moment[j, i, L] = rng.uniform(-0.5, 0.5)
+    return {"channel_l": channel_l, "max_l": max_l, "radial_grid": r, "aug_moment": moment.ravel(),
+            "compensation_r2": r2}
+
+
+def projected_amplitudes(atoms: int, dim: int, bands: int, seed: int = 43) -> np.ndarray:
+    """Seeded projector amplitudes P = B psi, (atoms*dim, bands) complex128 column-major."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p = rng.standard_normal((atoms * dim, bands)) + 1j * rng.standard_normal((atoms * dim, bands))
+    return np.asfortranarray(0.3 * p)

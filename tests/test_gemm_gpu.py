@@ -45,3 +45,25 @@ def test_mixed_gemm_is_deterministic(context):
     first = complex_gemm(context, a, b, precision="mixed")
     second = complex_gemm(context, a, b, precision="mixed")
     assert np.array_equal(first, second)
+
+
+@pytest.mark.parametrize("add", [0, 1])
+def test_host_gemm_on_submatrix_leaves_other_rows(context, add):
+    """C is a row block of a taller host matrix (ldc > m), as in the reference's
+    per-atom products into a shared projection array: only the block changes."""
+    import ctypes
+    from sdft_b200 import _capi as C
+    rng = np.random.Generator(np.random.PCG64(17))
+    m, n, k, ldc, offset = 8, 13, 8, 40, 16
+    a = np.asfortranarray(rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k)))
+    b = np.asfortranarray(rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n)))
+    full = np.asfortranarray(rng.standard_normal((ldc, n)) + 1j * rng.standard_normal((ldc, n)))
+    expected = full.copy(order="F")
+    expected[offset:offset + m] = a @ b + (expected[offset:offset + m] if add else 0)
+    base = full.ctypes.data + 16 * offset
+    C.check(C.library().sdft_b200_complex_gemm(context.handle, 0, 0, m, n, k, ctypes.c_void_p(a.ctypes.data), m,
+                                               ctypes.c_void_p(b.ctypes.data), k, ctypes.c_void_p(base), ldc, C.FP64,
+                                               add, C.HOST))
+    assert np.array_equal(full[:offset], expected[:offset])
+    assert np.array_equal(full[offset + m:], expected[offset + m:])
+    assert relative_error(full[offset:offset + m], expected[offset:offset + m]) < 1e-14
