@@ -317,11 +317,13 @@ def fused_local_roofline(op, inputs, stream):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     n0, n1, n2 = op.shape
-    slots = op.active_rows
-    # algorithmic bytes per column: FP64 psi in + T psi re-read + FP64 out, plus
-    # one FP32 slab write+read between plane and pencil passes, each direction.
-    per_column = 3 * 16 * op.npw + 2 * (2 * 8 * slots * n1 * n2)
-    algorithmic = per_column * cols + 4 * n0 * n1 * n2
+    grid = n0 * n1 * n2
+    # Algorithmic bytes per column: read psi and write H~psi (FP64 complex,
+    # 16 B) plus one full-grid FP32 write+read for each of the two transform
+    # halves; V(r) (FP32) once per launch. The pruned slab moves fewer grid
+    # bytes than this (active i0 rows only).
+    per_column = 2 * 16 * op.npw + 2 * (2 * 8 * grid)
+    algorithmic = per_column * cols + 4 * grid
     achieved = algorithmic / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "kernel": "fused local H~psi (plane_in + pencil + plane_out), FP32, 160 columns",
@@ -365,6 +367,44 @@ def cpu_baseline(inputs):
                       f"({seconds:.1f} s), extrapolated to its {full}-iteration solve of this pencil"}
 
 
+def run_case(args):
+    """A few launches of one kernel family on the bench workload, for profiling
+    captures (no timing, no JSON): local, pair, project, density, pbe."""
+    import numpy as np
+    import torch
+    from sdft_b200 import density, synthetic
+    from sdft_b200.operator import Context, PlaneWaveOperator
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = Context(0, stream.cuda_stream)
+    inputs = load_inputs()
+    cols = args.columns
+    if args.case in ("local", "pair", "project"):
+        op = PlaneWaveOperator(ctx, inputs)
+        x = torch.randn(cols, op.npw, dtype=torch.complex128, device="cuda").T
+        for _ in range(args.repeat):
+            if args.case == "local":
+                op.local_apply(x, precision=args.precision)
+            elif args.case == "pair":
+                op.apply_pair(x, precision=args.precision)
+            else:
+                op.project(x, precision=args.precision)
+        torch.cuda.synchronize()
+        op.close()
+    elif args.case == "density":
+        support = synthetic.density_support(inputs, args.factor)
+        psi = torch.from_numpy(synthetic.band_coefficients(inputs, cols)).cuda()
+        for _ in range(args.repeat):
+            density.band_density(ctx, inputs.hkl, psi, np.full(cols, 2.0), inputs.volume, support)
+        torch.cuda.synchronize()
+    elif args.case == "pbe":
+        n = np.exp(np.linspace(-20, 1, cols * 65536))
+        for _ in range(args.repeat):
+            density.pbe_points(ctx, n, 0.3 * n)
+    ctx.close()
+    print("case", args.case, "done")
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
@@ -372,8 +412,16 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
+    parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe"],
+                        help="run a few launches of one kernel family for a profiler capture and exit")
+    parser.add_argument("--columns", type=int, default=32, help="columns (bands) for --case")
+    parser.add_argument("--repeat", type=int, default=2, help="repetitions for --case")
+    parser.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="precision for --case")
+    parser.add_argument("--factor", type=float, default=16.0, help="density support factor f for --case density")
     args = parser.parse_args()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
