@@ -162,6 +162,39 @@ SDFT_B200_API sdft_b200_status sdft_b200_band_density(sdft_b200_context* context
                                                       double volume, const int32_t* support, size_t count,
                                                       double* out, int memory);
 
+/* One-centre occupations of `atoms` atoms with `rows` projectors each:
+ * out[a][i][j] = sum_n occupations[n] P[a*rows+i, n] conj(P[a*rows+j, n])
+ * (row-major rows x rows per atom). amplitudes: (atoms*rows) x bands complex,
+ * column-major with column stride `stride` >= atoms*rows (the all-atom FP64
+ * projection B psi); occupations: host, in [0, 2]. amplitudes and out follow
+ * `memory`. Replaces: onsite_density_from_amplitudes, src/onsite_density.hpp:10-36
+ * (called per atom on a row view of one projection). */
+SDFT_B200_API sdft_b200_status sdft_b200_onsite_density(sdft_b200_context* context, size_t rows, size_t atoms,
+                                                        size_t bands, const double* amplitudes, size_t stride,
+                                                        const double* occupations, double* out, int memory);
+
+/* Compensation charge of atoms sharing one PAW augmentation on a reciprocal
+ * support. create: lattice (3 lattice vectors as rows, bohr), fractional atom
+ * positions (atoms x 3), keys (count x 3), the radial mesh (Angstrom) and
+ * g_L(r) r^2 shapes ((max_l+1) x radial), and the (L,M) transform of the
+ * one-centre occupation ((max_l+1)^2 x dimension^2 complex, entry
+ * [LM][i*dimension+j] = the LM moment of the unit occupation at (i,j), i.e.
+ * the reference's density_transform_). Form factors are integrated on the
+ * device at creation. All host arrays; copied. density: onsite is atoms x
+ * dimension^2 complex row-major Hermitian occupations, out is count complex
+ * values in key order; both follow `memory`.
+ * Replaces: PawCompensationOperator(augmentation, lattice, position, keys,
+ * Codata, shared) and PawCompensationOperator::density_sum,
+ * src/paw_compensation.hpp:14-27 (src/paw_compensation.cpp:185-342,465-524). */
+typedef struct sdft_b200_compensation sdft_b200_compensation;
+SDFT_B200_API sdft_b200_status sdft_b200_compensation_create(
+    sdft_b200_context* context, const double lattice[9], size_t atoms, const double* fractional,
+    const int32_t* keys, size_t count, int max_l, size_t radial, const double* radial_grid,
+    const double* compensation_r2, size_t dimension, const double* transform, sdft_b200_compensation** out);
+SDFT_B200_API sdft_b200_status sdft_b200_compensation_destroy(sdft_b200_compensation* charge);
+SDFT_B200_API sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensation* charge, const double* onsite,
+                                                              double* out, int memory);
+
 enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
 
 /* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with

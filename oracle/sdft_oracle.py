@@ -324,3 +324,119 @@ def plane_wave_density(hkl, coefficients, occupations, volume, support, fast: bo
         density += f / volume * (field.real * field.real + field.imag * field.imag)
     transformed = forward_fft(density.reshape(shape).astype(np.complex128)).ravel()
     return transformed[index_map(support, shape)] / count
+
+
+# --- One-centre occupations and compensation charge ---------------------------
+# src/onsite_density.hpp:10-36, src/paw_compensation.cpp:51-139,185-342,465-524,
+# src/paw_augmentation.cpp:490-525.
+
+BOHR_PER_ANGSTROM = 1.8897261254578281  # CODATA convention (src/atomic_units.hpp:10-14)
+
+
+def onsite_density(amplitudes, occupations) -> np.ndarray:
+    """rho_ij = sum_n f_n P_in conj(P_jn) for one atom's rows (src/onsite_density.hpp:13-36)."""
+    p = np.asarray(amplitudes, dtype=np.complex128)
+    f = np.asarray(occupations, dtype=np.float64)
+    if np.any(~np.isfinite(f)) or np.any(f < 0) or np.any(f > 2):
+        raise ValueError("invalid projected onsite occupation")
+    if not (np.all(np.isfinite(p.real)) and np.all(np.isfinite(p.imag))):
+        raise ValueError("nonfinite onsite projection")
+    return (p * f[None, :]) @ p.conj().T
+
+
+def radial_weights(r) -> np.ndarray:
+    """Simpson panels from the outer end on a logarithmic mesh, else trapezoids (src/paw_compensation.cpp:51-74)."""
+    r = np.asarray(r, dtype=np.float64)
+    h = math.log(r[1] / r[0])
+    logarithmic = np.isfinite(h) and h > 0 and np.all(np.abs(np.log(r[1:] / r[:-1]) - h) < 2e-7)
+    w = np.zeros(r.size)
+    if logarithmic:
+        k = r.size
+        while k >= 3:
+            w[k - 1] += r[k - 1] * h / 3.0
+            w[k - 2] = 4.0 * r[k - 2] * h / 3.0
+            w[k - 3] = r[k - 3] * h / 3.0
+            if k == 3:
+                break
+            k -= 2
+    else:
+        d = np.diff(r) / 2.0
+        w[:-1] += d
+        w[1:] += d
+    return w
+
+
+def real_harmonic(l: int, m: int, q: np.ndarray) -> np.ndarray:
+    """Real harmonics without the Condon-Shortley phase (src/paw_compensation.cpp:116-139); q (n,3)."""
+    q = np.asarray(q, dtype=np.float64).reshape(-1, 3)
+    radius = np.sqrt(np.sum(q * q, axis=1))
+    small = radius < 1e-14
+    safe = np.where(small, 1.0, radius)
+    z = np.clip(q[:, 2] / safe, -1.0, 1.0)
+    s = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    order = abs(m)
+    pmm = np.ones_like(z)
+    for k in range(1, order + 1):
+        pmm = pmm * ((2.0 * k - 1.0) * s)
+    value = pmm
+    if l > order:
+        previous = pmm
+        value = (2.0 * order + 1.0) * z * pmm
+        for degree in range(order + 2, l + 1):
+            nxt = ((2.0 * degree - 1.0) * z * value - (degree + order - 1.0) * previous) / (degree - order)
+            previous, value = value, nxt
+    factor = math.sqrt((2 * l + 1) / (4 * math.pi) * math.exp(math.lgamma(l - order + 1) - math.lgamma(l + order + 1)))
+    factor *= math.sqrt(2.0) if order else 1.0
+    angle = order * np.arctan2(q[:, 1], q[:, 0])
+    out = factor * value * (np.sin(angle) if m < 0 else np.cos(angle))
+    return np.where(small, (1.0 / math.sqrt(4 * math.pi)) if l == 0 else 0.0, out)
+
+
+def _reciprocal(lattice):
+    a = np.asarray(lattice, dtype=np.float64).reshape(3, 3)
+    volume = float(np.dot(a[0], np.cross(a[1], a[2])))
+    b = 2 * math.pi / volume * np.array([np.cross(a[1], a[2]), np.cross(a[2], a[0]), np.cross(a[0], a[1])])
+    return a, b, abs(volume)
+
+
+def compensation_form(lattice, keys, augmentation) -> np.ndarray:
+    """Compact F_LM(G) = nonzero part of 4 pi (-i)^L Y_LM(G^) int g_L r^2 j_L(|G| r) dr, shape (lms, count)
+    (src/paw_compensation.cpp:254-301)."""
+    from scipy.special import spherical_jn
+    _, b, _ = _reciprocal(lattice)
+    keys = np.asarray(keys).reshape(-1, 3).astype(np.float64)
+    q = keys @ b
+    radius = np.sqrt(np.sum(q * q, axis=1)) * BOHR_PER_ANGSTROM
+    r = np.asarray(augmentation["radial_grid"], dtype=np.float64)
+    r2 = np.asarray(augmentation["compensation_r2"], dtype=np.float64)
+    w = radial_weights(r)
+    shells, inverse = np.unique(radius, return_inverse=True)
+    max_l = int(augmentation["max_l"])
+    form = np.zeros(((max_l + 1) ** 2, keys.shape[0]))
+    for L in range(max_l + 1):
+        integral = (spherical_jn(L, np.outer(shells, r)) * (w * r2[L])[None, :]).sum(axis=1)
+        if L == 0:
+            integral = np.where(shells < 1e-14, 1.0, integral)
+        sign = 1.0 if L % 4 in (0, 3) else -1.0
+        for M in range(-L, L + 1):
+            form[L * L + M + L] = sign * 4 * math.pi * real_harmonic(L, M, q) * integral[inverse]
+    return form
+
+
+def compensation_density(lattice, fractional, keys, augmentation, transform, onsite) -> np.ndarray:
+    """sum_a exp(-i G.tau_a)/Omega sum_LM F_LM(G) M_a,LM with M_a = transform . rho_a (src/paw_compensation.cpp:465-524)."""
+    a, b, volume = _reciprocal(lattice)
+    keys = np.asarray(keys).reshape(-1, 3)
+    q = keys.astype(np.float64) @ b
+    form = compensation_form(lattice, keys, augmentation)
+    max_l = int(augmentation["max_l"])
+    imaginary = np.array([L % 2 for L in range(max_l + 1) for _ in range(2 * L + 1)], dtype=bool)
+    complex_form = np.where(imaginary[:, None], 1j * form, form)
+    rho = np.asarray(onsite, dtype=np.complex128).reshape(len(fractional), -1)
+    moments = rho @ np.asarray(transform).T  # (atoms, lms)
+    positions = np.asarray(fractional, dtype=np.float64).reshape(-1, 3) @ a
+    total = np.zeros(keys.shape[0], dtype=np.complex128)
+    for atom in range(positions.shape[0]):
+        phase = np.exp(-1j * (q @ positions[atom]))
+        total += phase * (moments[atom] @ complex_form) / volume
+    return total

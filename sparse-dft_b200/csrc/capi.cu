@@ -8,6 +8,7 @@
 #include "../../include/sdft_b200.h"
 #include "davidson.cuh"
 #include "band_density.cuh"
+#include "paw_density.cuh"
 #include "operator.cuh"
 
 struct sdft_b200_context {
@@ -16,6 +17,10 @@ struct sdft_b200_context {
 struct sdft_b200_operator {
   std::unique_ptr<sdft_b200::DeviceOperator> impl;
   std::unique_ptr<sdft_b200::DavidsonSolver> solver;  // workspace reused across solves
+};
+
+struct sdft_b200_compensation {
+  std::unique_ptr<sdft_b200::CompensationCharge> impl;
 };
 
 namespace {
@@ -366,6 +371,91 @@ sdft_b200_status sdft_b200_band_density(sdft_b200_context* context, const int32_
     SDFT_CUDA(cudaMemcpyAsync(din, psi, sizeof(C) * npw * bands, cudaMemcpyHostToDevice, ctx.stream));
     sdft_b200::band_density(ctx, hkl, npw, din, occupations, bands, volume, support, count, dout);
     SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
+sdft_b200_status sdft_b200_onsite_density(sdft_b200_context* context, size_t rows, size_t atoms, size_t bands,
+                                         const double* amplitudes, size_t stride, const double* occupations,
+                                         double* out, int memory) {
+  return guarded([&] {
+    require(context && amplitudes && occupations && out && rows && atoms && bands && stride >= rows * atoms,
+            "invalid projected onsite density dimensions");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    using C = sdft_b200::Cx<double>;
+    const std::size_t outputs = atoms * rows * rows;
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      sdft_b200::onsite_density(ctx, rows, atoms, bands, reinterpret_cast<const C*>(amplitudes), stride, occupations,
+                                reinterpret_cast<C*>(out));
+      return;
+    }
+    require(memory == SDFT_B200_MEMORY_HOST, "memory must be host or device");
+    const std::size_t in_count = stride * (bands - 1) + rows * atoms;
+    auto* din = static_cast<C*>(ctx.staging_in.reserve(sizeof(C) * in_count));
+    auto* dout = static_cast<C*>(ctx.staging_out.reserve(sizeof(C) * outputs));
+    SDFT_CUDA(cudaMemcpyAsync(din, amplitudes, sizeof(C) * in_count, cudaMemcpyHostToDevice, ctx.stream));
+    sdft_b200::onsite_density(ctx, rows, atoms, bands, din, stride, occupations, dout);
+    SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * outputs, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
+sdft_b200_status sdft_b200_compensation_create(sdft_b200_context* context, const double lattice[9], size_t atoms,
+                                               const double* fractional, const int32_t* keys, size_t count,
+                                               int max_l, size_t radial, const double* radial_grid,
+                                               const double* compensation_r2, size_t dimension,
+                                               const double* transform, sdft_b200_compensation** out) {
+  return guarded([&] {
+    require(context && out, "invalid PAW compensation dimensions");
+    *out = nullptr;
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    sdft_b200::CompensationInput in;
+    in.lattice = lattice;
+    in.atoms = atoms;
+    in.fractional = fractional;
+    in.keys = keys;
+    in.count = count;
+    in.max_l = max_l;
+    in.radial = radial;
+    in.radial_grid = radial_grid;
+    in.compensation_r2 = compensation_r2;
+    in.dimension = dimension;
+    in.transform = transform;
+    auto charge = std::make_unique<sdft_b200_compensation>();
+    charge->impl = std::make_unique<sdft_b200::CompensationCharge>(ctx, in);
+    *out = charge.release();
+  });
+}
+
+sdft_b200_status sdft_b200_compensation_destroy(sdft_b200_compensation* charge) {
+  return guarded([&] {
+    if (!charge) return;
+    SDFT_CUDA(cudaSetDevice(charge->impl->context().device));
+    delete charge;
+  });
+}
+
+sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensation* charge, const double* onsite, double* out,
+                                                int memory) {
+  return guarded([&] {
+    require(charge && onsite && out, "invalid PAW compensation dimensions");
+    auto& c = *charge->impl;
+    auto& ctx = c.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    using C = sdft_b200::Cx<double>;
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      c.density(reinterpret_cast<const C*>(onsite), reinterpret_cast<C*>(out));
+      return;
+    }
+    require(memory == SDFT_B200_MEMORY_HOST, "memory must be host or device");
+    const std::size_t in_count = c.atoms() * c.dimension() * c.dimension();
+    auto* din = static_cast<C*>(ctx.staging_in.reserve(sizeof(C) * in_count));
+    auto* dout = static_cast<C*>(ctx.staging_out.reserve(sizeof(C) * c.count()));
+    SDFT_CUDA(cudaMemcpyAsync(din, onsite, sizeof(C) * in_count, cudaMemcpyHostToDevice, ctx.stream));
+    c.density(din, dout);
+    SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * c.count(), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.synchronize();
   });
 }

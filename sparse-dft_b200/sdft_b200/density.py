@@ -51,3 +51,70 @@ def band_density(context: Context, hkl, coefficients, occupations, volume: float
                                        occ.ctypes.data_as(C.D), occ.size, float(volume), sup.ctypes.data_as(C.I32),
                                        sup.shape[0], pout, memory))
     return out
+
+
+def onsite_density(context: Context, amplitudes, rows: int, occupations) -> np.ndarray:
+    """(atoms, rows, rows) one-centre occupations from the all-atom projection
+    (atoms*rows, bands), the reference's onsite_density_from_amplitudes per atom."""
+    lib = C.library()
+    p = np.asfortranarray(amplitudes, dtype=np.complex128)
+    occ = np.ascontiguousarray(occupations, dtype=np.float64).ravel()
+    total, bands = p.shape
+    if total % rows or bands != occ.size:
+        raise ValueError("amplitudes must be (atoms*rows, bands) with one occupation per band")
+    atoms = total // rows
+    out = np.zeros((atoms, rows, rows), dtype=np.complex128)
+    C.check(lib.sdft_b200_onsite_density(context.handle, rows, atoms, bands, ctypes.c_void_p(p.ctypes.data), total,
+                                         occ.ctypes.data_as(C.D), ctypes.c_void_p(out.ctypes.data), C.HOST))
+    return out
+
+
+class CompensationCharge:
+    """Device compensation charge of atoms sharing one augmentation on a
+    reciprocal support (the reference's PawCompensationOperator::density_sum)."""
+
+    def __init__(self, context: Context, lattice, fractional, keys, augmentation: dict, transform):
+        lib = C.library()
+        self._lib = lib
+        self.context = context
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        frac = np.ascontiguousarray(fractional, dtype=np.float64).reshape(-1, 3)
+        self.keys = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+        r = np.ascontiguousarray(augmentation["radial_grid"], dtype=np.float64)
+        r2 = np.ascontiguousarray(augmentation["compensation_r2"], dtype=np.float64)
+        t = np.ascontiguousarray(transform, dtype=np.complex128)
+        self.atoms = frac.shape[0]
+        self.dimension = int(round(np.sqrt(t.shape[1])))
+        handle = ctypes.c_void_p()
+        C.check(lib.sdft_b200_compensation_create(
+            context.handle, lat.ctypes.data_as(C.D), self.atoms, frac.ctypes.data_as(C.D),
+            self.keys.ctypes.data_as(C.I32), self.keys.shape[0], int(augmentation["max_l"]), r.size,
+            r.ctypes.data_as(C.D), r2.ctypes.data_as(C.D), self.dimension, t.view(np.float64).ctypes.data_as(C.D),
+            ctypes.byref(handle)))
+        self.handle = handle
+
+    def density(self, onsite):
+        """onsite: (atoms, dim, dim) numpy (host path) or a torch CUDA tensor (device path)."""
+        if getattr(onsite, "is_cuda", False):
+            import torch
+            rho = onsite.contiguous()
+            out = torch.empty(self.keys.shape[0], dtype=torch.complex128, device=rho.device)
+            C.check(self._lib.sdft_b200_compensation_density(self.handle, ctypes.c_void_p(rho.data_ptr()),
+                                                             ctypes.c_void_p(out.data_ptr()), C.DEVICE))
+            return out
+        rho = np.ascontiguousarray(onsite, dtype=np.complex128)
+        out = np.zeros(self.keys.shape[0], dtype=np.complex128)
+        C.check(self._lib.sdft_b200_compensation_density(self.handle, ctypes.c_void_p(rho.ctypes.data),
+                                                         ctypes.c_void_p(out.ctypes.data), C.HOST))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.sdft_b200_compensation_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

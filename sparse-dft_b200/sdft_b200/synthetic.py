@@ -355,3 +355,39 @@ def projected_amplitudes(atoms: int, dim: int, bands: int, seed: int = 43) -> np
     rng = np.random.Generator(np.random.PCG64(seed))
     p = rng.standard_normal((atoms * dim, bands)) + 1j * rng.standard_normal((atoms * dim, bands))
     return np.asfortranarray(0.3 * p)
+
+
+def real_gaunt(l1: int, m1: int, l2: int, m2: int, L: int, M: int) -> float:
+    """int Y_l1m1 Y_l2m2 Y_LM dOmega over the sphere by Gauss-Legendre (16) x uniform-phi (32)
+    quadrature, exact for the polynomial degrees of L <= 6 products."""
+    x, wx = np.polynomial.legendre.leggauss(16)
+    phi = np.arange(32) * (2 * math.pi / 32)
+    theta = np.arccos(x)
+    q = np.stack([np.outer(np.sin(theta), np.cos(phi)).ravel(), np.outer(np.sin(theta), np.sin(phi)).ravel(),
+                  np.repeat(np.cos(theta), phi.size)], axis=1)
+    weight = np.repeat(wx, phi.size) * (2 * math.pi / 32)
+    return float(np.sum(weight * real_harmonic(l1, m1, q) * real_harmonic(l2, m2, q) * real_harmonic(L, M, q)))
+
+
+def lm_transform(aug: dict) -> np.ndarray:
+    """(L,M) moments of each unit one-centre occupation, [LM, ii*dim+jj] =
+    aug_moment(i, j, L) G(l_i m, l_j m' | L M): the compensation transform the
+    reference builds from paw_lm_moments_from_density (src/paw_augmentation.cpp:490-525,
+    src/paw_compensation.cpp:228-236), here from the real Gaunt coefficients by quadrature."""
+    ch = [int(v) for v in aug["channel_l"]]
+    max_l = int(aug["max_l"])
+    moment = np.asarray(aug["aug_moment"], dtype=np.float64).reshape(len(ch), len(ch), max_l + 1)
+    offset = np.concatenate([[0], np.cumsum([2 * l + 1 for l in ch])])
+    dim = int(offset[-1])
+    out = np.zeros(((max_l + 1) ** 2, dim * dim), dtype=np.complex128)
+    for i, li in enumerate(ch):
+        for j, lj in enumerate(ch):
+            for m in range(-li, li + 1):
+                for mp in range(-lj, lj + 1):
+                    e = (offset[i] + m + li) * dim + offset[j] + mp + lj
+                    for L in range(abs(li - lj), min(max_l, li + lj) + 1):
+                        for M in range(-L, L + 1):
+                            g = real_gaunt(li, m, lj, mp, L, M)
+                            if abs(g) > 1e-12:
+                                out[L * L + M + L, e] += moment[i, j, L] * g
+    return out

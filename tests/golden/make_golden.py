@@ -127,6 +127,23 @@ def density_fixture(lib, inputs, name, factor, bands):
     print("density", name, "support", support.shape[0])
 
 
+def compensation_fixture(lib, inputs, name, factor, bands):
+    """Reference onsite_density_from_amplitudes (src/onsite_density.hpp:13), the (L,M)
+    transform and PawCompensationOperator::density_sum (src/paw_compensation.cpp:465)."""
+    aug = synthetic.augmentation()
+    atoms = inputs.positions.shape[0]
+    rows = int(np.sum(2 * aug["channel_l"] + 1))
+    amplitudes = synthetic.projected_amplitudes(atoms, rows, bands)
+    occ = density_occupations(bands)
+    onsite = np.stack([lib.onsite_density(amplitudes[a * rows:(a + 1) * rows], occ) for a in range(atoms)])
+    transform = lib.lm_transform(aug)
+    keys = synthetic.density_support(inputs, factor)
+    charge = lib.compensation_density(inputs.lattice, inputs.positions, keys, aug, onsite)
+    np.savez_compressed(HERE / f"compensation_{name}.npz", occupations=occ, onsite=onsite, transform=transform,
+                        factor=np.array(factor), bands=np.array(bands), charge=charge)
+    print("compensation", name, "keys", keys.shape[0])
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
@@ -137,6 +154,7 @@ def main():
     pbe_fixture(lib)
     density_fixture(lib, synthetic.tiny(), "tiny", 4.0, 6)
     density_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
+    compensation_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

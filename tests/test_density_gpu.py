@@ -181,3 +181,84 @@ def test_band_density_edge_cases(context):
     # The context stays usable after every rejected call.
     again = density.band_density(context, x.hkl, c, np.ones(3), x.volume, support)
     assert np.all(np.isfinite(again))
+
+
+# --- one-centre occupations and compensation charge ----------------------------
+
+def _compensation_inputs(x, bands, factor):
+    from sdft_b200 import synthetic
+    aug = synthetic.augmentation()
+    rows = int(np.sum(2 * aug["channel_l"] + 1))
+    amplitudes = synthetic.projected_amplitudes(x.positions.shape[0], rows, bands)
+    return aug, rows, amplitudes, synthetic.density_support(x, factor)
+
+
+def test_onsite_density_matches_reference_fixture(context, golden):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    g = golden("compensation_si8")
+    _, rows, amplitudes, _ = _compensation_inputs(synthetic.si8(), int(g["bands"]), float(g["factor"]))
+    onsite = density.onsite_density(context, amplitudes, rows, g["occupations"])
+    assert relative_error(onsite, g["onsite"]) < 1e-13
+
+
+def test_compensation_matches_reference_fixture(context, golden):
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    g = golden("compensation_si8")
+    x = synthetic.si8()
+    aug, _, _, keys = _compensation_inputs(x, int(g["bands"]), float(g["factor"]))
+    charge = density.CompensationCharge(context, x.lattice, x.positions, keys, aug, g["transform"])
+    out = charge.density(g["onsite"])
+    charge.close()
+    assert relative_error(out, g["charge"]) < 1e-12
+
+
+def test_compensation_si64_f16_matches_oracle_and_device_path(context):
+    """Config-size support (Si64, f = 16: ~1.07 M keys, 64 atoms) from 128 occupied bands."""
+    import torch
+    from conftest import relative_error
+    from sdft_b200 import density, synthetic
+    x = synthetic.si64()
+    aug, rows, amplitudes, keys = _compensation_inputs(x, 128, 16.0)
+    occ = np.full(128, 2.0)
+    onsite = density.onsite_density(context, amplitudes, rows, occ)
+    transform = synthetic.lm_transform(aug)
+    charge = density.CompensationCharge(context, x.lattice, x.positions, keys, aug, transform)
+    out = charge.density(onsite)
+    sub = slice(0, None, 97)  # oracle on a strided subset of the keys
+    expected = sdft_oracle.compensation_density(x.lattice, x.positions, keys[sub], aug, transform, onsite)
+    assert relative_error(out[sub], expected) < 1e-12
+    device = charge.density(torch.from_numpy(onsite).cuda())
+    assert np.array_equal(device.cpu().numpy(), out)
+    # n(-G) = conj n(G) for a Hermitian occupation.
+    position = {tuple(k): i for i, k in enumerate(keys.tolist())}
+    mirror = np.array([position[(-h, -k, -l)] for h, k, l in keys[sub].tolist()])
+    assert np.max(np.abs(out[mirror] - np.conj(out[sub]))) < 1e-12 * np.max(np.abs(out))
+    charge.close()
+
+
+def test_onsite_and_compensation_reject_invalid_inputs(context):
+    from sdft_b200 import _capi, density, synthetic
+    x = synthetic.si8()
+    aug, rows, amplitudes, keys = _compensation_inputs(x, 4, 1.0)
+    with pytest.raises(_capi.InvalidArgument, match="invalid projected onsite occupation"):
+        density.onsite_density(context, amplitudes, rows, [2.0, 2.1, 1.0, 0.0])
+    bad = amplitudes.copy()
+    bad[3, 1] = np.inf
+    with pytest.raises(_capi.InvalidArgument, match="nonfinite onsite projection"):
+        density.onsite_density(context, bad, rows, np.ones(4))
+    transform = synthetic.lm_transform(aug)
+    charge = density.CompensationCharge(context, x.lattice, x.positions, keys, aug, transform)
+    onsite = density.onsite_density(context, amplitudes, rows, np.ones(4))
+    skew = onsite.copy()
+    skew[0, 1, 2] += 1e-6
+    with pytest.raises(_capi.InvalidArgument, match="finite and Hermitian"):
+        charge.density(skew)
+    assert np.all(np.isfinite(charge.density(onsite)))
+    charge.close()
+    with pytest.raises(_capi.InvalidArgument, match="singular PAW compensation lattice"):
+        density.CompensationCharge(context, np.zeros((3, 3)), x.positions, keys, aug, transform)
+    with pytest.raises(_capi.InvalidArgument, match="radial mesh"):
+        bad_aug = dict(aug, radial_grid=aug["radial_grid"][::-1].copy())
+        density.CompensationCharge(context, x.lattice, x.positions, keys, bad_aug, transform)

@@ -123,3 +123,33 @@ def test_band_density_grid_rule_matches_reference_cases():
     # min/max are seeded at 0: a basis on one side of the origin still counts from 0.
     hkl = np.array([[2, 3, 4], [5, 3, 4]])
     assert sdft_oracle.density_grid_shape(hkl, np.array([[0, 0, 0]])) == (11, 7, 9)
+
+
+def test_onsite_and_compensation_restatements_match_golden(golden):
+    g = golden("compensation_si8")
+    x = synthetic.si8()
+    aug = synthetic.augmentation()
+    rows = int(np.sum(2 * aug["channel_l"] + 1))
+    amplitudes = synthetic.projected_amplitudes(x.positions.shape[0], rows, int(g["bands"]))
+    onsite = np.stack([sdft_oracle.onsite_density(amplitudes[a * rows:(a + 1) * rows], g["occupations"])
+                       for a in range(x.positions.shape[0])])
+    assert relative_error(onsite, g["onsite"]) < 1e-14
+    # The synthetic (L,M) transform (Gaunt coefficients by quadrature) is the reference's.
+    assert np.max(np.abs(synthetic.lm_transform(aug) - g["transform"])) < 1e-14
+    keys = synthetic.density_support(x, float(g["factor"]))
+    charge = sdft_oracle.compensation_density(x.lattice, x.positions, keys, aug, g["transform"], g["onsite"])
+    assert relative_error(charge, g["charge"]) < 1e-13
+
+
+def test_compensation_restatement_matches_live_reference_off_gamma_lattice(reference):
+    """A non-cubic cell and a complex (non-real) occupation, against the reference itself."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    lattice = np.array([[6.0, 0.4, 0.0], [0.3, 7.0, 0.2], [0.0, -0.5, 6.5]])
+    fractional = rng.uniform(0, 1, (3, 3))
+    keys = np.array([(h, k, l) for h in range(-4, 5) for k in range(-4, 5) for l in range(-4, 5)], dtype=np.int32)
+    aug = synthetic.augmentation(seed=5)
+    m = rng.standard_normal((3, 8, 8)) + 1j * rng.standard_normal((3, 8, 8))
+    onsite = m + np.conj(np.transpose(m, (0, 2, 1)))
+    expected = reference.compensation_density(lattice, fractional, keys, aug, onsite)
+    charge = sdft_oracle.compensation_density(lattice, fractional, keys, aug, synthetic.lm_transform(aug), onsite)
+    assert relative_error(charge, expected) < 1e-13
