@@ -83,6 +83,22 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op
  * Replaces: PlaneWaveOperator::fft_grid_points, src/plane_wave_operator.hpp:38. */
 SDFT_B200_API sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t shape[3], size_t* grid_points,
                                          size_t* projectors, size_t* npw, size_t* active_rows);
+/* Local part of H~ (y = T o x + (1/N) FFT_fwd(V(r) . FFT_bwd(scatter x))) on
+ * DEVICE pointers x, y (npw x columns, ld npw), with no allocation of any
+ * kind: the FFT slab and twiddle tables live in a fixed 32 MiB static device
+ * array per device, looked up once per device by the first call (which must
+ * therefore come before any stream capture on that device). A call whose
+ * slab (active rows x n1 x n2 x columns complex values of the precision)
+ * exceeds the array is rejected with INVALID_ARGUMENT naming the column
+ * limit. Nothing in the array has to start at zero. All calls on one device
+ * share the array: calls whose work overlaps in time on different streams,
+ * threads or contexts race; calls on one stream are ordered. Same results as
+ * sdft_b200_apply_local. For callers that must not allocate (memory reserved
+ * up front, or no room for the device-wide synchronisation of cudaFree).
+ * No reference counterpart: the reference allocates its FFT work arrays per
+ * call (src/compute_cuda.cu:141-177). */
+SDFT_B200_API sdft_b200_status sdft_b200_apply_local_noalloc(sdft_b200_operator* op, const double* x,
+                                                             size_t columns, double* y, int precision);
 /* Sphere-to-grid index map (npw values), T (Hartree), H and S diagonals
  * (npw each), V(r) (grid_points values); any pointer may be NULL.
  * Replaces: the Impl members indices/kinetic/h_diagonal/s_diagonal/local_real,

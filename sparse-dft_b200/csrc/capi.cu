@@ -228,6 +228,18 @@ sdft_b200_status sdft_b200_apply_local(sdft_b200_operator* op, const double* x, 
   });
 }
 
+sdft_b200_status sdft_b200_apply_local_noalloc(sdft_b200_operator* op, const double* x, size_t columns, double* y,
+                                               int precision) {
+  return guarded([&] {
+    require(op && x && y && columns && x != y, "invalid direct plane-wave input/output buffers");
+    require(columns <= static_cast<size_t>(INT32_MAX), "too many columns");
+    auto& o = *op->impl;
+    SDFT_CUDA(cudaSetDevice(o.context().device));
+    sdft_b200::apply_local_noalloc(o, reinterpret_cast<const Cx<double>*>(x), static_cast<int>(columns),
+                                   reinterpret_cast<Cx<double>*>(y), precision_of(precision));
+  });
+}
+
 sdft_b200_status sdft_b200_operator_arrays(const sdft_b200_operator* op, uint64_t* indices, double* kinetic,
                                            double* h_diagonal, double* s_diagonal, double* local_potential) {
   return guarded([&] {

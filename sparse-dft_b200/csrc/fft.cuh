@@ -299,4 +299,9 @@ __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_strid
 template <typename T>
 const Cx<T>* device_twiddles(int n);
 
+// The same table values written into caller memory on the host (no device
+// allocation, no cache).
+template <typename T>
+void host_twiddles(int n, Cx<T>* out);
+
 }  // namespace sdft_b200

@@ -83,6 +83,17 @@ const Cx<T>* device_twiddles(int n) {
   return static_cast<const Cx<T>*>(ptr);
 }
 
+template <typename T>
+void host_twiddles(int n, Cx<T>* out) {
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; ++m) {
+    const long double angle = two_pi * static_cast<long double>(m) / static_cast<long double>(n);
+    out[m] = Cx<T>{static_cast<T>(std::cos(angle)), static_cast<T>(-std::sin(angle))};
+  }
+}
+
+template void host_twiddles<float>(int, Cx<float>*);
+template void host_twiddles<double>(int, Cx<double>*);
 template const Cx<float>* device_twiddles<float>(int);
 template const Cx<double>* device_twiddles<double>(int);
 

@@ -381,6 +381,56 @@ void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t s
   else fft3d_impl<T, false>(grid, n, batch, stream);
 }
 
+template <typename T>
+void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns,
+                              const T* potential, const double* kinetic, Cx<double>* y, long long ldy,
+                              Cx<T>* slab, const Cx<T>* const twiddle[3], cudaStream_t stream) {
+  if (columns <= 0) return;
+  if (std::max({plan.n[0], plan.n[1], plan.n[2]}) > 128)
+    throw InvalidArgument("operator FFT grid axes above 128 points are not supported");
+  LocalArgs<T> a{};
+  a.n0 = plan.n[0];
+  a.n1 = plan.n[1];
+  a.n2 = plan.n[2];
+  a.n2p = plan.n2p;
+  a.slots = plan.slots;
+  a.krows = plan.krows;
+  a.n12 = static_cast<long long>(plan.n[1]) * plan.n[2];
+  a.slot_row = plan.slot_row;
+  a.point_offset = plan.point_offset;
+  a.point_g = plan.point_g;
+  a.point_smem = plan.point_smem;
+  a.krow = plan.krow;
+  a.p0 = plan.line[0];
+  a.p1 = plan.line[1];
+  a.p2 = plan.line[2];
+  a.tw0 = twiddle[0];
+  a.tw1 = twiddle[1];
+  a.tw2 = twiddle[2];
+  const std::size_t plane_smem =
+      sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + 2 * static_cast<std::size_t>(plan.n[1]) * plan.n2p);
+  const std::size_t pencil_smem =
+      sizeof(Cx<T>) * (plan.n[0] + 2 * static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
+  allow_smem(plane_in_kernel<T>, plane_smem);
+  allow_smem(pencil_kernel<T>, pencil_smem);
+  allow_smem(plane_out_kernel<T>, plane_smem);
+  const dim3 planes(plan.slots, columns);
+  plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
+  SDFT_LAUNCH("plane_in_kernel");
+  const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
+  pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+  SDFT_LAUNCH("pencil_kernel");
+  plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
+                                                                static_cast<double>(plan.count), y, ldy);
+  SDFT_LAUNCH("plane_out_kernel");
+}
+
+template void local_hamiltonian_preset<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,
+                                              const double*, Cx<double>*, long long, Cx<float>*,
+                                              const Cx<float>* const[3], cudaStream_t);
+template void local_hamiltonian_preset<double>(const SpherePlan&, const Cx<double>*, long long, int, const double*,
+                                               const double*, Cx<double>*, long long, Cx<double>*,
+                                               const Cx<double>* const[3], cudaStream_t);
 template void local_hamiltonian<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,
                                        const double*, Cx<double>*, long long, Cx<float>*, cudaStream_t);
 template void local_hamiltonian<double>(const SpherePlan&, const Cx<double>*, long long, int, const double*,

@@ -42,6 +42,13 @@ void local_hamiltonian(const SpherePlan& plan, const Cx<double>* x, long long ld
                        const T* potential, const double* kinetic, Cx<double>* y, long long ldy,
                        Cx<T>* slab, cudaStream_t stream);
 
+// local_hamiltonian with caller-provided twiddle tables (twiddle[a] holds
+// plan.n[a] values) and slab; launches kernels only, allocates nothing.
+template <typename T>
+void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns,
+                              const T* potential, const double* kinetic, Cx<double>* y, long long ldy,
+                              Cx<T>* slab, const Cx<T>* const twiddle[3], cudaStream_t stream);
+
 // In-place unnormalised 3D FFT of `batch` contiguous row-major grids.
 template <typename T>
 void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream);

@@ -1,0 +1,88 @@
+// Fused local H~psi on device arrays with no allocation of any kind in the
+// call: the slab between the plane and pencil passes and the three twiddle
+// tables live in one file-scope device array of fixed size, whose address is
+// looked up once per device with cudaGetSymbolAddress.
+//
+// For callers that must not allocate: a serving loop that has reserved the
+// device's memory up front (pools sized to HBM), or one that cannot accept the
+// device-wide synchronisation that cudaMalloc/cudaFree imply. The regular
+// entry point grows its slab with cudaMalloc on first use of a larger block.
+//
+// Scratch contract:
+//   - capacity kNoAllocScratchBytes (32 MiB) per device; the twiddle tables
+//     take the first kTwiddleBytes, the slab the rest. A call whose slab
+//     (slots * n1 * n2 * columns complex values) does not fit is rejected.
+//   - nothing in it has to start at zero: each call writes the tables, and
+//     the plane pass writes every slab entry before the pencil pass reads it.
+//   - all calls on one device share it: two calls whose work overlaps in time
+//     (different streams, threads or contexts on the same device) race on it.
+//     Calls issued on one stream are ordered and safe.
+#include <mutex>
+#include <string>
+
+#include "operator.cuh"
+
+namespace sdft_b200 {
+
+namespace {
+
+constexpr std::size_t kNoAllocScratchBytes = std::size_t(32) << 20;
+constexpr std::size_t kTwiddleBytes = 32 * 1024;  // 3 tables x 512 x 16 B, rounded up
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_setup_mutex;
+void* g_scratch_address[kMaxDevices] = {};
+
+// Once per device, with that device current. The first call on a device does
+// this look-up, so it must come before any stream capture on that device.
+unsigned char* scratch_for(int device) {
+  if (device < 0 || device >= kMaxDevices) throw InvalidArgument("device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_scratch_address[device]) {
+    void* address = nullptr;
+    SDFT_CUDA(cudaGetSymbolAddress(&address, g_noalloc_scratch));
+    g_scratch_address[device] = address;
+  }
+  return static_cast<unsigned char*>(g_scratch_address[device]);
+}
+
+template <typename T>
+void run(DeviceOperator& op, const Cx<double>* x, int columns, Cx<double>* y, const T* potential) {
+  Context& ctx = op.context();
+  const SpherePlan& plan = op.plan();
+  const std::size_t per_column = sizeof(Cx<T>) * plan.slab_elements(1);
+  const std::size_t capacity = kNoAllocScratchBytes - kTwiddleBytes;
+  if (per_column * static_cast<std::size_t>(columns) > capacity)
+    throw InvalidArgument("no-allocation local apply: " + std::to_string(columns) + " columns need " +
+                          std::to_string(per_column * static_cast<std::size_t>(columns)) +
+                          " slab bytes, above the 32 MiB static scratch; at most " +
+                          std::to_string(capacity / per_column) + " columns per call for this operator");
+  unsigned char* scratch = scratch_for(ctx.device);
+  // Same table values as the cached tables of the regular path.
+  Cx<T> host[3][kMaxLine];
+  std::size_t offset = 0;
+  const Cx<T>* twiddle[3];
+  for (int a = 0; a < 3; ++a) {
+    const int n = plan.n[a];
+    host_twiddles<T>(n, host[a]);
+    auto* dst = reinterpret_cast<Cx<T>*>(scratch + offset);
+    SDFT_CUDA(cudaMemcpyAsync(dst, host[a], sizeof(Cx<T>) * n, cudaMemcpyHostToDevice, ctx.stream));
+    twiddle[a] = dst;
+    offset += sizeof(Cx<T>) * kMaxLine;
+  }
+  auto* slab = reinterpret_cast<Cx<T>*>(scratch + kTwiddleBytes);
+  local_hamiltonian_preset<T>(plan, x, op.npw(), columns, potential, op.device_kinetic(), y, op.npw(), slab, twiddle,
+                              ctx.stream);
+}
+
+}  // namespace
+
+void apply_local_noalloc(DeviceOperator& op, const Cx<double>* x, int columns, Cx<double>* y, Precision precision) {
+  if (columns <= 0) throw InvalidArgument("invalid direct plane-wave input/output buffers");
+  if (precision == Precision::FP64) run<double>(op, x, columns, y, op.device_potential64());
+  else run<float>(op, x, columns, y, op.device_potential32());
+}
+
+}  // namespace sdft_b200

@@ -72,6 +72,11 @@ void accelerator_paw_pair(Context& ctx, std::uint64_t identity, std::size_t npw,
                           std::size_t columns, const double* b, const double* d, const double* q, const double* input,
                           double* h, double* s, Precision precision, std::uint64_t projector_identity);
 
+class DeviceOperator;
+// Local part of H~ on device arrays with all scratch in a static device array
+// (local_noalloc.cu); allocates nothing.
+void apply_local_noalloc(DeviceOperator& op, const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
+
 // PBE per point on device arrays (pbe.cu): out holds 7 values per point.
 void pbe_points(Context& ctx, const double* density, const double* gradient, std::size_t count, double* out);
 
@@ -120,6 +125,8 @@ class DeviceOperator {
   const std::vector<std::uint64_t>& indices() const { return h_indices_; }
   const std::vector<double>& local_real() const { return h_local_real_; }
   const double* device_kinetic() const { return kinetic_; }
+  const double* device_potential64() const { return v64_; }
+  const float* device_potential32() const { return v32_; }
 
   // Device-pointer applies on ctx.stream; x, y are npw x columns (ld npw).
   void apply_hamiltonian(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);

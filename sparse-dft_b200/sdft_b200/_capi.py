@@ -100,6 +100,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_operator_destroy", [P])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])
     fn("sdft_b200_pbe_points", [P, P, P, SZ, P, ctypes.c_int])
     fn("sdft_b200_band_density", [P, I32, SZ, P, D, SZ, ctypes.c_double, I32, SZ, P, ctypes.c_int])
     fn("sdft_b200_onsite_density", [P, SZ, SZ, SZ, P, SZ, D, P, ctypes.c_int])

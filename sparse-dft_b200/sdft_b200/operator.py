@@ -172,6 +172,16 @@ class PlaneWaveOperator:
         C.check(self._lib.sdft_b200_apply_local(self.handle, ptr, cols, yptr, _precision(precision), mem))
         return y
 
+    def local_apply_noalloc(self, x, out, precision="fp64"):
+        """local_apply on torch CUDA blocks with all scratch in the library's static
+        device array (no allocation in the call; see sdft_b200_apply_local_noalloc)."""
+        ptr, cols, mem, _ = self._block(x)
+        optr, ocols, omem, _ = self._block(out)
+        if mem != C.DEVICE or omem != C.DEVICE or ocols != cols:
+            raise ValueError("x and out must be device blocks with the same column count")
+        C.check(self._lib.sdft_b200_apply_local_noalloc(self.handle, ptr, cols, optr, _precision(precision)))
+        return out
+
     def apply_pair(self, x, precision="fp64"):
         ptr, cols, mem, keep = self._block(x)
         hy, sy = self._like(keep), self._like(keep)

@@ -1,0 +1,75 @@
+"""sdft_b200_apply_local_noalloc: the fused local H~psi with its slab and
+twiddle tables in the library's static device array. Collected last (file
+name), and self-contained so that it also passes alone in a fresh process.
+
+Checks: the same results as sdft_b200_apply_local on two calls in a row in
+each precision, no change in free device memory across calls after the
+first (set-up) call, and a clear rejection of a block beyond the array."""
+import numpy as np
+import pytest
+
+from conftest import probe_block
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def si8_operator():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from sdft_b200 import synthetic
+    from sdft_b200.operator import Context, PlaneWaveOperator
+    ctx = Context(0)
+    op = PlaneWaveOperator(ctx, synthetic.si8())
+    yield op
+    op.close()
+    ctx.close()
+
+
+def _device_block(npw, columns, seed):
+    import torch
+    x = probe_block(npw, columns, seed)
+    return torch.from_numpy(x.T.copy()).cuda().T  # column-major, ld npw
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_noalloc_matches_regular_entry_point(si8_operator, precision):
+    import torch
+    op = si8_operator
+    for call, seed in enumerate((3, 4)):
+        x = _device_block(op.npw, 24, seed)
+        regular = op.local_apply(x, out=torch.empty((24, op.npw), dtype=torch.complex128, device="cuda").T,
+                                 precision=precision)
+        static = op.local_apply_noalloc(x, torch.empty((24, op.npw), dtype=torch.complex128, device="cuda").T,
+                                        precision=precision)
+        torch.cuda.synchronize()
+        assert torch.equal(static, regular), f"call {call}: results differ from sdft_b200_apply_local"
+
+
+def test_noalloc_calls_leave_free_memory_unchanged(si8_operator):
+    import torch
+    op = si8_operator
+    x = _device_block(op.npw, 16, 5)
+    y = torch.empty((16, op.npw), dtype=torch.complex128, device="cuda").T
+    op.local_apply_noalloc(x, y, precision="mixed")  # set-up call
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for precision in ("mixed", "fp64", "mixed"):
+        op.local_apply_noalloc(x, y, precision=precision)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+
+def test_noalloc_rejects_blocks_beyond_the_static_array(si8_operator):
+    import torch
+    from sdft_b200 import _capi
+    op = si8_operator
+    columns = 1000  # ~1 GB of FP64 slab for Si8, far above 32 MiB
+    x = torch.zeros((columns, op.npw), dtype=torch.complex128, device="cuda").T
+    y = torch.empty_like(x.T).T
+    with pytest.raises(_capi.InvalidArgument, match="static scratch; at most [0-9]+ columns"):
+        op.local_apply_noalloc(x, y, precision="fp64")
+    small = _device_block(op.npw, 2, 6)
+    out = op.local_apply_noalloc(small, torch.empty((2, op.npw), dtype=torch.complex128, device="cuda").T)
+    assert torch.isfinite(torch.view_as_real(out)).all()
