@@ -7,6 +7,8 @@
 
 #include "../../include/sdft_b200.h"
 #include "davidson.cuh"
+#include "dense.cuh"
+#include "eigensolver.cuh"
 #include "band_density.cuh"
 #include "paw_density.cuh"
 #include "operator.cuh"
@@ -468,6 +470,46 @@ sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensation* charge, 
     SDFT_CUDA(cudaMemcpyAsync(din, onsite, sizeof(C) * in_count, cudaMemcpyHostToDevice, ctx.stream));
     c.density(din, dout);
     SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * c.count(), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
+sdft_b200_status sdft_b200_rayleigh_ritz(sdft_b200_context* context, size_t n, size_t requested, const double* h,
+                                        const double* s, double* values, double* vectors, int memory) {
+  return guarded([&] {
+    require(context && h && s && values && vectors && n && requested <= n, "invalid Rayleigh-Ritz dimensions");
+    require(n <= 46340, "invalid Rayleigh-Ritz dimensions");
+    require(memory == SDFT_B200_MEMORY_HOST || memory == SDFT_B200_MEMORY_DEVICE, "memory must be host or device");
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    using C = sdft_b200::Cx<double>;
+    const int m = static_cast<int>(n);
+    const int count = requested ? static_cast<int>(requested) : m;
+    const std::size_t mm = n * n;
+    auto* buffers = static_cast<C*>(ctx.staging_in.reserve(sizeof(C) * 4 * mm));
+    C* hw = buffers;
+    C* sw = buffers + mm;
+    C* staged = buffers + 2 * mm;
+    auto* dvalues = static_cast<double*>(ctx.staging_out.reserve(sizeof(double) * n));
+    const C* hin = reinterpret_cast<const C*>(h);
+    const C* sin = reinterpret_cast<const C*>(s);
+    if (memory == SDFT_B200_MEMORY_HOST) {
+      SDFT_CUDA(cudaMemcpyAsync(staged, h, sizeof(C) * mm, cudaMemcpyHostToDevice, ctx.stream));
+      SDFT_CUDA(cudaMemcpyAsync(staged + mm, s, sizeof(C) * mm, cudaMemcpyHostToDevice, ctx.stream));
+      hin = staged;
+      sin = staged + mm;
+    }
+    sdft_b200::hermitian_from_lower(hin, m, hw, m, m, ctx.stream);
+    sdft_b200::hermitian_from_lower(sin, m, sw, m, m, ctx.stream);
+    sdft_b200::generalized_lowest(ctx.blas, ctx.solver, hw, sw, m, count, dvalues, hw, ctx.eigen, sdft_b200::rr_mode(),
+                                  ctx.stream);
+    if (memory == SDFT_B200_MEMORY_HOST) {
+      SDFT_CUDA(cudaMemcpyAsync(values, dvalues, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx.stream));
+      SDFT_CUDA(cudaMemcpyAsync(vectors, hw, sizeof(C) * n * count, cudaMemcpyDeviceToHost, ctx.stream));
+    } else {
+      SDFT_CUDA(cudaMemcpyAsync(values, dvalues, sizeof(double) * count, cudaMemcpyDeviceToDevice, ctx.stream));
+      SDFT_CUDA(cudaMemcpyAsync(vectors, hw, sizeof(C) * n * count, cudaMemcpyDeviceToDevice, ctx.stream));
+    }
     ctx.synchronize();
   });
 }

@@ -190,47 +190,9 @@ void DavidsonSolver::rayleigh_ritz() {
   auto* b = as<Cx<double>>(rr_b_, static_cast<std::size_t>(capacity_) * capacity_);
   hermitian_part(ch_, capacity_, a, m, m, st);
   hermitian_part(cs_, capacity_, b, m, m, st);
-  int lwork = 0;
-  int* info = as<int>(info_, 4);
-  // Only the lowest min(m, 2 roots) Ritz pairs are ever used (rotation and
-  // thick restart), so the subset form (default) is equivalent to the full one.
-  static const bool full = [] {
-    const char* v = std::getenv("SDFT_B200_RR");
-    if (v && std::string(v) != "subset" && std::string(v) != "full")
-      throw InvalidArgument("SDFT_B200_RR must be subset or full");
-    return v && std::string(v) == "full";
-  }();
-  const int wanted = std::min(m, 2 * roots_);
-  if (full || wanted == m) {
-    check_solver(cusolverDnZhegvd_bufferSize(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                             CUBLAS_FILL_MODE_LOWER, m, reinterpret_cast<cuDoubleComplex*>(a), m,
-                                             reinterpret_cast<cuDoubleComplex*>(b), m, w_, &lwork),
-                 "zhegvd_bufferSize");
-    auto* work = as<cuDoubleComplex>(rr_work_, static_cast<std::size_t>(lwork));
-    check_solver(cusolverDnZhegvd(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
-                                  m, reinterpret_cast<cuDoubleComplex*>(a), m, reinterpret_cast<cuDoubleComplex*>(b), m,
-                                  w_, work, lwork, info),
-                 "zhegvd");
-  } else {
-    int found = 0;
-    check_solver(cusolverDnZhegvdx_bufferSize(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                              CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_LOWER, m,
-                                              reinterpret_cast<cuDoubleComplex*>(a), m,
-                                              reinterpret_cast<cuDoubleComplex*>(b), m, 0.0, 0.0, 1, wanted, &found,
-                                              w_, &lwork),
-                 "zhegvdx_bufferSize");
-    auto* work = as<cuDoubleComplex>(rr_work_, static_cast<std::size_t>(lwork));
-    check_solver(cusolverDnZhegvdx(ctx.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
-                                   CUBLAS_FILL_MODE_LOWER, m, reinterpret_cast<cuDoubleComplex*>(a), m,
-                                   reinterpret_cast<cuDoubleComplex*>(b), m, 0.0, 0.0, 1, wanted, &found, w_, work,
-                                   lwork, info),
-                 "zhegvdx");
-    if (found != wanted) throw std::runtime_error("selected generalized Ritz failed: found " + std::to_string(found));
-  }
-  int host_info = 0;
-  SDFT_CUDA(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  // Only the lowest min(m, 2 roots) Ritz pairs are ever used (rotation and thick restart).
+  generalized_lowest(ctx.blas, ctx.solver, a, b, m, std::min(m, 2 * roots_), w_, a, eigen_, rr_mode(), st);
   values_ = download(w_, std::min(m, roots_));
-  if (host_info) throw std::runtime_error("Davidson Rayleigh-Ritz failed: info=" + std::to_string(host_info));
   ++stats_.rayleigh_ritz;
   stats_.rr_seconds += now() - t0;
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <vector>
 
+#include "eigensolver.cuh"
 #include "operator.cuh"
 
 namespace sdft_b200 {
@@ -58,6 +59,7 @@ class DavidsonSolver {
   bool exact_mode_ = true, incremental_ = true, strict_projection_ = false;
   double tolerance_ = 1e-10;
   Scratch basis_, hbasis_, sbasis_, cached_h_, cached_s_, rr_a_, rr_b_, rr_w_, rr_work_, info_;
+  EigenWorkspace eigen_;
   Scratch xs_, sxs_, hxs_, res_, block_, metric_, original_, projections_, gram_, small_, order_, select_;
   Cx<double>* v_ = nullptr;
   Cx<double>* hv_ = nullptr;

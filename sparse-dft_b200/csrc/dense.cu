@@ -68,6 +68,20 @@ __global__ void hermitian_part_kernel(const Cx<double>* __restrict__ src, long l
   }
 }
 
+__global__ void hermitian_from_lower_kernel(const Cx<double>* __restrict__ src, long long lds,
+                                            Cx<double>* __restrict__ dst, long long ldd, int m) {
+  const long long total = static_cast<long long>(m) * m;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(idx % m), j = static_cast<int>(idx / m);
+    Cx<double> v;
+    if (i > j) v = src[i + j * lds];
+    else if (i < j) v = Cx<double>{src[j + i * lds].re, -src[j + i * lds].im};
+    else v = Cx<double>{src[i + j * lds].re, 0.0};
+    dst[i + j * ldd] = v;
+  }
+}
+
 __global__ void column_norms_kernel(const Cx<double>* __restrict__ a, long long lda, int rows, double* __restrict__ out) {
   __shared__ double shared[kReduceThreads];
   const Cx<double>* col = a + blockIdx.x * lda;
@@ -219,6 +233,15 @@ __global__ void copy_block_kernel(const Cx<double>* __restrict__ src, long long 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) dst[d + i] = src[s + i];
 }
 
+__global__ void add_block_kernel(const Cx<double>* __restrict__ src, long long lds, Cx<double>* __restrict__ dst,
+                                 long long ldd, int rows) {
+  const long long s = blockIdx.y * lds, d = blockIdx.y * ldd;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const Cx<double> x = src[s + i], y = dst[d + i];
+    dst[d + i] = Cx<double>{y.re + x.re, y.im + x.im};
+  }
+}
+
 __global__ void gather_columns_kernel(const Cx<double>* __restrict__ src, long long lds, int rows,
                                       const int* __restrict__ index, Cx<double>* __restrict__ dst, long long ldd) {
   const long long s = index[blockIdx.y] * lds, d = blockIdx.y * ldd;
@@ -242,6 +265,14 @@ void hermitian_part(const Cx<double>* src, long long lds, Cx<double>* dst, long 
   hermitian_part_kernel<<<static_cast<unsigned>(std::min<long long>(ceil_div(total, 256), 4096)), 256, 0, stream>>>(
       src, lds, dst, ldd, m);
   SDFT_LAUNCH("hermitian_part_kernel");
+}
+
+void hermitian_from_lower(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int m,
+                          cudaStream_t stream) {
+  const long long total = static_cast<long long>(m) * m;
+  hermitian_from_lower_kernel<<<static_cast<unsigned>(std::min<long long>(ceil_div(total, 256), 4096)), 256, 0,
+                                stream>>>(src, lds, dst, ldd, m);
+  SDFT_LAUNCH("hermitian_from_lower_kernel");
 }
 
 void column_norms(const Cx<double>* a, long long lda, int rows, int cols, double* out, cudaStream_t stream) {
@@ -297,6 +328,13 @@ void copy_block(const Cx<double>* src, long long lds, Cx<double>* dst, long long
   if (cols <= 0 || rows <= 0) return;
   copy_block_kernel<<<column_grid(rows, cols), 256, 0, stream>>>(src, lds, dst, ldd, rows);
   SDFT_LAUNCH("copy_block_kernel");
+}
+
+void add_block(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int rows, int cols,
+               cudaStream_t stream) {
+  if (cols <= 0 || rows <= 0) return;
+  add_block_kernel<<<column_grid(rows, cols), 256, 0, stream>>>(src, lds, dst, ldd, rows);
+  SDFT_LAUNCH("add_block_kernel");
 }
 
 void gather_columns(const Cx<double>* src, long long lds, int rows, const int* index, int count, Cx<double>* dst,

@@ -7,6 +7,12 @@ namespace sdft_b200 {
 // dst(m x m, ldd) = (src + src^H)/2.
 void hermitian_part(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int m, cudaStream_t stream);
 
+// dst = the Hermitian matrix whose lower triangle is src's (LAPACK 'L'
+// convention: the upper triangle and the imaginary part of the diagonal of
+// src are not referenced).
+void hermitian_from_lower(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int m,
+                          cudaStream_t stream);
+
 // out[c] = ||A(:,c)||_2 for `cols` columns of length `rows`.
 void column_norms(const Cx<double>* a, long long lda, int rows, int cols, double* out, cudaStream_t stream);
 
@@ -42,6 +48,9 @@ void broad_seed_block(int rows, int cols, unsigned long long first_draw, const i
                       long long ld, cudaStream_t stream);
 
 // dst(rows x cols, ldd) = src(rows x cols, lds).
+// dst += src (rows x cols blocks).
+void add_block(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int rows, int cols,
+               cudaStream_t stream);
 void copy_block(const Cx<double>* src, long long lds, Cx<double>* dst, long long ldd, int rows, int cols,
                 cudaStream_t stream);
 

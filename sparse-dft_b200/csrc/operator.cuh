@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "eigensolver.cuh"
 #include "gemm.cuh"
 #include "local_hamiltonian.cuh"
 #include "umma_gemm.cuh"
@@ -57,6 +58,7 @@ struct Context {
   TensorCoreWorkspace tc;
   AcceleratorCache accel;
   DensityCache density;
+  EigenWorkspace eigen;
   explicit Context(int device, cudaStream_t stream);
   ~Context();
   Context(const Context&) = delete;

@@ -272,39 +272,55 @@ __device__ __forceinline__ void split3(double x, std::uint16_t t[3]) {
   t[2] = __bfloat16_as_ushort(h2);
 }
 
+// Stores P (lo, hi) uint16 pairs at dst with 8-byte stores when P is even
+// (dst is then 8-byte aligned: rows are 128-byte aligned and each value
+// takes 4P bytes), else 4-byte stores.
+template <int P>
+__device__ __forceinline__ void store_pairs(std::uint16_t* dst, const std::uint32_t (&pairs)[P]) {
+  if constexpr (P % 2 == 0) {
+    auto* d = reinterpret_cast<uint2*>(dst);
+#pragma unroll
+    for (int q = 0; q < P / 2; ++q) d[q] = make_uint2(pairs[2 * q], pairs[2 * q + 1]);
+  } else {
+    auto* d = reinterpret_cast<std::uint32_t*>(dst);
+#pragma unroll
+    for (int q = 0; q < P; ++q) d[q] = pairs[q];
+  }
+}
+
+__device__ __forceinline__ std::uint32_t pair(std::uint16_t lo, std::uint16_t hi) {
+  return static_cast<std::uint32_t>(lo) | (static_cast<std::uint32_t>(hi) << 16);
+}
+
 // Writes the 2P A-side entries of one complex value.
 template <int P>
 __device__ __forceinline__ void write_a(std::uint16_t* dst, Cx<double> v) {
   std::uint16_t re[3], im[3];
   split3(v.re, re);
   split3(v.im, im);
+  std::uint32_t pairs[P];
 #pragma unroll
-  for (int p = 0; p < P; ++p) {
-    dst[2 * p] = re[term_a(p)];
-    dst[2 * p + 1] = im[term_a(p)];
-  }
+  for (int p = 0; p < P; ++p) pairs[p] = pair(re[term_a(p)], im[term_a(p)]);
+  store_pairs<P>(dst, pairs);
 }
 
+// One row i of A per blockIdx.y; threads stride over k.
 template <int P, bool CONJ_T>
 __global__ void pack_a_direct_kernel(const Cx<double>* __restrict__ src, long long lds, int rows, int k,
                                      std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
   // CONJ_T: A[i,k] = conj(src[k + i*lds]) (k contiguous in the source).
-  const long long total = static_cast<long long>(rows) * k;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long i = idx / k, kk = idx % k;
-    Cx<double> v = src[kk + i * lds];
+  const int i = blockIdx.y;
+  const Cx<double>* in = src + static_cast<long long>(i) * lds;
+  std::uint16_t* row = out + static_cast<long long>(i) * ldo;
+  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
+    Cx<double> v = in[kk];
     if (CONJ_T) v.im = -v.im;
-    write_a<P>(out + i * ldo + kk * 2 * P, v);
+    write_a<P>(row + static_cast<long long>(kk) * 2 * P, v);
   }
-  // zero padding [2Pk, kexp) of every row
-  const long long pad = kexp - 2LL * P * k;
-  const long long ptotal = static_cast<long long>(rows) * pad;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < ptotal;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long i = idx / pad, q = idx % pad;
-    out[i * ldo + 2LL * P * k + q] = 0;
-  }
+  // zero padding [2Pk, kexp) of the row
+  for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
+       q += static_cast<long long>(gridDim.x) * blockDim.x)
+    row[q] = 0;
 }
 
 // A[i,k] = src[i + k*lds] (rows contiguous): 32x32 shared-memory transpose.
@@ -334,33 +350,41 @@ __global__ void zero_pad_kernel(std::uint16_t* __restrict__ out, long long ldo, 
     out[(idx / pad) * ldo + from + idx % pad] = 0;
 }
 
+// One source column j per blockIdx.y (two expanded rows); threads stride over k.
 template <int P>
 __global__ void pack_b_kernel(const Cx<double>* __restrict__ src, long long ldb, int k, int n,
                               std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
-  const long long total = static_cast<long long>(n) * k;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long j = idx / k, kk = idx % k;
-    const Cx<double> v = src[kk + j * ldb];
+  const int j = blockIdx.y;
+  const Cx<double>* in = src + static_cast<long long>(j) * ldb;
+  std::uint16_t* row0 = out + (2LL * j) * ldo;
+  std::uint16_t* row1 = row0 + ldo;
+  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
+    const Cx<double> v = in[kk];
     std::uint16_t re[3], im[3];
     split3(v.re, re);
     split3(v.im, im);
-    std::uint16_t* row0 = out + (2 * j) * ldo + kk * 2 * P;
-    std::uint16_t* row1 = row0 + ldo;
+    std::uint32_t p0[P], p1[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
       const int t = term_b(p);
-      row0[2 * p] = re[t];
-      row0[2 * p + 1] = im[t] ^ 0x8000u;  // -Im (sign flip is exact)
-      row1[2 * p] = im[t];
-      row1[2 * p + 1] = re[t];
+      p0[p] = pair(re[t], im[t] ^ 0x8000u);  // [Re, -Im] (sign flip is exact)
+      p1[p] = pair(im[t], re[t]);            // [Im, Re]
     }
+    store_pairs<P>(row0 + static_cast<long long>(kk) * 2 * P, p0);
+    store_pairs<P>(row1 + static_cast<long long>(kk) * 2 * P, p1);
   }
-  const long long pad = kexp - 2LL * P * k;
-  const long long ptotal = 2LL * n * pad;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < ptotal;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x)
-    out[(idx / pad) * ldo + 2LL * P * k + idx % pad] = 0;
+  for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    row0[q] = 0;
+    row1[q] = 0;
+  }
+}
+
+// Blocks along a row of `length` entries when `rows` rows run side by side:
+// enough CTAs in total for ~16 per SM, at least one per row.
+unsigned row_blocks(long long length, int rows) {
+  const long long per_row = std::max<long long>(1, (148LL * 16 + rows - 1) / rows);
+  return static_cast<unsigned>(std::max<long long>(1, std::min<long long>(per_row, (length + 255) / 256)));
 }
 
 unsigned grid_for(long long total) {
@@ -425,11 +449,12 @@ void pack_a(Op aop, const Cx<double>* src, long long lds, int rows, int k, Split
             long long ldo, cudaStream_t stream) {
   const long long kexp = expanded_k(k, split);
   if (aop == Op::C) {
-    const long long total = static_cast<long long>(rows) * std::max<long long>(k, kexp - 2LL * split_terms(split) * k);
+    if (rows > 65535) throw InvalidArgument("packed operand has more than 65535 rows");
+    const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), rows), rows);
     if (split == Split::BF16x3)
-      pack_a_direct_kernel<3, true><<<grid_for(total), 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
+      pack_a_direct_kernel<3, true><<<grid, 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
     else
-      pack_a_direct_kernel<6, true><<<grid_for(total), 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
+      pack_a_direct_kernel<6, true><<<grid, 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
     SDFT_LAUNCH("pack_a_direct_kernel");
     return;
   }
@@ -462,9 +487,10 @@ void pack_a_columns(const Cx<double>* src, long long lds, int rows, int first, i
 void pack_b(const Cx<double>* src, long long ldb, int k, int n, Split split, std::uint16_t* out, long long ldo,
             cudaStream_t stream) {
   const long long kexp = expanded_k(k, split);
-  const long long total = static_cast<long long>(n) * std::max<long long>(k, 2 * (kexp - 2LL * split_terms(split) * k));
-  if (split == Split::BF16x3) pack_b_kernel<3><<<grid_for(total), 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
-  else pack_b_kernel<6><<<grid_for(total), 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
+  if (n > 65535) throw InvalidArgument("packed operand has more than 65535 columns");
+  const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), n), n);
+  if (split == Split::BF16x3) pack_b_kernel<3><<<grid, 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
+  else pack_b_kernel<6><<<grid, 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
   SDFT_LAUNCH("pack_b_kernel");
 }
 

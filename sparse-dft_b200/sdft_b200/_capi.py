@@ -102,6 +102,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])
     fn("sdft_b200_pbe_points", [P, P, P, SZ, P, ctypes.c_int])
+    fn("sdft_b200_rayleigh_ritz", [P, SZ, SZ, P, P, P, P, ctypes.c_int])
     fn("sdft_b200_band_density", [P, I32, SZ, P, D, SZ, ctypes.c_double, I32, SZ, P, ctypes.c_int])
     fn("sdft_b200_onsite_density", [P, SZ, SZ, SZ, P, SZ, D, P, ctypes.c_int])
     fn("sdft_b200_compensation_create", [P, D, SZ, D, I32, SZ, ctypes.c_int, SZ, D, D, SZ, D, ctypes.POINTER(P)])

@@ -244,3 +244,22 @@ def complex_gemm(context: Context, a, b, adjoint_a: bool = False, precision="fp6
                                        a.shape[0], ctypes.c_void_p(b.ctypes.data), b.shape[0],
                                        ctypes.c_void_p(out.ctypes.data), m, _precision(precision), int(add), C.HOST))
     return out
+
+
+def rayleigh_ritz(context: Context, h, s, requested: int = 0):
+    """Lowest `requested` (0 = all) solutions of H y = e S y for n x n Hermitian
+    H and S (lower triangles referenced), the reference's rayleigh_ritz. Returns
+    (values, vectors) with S-orthonormal vector columns (host arrays)."""
+    lib = C.library()
+    h = np.asfortranarray(h, dtype=np.complex128)
+    s = np.asfortranarray(s, dtype=np.complex128)
+    n = h.shape[0]
+    if h.shape != (n, n) or s.shape != (n, n):
+        raise ValueError("h and s must be square and of the same order")
+    count = requested or n
+    values = np.zeros(count)
+    vectors = np.zeros((n, count), dtype=np.complex128, order="F")
+    C.check(lib.sdft_b200_rayleigh_ritz(context.handle, n, requested, ctypes.c_void_p(h.ctypes.data),
+                                        ctypes.c_void_p(s.ctypes.data), ctypes.c_void_p(values.ctypes.data),
+                                        ctypes.c_void_p(vectors.ctypes.data), C.HOST))
+    return values, vectors
