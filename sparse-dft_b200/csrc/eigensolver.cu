@@ -4,20 +4,24 @@
 // 1. tridiagonalize_kernel: one cooperative launch, one CTA per SM, columns
 //    distributed cyclically and held in shared memory. Step j of the
 //    Householder reduction (LAPACK zhetd2, lower, H_j = I - tau v v^H with
-//    v[j+1] = 1) needs one grid-wide barrier: every CTA recomputes the
-//    reflector from the published column j (plus the previous rank-2 update)
-//    redundantly, computes p = tau A22 v for its own columns, publishes p and
-//    its share of p^H v, and after the barrier forms w = p - tau/2 (p^H v) v
-//    and updates its columns. Exchange buffers are double-buffered by step
-//    parity. The barrier is a counting barrier with a time limit: on expiry
-//    an error word is set and every CTA returns.
-// 2. bisect_kernel: one warp per wanted eigenvalue, 32-point multisection on
-//    Sturm counts of the tridiagonal matrix.
+//    v[j+1] = 1) needs one grid-wide barrier: after it every CTA forms
+//    w = p - tau/2 (p^H v) v from the published p and shares of p^H v,
+//    recomputes the next reflector redundantly from the published next column
+//    (plus this rank-2 update), then in one pass over its own columns applies
+//    the update and accumulates p = tau A22 v for the next reflector, and
+//    publishes p, its share of p^H v and the column after next. Exchange
+//    buffers are double-buffered by step parity. The barrier is a counting
+//    barrier with a time limit: on expiry an error word is set and every CTA
+//    returns.
+// 2. bisect_kernel: one warp per wanted eigenvalue, 64-point multisection on
+//    division-free Sturm counts of the tridiagonal matrix.
 // 3. inverse_iteration_kernel: one thread per cluster of eigenvalues closer
-//    than 1e-9 of the matrix scale; LU with partial pivoting of T - lambda I,
-//    three solves, Gram-Schmidt against earlier members of the cluster.
-// 4. backtransform_kernel: the reflectors applied to the tridiagonal
-//    eigenvectors in reverse order, four columns per CTA in shared memory.
+//    than 1e-9 of the matrix scale, factors in shared memory; LU with partial
+//    pivoting of T - lambda I, two solves, Gram-Schmidt against earlier
+//    members of the cluster.
+// 4. reflector_blocks_kernel + backtransform_kernel: the reflectors in
+//    blocks of 32 as I - V T V^H (compact WY), applied to the tridiagonal
+//    eigenvectors from the last block to the first.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -34,8 +38,11 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxCpc = 12;
+constexpr int kMaxCpc = 10;
+constexpr int kRowsPerThread = 5;  // rows per thread held in registers: m <= 1280
 constexpr int kBackColumns = 4;
+constexpr int kReflectorBlock = 32;
+constexpr int kInvitThreads = 4;
 constexpr unsigned long long kWaitNs = 2000000000ULL;
 constexpr double kClusterTolerance = 1e-9;
 
@@ -136,166 +143,282 @@ struct TridiagArgs {
   unsigned int* arrive;
 };
 
+struct StepScalars {
+  Cx<double> tau, scale, alpha_in;
+  double beta, diag;
+  int trivial;
+};
+
+// Rows r = tid + kThreads k of the reflector and rank-2 vectors live in
+// registers; own columns c = cta + G s in shared memory. Step j+1's reflector
+// is formed before step j's rank-2 update, so the update of each own column
+// and its product with the next reflector share one pass.
 __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int R = kRowsPerThread;
   const int m = t.m, G = t.grid, cpc = t.cpc, cta = blockIdx.x, tid = threadIdx.x;
   Cx<double>* cols = reinterpret_cast<Cx<double>*>(smem_raw);
-  Cx<double>* v = cols + static_cast<long long>(cpc) * m;
-  Cx<double>* w = v + m;
-  Cx<double>* red = w + m;             // kWarps * kMaxCpc
-  Cx<double>* res = red + kWarps * kMaxCpc;  // kMaxCpc
-  double* rred = reinterpret_cast<double*>(res + kMaxCpc);  // kWarps
+  Cx<double>* red = cols + static_cast<long long>(cpc) * m;  // kWarps * kMaxCpc
+  Cx<double>* res = red + kWarps * kMaxCpc;                   // kMaxCpc
+  Cx<double>* colv = res + kMaxCpc;                           // v at own column indices
+  Cx<double>* colw = colv + kMaxCpc;                          // w at own column indices
+  double* rred = reinterpret_cast<double*>(colw + kMaxCpc);   // kWarps
   __shared__ int ok;
-  __shared__ Cx<double> shared_tau, shared_scale;
-  __shared__ double shared_beta;
-  __shared__ int shared_trivial;
+  __shared__ StepScalars sc;
+  __shared__ Cx<double> head_v, head_w;  // v[j+1], w[j+1]
 
+  int slot_of_row[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int r = tid + k * kThreads;
+    slot_of_row[k] = (r < m && r >= cta && (r - cta) % G == 0) ? (r - cta) / G : -1;
+  }
   for (int s = 0; s < cpc; ++s) {
     const int c = cta + s * G;
     if (c < m)
       for (int r = tid; r < m; r += kThreads) cols[static_cast<long long>(s) * m + r] = t.a[r + static_cast<long long>(c) * m];
   }
-  __syncthreads();
 
-  for (int j = 0; j < m - 1; ++j) {
-    // P1: column j with updates 0..j-1 into w (rows j..m-1); reflector j.
-    Cx<double> vj{0.0, 0.0}, wj{0.0, 0.0};
-    if (j > 0) {
-      vj = v[j];
-      wj = w[j];
-    }
-    __syncthreads();
+  Cx<double> v[R], w[R], vn[R], col[R];
+
+  // Reflector of column jc from col[] (rows >= jc): vn[] for rows >= jc+1,
+  // the shared scalars, and CTA 0's outputs.
+  auto reflect = [&](int jc) {
     double part = 0.0;
-    const Cx<double>* src = t.colbuf + static_cast<long long>(j & 1) * m;
-    for (int r = j + tid; r < m; r += kThreads) {
-      Cx<double> c;
-      if (j == 0) {
-        c = t.a[r];
-      } else {
-        const double2 q = __ldcg(reinterpret_cast<const double2*>(src + r));
-        c = Cx<double>{q.x, q.y};
-        c = csub(c, cadd(cmulz(v[r], cconj(wj)), cmulz(w[r], cconj(vj))));
-      }
-      w[r] = c;
-      if (r >= j + 2) part += c.re * c.re + c.im * c.im;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int r = tid + k * kThreads;
+      if (r < m && r >= jc + 2) part += col[k].re * col[k].re + col[k].im * col[k].im;
+      if (r == jc + 1) sc.alpha_in = col[k];
+      if (r == jc) sc.diag = col[k].re;
     }
     const double xnorm2 = block_sum_real(part, rred);
     if (tid == 0) {
-      const Cx<double> alpha = w[j + 1];
+      const Cx<double> alpha = sc.alpha_in;
       if (xnorm2 == 0.0 && alpha.im == 0.0) {
-        shared_trivial = 1;
-        shared_tau = Cx<double>{0.0, 0.0};
-        shared_beta = alpha.re;
-        shared_scale = Cx<double>{0.0, 0.0};
+        sc.trivial = 1;
+        sc.tau = Cx<double>{0.0, 0.0};
+        sc.beta = alpha.re;
+        sc.scale = Cx<double>{0.0, 0.0};
       } else {
         const double beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + xnorm2), alpha.re);
-        shared_trivial = 0;
-        shared_tau = Cx<double>{(beta - alpha.re) / beta, -alpha.im / beta};
-        shared_beta = beta;
+        sc.trivial = 0;
+        sc.tau = Cx<double>{(beta - alpha.re) / beta, -alpha.im / beta};
+        sc.beta = beta;
         // 1 / (alpha - beta)
         const double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
-        shared_scale = Cx<double>{dr / den, -di / den};
+        sc.scale = Cx<double>{dr / den, -di / den};
       }
       if (cta == 0) {
-        t.d[j] = w[j].re;
-        t.e[j] = shared_beta;
-        t.tau[j] = shared_tau;
+        t.d[jc] = sc.diag;
+        t.e[jc] = sc.beta;
+        t.tau[jc] = sc.tau;
       }
     }
     __syncthreads();
-    const Cx<double> tau = shared_tau, scale = shared_scale;
-    const int trivial = shared_trivial;
-    for (int r = j + 1 + tid; r < m; r += kThreads) {
-      const Cx<double> vr = r == j + 1 ? Cx<double>{1.0, 0.0} : (trivial ? Cx<double>{0.0, 0.0} : cmulz(w[r], scale));
-      v[r] = vr;
-      if (cta == 0) t.reflectors[r + static_cast<long long>(j) * m] = vr;
+    const Cx<double> scale = sc.scale;
+    const int trivial = sc.trivial;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int r = tid + k * kThreads;
+      Cx<double> vr{0.0, 0.0};
+      if (r == jc + 1) vr = Cx<double>{1.0, 0.0};
+      else if (r > jc + 1 && r < m && !trivial) vr = cmulz(col[k], scale);
+      vn[k] = vr;
+      if (cta == 0 && r > jc && r < m) t.reflectors[r + static_cast<long long>(jc) * m] = vr;
     }
-    __syncthreads();
+  };
 
-    // P2: p[c] = tau sum_r conj(A[r,c]) v[r] for own columns c >= j+1.
-    Cx<double> acc[kMaxCpc];
-#pragma unroll
-    for (int s = 0; s < kMaxCpc; ++s) acc[s] = Cx<double>{0.0, 0.0};
-    if (!trivial) {
-      for (int r = j + 1 + tid; r < m; r += kThreads) {
-        const Cx<double> vr = v[r];
-#pragma unroll
-        for (int s = 0; s < kMaxCpc; ++s) {
-          const int c = cta + s * G;
-          if (s < cpc && c > j && c < m) acc[s] = cadd(acc[s], cdot1(cols[static_cast<long long>(s) * m + r], vr));
-        }
-      }
-    }
+  // p for own columns c > jc and the CTA share of p^H v (v at own columns in colv).
+  auto publish = [&](int jc, Cx<double> (&acc)[kMaxCpc]) {
     block_sum<kMaxCpc>(acc, cpc, red, res);
-    if (tid == 0) {
-      Cx<double> dot{0.0, 0.0};
-      for (int s = 0; s < cpc; ++s) {
-        const int c = cta + s * G;
-        if (c > j && c < m) {
-          const Cx<double> p = cmulz(tau, res[s]);
-          t.pbuf[static_cast<long long>(j & 1) * m + c] = p;
-          dot = cadd(dot, cdot1(p, v[c]));
-        }
-      }
-      t.dotbuf[static_cast<long long>(j & 1) * G + cta] = dot;
-    }
-    // Publish column j+1 (updates 0..j-1) for the next step.
-    if ((j + 1) % G == cta) {
-      const int s1 = (j + 1) / G;
-      Cx<double>* dst = t.colbuf + static_cast<long long>((j + 1) & 1) * m;
-      for (int r = j + 1 + tid; r < m; r += kThreads) dst[r] = cols[static_cast<long long>(s1) * m + r];
-    }
-    __threadfence();
-    if (!grid_barrier(t.arrive, static_cast<unsigned int>(G) * static_cast<unsigned int>(j + 1), &ok)) return;
-
-    // P3: w = p - tau/2 (p^H v) v.
     if (tid < 32) {
-      Cx<double> s{0.0, 0.0};
-      const double* db = reinterpret_cast<const double*>(t.dotbuf + static_cast<long long>(j & 1) * G);
-      for (int g = tid; g < G; g += 32) s = cadd(s, Cx<double>{__ldcg(db + 2 * g), __ldcg(db + 2 * g + 1)});
+      Cx<double> dot{0.0, 0.0};
+      const int c = cta + tid * G;
+      if (tid < cpc && c > jc && c < m) {
+        const Cx<double> p = cmulz(sc.tau, res[tid]);
+        t.pbuf[static_cast<long long>(jc & 1) * m + c] = p;
+        dot = cdot1(p, colv[tid]);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
-        s.re += __shfl_xor_sync(0xffffffffu, s.re, o);
-        s.im += __shfl_xor_sync(0xffffffffu, s.im, o);
+        dot.re += __shfl_xor_sync(0xffffffffu, dot.re, o);
+        dot.im += __shfl_xor_sync(0xffffffffu, dot.im, o);
       }
-      if (tid == 0) res[0] = cmulz(Cx<double>{-0.5 * tau.re, -0.5 * tau.im}, s);
+      if (tid == 0) t.dotbuf[static_cast<long long>(jc & 1) * G + cta] = dot;
+    }
+  };
+
+  // Step 0: reflector of column 0, p_0 over own columns, column 1 published.
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    const int r = tid + k * kThreads;
+    col[k] = r < m ? t.a[r] : Cx<double>{0.0, 0.0};
+  }
+  __syncthreads();
+  reflect(0);
+#pragma unroll
+  for (int k = 0; k < R; ++k) {
+    v[k] = vn[k];
+    if (slot_of_row[k] >= 0) colv[slot_of_row[k]] = v[k];
+  }
+  {
+    Cx<double> acc[kMaxCpc];
+#pragma unroll
+    for (int q = 0; q < kMaxCpc; ++q) acc[q] = Cx<double>{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < kMaxCpc; ++q) {
+      const int c = cta + q * G;
+      if (q >= cpc || c < 1 || c >= m) continue;
+      const Cx<double>* a = cols + static_cast<long long>(q) * m;
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int r = tid + k * kThreads;
+        if (r >= 1 && r < m) acc[q] = cadd(acc[q], cdot1(a[r], v[k]));
+      }
+    }
+    __syncthreads();  // colv visible
+    publish(0, acc);
+    if (1 % G == cta)
+      for (int r = 1 + tid; r < m; r += kThreads) t.colbuf[m + r] = cols[static_cast<long long>(1 / G) * m + r];
+  }
+  if (!grid_barrier(t.arrive, static_cast<unsigned int>(G), &ok)) return;
+
+  for (int j = 0; j < m - 1; ++j) {
+    const bool last = j == m - 2;
+    // w = p - tau/2 (p^H v) v; column j+1 (updates 0..j-1) prefetched.
+    const double2* pb = reinterpret_cast<const double2*>(t.pbuf + static_cast<long long>(j & 1) * m);
+    const double2* cb = reinterpret_cast<const double2*>(t.colbuf + static_cast<long long>((j + 1) & 1) * m);
+    const int trivial = sc.trivial;
+    const Cx<double> tau = sc.tau;
+    Cx<double> pv[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int r = tid + k * kThreads;
+      pv[k] = Cx<double>{0.0, 0.0};
+      col[k] = Cx<double>{0.0, 0.0};
+      if (r > j && r < m) {
+        if (!trivial) {
+          const double2 q = __ldcg(pb + r);
+          pv[k] = Cx<double>{q.x, q.y};
+        }
+        if (!last) {
+          const double2 q = __ldcg(cb + r);
+          col[k] = Cx<double>{q.x, q.y};
+        }
+      }
+    }
+    if (tid < 32) {
+      Cx<double> sum{0.0, 0.0};
+      if (!trivial) {
+        const double2* db = reinterpret_cast<const double2*>(t.dotbuf + static_cast<long long>(j & 1) * G);
+        for (int g = tid; g < G; g += 32) {
+          const double2 q = __ldcg(db + g);
+          sum = cadd(sum, Cx<double>{q.x, q.y});
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sum.re += __shfl_xor_sync(0xffffffffu, sum.re, o);
+          sum.im += __shfl_xor_sync(0xffffffffu, sum.im, o);
+        }
+      }
+      if (tid == 0) res[0] = cmulz(Cx<double>{-0.5 * tau.re, -0.5 * tau.im}, sum);
     }
     __syncthreads();
     const Cx<double> alpha = res[0];
-    const double* pb = reinterpret_cast<const double*>(t.pbuf + static_cast<long long>(j & 1) * m);
-    for (int r = j + 1 + tid; r < m; r += kThreads) {
-      const Cx<double> p = trivial ? Cx<double>{0.0, 0.0} : Cx<double>{__ldcg(pb + 2 * r), __ldcg(pb + 2 * r + 1)};
-      w[r] = cadd(p, cmulz(alpha, v[r]));
-    }
-    __syncthreads();
-
-    // P4: own columns -= v w^H + w v^H.
-    if (!trivial) {
-      for (int s = 0; s < cpc; ++s) {
-        const int c = cta + s * G;
-        if (c <= j || c >= m) continue;
-        const Cx<double> wc = cconj(w[c]), vc = cconj(v[c]);
-        Cx<double>* col = cols + static_cast<long long>(s) * m;
-        for (int r = j + 1 + tid; r < m; r += kThreads) col[r] = csub(col[r], cadd(cmulz(v[r], wc), cmulz(w[r], vc)));
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int r = tid + k * kThreads;
+      w[k] = (r > j && r < m) ? cadd(pv[k], cmulz(alpha, v[k])) : Cx<double>{0.0, 0.0};
+      if (slot_of_row[k] >= 0) colw[slot_of_row[k]] = w[k];
+      if (r == j + 1) {
+        head_v = v[k];
+        head_w = w[k];
       }
     }
     __syncthreads();
+
+    // Step j+1's reflector from column j+1 with update j applied.
+    if (!last) {
+      const Cx<double> hv = cconj(head_v), hw = cconj(head_w);
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int r = tid + k * kThreads;
+        if (r > j && r < m) col[k] = csub(col[k], cadd(cmulz(v[k], hw), cmulz(w[k], hv)));
+      }
+      reflect(j + 1);
+    }
+
+    // Update j on own columns c > j; p_{j+1} partial sums over rows/columns > j+1.
+    Cx<double> acc[kMaxCpc];
+#pragma unroll
+    for (int q = 0; q < kMaxCpc; ++q) acc[q] = Cx<double>{0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < kMaxCpc; ++q) {
+      const int c = cta + q * G;
+      if (q >= cpc || c <= j || c >= m) continue;
+      const Cx<double> wc = cconj(colw[q]), vc = cconj(colv[q]);
+      Cx<double>* a = cols + static_cast<long long>(q) * m;
+      const bool dot_column = !last && c > j + 1;
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int r = tid + k * kThreads;
+        if (r > j && r < m) {
+          Cx<double> x = a[r];
+          if (!trivial) {
+            x = csub(x, cadd(cmulz(v[k], wc), cmulz(w[k], vc)));
+            a[r] = x;
+          }
+          if (dot_column && r > j + 1) acc[q] = cadd(acc[q], cdot1(x, vn[k]));
+        }
+      }
+    }
+    if (last) break;
+    __syncthreads();  // every thread is done with colv/colw of step j
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      v[k] = vn[k];
+      if (slot_of_row[k] >= 0) colv[slot_of_row[k]] = v[k];
+    }
+    __syncthreads();
+    publish(j + 1, acc);
+    // Column j+2 (updates 0..j) for step j+2.
+    if (j + 2 < m && (j + 2) % G == cta) {
+      const long long slot = (j + 2) / G;
+      Cx<double>* dst = t.colbuf + static_cast<long long>((j + 2) & 1) * m;
+      for (int r = j + 2 + tid; r < m; r += kThreads) dst[r] = cols[slot * m + r];
+    }
+    if (!grid_barrier(t.arrive, static_cast<unsigned int>(G) * static_cast<unsigned int>(j + 2), &ok)) return;
   }
+  __syncthreads();
   if ((m - 1) % G == cta && tid == 0) t.d[m - 1] = cols[static_cast<long long>((m - 1) / G) * m + m - 1].re;
 }
 
+// Number of eigenvalues of the tridiagonal (d, e) below x: sign changes of
+// the Sturm sequence p_0 = 1, p_1 = d_0 - x, p_i = (d_{i-1} - x) p_{i-1} -
+// e_{i-2}^2 p_{i-2}, kept in range by exact power-of-two rescaling. A p_i
+// below pivmin |p_{i-1}| counts as a sign change (the q = -pivmin convention
+// of the quotient form q_i = p_i / p_{i-1}).
 __device__ int sturm_count(const double* d, const double* e2, int m, double x, double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) <= pivmin) q = -pivmin;
-  int count = q < 0.0;
+  double p0 = 1.0, p1 = d[0] - x;
+  if (fabs(p1) <= pivmin) p1 = -pivmin;
+  int count = p1 < 0.0;
   for (int i = 1; i < m; ++i) {
-    q = (d[i] - x) - e2[i - 1] / q;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    count += q < 0.0;
+    double p2 = fma(d[i] - x, p1, -e2[i - 1] * p0);
+    if (fabs(p2) <= pivmin * fabs(p1)) p2 = -pivmin * p1;
+    count += (p2 < 0.0) != (p1 < 0.0);
+    p0 = p1;
+    p1 = p2;
+    // Exact rescaling by 2^-400 / 2^400.
+    const double mag = fabs(p1);
+    const double f = mag > 0x1p+400 ? 0x1p-400 : (mag < 0x1p-400 ? 0x1p+400 : 1.0);
+    p0 *= f;
+    p1 *= f;
   }
   return count;
 }
 
+// One warp per wanted eigenvalue; 32 x P points per round (P per lane).
 __global__ void bisect_kernel(const double* __restrict__ d, const double* __restrict__ e, int m, int wanted,
                               double* __restrict__ values) {
   extern __shared__ double sm[];
@@ -309,7 +432,6 @@ __global__ void bisect_kernel(const double* __restrict__ d, const double* __rest
   const int lane = threadIdx.x & 31;
   const int k = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (k >= wanted) return;
-  // Gershgorin bounds and pivot guard (the same in every warp).
   double lo = DBL_MAX, hi = -DBL_MAX, emax = 0.0;
   for (int i = lane; i < m; i += 32) {
     const double left = i > 0 ? fabs(e[i - 1]) : 0.0, right = i + 1 < m ? fabs(e[i]) : 0.0;
@@ -327,17 +449,23 @@ __global__ void bisect_kernel(const double* __restrict__ d, const double* __rest
   const double pad = 4.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin;
   lo -= pad;
   hi += pad;
+  constexpr int P = 2;
   for (int round = 0; round < 64; ++round) {
     const double width = hi - lo;
     if (width <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) || width <= pivmin) break;
-    const double x = lo + (lane + 1) * (width / 33.0);
-    const int count = sturm_count(sd, se2, m, x, pivmin);
-    const unsigned above = __ballot_sync(0xffffffffu, count > k);
-    const int first = above ? __ffs(above) - 1 : 32;
-    const double x_prev = __shfl_sync(0xffffffffu, x, first > 0 ? first - 1 : 0);
-    const double x_first = __shfl_sync(0xffffffffu, x, first < 32 ? first : 31);
-    const double new_lo = first == 0 ? lo : x_prev;
-    const double new_hi = first == 32 ? hi : x_first;
+    const double step = width / (32 * P + 1);
+    // point q of lane l is lo + (q * 32 + l + 1) step: increasing over (q, l).
+    unsigned masks[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q)
+      masks[q] = __ballot_sync(0xffffffffu, sturm_count(sd, se2, m, lo + (q * 32 + lane + 1) * step, pivmin) > k);
+    int above = -1;  // first point index with count > k
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q)
+      if (masks[q]) above = q * 32 + __ffs(masks[q]) - 1;
+    double new_lo = lo, new_hi = hi;
+    if (above >= 0) new_hi = lo + (above + 1) * step;
+    if (above != 0) new_lo = lo + (above < 0 ? 32 * P : above) * step;
     if (new_lo == lo && new_hi == hi) break;
     lo = new_lo;
     hi = new_hi;
@@ -354,11 +482,24 @@ __device__ __forceinline__ double start_entry(int k, int i) {
   return static_cast<double>(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
-// Work layout: field f, row i, vector q at ((f * m + i) * wanted + q).
+// One thread per cluster start, kInvitThreads threads per CTA, each with its
+// LU factors and vector in shared memory: reciprocal pivots, the two U
+// superdiagonals, multipliers, z and pivot flags (bytes). Members of a
+// cluster after the first are orthogonalised against the earlier ones
+// (stored in zt) after each solve.
 __global__ void inverse_iteration_kernel(const double* __restrict__ d, const double* __restrict__ e, int m, int wanted,
-                                         const double* __restrict__ values, double* __restrict__ work,
-                                         double* __restrict__ zt) {
+                                         const double* __restrict__ values, double* __restrict__ zt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double* base = reinterpret_cast<double*>(smem_raw) + static_cast<long long>(threadIdx.x) * 5 * m;
+  double* rinv = base;
+  double* u1 = base + m;
+  double* u2 = base + 2 * m;
+  double* mult = base + 3 * m;
+  double* z = base + 4 * m;
+  unsigned char* piv =
+      reinterpret_cast<unsigned char*>(reinterpret_cast<double*>(smem_raw) + static_cast<long long>(blockDim.x) * 5 * m) +
+      static_cast<long long>(threadIdx.x) * m;
   if (k >= wanted) return;
   double norm = 0.0;
   for (int i = 0; i < m; ++i) norm = fmax(norm, fabs(d[i]) + (i + 1 < m ? fabs(e[i]) : 0.0));
@@ -370,108 +511,222 @@ __global__ void inverse_iteration_kernel(const double* __restrict__ d, const dou
   const long long W = wanted;
   for (int q = k; q <= end; ++q) {
     const double lam = values[q];
-    double* u0 = work + (0LL * m) * W + q;
-    double* u1 = work + (1LL * m) * W + q;
-    double* u2 = work + (2LL * m) * W + q;
-    double* mult = work + (3LL * m) * W + q;
-    double* piv = work + (4LL * m) * W + q;
     // LU of T - lam I with partial pivoting (rows i, i+1 swapped when |sub| wins).
     double cur_d = d[0] - lam, cur_u = m > 1 ? e[0] : 0.0;
     for (int i = 0; i + 1 < m; ++i) {
       const double nd = d[i + 1] - lam, nu = i + 2 < m ? e[i + 1] : 0.0, l = e[i];
       if (fabs(cur_d) >= fabs(l)) {
         if (fabs(cur_d) < tiny) cur_d = copysign(tiny, cur_d == 0.0 ? 1.0 : cur_d);
-        const double mu = l / cur_d;
-        u0[i * W] = cur_d;
-        u1[i * W] = cur_u;
-        u2[i * W] = 0.0;
-        mult[i * W] = mu;
-        piv[i * W] = 0.0;
-        cur_d = nd - mu * cur_u;
+        const double r = 1.0 / cur_d;
+        rinv[i] = r;
+        u1[i] = cur_u;
+        u2[i] = 0.0;
+        mult[i] = l * r;
+        piv[i] = 0;
+        cur_d = nd - mult[i] * cur_u;
         cur_u = nu;
       } else {
         const double mu = cur_d / l;
-        u0[i * W] = l;
-        u1[i * W] = nd;
-        u2[i * W] = nu;
-        mult[i * W] = mu;
-        piv[i * W] = 1.0;
+        rinv[i] = 1.0 / l;
+        u1[i] = nd;
+        u2[i] = nu;
+        mult[i] = mu;
+        piv[i] = 1;
         cur_d = cur_u - mu * nd;
         cur_u = -mu * nu;
       }
     }
     if (fabs(cur_d) < tiny) cur_d = copysign(tiny, cur_d == 0.0 ? 1.0 : cur_d);
-    u0[(m - 1) * W] = cur_d;
-    double* z = zt + q;
-    for (int i = 0; i < m; ++i) z[i * W] = start_entry(q, i);
-    for (int it = 0; it < 3; ++it) {
+    rinv[m - 1] = 1.0 / cur_d;
+    for (int i = 0; i < m; ++i) z[i] = start_entry(q, i);
+    for (int it = 0; it < 2; ++it) {
       for (int i = 0; i + 1 < m; ++i) {
-        if (piv[i * W] != 0.0) {
-          const double tmp = z[i * W];
-          z[i * W] = z[(i + 1) * W];
-          z[(i + 1) * W] = tmp;
+        double a = z[i], b = z[i + 1];
+        if (piv[i]) {
+          const double tmp = a;
+          a = b;
+          b = tmp;
         }
-        z[(i + 1) * W] -= mult[i * W] * z[i * W];
+        z[i] = a;
+        z[i + 1] = b - mult[i] * a;
       }
-      z[(m - 1) * W] /= u0[(m - 1) * W];
-      if (m > 1) z[(m - 2) * W] = (z[(m - 2) * W] - u1[(m - 2) * W] * z[(m - 1) * W]) / u0[(m - 2) * W];
-      for (int i = m - 3; i >= 0; --i)
-        z[i * W] = (z[i * W] - u1[i * W] * z[(i + 1) * W] - u2[i * W] * z[(i + 2) * W]) / u0[i * W];
+      double z2 = z[m - 1] * rinv[m - 1];
+      z[m - 1] = z2;
+      double z1 = 0.0;
+      if (m > 1) {
+        z1 = (z[m - 2] - u1[m - 2] * z2) * rinv[m - 2];
+        z[m - 2] = z1;
+      }
+      for (int i = m - 3; i >= 0; --i) {
+        const double zi = (z[i] - u1[i] * z1 - u2[i] * z2) * rinv[i];
+        z[i] = zi;
+        z2 = z1;
+        z1 = zi;
+      }
       for (int p = k; p < q; ++p) {
         double dot = 0.0;
-        for (int i = 0; i < m; ++i) dot += zt[i * W + p] * z[i * W];
-        for (int i = 0; i < m; ++i) z[i * W] -= dot * zt[i * W + p];
+        for (int i = 0; i < m; ++i) dot += zt[i * W + p] * z[i];
+        for (int i = 0; i < m; ++i) z[i] -= dot * zt[i * W + p];
       }
       double nrm = 0.0;
-      for (int i = 0; i < m; ++i) nrm += z[i * W] * z[i * W];
+      for (int i = 0; i < m; ++i) nrm += z[i] * z[i];
       const double inv = 1.0 / sqrt(nrm);
-      for (int i = 0; i < m; ++i) z[i * W] *= inv;
+      for (int i = 0; i < m; ++i) z[i] *= inv;
     }
+    for (int i = 0; i < m; ++i) zt[i * W + q] = z[i];
   }
 }
 
+// Compact WY factor of each block of kReflectorBlock reflectors:
+// H_j0 ... H_j0+nb-1 = I - V T V^H (LAPACK zlarft, forward, columnwise),
+// T upper triangular, from the block's Gram matrix V^H V. One CTA per block.
+__global__ void __launch_bounds__(kThreads) reflector_blocks_kernel(const Cx<double>* __restrict__ reflectors,
+                                                                    const Cx<double>* __restrict__ tau, int m,
+                                                                    Cx<double>* __restrict__ tfac) {
+  constexpr int NB = kReflectorBlock, CH = 16;
+  __shared__ Cx<double> vs[CH][NB + 1];
+  __shared__ Cx<double> gram[NB][NB + 1];
+  __shared__ Cx<double> tmat[NB][NB + 1];
+  const int j0 = blockIdx.x * NB;
+  const int nb = min(NB, m - 1 - j0);
+  const int tid = threadIdx.x;
+  Cx<double> acc[4];
+  int pa[4], pb[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    acc[q] = Cx<double>{0.0, 0.0};
+    const int idx = tid + q * kThreads;  // over NB*NB
+    pa[q] = idx / NB;
+    pb[q] = idx % NB;
+  }
+  for (int r0 = j0 + 1; r0 < m; r0 += CH) {
+    for (int idx = tid; idx < CH * NB; idx += kThreads) {
+      const int rr = idx % CH, c = idx / CH, r = r0 + rr;
+      Cx<double> val{0.0, 0.0};
+      if (c < nb && r < m && r >= j0 + c + 1) val = reflectors[r + static_cast<long long>(j0 + c) * m];
+      vs[rr][c] = val;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q])
+        for (int rr = 0; rr < CH; ++rr) acc[q] = cadd(acc[q], cdot1(vs[rr][pa[q]], vs[rr][pb[q]]));
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q]) {
+      gram[pa[q]][pb[q]] = acc[q];
+      gram[pb[q]][pa[q]] = cconj(acc[q]);
+    }
+  for (int idx = tid; idx < NB * NB; idx += kThreads) tmat[idx / NB][idx % NB] = Cx<double>{0.0, 0.0};
+  __syncthreads();
+  // T(i,i) = tau_i; T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
+  for (int i = 0; i < nb; ++i) {
+    const Cx<double> ti = tau[j0 + i];
+    if (tid < i) {
+      Cx<double> sum{0.0, 0.0};
+      for (int c = tid; c < i; ++c) sum = cadd(sum, cmulz(tmat[tid][c], gram[c][i]));
+      tmat[tid][i] = cmulz(Cx<double>{-ti.re, -ti.im}, sum);
+    }
+    if (tid == 0) tmat[i][i] = ti;
+    __syncthreads();
+  }
+  for (int idx = tid; idx < NB * NB; idx += kThreads)
+    tfac[static_cast<long long>(blockIdx.x) * NB * NB + idx] = tmat[idx / NB][idx % NB];
+}
+
+// X = Q Z with Q = H_0 ... H_{m-2}: the reflector blocks applied from the
+// last to the first, Z <- Z - V (T (V^H Z)), kBackColumns columns of Z per
+// CTA in shared memory.
 __global__ void __launch_bounds__(kThreads) backtransform_kernel(const Cx<double>* __restrict__ reflectors,
-                                                                 const Cx<double>* __restrict__ tau, int m, int wanted,
-                                                                 const double* __restrict__ zt,
+                                                                 const Cx<double>* __restrict__ tfac, int m,
+                                                                 int wanted, const double* __restrict__ zt,
                                                                  Cx<double>* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int NB = kBackColumns;
+  constexpr int NB = kBackColumns, RB = kReflectorBlock, PER_WARP = RB / kWarps;
   Cx<double>* z = reinterpret_cast<Cx<double>*>(smem_raw);  // m x NB, row-major
-  Cx<double>* red = z + static_cast<long long>(m) * NB;     // kWarps * NB
-  Cx<double>* res = red + kWarps * NB;                       // NB
+  __shared__ Cx<double> wsh[RB][NB];
+  __shared__ Cx<double> ush[RB][NB];
+  __shared__ Cx<double> tsh[RB][RB + 1];
   const int q0 = blockIdx.x * NB;
   const int count = min(NB, wanted - q0);
-  for (int idx = threadIdx.x; idx < m * NB; idx += kThreads) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int idx = tid; idx < m * NB; idx += kThreads) {
     const int i = idx / NB, c = idx - i * NB;
     z[idx] = Cx<double>{c < count ? zt[static_cast<long long>(i) * wanted + q0 + c] : 0.0, 0.0};
   }
-  __syncthreads();
-  for (int j = m - 2; j >= 0; --j) {
-    const Cx<double> t = tau[j];
-    if (t.re == 0.0 && t.im == 0.0) continue;
-    const Cx<double>* v = reflectors + static_cast<long long>(j) * m;
-    Cx<double> acc[NB];
+  const int blocks = (m - 1 + RB - 1) / RB;
+  const int a = tid / NB, c = tid % NB;  // (reflector, column) of the T W product
+  for (int b = blocks - 1; b >= 0; --b) {
+    const int j0 = b * RB;
+    const int nb = min(RB, m - 1 - j0);
+    for (int idx = tid; idx < RB * RB; idx += kThreads)
+      tsh[idx / RB][idx % RB] = tfac[static_cast<long long>(b) * RB * RB + idx];
+    __syncthreads();
+    // W(a, c) = sum_r conj(V(r, j0+a)) Z(r, c): warp w takes reflectors
+    // PER_WARP w .. PER_WARP w + PER_WARP - 1, lanes split the rows.
+    {
+      Cx<double> acc[PER_WARP][NB];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) acc[c] = Cx<double>{0.0, 0.0};
-    for (int r = j + 1 + threadIdx.x; r < m; r += kThreads) {
-      const Cx<double> vr = v[r];
+      for (int q = 0; q < PER_WARP; ++q)
 #pragma unroll
-      for (int c = 0; c < NB; ++c) acc[c] = cadd(acc[c], cdot1(vr, z[r * NB + c]));
+        for (int cc = 0; cc < NB; ++cc) acc[q][cc] = Cx<double>{0.0, 0.0};
+      for (int r = j0 + 1 + lane; r < m; r += 32) {
+        Cx<double> zr[NB];
+#pragma unroll
+        for (int cc = 0; cc < NB; ++cc) zr[cc] = z[r * NB + cc];
+#pragma unroll
+        for (int q = 0; q < PER_WARP; ++q) {
+          const int aa = warp * PER_WARP + q;
+          if (aa < nb && r >= j0 + aa + 1) {
+            const Cx<double> vr = reflectors[r + static_cast<long long>(j0 + aa) * m];
+#pragma unroll
+            for (int cc = 0; cc < NB; ++cc) acc[q][cc] = cadd(acc[q][cc], cdot1(vr, zr[cc]));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < PER_WARP; ++q)
+#pragma unroll
+        for (int cc = 0; cc < NB; ++cc) {
+          double re = acc[q][cc].re, im = acc[q][cc].im;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+          }
+          if (lane == 0) wsh[warp * PER_WARP + q][cc] = Cx<double>{re, im};
+        }
     }
-    block_sum<NB>(acc, NB, red, res);
-    Cx<double> coef[NB];
+    __syncthreads();
+    // U = T W (T upper triangular)
+    if (a < RB) {
+      Cx<double> sum{0.0, 0.0};
+      if (a < nb)
+        for (int k2 = a; k2 < nb; ++k2) sum = cadd(sum, cmulz(tsh[a][k2], wsh[k2][c]));
+      ush[a][c] = sum;
+    }
+    __syncthreads();
+    // Z(r, :) -= sum_a V(r, j0+a) U(a, :), reflector a touching rows >= j0+a+1
+    for (int r = j0 + 1 + tid; r < m; r += kThreads) {
+      Cx<double> delta[NB];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) coef[c] = cmulz(t, res[c]);
-    for (int r = j + 1 + threadIdx.x; r < m; r += kThreads) {
-      const Cx<double> vr = v[r];
+      for (int cc = 0; cc < NB; ++cc) delta[cc] = Cx<double>{0.0, 0.0};
+      const int top = min(nb, r - j0);
+      for (int aa = 0; aa < top; ++aa) {
+        const Cx<double> vr = reflectors[r + static_cast<long long>(j0 + aa) * m];
 #pragma unroll
-      for (int c = 0; c < NB; ++c) z[r * NB + c] = csub(z[r * NB + c], cmulz(vr, coef[c]));
+        for (int cc = 0; cc < NB; ++cc) delta[cc] = cadd(delta[cc], cmulz(vr, ush[aa][cc]));
+      }
+#pragma unroll
+      for (int cc = 0; cc < NB; ++cc) z[r * NB + cc] = csub(z[r * NB + cc], delta[cc]);
     }
     __syncthreads();
   }
-  for (int idx = threadIdx.x; idx < m * NB; idx += kThreads) {
-    const int i = idx / NB, c = idx - i * NB;
-    if (c < count) out[i + static_cast<long long>(q0 + c) * m] = z[idx];
+  for (int idx = tid; idx < m * NB; idx += kThreads) {
+    const int i = idx / NB, cc = idx - i * NB;
+    if (cc < count) out[i + static_cast<long long>(q0 + cc) * m] = z[idx];
   }
 }
 
@@ -518,11 +773,19 @@ int sm_count() {
 }
 
 std::size_t tridiag_smem(int m, int cpc) {
-  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc + 2) * m + kWarps * kMaxCpc + kMaxCpc) +
+  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc) * m + kWarps * kMaxCpc + 3 * kMaxCpc) +
          sizeof(double) * kWarps;
 }
 
 constexpr std::size_t kSmemLimit = 227 * 1024;
+
+std::size_t invit_smem(int m) { return static_cast<std::size_t>(kInvitThreads) * (5 * sizeof(double) + 1) * m; }
+
+std::size_t back_smem(int m) { return sizeof(Cx<double>) * static_cast<std::size_t>(m) * kBackColumns; }
+
+// Static shared memory of backtransform_kernel (W, U and T tiles).
+constexpr std::size_t kBackStatic =
+    sizeof(Cx<double>) * (2 * kReflectorBlock * kBackColumns + kReflectorBlock * (kReflectorBlock + 1));
 
 }  // namespace
 
@@ -532,7 +795,9 @@ int hermitian_eigen_max_order() {
   for (int m = 2; m <= 4096; ++m) {
     const int grid = std::min(g, m);
     const int cpc = (m + grid - 1) / grid;
-    if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit) break;
+    if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit || m > kRowsPerThread * kThreads ||
+        invit_smem(m) > kSmemLimit || back_smem(m) + kBackStatic > kSmemLimit)
+      break;
     best = m;
   }
   return best;
@@ -582,19 +847,26 @@ void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<doubl
                   stream>>>(d, e, m, wanted, values);
   SDFT_LAUNCH("bisect_kernel");
 
-  const std::size_t vbytes = sizeof(double) * static_cast<std::size_t>(wanted) * mm * 6;
-  auto* vbase = static_cast<double*>(ws.vectors.reserve(vbytes));
-  double* work = vbase;
-  double* zt = vbase + static_cast<std::size_t>(wanted) * mm * 5;
-  inverse_iteration_kernel<<<static_cast<unsigned>(ceil_div(wanted, 64)), 64, 0, stream>>>(d, e, m, wanted, values,
-                                                                                          work, zt);
+  const int blocks = static_cast<int>(ceil_div(m - 1, kReflectorBlock));
+  const std::size_t vbytes = sizeof(double) * static_cast<std::size_t>(wanted) * mm +
+                             sizeof(Cx<double>) * static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
+  auto* zt = static_cast<double*>(ws.vectors.reserve(vbytes));
+  auto* tfac = reinterpret_cast<Cx<double>*>(zt + static_cast<std::size_t>(wanted) * mm);
+  const std::size_t inv_smem = invit_smem(m);
+  SDFT_CUDA(cudaFuncSetAttribute(inverse_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(inv_smem)));
+  inverse_iteration_kernel<<<static_cast<unsigned>(ceil_div(wanted, kInvitThreads)), kInvitThreads, inv_smem,
+                             stream>>>(d, e, m, wanted, values, zt);
   SDFT_LAUNCH("inverse_iteration_kernel");
 
-  const std::size_t back_smem = sizeof(Cx<double>) * (mm * kBackColumns + kWarps * kBackColumns + kBackColumns);
+  reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(reflectors, tau, m, tfac);
+  SDFT_LAUNCH("reflector_blocks_kernel");
+
+  const std::size_t bsmem = back_smem(m);
   SDFT_CUDA(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(back_smem)));
-  backtransform_kernel<<<static_cast<unsigned>(ceil_div(wanted, kBackColumns)), kThreads, back_smem, stream>>>(
-      reflectors, tau, m, wanted, zt, vectors);
+                                 static_cast<int>(bsmem)));
+  backtransform_kernel<<<static_cast<unsigned>(ceil_div(wanted, kBackColumns)), kThreads, bsmem, stream>>>(
+      reflectors, tfac, m, wanted, zt, vectors);
   SDFT_LAUNCH("backtransform_kernel");
 
   unsigned int error = 0;

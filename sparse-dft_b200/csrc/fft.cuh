@@ -237,38 +237,91 @@ __device__ __forceinline__ void pp_butterflies(const Cx<T>* src_line, Cx<T>* dst
   }
 }
 
-// One butterfly (line offset `offset`, index j) of a ping-pong stage.
+// Radix-R DFT on v with the stage's roots held in registers:
+// roots[p] = exp(-2 pi i p / R) for p = 1..R-1 (forward sign).
 template <typename T, int R, bool INV>
-__device__ __forceinline__ void pp_butterfly(const Cx<T>* src, Cx<T>* dst, int offset, int j, int es, int n, int ns,
-                                             const Cx<T>* tw) {
-  const int m = n / R, twstride = n / (ns * R), unit = n / R;
-  const int k = j % ns;
-  const Cx<T>* in = src + offset;
-  Cx<T> v[R];
+__device__ __forceinline__ void radix_dft_roots(Cx<T>* v, const Cx<T>* roots) {
+  if constexpr (R == 2 || R == 4) {
+    radix_dft<T, R, INV>(v, nullptr, 0);
+  } else {
+    constexpr int H = (R - 1) / 2;
+    Cx<T> a[H], b[H];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    Cx<T> x = in[(j + r * m) * es];
-    if (r > 0 && k > 0) x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
-    v[r] = x;
+    for (int r = 1; r <= H; ++r) {
+      a[r - 1] = v[r] + v[R - r];
+      b[r - 1] = v[r] - v[R - r];
+    }
+    const Cx<T> x0 = v[0];
+    Cx<T> sum = x0;
+#pragma unroll
+    for (int r = 0; r < H; ++r) sum = sum + a[r];
+    v[0] = sum;
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+      T cre = x0.re, cim = x0.im, sre = 0, sim = 0;
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const Cx<T> w = roots[(r * q) % R];  // cos, -sin (forward)
+        cre += a[r - 1].re * w.re;
+        cim += a[r - 1].im * w.re;
+        const T s = INV ? -w.im : w.im;
+        sre -= b[r - 1].im * s;
+        sim += b[r - 1].re * s;
+      }
+      v[q] = Cx<T>{cre + sre, cim + sim};
+      v[R - q] = Cx<T>{cre - sre, cim - sim};
+    }
   }
-  radix_dft<T, R, INV>(v, tw, unit);
-  const int base = (j / ns) * ns * R + k;
-  Cx<T>* out = dst + offset;
-#pragma unroll
-  for (int r = 0; r < R; ++r) out[(base + r * ns) * es] = v[r];
 }
 
+// One ping-pong stage over `count` lines (line offset rows[t] or t, times
+// line_stride). Work items (butterfly j, line t) = divmod(item, count) with
+// lines fastest; each thread walks items tid, tid + blockDim, ... and
+// advances (j, t) and (j / ns, j mod ns) incrementally, so the loop carries
+// no integer division. The stage's radix roots sit in registers.
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void pp_stage_flat(const Cx<T>* src, Cx<T>* dst, int count, int line_stride, int es,
                                               const int* rows, int n, int ns, const Cx<T>* tw) {
-  // Work items (line, butterfly) with lines fastest: consecutive threads hit
-  // consecutive lines at the same butterfly, so all lanes stay busy.
   const int m = n / R;
   const int items = count * m;
-  for (int item = threadIdx.x; item < items; item += blockDim.x) {
-    const int j = item / count, t = item - j * count;
+  int item = threadIdx.x;
+  if (item >= items) return;
+  const int twstride = n / (ns * R);
+  Cx<T> roots[R];
+#pragma unroll
+  for (int p = 1; p < R; ++p) roots[p] = tw[p * m];
+  const int step = blockDim.x;
+  const int dj = step / count, dt = step - dj * count;
+  const int djq = dj / ns, djk = dj - djq * ns;
+  int j = item / count, t = item - j * count;
+  int jq = j / ns, jk = j - jq * ns;
+  for (; item < items; item += step) {
     const int offset = (rows ? rows[t] : t) * line_stride;
-    pp_butterfly<T, R, INV>(src, dst, offset, j, es, n, ns, tw);
+    const Cx<T>* in = src + offset;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      Cx<T> x = in[(j + r * m) * es];
+      if (r > 0 && jk > 0) x = cmul(x, twiddle<T, INV>(tw, r * jk * twstride));
+      v[r] = x;
+    }
+    radix_dft_roots<T, R, INV>(v, roots);
+    Cx<T>* out = dst + offset + (jq * ns * R + jk) * es;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[r * ns * es] = v[r];
+    t += dt;
+    j += dj;
+    jk += djk;
+    jq += djq;
+    if (t >= count) {
+      t -= count;
+      ++j;
+      ++jk;
+    }
+    if (jk >= ns) {
+      jk -= ns;
+      ++jq;
+    }
   }
 }
 
