@@ -215,11 +215,11 @@ SDFT_B200_API sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensa
  * `requested` (0 = all n) solutions of H y = e S y, H and S n x n Hermitian
  * (lower triangles referenced, column-major), S positive definite. values:
  * count = requested ? requested : n ascending eigenvalues; vectors: n x count
- * column-major, S-orthonormal. For S within 1e-6 of the identity the device
+ * column-major, S-orthonormal. For S within 1e-5 of the identity the device
  * eigensolver runs (Householder tridiagonalisation in one cooperative
- * kernel, multisection, inverse iteration) after a first-order Loewdin
- * reduction; otherwise, or for n above the device solver's limit, cuSOLVER
- * zhegvdx/zhegvd. memory applies to h, s, values and vectors.
+ * kernel, multisection, inverse iteration, compact-WY back-transform) after a
+ * first- or second-order Loewdin reduction; otherwise, or for n above the
+ * device solver's limit, cuSOLVER zhegvdx/zhegvd. memory applies to h, s, values and vectors.
  * Replaces: rayleigh_ritz(h, s, requested), src/pw_core.cpp:56-136. */
 SDFT_B200_API sdft_b200_status sdft_b200_rayleigh_ritz(sdft_b200_context* context, size_t n, size_t requested,
                                                        const double* h, const double* s, double* values,

@@ -19,12 +19,13 @@
 //    than 1e-9 of the matrix scale, factors in shared memory; LU with partial
 //    pivoting of T - lambda I, two solves, Gram-Schmidt against earlier
 //    members of the cluster.
-// 4. reflector_blocks_kernel + backtransform_kernel: the reflectors in
-//    blocks of 32 as I - V T V^H (compact WY), applied to the tridiagonal
-//    eigenvectors from the last block to the first.
+// 4. reflector_blocks_kernel: the reflectors in blocks of 64 as
+//    I - V T V^H (compact WY); the blocks are applied to the tridiagonal
+//    eigenvectors from the last to the first with three cuBLAS ZGEMMs each.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -40,8 +41,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxCpc = 10;
 constexpr int kRowsPerThread = 5;  // rows per thread held in registers: m <= 1280
-constexpr int kBackColumns = 4;
-constexpr int kReflectorBlock = 32;
+constexpr int kReflectorBlock = 64;
 constexpr int kInvitThreads = 4;
 constexpr unsigned long long kWaitNs = 2000000000ULL;
 constexpr double kClusterTolerance = 1e-9;
@@ -103,16 +103,19 @@ __device__ double block_sum_real(double v, double* scratch) {
 }
 
 // Counting grid barrier with a time limit. Returns false (and every CTA
-// should return) when the limit expired here or the error word is set.
+// should return) when the limit expired here or the error word is set. The
+// CTA's writes (ordered before thread 0 by __syncthreads) are released by the
+// arrival; the acquire fence after the wait orders the reads that follow.
 __device__ bool grid_barrier(unsigned int* arrive, unsigned int target, int* ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(arrive, 1u);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(arrive) : "memory");
     const unsigned long long start = global_ns();
     int good = 1;
     while (true) {
-      if (*reinterpret_cast<volatile unsigned int*>(arrive) >= target) break;
+      unsigned int cur;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(arrive) : "memory");
+      if (cur >= target) break;
       if (*reinterpret_cast<volatile unsigned int*>(&g_eigen_error) != 0u) {
         good = 0;
         break;
@@ -123,7 +126,7 @@ __device__ bool grid_barrier(unsigned int* arrive, unsigned int target, int* ok)
         break;
       }
     }
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     *ok = good;
   }
   __syncthreads();
@@ -579,21 +582,23 @@ __global__ void inverse_iteration_kernel(const double* __restrict__ d, const dou
 
 // Compact WY factor of each block of kReflectorBlock reflectors:
 // H_j0 ... H_j0+nb-1 = I - V T V^H (LAPACK zlarft, forward, columnwise),
-// T upper triangular, from the block's Gram matrix V^H V. One CTA per block.
+// T upper triangular (column-major, leading dimension kReflectorBlock), from
+// the block's Gram matrix V^H V. One CTA per block.
 __global__ void __launch_bounds__(kThreads) reflector_blocks_kernel(const Cx<double>* __restrict__ reflectors,
                                                                     const Cx<double>* __restrict__ tau, int m,
                                                                     Cx<double>* __restrict__ tfac) {
-  constexpr int NB = kReflectorBlock, CH = 16;
-  __shared__ Cx<double> vs[CH][NB + 1];
-  __shared__ Cx<double> gram[NB][NB + 1];
-  __shared__ Cx<double> tmat[NB][NB + 1];
+  constexpr int NB = kReflectorBlock, CH = 16, LD = NB + 1, PAIRS = NB * NB / kThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* vs = reinterpret_cast<Cx<double>*>(smem_raw);  // CH x LD
+  Cx<double>* gram = vs + CH * LD;                            // NB x LD
+  Cx<double>* tmat = gram + NB * LD;                          // NB x LD
   const int j0 = blockIdx.x * NB;
   const int nb = min(NB, m - 1 - j0);
   const int tid = threadIdx.x;
-  Cx<double> acc[4];
-  int pa[4], pb[4];
+  Cx<double> acc[PAIRS];
+  int pa[PAIRS], pb[PAIRS];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < PAIRS; ++q) {
     acc[q] = Cx<double>{0.0, 0.0};
     const int idx = tid + q * kThreads;  // over NB*NB
     pa[q] = idx / NB;
@@ -604,129 +609,48 @@ __global__ void __launch_bounds__(kThreads) reflector_blocks_kernel(const Cx<dou
       const int rr = idx % CH, c = idx / CH, r = r0 + rr;
       Cx<double> val{0.0, 0.0};
       if (c < nb && r < m && r >= j0 + c + 1) val = reflectors[r + static_cast<long long>(j0 + c) * m];
-      vs[rr][c] = val;
+      vs[rr * LD + c] = val;
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < PAIRS; ++q)
       if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q])
-        for (int rr = 0; rr < CH; ++rr) acc[q] = cadd(acc[q], cdot1(vs[rr][pa[q]], vs[rr][pb[q]]));
+        for (int rr = 0; rr < CH; ++rr) acc[q] = cadd(acc[q], cdot1(vs[rr * LD + pa[q]], vs[rr * LD + pb[q]]));
     __syncthreads();
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < PAIRS; ++q)
     if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q]) {
-      gram[pa[q]][pb[q]] = acc[q];
-      gram[pb[q]][pa[q]] = cconj(acc[q]);
+      gram[pa[q] * LD + pb[q]] = acc[q];
+      gram[pb[q] * LD + pa[q]] = cconj(acc[q]);
     }
-  for (int idx = tid; idx < NB * NB; idx += kThreads) tmat[idx / NB][idx % NB] = Cx<double>{0.0, 0.0};
+  for (int idx = tid; idx < NB * NB; idx += kThreads) tmat[(idx / NB) * LD + idx % NB] = Cx<double>{0.0, 0.0};
   __syncthreads();
   // T(i,i) = tau_i; T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
   for (int i = 0; i < nb; ++i) {
     const Cx<double> ti = tau[j0 + i];
     if (tid < i) {
       Cx<double> sum{0.0, 0.0};
-      for (int c = tid; c < i; ++c) sum = cadd(sum, cmulz(tmat[tid][c], gram[c][i]));
-      tmat[tid][i] = cmulz(Cx<double>{-ti.re, -ti.im}, sum);
+      for (int c = tid; c < i; ++c) sum = cadd(sum, cmulz(tmat[tid * LD + c], gram[c * LD + i]));
+      tmat[tid * LD + i] = cmulz(Cx<double>{-ti.re, -ti.im}, sum);
     }
-    if (tid == 0) tmat[i][i] = ti;
+    if (tid == 0) tmat[i * LD + i] = ti;
     __syncthreads();
   }
-  for (int idx = tid; idx < NB * NB; idx += kThreads)
-    tfac[static_cast<long long>(blockIdx.x) * NB * NB + idx] = tmat[idx / NB][idx % NB];
+  for (int idx = tid; idx < NB * NB; idx += kThreads) {
+    const int col = idx / NB, row = idx % NB;
+    tfac[static_cast<long long>(blockIdx.x) * NB * NB + idx] = tmat[row * LD + col];
+  }
 }
 
-// X = Q Z with Q = H_0 ... H_{m-2}: the reflector blocks applied from the
-// last to the first, Z <- Z - V (T (V^H Z)), kBackColumns columns of Z per
-// CTA in shared memory.
-__global__ void __launch_bounds__(kThreads) backtransform_kernel(const Cx<double>* __restrict__ reflectors,
-                                                                 const Cx<double>* __restrict__ tfac, int m,
-                                                                 int wanted, const double* __restrict__ zt,
-                                                                 Cx<double>* __restrict__ out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int NB = kBackColumns, RB = kReflectorBlock, PER_WARP = RB / kWarps;
-  Cx<double>* z = reinterpret_cast<Cx<double>*>(smem_raw);  // m x NB, row-major
-  __shared__ Cx<double> wsh[RB][NB];
-  __shared__ Cx<double> ush[RB][NB];
-  __shared__ Cx<double> tsh[RB][RB + 1];
-  const int q0 = blockIdx.x * NB;
-  const int count = min(NB, wanted - q0);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int idx = tid; idx < m * NB; idx += kThreads) {
-    const int i = idx / NB, c = idx - i * NB;
-    z[idx] = Cx<double>{c < count ? zt[static_cast<long long>(i) * wanted + q0 + c] : 0.0, 0.0};
-  }
-  const int blocks = (m - 1 + RB - 1) / RB;
-  const int a = tid / NB, c = tid % NB;  // (reflector, column) of the T W product
-  for (int b = blocks - 1; b >= 0; --b) {
-    const int j0 = b * RB;
-    const int nb = min(RB, m - 1 - j0);
-    for (int idx = tid; idx < RB * RB; idx += kThreads)
-      tsh[idx / RB][idx % RB] = tfac[static_cast<long long>(b) * RB * RB + idx];
-    __syncthreads();
-    // W(a, c) = sum_r conj(V(r, j0+a)) Z(r, c): warp w takes reflectors
-    // PER_WARP w .. PER_WARP w + PER_WARP - 1, lanes split the rows.
-    {
-      Cx<double> acc[PER_WARP][NB];
-#pragma unroll
-      for (int q = 0; q < PER_WARP; ++q)
-#pragma unroll
-        for (int cc = 0; cc < NB; ++cc) acc[q][cc] = Cx<double>{0.0, 0.0};
-      for (int r = j0 + 1 + lane; r < m; r += 32) {
-        Cx<double> zr[NB];
-#pragma unroll
-        for (int cc = 0; cc < NB; ++cc) zr[cc] = z[r * NB + cc];
-#pragma unroll
-        for (int q = 0; q < PER_WARP; ++q) {
-          const int aa = warp * PER_WARP + q;
-          if (aa < nb && r >= j0 + aa + 1) {
-            const Cx<double> vr = reflectors[r + static_cast<long long>(j0 + aa) * m];
-#pragma unroll
-            for (int cc = 0; cc < NB; ++cc) acc[q][cc] = cadd(acc[q][cc], cdot1(vr, zr[cc]));
-          }
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < PER_WARP; ++q)
-#pragma unroll
-        for (int cc = 0; cc < NB; ++cc) {
-          double re = acc[q][cc].re, im = acc[q][cc].im;
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            re += __shfl_xor_sync(0xffffffffu, re, o);
-            im += __shfl_xor_sync(0xffffffffu, im, o);
-          }
-          if (lane == 0) wsh[warp * PER_WARP + q][cc] = Cx<double>{re, im};
-        }
-    }
-    __syncthreads();
-    // U = T W (T upper triangular)
-    if (a < RB) {
-      Cx<double> sum{0.0, 0.0};
-      if (a < nb)
-        for (int k2 = a; k2 < nb; ++k2) sum = cadd(sum, cmulz(tsh[a][k2], wsh[k2][c]));
-      ush[a][c] = sum;
-    }
-    __syncthreads();
-    // Z(r, :) -= sum_a V(r, j0+a) U(a, :), reflector a touching rows >= j0+a+1
-    for (int r = j0 + 1 + tid; r < m; r += kThreads) {
-      Cx<double> delta[NB];
-#pragma unroll
-      for (int cc = 0; cc < NB; ++cc) delta[cc] = Cx<double>{0.0, 0.0};
-      const int top = min(nb, r - j0);
-      for (int aa = 0; aa < top; ++aa) {
-        const Cx<double> vr = reflectors[r + static_cast<long long>(j0 + aa) * m];
-#pragma unroll
-        for (int cc = 0; cc < NB; ++cc) delta[cc] = cadd(delta[cc], cmulz(vr, ush[aa][cc]));
-      }
-#pragma unroll
-      for (int cc = 0; cc < NB; ++cc) z[r * NB + cc] = csub(z[r * NB + cc], delta[cc]);
-    }
-    __syncthreads();
-  }
-  for (int idx = tid; idx < m * NB; idx += kThreads) {
-    const int i = idx / NB, cc = idx - i * NB;
-    if (cc < count) out[i + static_cast<long long>(q0 + cc) * m] = z[idx];
+// X (complex, column-major, leading dimension m) from the row-major real
+// tridiagonal eigenvectors zt (m x wanted).
+__global__ void complex_columns_kernel(const double* __restrict__ zt, int m, int wanted, Cx<double>* __restrict__ x) {
+  const long long total = static_cast<long long>(m) * wanted;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long i = idx % m, q = idx / m;
+    x[idx] = Cx<double>{zt[i * wanted + q], 0.0};
   }
 }
 
@@ -744,6 +668,17 @@ __global__ void identity_deviation_kernel(Cx<double>* __restrict__ b, int m, uns
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(0xffffffffu, local, o));
   if ((threadIdx.x & 31) == 0) atomicMax(max_bits, static_cast<unsigned long long>(__double_as_longlong(local)));
+}
+
+// c <- I - e/2 + 3/8 c (c holds E^2 on entry)
+__global__ void lowdin_second_order_kernel(const Cx<double>* __restrict__ e, Cx<double>* __restrict__ c, int m) {
+  const long long total = static_cast<long long>(m) * m;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long i = idx % m, j = idx / m;
+    const Cx<double> x = e[idx], y = c[idx];
+    c[idx] = Cx<double>{(i == j ? 1.0 : 0.0) - 0.5 * x.re + 0.375 * y.re, -0.5 * x.im + 0.375 * y.im};
+  }
 }
 
 __global__ void add_identity_kernel(Cx<double>* __restrict__ b, int m) {
@@ -781,11 +716,7 @@ constexpr std::size_t kSmemLimit = 227 * 1024;
 
 std::size_t invit_smem(int m) { return static_cast<std::size_t>(kInvitThreads) * (5 * sizeof(double) + 1) * m; }
 
-std::size_t back_smem(int m) { return sizeof(Cx<double>) * static_cast<std::size_t>(m) * kBackColumns; }
-
-// Static shared memory of backtransform_kernel (W, U and T tiles).
-constexpr std::size_t kBackStatic =
-    sizeof(Cx<double>) * (2 * kReflectorBlock * kBackColumns + kReflectorBlock * (kReflectorBlock + 1));
+constexpr std::size_t kBlockSmem = sizeof(Cx<double>) * (16 + 2 * kReflectorBlock) * (kReflectorBlock + 1);
 
 }  // namespace
 
@@ -796,15 +727,15 @@ int hermitian_eigen_max_order() {
     const int grid = std::min(g, m);
     const int cpc = (m + grid - 1) / grid;
     if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit || m > kRowsPerThread * kThreads ||
-        invit_smem(m) > kSmemLimit || back_smem(m) + kBackStatic > kSmemLimit)
+        invit_smem(m) > kSmemLimit)
       break;
     best = m;
   }
   return best;
 }
 
-void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws,
-                      cudaStream_t stream) {
+void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors,
+                      EigenWorkspace& ws, cudaStream_t stream) {
   if (m < 2 || wanted < 1 || wanted > m) throw InvalidArgument("invalid Hermitian eigenproblem size");
   const int grid = std::min(sm_count(), m);
   const int cpc = (m + grid - 1) / grid;
@@ -824,6 +755,8 @@ void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<doubl
   Cx<double>* pbuf = colbuf + 2 * mm;
   Cx<double>* dotbuf = pbuf + 2 * mm;
   SDFT_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned int), stream));
+  // Entries above each reflector's unit element stay zero for the block products.
+  SDFT_CUDA(cudaMemsetAsync(reflectors, 0, sizeof(Cx<double>) * mm * mm, stream));
   const unsigned int zero = 0;
   SDFT_CUDA(cudaMemcpyToSymbolAsync(g_eigen_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, stream));
 
@@ -848,10 +781,14 @@ void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<doubl
   SDFT_LAUNCH("bisect_kernel");
 
   const int blocks = static_cast<int>(ceil_div(m - 1, kReflectorBlock));
-  const std::size_t vbytes = sizeof(double) * static_cast<std::size_t>(wanted) * mm +
-                             sizeof(Cx<double>) * static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
+  const std::size_t vbytes =
+      sizeof(double) * static_cast<std::size_t>(wanted) * mm +
+      sizeof(Cx<double>) * (static_cast<std::size_t>(blocks) + 2 * static_cast<std::size_t>(wanted)) * kReflectorBlock *
+          kReflectorBlock;
   auto* zt = static_cast<double*>(ws.vectors.reserve(vbytes));
   auto* tfac = reinterpret_cast<Cx<double>*>(zt + static_cast<std::size_t>(wanted) * mm);
+  Cx<double>* wtmp = tfac + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
+  Cx<double>* utmp = wtmp + static_cast<std::size_t>(wanted) * kReflectorBlock;
   const std::size_t inv_smem = invit_smem(m);
   SDFT_CUDA(cudaFuncSetAttribute(inverse_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(inv_smem)));
@@ -859,15 +796,27 @@ void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<doubl
                              stream>>>(d, e, m, wanted, values, zt);
   SDFT_LAUNCH("inverse_iteration_kernel");
 
-  reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, 0, stream>>>(reflectors, tau, m, tfac);
+  SDFT_CUDA(cudaFuncSetAttribute(reflector_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kBlockSmem)));
+  reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, kBlockSmem, stream>>>(reflectors, tau, m, tfac);
   SDFT_LAUNCH("reflector_blocks_kernel");
 
-  const std::size_t bsmem = back_smem(m);
-  SDFT_CUDA(cudaFuncSetAttribute(backtransform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(bsmem)));
-  backtransform_kernel<<<static_cast<unsigned>(ceil_div(wanted, kBackColumns)), kThreads, bsmem, stream>>>(
-      reflectors, tfac, m, wanted, zt, vectors);
-  SDFT_LAUNCH("backtransform_kernel");
+  // X = Q Z: blocks from the last to the first, X <- X - V (T (V^H X)) on rows > j0.
+  const long long total = static_cast<long long>(m) * wanted;
+  complex_columns_kernel<<<static_cast<unsigned>(std::min<long long>(ceil_div(total, 256), 148 * 8)), 256, 0,
+                           stream>>>(zt, m, wanted, vectors);
+  SDFT_LAUNCH("complex_columns_kernel");
+  for (int b = blocks - 1; b >= 0; --b) {
+    const int j0 = b * kReflectorBlock;
+    const int nb = std::min(kReflectorBlock, m - 1 - j0);
+    const int rows = m - 1 - j0;
+    const Cx<double>* vb = reflectors + (j0 + 1) + static_cast<long long>(j0) * m;
+    Cx<double>* xs = vectors + (j0 + 1);
+    const Cx<double>* tb = tfac + static_cast<long long>(b) * kReflectorBlock * kReflectorBlock;
+    zgemm(blas, Op::C, Op::N, nb, wanted, rows, vb, m, xs, m, wtmp, kReflectorBlock, false);
+    zgemm(blas, Op::N, Op::N, nb, wanted, nb, tb, kReflectorBlock, wtmp, kReflectorBlock, utmp, kReflectorBlock, false);
+    zgemm(blas, Op::N, Op::N, rows, wanted, nb, vb, m, utmp, kReflectorBlock, xs, m, true, -1.0);
+  }
 
   unsigned int error = 0;
   SDFT_CUDA(cudaMemcpyFromSymbolAsync(&error, g_eigen_error, sizeof(error), 0, cudaMemcpyDeviceToHost, stream));
@@ -888,6 +837,13 @@ double identity_deviation(Cx<double>* b, int m, EigenWorkspace& ws, cudaStream_t
   double value;
   std::memcpy(&value, &host, sizeof(value));
   return value;
+}
+
+void lowdin_second_order(const Cx<double>* e, Cx<double>* c, int m, cudaStream_t stream) {
+  const long long total = static_cast<long long>(m) * m;
+  lowdin_second_order_kernel<<<static_cast<unsigned>(std::min<long long>(ceil_div(total, 256), 148 * 8)), 256, 0,
+                               stream>>>(e, c, m);
+  SDFT_LAUNCH("lowdin_second_order_kernel");
 }
 
 void add_identity(Cx<double>* b, int m, cudaStream_t stream) {
@@ -915,13 +871,18 @@ void check_solver(cusolverStatus_t status, const char* what) {
 
 void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<double>* h, Cx<double>* s, int m,
                         int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws, RitzSolver mode,
-                        cudaStream_t st) {
+                        cudaStream_t st, double max_deviation) {
   if (m < 1 || wanted < 1 || wanted > m) throw InvalidArgument("invalid Rayleigh-Ritz dimensions");
   const std::size_t mm = static_cast<std::size_t>(m);
   if (mode == RitzSolver::Device && m >= 2 && m <= hermitian_eigen_max_order()) {
     const double deviation = identity_deviation(s, m, ws, st);
     if (!std::isfinite(deviation)) throw NonFinite("Rayleigh-Ritz overlap is not finite");
-    if (deviation <= 1e-6) {
+    static const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
+    if (trace)
+      std::fprintf(stderr, "rayleigh-ritz m=%d |S-I|max=%.3e path=%s\n", m, deviation,
+                   deviation <= 1e-8 ? "device" : deviation <= max_deviation ? "device-loewdin2" : "cusolver");
+    if (deviation <= 1e-8) {
+      // First order: H' = H - (E H + H E)/2, y -> y - E y / 2 (error O(|E|^2) <= 1e-16).
       const bool correct = deviation > 1e-14;
       Cx<double>* f = nullptr;
       if (correct) {
@@ -929,12 +890,24 @@ void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<doubl
         zgemm(blas, Op::N, Op::N, m, m, m, s, m, h, m, f, m, false);
         lowdin_combine(h, f, m, st);
       }
-      hermitian_lowest(h, m, wanted, values, vectors, ws, st);
+      hermitian_lowest(blas, h, m, wanted, values, vectors, ws, st);
       if (correct) {
-        // y -> y - E y / 2
         zgemm(blas, Op::N, Op::N, m, wanted, m, s, m, vectors, m, f, m, false, -0.5);
         add_block(f, m, vectors, m, m, wanted, st);
       }
+      return;
+    }
+    if (deviation <= max_deviation) {
+      // Second order: C = I - E/2 + 3/8 E^2 = S^(-1/2) + O(|E|^3); H' = C H C, y -> C y.
+      auto* f = static_cast<Cx<double>*>(ws.product.reserve(sizeof(Cx<double>) * mm * mm));
+      auto* c = static_cast<Cx<double>*>(ws.product2.reserve(sizeof(Cx<double>) * mm * mm));
+      zgemm(blas, Op::N, Op::N, m, m, m, s, m, s, m, c, m, false);
+      lowdin_second_order(s, c, m, st);
+      zgemm(blas, Op::N, Op::N, m, m, m, c, m, h, m, f, m, false);
+      zgemm(blas, Op::N, Op::N, m, m, m, f, m, c, m, h, m, false);
+      hermitian_lowest(blas, h, m, wanted, values, vectors, ws, st);
+      zgemm(blas, Op::N, Op::N, m, wanted, m, c, m, vectors, m, f, m, false);
+      copy_block(f, m, vectors, m, m, wanted, st);
       return;
     }
     // Far from S-orthonormal: restore S and solve the pencil with cuSOLVER.

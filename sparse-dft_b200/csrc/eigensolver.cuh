@@ -17,7 +17,8 @@ struct EigenWorkspace {
   Scratch tridiagonal;  // d, e, tau, reflectors, exchange buffers, barrier words
   Scratch vectors;      // tridiagonal eigenvectors and inverse-iteration factors
   Scratch scalar;       // reduction word
-  Scratch product;      // m x m product for the overlap correction
+  Scratch product;      // m x m products for the overlap correction
+  Scratch product2;
   Scratch solver_work;  // cuSOLVER workspace and info word (generalized fallback)
 };
 
@@ -33,22 +34,24 @@ int hermitian_eigen_max_order();
 // m; overwritten. On return values[0..wanted) (device) holds the lowest
 // eigenvalues in ascending order and vectors (m x wanted, leading dimension
 // m, device; may alias a) the orthonormal eigenvectors. m must not exceed
-// hermitian_eigen_max_order().
-void hermitian_lowest(Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws,
-                      cudaStream_t stream);
+// hermitian_eigen_max_order(). blas must be bound to `stream`.
+void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors,
+                      EigenWorkspace& ws, cudaStream_t stream);
 
 // Lowest `wanted` pairs of the Hermitian pencil H y = e S y (the reference's
 // rayleigh_ritz, src/pw_core.cpp:56-136). h, s: m x m, both triangles,
 // leading dimension m, device; both overwritten. values: device, at least
 // `wanted` (all m for RitzSolver::Full); vectors: m x wanted (m x m for
 // Full), leading dimension m, may alias h, S-orthonormal.
-// Device solver: S = I + E with max |E| <= 1e-6 is reduced by the first-order
-// Loewdin transform C = I - E/2 (H' = H - (E H + H E)/2, y -> y - E y/2, exact
-// to O(|E|^2)), skipped when max |E| <= 1e-14; otherwise, or when m exceeds
-// hermitian_eigen_max_order(), cuSOLVER zhegvdx solves the pencil.
+// Device solver on S = I + E: nothing when max |E| <= 1e-14; the
+// first-order Loewdin transform C = I - E/2 (H' = H - (E H + H E)/2,
+// y -> y - E y/2, error O(|E|^2)) up to 1e-8; the second-order C = I - E/2 +
+// 3/8 E^2 (H' = C H C, y -> C y, error O(|E|^3)) up to max_deviation.
+// Beyond that, or when m exceeds hermitian_eigen_max_order(), cuSOLVER
+// zhegvdx solves the pencil.
 void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<double>* h, Cx<double>* s, int m,
                         int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws, RitzSolver mode,
-                        cudaStream_t stream);
+                        cudaStream_t stream, double max_deviation = 1e-5);
 
 // b <- b - I (m x m, leading dimension m); returns max |entry| of the result.
 double identity_deviation(Cx<double>* b, int m, EigenWorkspace& ws, cudaStream_t stream);

@@ -46,7 +46,7 @@ def test_identity_overlap(context, n, requested):
     check(context, h, s, requested)
 
 
-@pytest.mark.parametrize("overlap", [1e-9, 5e-7])
+@pytest.mark.parametrize("overlap", [1e-9, 5e-7, 3e-6])
 def test_near_identity_overlap_uses_loewdin(context, overlap):
     rng = np.random.Generator(np.random.PCG64(11))
     h, s = pencil(500, rng, overlap=overlap)
