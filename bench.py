@@ -266,6 +266,10 @@ def run_b200(args):
     # host arrays, solve, eigenvectors read back, every step.
     e2e = end_to_end(ctx, inputs, stream, steps=max(1, min(args.steps, 2)))
 
+    density_rows = None
+    if rank == 0 and world == 1 and not args.no_density:
+        density_rows = density_side(ctx, inputs, stream, roofline["peak"])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(inputs)
@@ -283,7 +287,7 @@ def run_b200(args):
                            "certified_pairs_per_solve": fp64_pairs / len(fp64_ms)},
             "mixed_over_fp64": statistics.median(fp64_ms) / statistics.median(step_ms),
             "solver_stats": stats, "clocks": clocks.summary(), "gpu_launches": int(launches),
-            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+            "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "density_side": density_rows,
         }
         print(json.dumps(line), flush=True)
     op.close()
@@ -333,6 +337,72 @@ def fused_local_roofline(op, inputs, stream):
             "traffic": traffic, "kernel": "fused local H~psi (plane_in + pencil + plane_out), FP32, 160 columns",
             "ms_per_launch": ms, "algorithmic_bytes": algorithmic,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+
+def density_side(ctx, inputs, stream, peak):
+    """Config-3 density-side rows on the Si64 cell, device-resident inputs, one
+    timed call each after a warm-up call (CUDA events on the library's stream):
+    band density of 128 occupied bands (f_n = 2) on the supports f = 4, 8, 16;
+    the compensation charge of 64 atoms on the f = 16 support from the one-centre
+    occupations of 128 bands; PBE on every point of the f = 16 density grid.
+    GB/s use the scope table's algorithmic bytes."""
+    import numpy as np
+    import torch
+    from sdft_b200 import density, synthetic
+    from sdft_b200.density import fast_length
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    bands = 128
+    psi = torch.from_numpy(synthetic.band_coefficients(inputs, bands)).cuda()
+    occ = np.full(bands, 2.0)
+    out = {"bands": bands, "band_density": {}}
+    grid16 = None
+    for factor in (4.0, 8.0, 16.0):
+        support = synthetic.density_support(inputs, factor)
+        ms, _ = timed(lambda: density.band_density(ctx, inputs.hkl, psi, occ, inputs.volume, support))
+        span = [int(2 * max(np.abs(support[:, a]).max(), inputs.hkl[:, a].max() - min(inputs.hkl[:, a].min(), 0)) + 1)
+                for a in range(3)]
+        n = [fast_length(max(3, v)) for v in span]
+        points = n[0] * n[1] * n[2]
+        grid16 = n
+        algorithmic = bands * (16 * inputs.npw + 2 * 2 * 16 * points) + 2 * 8 * points
+        gbs = algorithmic / (ms * 1e-3) / 1e9
+        out["band_density"][f"f{int(factor)}"] = {"grid": n, "support": int(support.shape[0]), "ms": ms,
+                                                  "achieved_gbs": gbs, "frac_of_hbm": gbs / peak}
+    # Compensation charge on the f = 16 support.
+    aug = synthetic.augmentation()
+    rows = int(np.sum(2 * aug["channel_l"] + 1))
+    atoms = inputs.positions.shape[0]
+    amplitudes = synthetic.projected_amplitudes(atoms, rows, bands)
+    onsite = density.onsite_density(ctx, amplitudes, rows, occ)
+    keys = synthetic.density_support(inputs, 16.0)
+    charge = density.CompensationCharge(ctx, inputs.lattice, inputs.positions, keys, aug, synthetic.lm_transform(aug))
+    rho = torch.from_numpy(onsite).cuda()
+    ms, _ = timed(lambda: charge.density(rho))
+    lms = (int(aug["max_l"]) + 1) ** 2
+    algorithmic = keys.shape[0] * (16 + 8 * lms)
+    out["compensation"] = {"keys": int(keys.shape[0]), "atoms": atoms, "ms": ms,
+                           "achieved_gbs": algorithmic / (ms * 1e-3) / 1e9,
+                           "atom_terms_per_s": keys.shape[0] * atoms / (ms * 1e-3)}
+    charge.close()
+    # PBE on every point of the f = 16 density grid.
+    points = grid16[0] * grid16[1] * grid16[2]
+    nval = torch.exp(torch.linspace(-20.0, 1.0, points, dtype=torch.float64, device="cuda"))
+    gval = 0.3 * nval
+    ms, _ = timed(lambda: density.pbe_points(ctx, nval, gval))
+    out["pbe"] = {"points": points, "ms": ms, "points_per_s": points / (ms * 1e-3),
+                  "achieved_gbs": points * 64 / (ms * 1e-3) / 1e9}
+    return out
 
 
 def end_to_end(ctx, inputs, stream, steps):
@@ -416,6 +486,7 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
+    parser.add_argument("--no-density", action="store_true", help="skip the density-side measurements")
     parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe"],
                         help="run a few launches of one kernel family for a profiler capture and exit")
     parser.add_argument("--columns", type=int, default=32, help="columns (bands) for --case")

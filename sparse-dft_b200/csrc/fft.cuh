@@ -325,6 +325,80 @@ __device__ __forceinline__ void pp_stage_flat(const Cx<T>* src, Cx<T>* dst, int 
   }
 }
 
+// ---- compile-time line length ------------------------------------------
+// The same Stockham stages with N, the radix sequence (4 first, then 2, 3,
+// 5, 7, as make_line_plan) and the line count known at compile time, so the
+// stage loops unroll and all index arithmetic folds to constants.
+__host__ __device__ constexpr int fixed_next_radix(int rest) {
+  return rest % 4 == 0 ? 4 : rest % 2 == 0 ? 2 : rest % 3 == 0 ? 3 : rest % 5 == 0 ? 5 : rest % 7 == 0 ? 7 : 0;
+}
+__host__ __device__ constexpr int fixed_stage_count(int n) {
+  int stages = 0;
+  for (int rest = n; rest > 1; rest /= fixed_next_radix(rest)) {
+    if (fixed_next_radix(rest) == 0) return -1;
+    ++stages;
+  }
+  return stages;
+}
+// Radix of stage s and the product of the radices before it.
+__host__ __device__ constexpr int fixed_radix(int n, int s) {
+  int rest = n;
+  for (int i = 0; i < s; ++i) rest /= fixed_next_radix(rest);
+  return fixed_next_radix(rest);
+}
+__host__ __device__ constexpr int fixed_ns(int n, int s) {
+  int ns = 1, rest = n;
+  for (int i = 0; i < s; ++i) {
+    const int r = fixed_next_radix(rest);
+    ns *= r;
+    rest /= r;
+  }
+  return ns;
+}
+
+template <typename T, int R, bool INV, int N, int NS, int COUNT, int THREADS>
+__device__ __forceinline__ void pp_stage_fixed(const Cx<T>* src, Cx<T>* dst, int line_stride, int es,
+                                               const Cx<T>* tw) {
+  constexpr int M = N / R, ITEMS = COUNT * M, TWSTRIDE = N / (NS * R);
+  Cx<T> roots[R];
+#pragma unroll
+  for (int p = 1; p < R; ++p) roots[p] = tw[p * M];
+#pragma unroll
+  for (int base = 0; base < ITEMS; base += THREADS) {
+    const int item = base + static_cast<int>(threadIdx.x);
+    if (ITEMS % THREADS != 0 && item >= ITEMS) break;
+    const int j = item / COUNT, t = item - j * COUNT;
+    const int jq = j / NS, jk = j - jq * NS;
+    const int offset = t * line_stride;
+    const Cx<T>* in = src + offset;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      Cx<T> x = in[(j + r * M) * es];
+      if (r > 0 && jk > 0) x = cmul(x, twiddle<T, INV>(tw, r * jk * TWSTRIDE));
+      v[r] = x;
+    }
+    radix_dft_roots<T, R, INV>(v, roots);
+    Cx<T>* out = dst + offset + (jq * NS * R + jk) * es;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[r * NS * es] = v[r];
+  }
+}
+
+// COUNT lines of length N (line t at t * line_stride, elements es apart),
+// ping-pong between src and dst; returns the buffer holding the result.
+template <typename T, bool INV, int N, int COUNT, int THREADS, int S = 0>
+__device__ __forceinline__ Cx<T>* fft_lines_fixed(Cx<T>* src, Cx<T>* dst, int line_stride, int es, const Cx<T>* tw) {
+  static_assert(fixed_stage_count(N) > 0, "line length must be 2/3/5/7-smooth");
+  if constexpr (S == fixed_stage_count(N)) {
+    return src;
+  } else {
+    pp_stage_fixed<T, fixed_radix(N, S), INV, N, fixed_ns(N, S), COUNT, THREADS>(src, dst, line_stride, es, tw);
+    __syncthreads();
+    return fft_lines_fixed<T, INV, N, COUNT, THREADS, S + 1>(dst, src, line_stride, es, tw);
+  }
+}
+
 template <typename T, bool INV>
 __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
                                const int* rows, const LinePlan& plan, const Cx<T>* tw) {

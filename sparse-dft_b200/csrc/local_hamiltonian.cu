@@ -112,6 +112,53 @@ __global__ void __launch_bounds__(kThreads) pencil_kernel(Cx<T>* __restrict__ sl
   }
 }
 
+// pencil_kernel for a compile-time axis length N0: every entry of the tile is
+// written once (slab value or zero), and the stages unroll with constant
+// index arithmetic.
+template <typename T, int N0>
+__global__ void __launch_bounds__(kThreads) pencil_fixed_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
+                                                                const T* __restrict__ potential) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TL = kPencilLines, STRIDE = TL + 1;
+  Cx<T>* tw0 = reinterpret_cast<Cx<T>*>(smem_raw);
+  Cx<T>* tile_a = tw0 + N0;
+  Cx<T>* tile_b = tile_a + N0 * STRIDE;
+  int* slot_of_row = reinterpret_cast<int*>(tile_b + N0 * STRIDE);
+  const long long kl0 = static_cast<long long>(blockIdx.x) * TL;
+  const int c = blockIdx.y;
+  const int lines = static_cast<int>(min(static_cast<long long>(TL), a.n12 - kl0));
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N0; i += kThreads) {
+    tw0[i] = a.tw0[i];
+    slot_of_row[i] = -1;
+  }
+  __syncthreads();
+  for (int s = tid; s < a.slots; s += kThreads) slot_of_row[a.slot_row[s]] = s;
+  __syncthreads();
+  Cx<T>* base = slab + static_cast<long long>(c) * a.slots * a.n12 + kl0;
+  for (int idx = tid; idx < N0 * TL; idx += kThreads) {
+    const int i = idx / TL, t = idx - i * TL;
+    const int s = slot_of_row[i];
+    tile_a[i * STRIDE + t] =
+        (s >= 0 && t < lines) ? base[static_cast<long long>(s) * a.n12 + t] : Cx<T>{0, 0};
+  }
+  __syncthreads();
+  Cx<T>* field = fft_lines_fixed<T, true, N0, TL, kThreads>(tile_a, tile_b, 1, STRIDE, tw0);
+  for (int idx = tid; idx < N0 * TL; idx += kThreads) {
+    const int i = idx / TL, t = idx - i * TL;
+    if (t < lines) {
+      const T v = potential[static_cast<long long>(i) * a.n12 + kl0 + t];
+      field[i * STRIDE + t] = cscale(field[i * STRIDE + t], v);
+    }
+  }
+  __syncthreads();
+  Cx<T>* back = fft_lines_fixed<T, false, N0, TL, kThreads>(field, field == tile_a ? tile_b : tile_a, 1, STRIDE, tw0);
+  for (int idx = tid; idx < a.slots * TL; idx += kThreads) {
+    const int s = idx / TL, t = idx - s * TL;
+    if (t < lines) base[static_cast<long long>(s) * a.n12 + t] = back[a.slot_row[s] * STRIDE + t];
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) plane_out_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                              const Cx<double>* __restrict__ x, long long ldx,
@@ -206,6 +253,37 @@ void allow_smem(Kernel kernel, std::size_t bytes) {
   SDFT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
 }
 
+// Pencil pass with the compile-time kernel for the common axis lengths.
+template <typename T>
+bool launch_pencil_fixed(const LocalArgs<T>& a, int columns, const T* potential, Cx<T>* slab, cudaStream_t stream) {
+  const std::size_t smem =
+      sizeof(Cx<T>) * (a.n0 + 2 * static_cast<std::size_t>(a.n0) * (kPencilLines + 1)) + sizeof(int) * a.n0;
+  const dim3 grid(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
+  auto go = [&](auto kernel) {
+    allow_smem(kernel, smem);
+    kernel<<<grid, kThreads, smem, stream>>>(slab, a, potential);
+    SDFT_LAUNCH("pencil_fixed_kernel");
+    return true;
+  };
+  switch (a.n0) {
+    case 35: return go(pencil_fixed_kernel<T, 35>);
+    case 36: return go(pencil_fixed_kernel<T, 36>);
+    case 45: return go(pencil_fixed_kernel<T, 45>);
+    case 48: return go(pencil_fixed_kernel<T, 48>);
+    case 60: return go(pencil_fixed_kernel<T, 60>);
+    case 64: return go(pencil_fixed_kernel<T, 64>);
+    case 70: return go(pencil_fixed_kernel<T, 70>);
+    case 72: return go(pencil_fixed_kernel<T, 72>);
+    case 80: return go(pencil_fixed_kernel<T, 80>);
+    case 81: return go(pencil_fixed_kernel<T, 81>);
+    case 84: return go(pencil_fixed_kernel<T, 84>);
+    case 90: return go(pencil_fixed_kernel<T, 90>);
+    case 96: return go(pencil_fixed_kernel<T, 96>);
+    default: return false;
+  }
+}
+
+
 template <typename T>
 LocalArgs<T> make_args(const SpherePlan& plan) {
   LocalArgs<T> a{};
@@ -246,8 +324,10 @@ void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long lo
   plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
   SDFT_LAUNCH("plane_in_kernel");
   const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
-  pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
-  SDFT_LAUNCH("pencil_kernel");
+  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
+    pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+    SDFT_LAUNCH("pencil_kernel");
+  }
   plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
                                                                 static_cast<double>(plan.count), y, ldy);
   SDFT_LAUNCH("plane_out_kernel");
@@ -418,8 +498,10 @@ void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long 
   plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
   SDFT_LAUNCH("plane_in_kernel");
   const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
-  pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
-  SDFT_LAUNCH("pencil_kernel");
+  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
+    pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+    SDFT_LAUNCH("pencil_kernel");
+  }
   plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
                                                                 static_cast<double>(plan.count), y, ldy);
   SDFT_LAUNCH("plane_out_kernel");

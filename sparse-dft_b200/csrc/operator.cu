@@ -44,6 +44,89 @@ double frobenius(const std::vector<C>& m) {
   for (const auto& v : m) s += std::norm(v);
   return std::sqrt(s);
 }
+
+// Row-major Sigma_np x NPW amplitudes (atom blocks of rows, the input layout)
+// to the column-major device B (ld Sigma_np), through 32 x 32 shared-memory
+// tiles so that both the reads and the writes are coalesced; a nonfinite entry
+// raises *bad.
+__global__ void paw_transpose_kernel(const Cx<double>* __restrict__ raw, int rows, int npw, Cx<double>* __restrict__ b,
+                                     unsigned int* bad) {
+  __shared__ Cx<double> tile[32][33];
+  const int g0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  unsigned int nonfinite = 0;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int r = r0 + dy, g = g0 + threadIdx.x;
+    if (r < rows && g < npw) {
+      const Cx<double> v = raw[static_cast<std::size_t>(r) * npw + g];
+      nonfinite |= !isfinite(v.re) || !isfinite(v.im);
+      tile[dy][threadIdx.x] = v;
+    }
+  }
+  __syncthreads();
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int g = g0 + dy, r = r0 + threadIdx.x;
+    if (r < rows && g < npw) b[r + static_cast<std::size_t>(g) * rows] = tile[threadIdx.x][dy];
+  }
+  if (__any_sync(0xffffffffu, nonfinite) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+}
+
+// h_diag[g] += Re(b_g^H D b_g), s_diag[g] += Re(b_g^H Q b_g) per atom, one
+// thread per plane wave, with the products and sums of the complex host loop
+// (atoms, rows i, columns j: db_i = sum_j D(i,j) b_j, hd = sum_i conj(b_i) db_i)
+// each rounded on its own, so the diagonals equal the host arithmetic's. The
+// symmetrised blocks are column-major (D(i,j) at i + j*np) and uniform over
+// the block's threads; the amplitudes are read row-major (coalesced).
+__global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ raw, int npw, int atoms,
+                                    const int* __restrict__ offsets, const long long* __restrict__ storage,
+                                    const Cx<double>* __restrict__ d, const Cx<double>* __restrict__ q,
+                                    double* __restrict__ h_diag, double* __restrict__ s_diag) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= npw) return;
+  double hdiag = h_diag[g], sdiag = s_diag[g];
+  for (int a = 0; a < atoms; ++a) {
+    const int base = offsets[a], np = offsets[a + 1] - offsets[a];
+    const Cx<double>* da = d + storage[a];
+    const Cx<double>* qa = q + storage[a];
+    const Cx<double>* col = raw + static_cast<std::size_t>(base) * npw + g;
+    double hr = 0, hi = 0, sr = 0, si = 0;
+    for (int i = 0; i < np; ++i) {
+      double dr = 0, di = 0, qr = 0, qi = 0;
+      for (int j = 0; j < np; ++j) {
+        const Cx<double> bj = col[static_cast<std::size_t>(j) * npw];
+        const Cx<double> dij = da[i + static_cast<std::size_t>(j) * np], qij = qa[i + static_cast<std::size_t>(j) * np];
+        dr = __dadd_rn(dr, __dsub_rn(__dmul_rn(dij.re, bj.re), __dmul_rn(dij.im, bj.im)));
+        di = __dadd_rn(di, __dadd_rn(__dmul_rn(dij.re, bj.im), __dmul_rn(dij.im, bj.re)));
+        qr = __dadd_rn(qr, __dsub_rn(__dmul_rn(qij.re, bj.re), __dmul_rn(qij.im, bj.im)));
+        qi = __dadd_rn(qi, __dadd_rn(__dmul_rn(qij.re, bj.im), __dmul_rn(qij.im, bj.re)));
+      }
+      // conj(b_i) * db: real part b.re*db.re - (-b.im)*db.im, imaginary part
+      // b.re*db.im + (-b.im)*db.re (only the real part reaches the diagonal,
+      // the imaginary part is summed as on the host for the same operation count).
+      const Cx<double> bi = col[static_cast<std::size_t>(i) * npw];
+      hr = __dadd_rn(hr, __dsub_rn(__dmul_rn(bi.re, dr), __dmul_rn(-bi.im, di)));
+      hi = __dadd_rn(hi, __dadd_rn(__dmul_rn(bi.re, di), __dmul_rn(-bi.im, dr)));
+      sr = __dadd_rn(sr, __dsub_rn(__dmul_rn(bi.re, qr), __dmul_rn(-bi.im, qi)));
+      si = __dadd_rn(si, __dadd_rn(__dmul_rn(bi.re, qi), __dmul_rn(-bi.im, qr)));
+    }
+    (void)hi;
+    (void)si;
+    hdiag = __dadd_rn(hdiag, hr);
+    sdiag = __dadd_rn(sdiag, sr);
+  }
+  h_diag[g] = hdiag;
+  s_diag[g] = sdiag;
+}
+
+void paw_prepare(const Cx<double>* raw, int rows, int npw, int atoms, const int* offsets, const long long* storage,
+                 const Cx<double>* d, const Cx<double>* q, Cx<double>* b, double* h_diag, double* s_diag,
+                 unsigned int* bad, cudaStream_t stream) {
+  const dim3 tiles((npw + 31) / 32, (rows + 31) / 32);
+  if (tiles.y > 65535u) throw Overflow("PAW projector tiles exceed the grid limit");
+  paw_transpose_kernel<<<tiles, dim3(32, 8), 0, stream>>>(raw, rows, npw, b, bad);
+  SDFT_LAUNCH("paw_transpose_kernel");
+  paw_diagonal_kernel<<<(npw + 127) / 128, 128, 0, stream>>>(raw, npw, atoms, offsets, storage, d, q, h_diag, s_diag);
+  SDFT_LAUNCH("paw_diagonal_kernel");
+}
 }  // namespace
 
 Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
@@ -241,20 +324,16 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
   offsets[atoms_] = static_cast<int>(total);
   if (total > 65536) throw InvalidArgument("too many PAW projectors");
   np_ = static_cast<int>(total);
-  std::vector<Cx<double>> all_b(static_cast<std::size_t>(np_) * in.npw), d_blocks(block_total), q_blocks(block_total);
+  std::vector<Cx<double>> d_blocks(block_total), q_blocks(block_total);
   {
-    std::size_t amp_offset = 0, blk_offset = 0;
+    std::size_t blk_offset = 0;
     for (int a = 0; a < atoms_; ++a) {
       const std::size_t np = in.projectors[a];
-      std::vector<C> b(np * in.npw), d(np * np), q(np * np);
-      for (std::size_t i = 0; i < np * in.npw; ++i)
-        b[i] = C(in.amplitudes[2 * (amp_offset + i)], in.amplitudes[2 * (amp_offset + i) + 1]);
+      std::vector<C> d(np * np), q(np * np);
       for (std::size_t i = 0; i < np * np; ++i) {
         d[i] = C(in.d[2 * (blk_offset + i)], in.d[2 * (blk_offset + i) + 1]);
         q[i] = C(in.q[2 * (blk_offset + i)], in.q[2 * (blk_offset + i) + 1]);
       }
-      for (const auto& v : b)
-        if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) throw InvalidArgument("nonfinite PAW projector/D/Q data");
       for (const auto* m : {&d, &q})
         for (const auto& v : *m)
           if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) throw InvalidArgument("nonfinite PAW projector/D/Q data");
@@ -272,39 +351,14 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
                << " Q_norm=" << frobenius(q) << " Q_asymmetry=" << qe;
         throw InvalidArgument(reason.str());
       }
-      std::vector<C> ds(np * np), qs(np * np);  // symmetrised, (i,j) row-major
+      // symmetrised, column-major device storage M(i,j) at i + j*np
       for (std::size_t i = 0; i < np; ++i)
         for (std::size_t j = 0; j < np; ++j) {
-          ds[i * np + j] = .5 * (d[i * np + j] + std::conj(d[j * np + i]));
-          qs[i * np + j] = .5 * (q[i * np + j] + std::conj(q[j * np + i]));
+          const C ds = .5 * (d[i * np + j] + std::conj(d[j * np + i]));
+          const C qs = .5 * (q[i * np + j] + std::conj(q[j * np + i]));
+          d_blocks[blk_offset + i + j * np] = Cx<double>{ds.real(), ds.imag()};
+          q_blocks[blk_offset + i + j * np] = Cx<double>{qs.real(), qs.imag()};
         }
-      // column-major device storage, M(i,j) at i + j*np
-      for (std::size_t i = 0; i < np; ++i)
-        for (std::size_t j = 0; j < np; ++j) {
-          d_blocks[blk_offset + i + j * np] = Cx<double>{ds[i * np + j].real(), ds[i * np + j].imag()};
-          q_blocks[blk_offset + i + j * np] = Cx<double>{qs[i * np + j].real(), qs[i * np + j].imag()};
-        }
-      // diagonal contributions Re(b_g^H D b_g), Re(b_g^H Q b_g)
-      for (std::size_t g = 0; g < in.npw; ++g) {
-        C hd = 0, sd = 0;
-        for (std::size_t i = 0; i < np; ++i) {
-          C db = 0, qb = 0;
-          for (std::size_t j = 0; j < np; ++j) {
-            db += ds[i * np + j] * b[j * in.npw + g];
-            qb += qs[i * np + j] * b[j * in.npw + g];
-          }
-          hd += std::conj(b[i * in.npw + g]) * db;
-          sd += std::conj(b[i * in.npw + g]) * qb;
-        }
-        h_diag_[g] += hd.real();
-        s_diag_[g] += sd.real();
-      }
-      for (std::size_t i = 0; i < np; ++i)
-        for (std::size_t g = 0; g < in.npw; ++g) {
-          const C v = b[i * in.npw + g];
-          all_b[(offsets[a] + i) + g * static_cast<std::size_t>(np_)] = Cx<double>{v.real(), v.imag()};
-        }
-      amp_offset += np * in.npw;
       blk_offset += np * np;
     }
   }
@@ -320,14 +374,41 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
   std::vector<float> v32(h_local_real_.begin(), h_local_real_.end());
   upload(v32_, v32);
   if (np_) {
-    upload(b_, all_b);
-    const Split split = search_split();
-    pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
-    pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
     upload(d_, d_blocks);
     upload(q_, q_blocks);
     upload(block_offsets_, offsets);
     upload(block_storage_, storage);
+    // B: the row-major per-atom amplitudes (the input layout) are uploaded as
+    // they are, checked and transposed on the device into the column-major
+    // Sigma_np x NPW matrix; the diagonals' PAW terms Re(b_g^H D b_g) and
+    // Re(b_g^H Q b_g) are summed on the device in the host order (atoms, rows,
+    // columns) with unfused products.
+    const std::size_t entries = static_cast<std::size_t>(np_) * npw_;
+    Cx<double>* raw = nullptr;
+    SDFT_CUDA(cudaMalloc(&raw, sizeof(Cx<double>) * entries));
+    SDFT_CUDA(cudaMemcpy(raw, in.amplitudes, sizeof(Cx<double>) * entries, cudaMemcpyHostToDevice));
+    SDFT_CUDA(cudaMalloc(&b_, sizeof(Cx<double>) * entries));
+    double* diag = nullptr;
+    unsigned int* flag = nullptr;
+    SDFT_CUDA(cudaMalloc(&diag, sizeof(double) * 2 * npw_ + 16));
+    flag = reinterpret_cast<unsigned int*>(diag + 2 * npw_);
+    SDFT_CUDA(cudaMemcpy(diag, h_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice));
+    SDFT_CUDA(cudaMemcpy(diag + npw_, s_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice));
+    SDFT_CUDA(cudaMemset(flag, 0, sizeof(unsigned int)));
+    paw_prepare(raw, np_, npw_, atoms_, block_offsets_, block_storage_, d_, q_, b_, diag, diag + npw_, flag,
+                ctx.stream);
+    unsigned int bad = 0;
+    SDFT_CUDA(cudaMemcpyAsync(&bad, flag, sizeof(bad), cudaMemcpyDeviceToHost, ctx.stream));
+    SDFT_CUDA(cudaMemcpyAsync(h_diag_.data(), diag, sizeof(double) * npw_, cudaMemcpyDeviceToHost, ctx.stream));
+    SDFT_CUDA(cudaMemcpyAsync(s_diag_.data(), diag + npw_, sizeof(double) * npw_, cudaMemcpyDeviceToHost,
+                              ctx.stream));
+    SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
+    cudaFree(raw);
+    cudaFree(diag);
+    if (bad) throw InvalidArgument("nonfinite PAW projector/D/Q data");
+    const Split split = search_split();
+    pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
+    pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
   }
   SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
 }

@@ -10,13 +10,38 @@ import numpy as np
 from . import _capi as C
 from .operator import Context
 
+def fast_length(minimum: int) -> int:
+    """Smallest 2/3/5/7-smooth length >= minimum (the density grid rounding)."""
+    n = minimum
+    while True:
+        r = n
+        for p in (2, 3, 5, 7):
+            while r % p == 0:
+                r //= p
+        if r == 1:
+            return n
+        n += 1
+
+
 PBE_FIELDS = ("energy_density", "energy_per_particle", "exchange_energy_density", "correlation_energy_density",
               "exchange_potential", "correlation_potential", "gradient_squared_coefficient")
 
 
-def pbe_points(context: Context, density, gradient) -> np.ndarray:
-    """(count, 7) PbeXcPoint fields for densities n > 0 and gradient magnitudes |grad n|."""
+def pbe_points(context: Context, density, gradient):
+    """(count, 7) PbeXcPoint fields for densities n > 0 and gradient magnitudes
+    |grad n|. numpy in, numpy out (host path); torch CUDA float64 tensors in,
+    a CUDA tensor out (device path)."""
     lib = C.library()
+    if getattr(density, "is_cuda", False):
+        import torch
+        n = density.contiguous().view(-1)
+        g = gradient.contiguous().view(-1)
+        if n.dtype != torch.float64 or g.dtype != torch.float64 or n.numel() != g.numel():
+            raise ValueError("density and gradient must be float64 tensors of the same length")
+        out = torch.empty((n.numel(), 7), dtype=torch.float64, device=n.device)
+        C.check(lib.sdft_b200_pbe_points(context.handle, ctypes.c_void_p(n.data_ptr()), ctypes.c_void_p(g.data_ptr()),
+                                         n.numel(), ctypes.c_void_p(out.data_ptr()), C.DEVICE))
+        return out
     n = np.ascontiguousarray(density, dtype=np.float64).ravel()
     g = np.ascontiguousarray(gradient, dtype=np.float64).ravel()
     if n.shape != g.shape:
