@@ -31,7 +31,8 @@ typedef enum {
   SDFT_B200_RUNTIME_ERROR = 3,    /* std::runtime_error (numerical failure) */
   SDFT_B200_CUDA_ERROR = 4,       /* runtime_error("CUDA: ...") / cuBLAS / cuSOLVER */
   SDFT_B200_OUT_OF_MEMORY = 5,    /* std::bad_alloc */
-  SDFT_B200_NONFINITE = 6         /* runtime_error on a nonfinite operator result */
+  SDFT_B200_NONFINITE = 6,        /* runtime_error on a nonfinite operator result */
+  SDFT_B200_NOT_READY = 7         /* a served solve has not finished within the wait */
 } sdft_b200_status;
 
 enum { SDFT_B200_PRECISION_FP64 = 0, SDFT_B200_PRECISION_MIXED = 1 };
@@ -274,6 +275,52 @@ typedef struct {
 SDFT_B200_API sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
                                                   const double* initial, double* eigenvalues, double* eigenvectors,
                                                   double* residuals, sdft_b200_davidson_stats* stats, int memory);
+
+/* ---- Solve server: continuous batching of independent solves ------------
+ * One request = one operator (one cell, one k-point) and its Davidson solve,
+ * copied in at submit. Requests wait in a FIFO queue and start when a worker
+ * slot is free and their estimated device footprint fits under memory_cap
+ * beside the solves already running; each worker owns a stream, cuBLAS and
+ * cuSOLVER handles and scratch, so admitted solves overlap on the device and
+ * each result is the one the request gives alone. The operator and Davidson
+ * state of a running solve stay resident until it finishes.
+ * Replaces: the concurrent k-team solves over distinct operators
+ * (src/scf_core.cpp:2974-3061), one PlaneWaveOperator + solve per team. */
+typedef struct sdft_b200_server sdft_b200_server;
+
+typedef struct {
+  int slot;                           /* worker that ran the solve */
+  size_t footprint;                   /* budgeted device bytes */
+  double submitted, started, finished; /* seconds since the server started */
+} sdft_b200_solve_timing;
+
+SDFT_B200_API sdft_b200_status sdft_b200_server_create(int device, uint64_t memory_cap, int slots,
+                                                       sdft_b200_server** out);
+/* Waits for the running solves; requests still queued are answered with an error. */
+SDFT_B200_API sdft_b200_status sdft_b200_server_destroy(sdft_b200_server* server);
+/* Arguments as sdft_b200_operator_create and sdft_b200_davidson (host
+ * arrays). INVALID_ARGUMENT when the footprint exceeds the cap. */
+SDFT_B200_API sdft_b200_status sdft_b200_server_submit(sdft_b200_server* server, size_t npw, const int32_t* hkl,
+                                                       const double* kinetic_ev, size_t potential_count,
+                                                       const int32_t* potential_hkl, const double* potential,
+                                                       size_t atoms, const uint64_t* projectors,
+                                                       const double* amplitudes, const double* d, const double* q,
+                                                       double hartree_to_ev, double regularization,
+                                                       const sdft_b200_davidson_options* options, int want_vectors,
+                                                       uint64_t* ticket);
+/* Waits up to timeout seconds (negative: no limit). NOT_READY when the solve
+ * is still queued or running; otherwise the solve's own status (its message
+ * through sdft_b200_last_error), with the outputs of sdft_b200_davidson
+ * (host memory; eigenvectors only when requested at submit, may be NULL). */
+SDFT_B200_API sdft_b200_status sdft_b200_server_wait(sdft_b200_server* server, uint64_t ticket, double timeout,
+                                                     double* eigenvalues, double* eigenvectors, double* residuals,
+                                                     sdft_b200_davidson_stats* stats,
+                                                     sdft_b200_solve_timing* timing);
+SDFT_B200_API sdft_b200_status sdft_b200_server_memory(const sdft_b200_server* server, uint64_t* cap,
+                                                       uint64_t* in_use, uint64_t* peak);
+/* The device bytes a solve is budgeted at by the server's admission. */
+SDFT_B200_API sdft_b200_status sdft_b200_solve_footprint(size_t npw, const int32_t* hkl, size_t projectors_total,
+                                                         size_t roots, int subspace_factor, uint64_t* bytes);
 
 #ifdef __cplusplus
 }

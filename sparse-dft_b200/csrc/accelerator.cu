@@ -133,7 +133,7 @@ void accelerator_paw_pair(Context& ctx, std::uint64_t identity, std::size_t npw,
   ctx.synchronize();
   c.projector_identity = projector_identity;
   c.onsite_identity = identity;
-  if (umma_error_flag_read_and_clear()) throw CudaError("tensor-core GEMM wait limit exceeded");
+  if (umma_error_flag()) throw CudaError("tensor-core GEMM wait limit exceeded");
 }
 
 }  // namespace sdft_b200

@@ -185,8 +185,8 @@ __global__ void gather_support_kernel(const Cx<double>* __restrict__ grid, int n
 
 template <typename Kernel>
 void allow(Kernel kernel, std::size_t bytes) {
-  if (bytes > 227 * 1024) throw InvalidArgument("density FFT tile does not fit in shared memory");
-  SDFT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  if (bytes > kMaxDynamicSmem) throw InvalidArgument("density FFT tile does not fit in shared memory");
+  allow_dynamic_smem(kernel, bytes);
 }
 
 std::size_t pencil_smem(int n0, int tl) {

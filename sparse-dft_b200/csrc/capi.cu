@@ -12,6 +12,7 @@
 #include "band_density.cuh"
 #include "paw_density.cuh"
 #include "operator.cuh"
+#include "server.cuh"
 
 struct sdft_b200_context {
   std::unique_ptr<sdft_b200::Context> impl;
@@ -24,9 +25,30 @@ struct sdft_b200_operator {
 struct sdft_b200_compensation {
   std::unique_ptr<sdft_b200::CompensationCharge> impl;
 };
+struct sdft_b200_server {
+  std::unique_ptr<sdft_b200::SolveServer> impl;
+};
 
 namespace {
 thread_local std::string last_error;
+
+void copy_stats(const sdft_b200::DavidsonStats& st, sdft_b200_davidson_stats* stats) {
+  stats->iterations = static_cast<size_t>(st.iterations);
+  stats->converged = st.converged ? 1 : 0;
+  stats->max_residual = st.max_residual;
+  stats->seconds = st.seconds;
+  stats->rayleigh_ritz_seconds = st.rr_seconds;
+  stats->h_columns_search = static_cast<size_t>(st.h_columns_search);
+  stats->h_columns_fp64 = static_cast<size_t>(st.h_columns_fp64);
+  stats->s_columns_search = static_cast<size_t>(st.s_columns_search);
+  stats->s_columns_fp64 = static_cast<size_t>(st.s_columns_fp64);
+  stats->rayleigh_ritz_calls = st.rayleigh_ritz;
+  stats->restarts = st.restarts;
+  stats->fp64_refreshes = st.fp64_refreshes;
+  stats->certifications = st.certifications;
+  stats->handoff_iteration = st.handoff_iteration;
+  stats->block_rank_fallbacks = st.block_rank_fallbacks;
+}
 
 template <typename F>
 sdft_b200_status guarded(F&& body) {
@@ -549,7 +571,7 @@ sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int
                          static_cast<long long>(ldc), add != 0, 1.0, sdft_b200::search_split(), ctx.tc, ctx.stream);
     stage.matrix_back(c, dc, m, n, ldc);
     ctx.synchronize();
-    if (sdft_b200::umma_error_flag_read_and_clear()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
+    if (sdft_b200::umma_error_flag()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
   });
 }
 
@@ -591,24 +613,112 @@ sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davi
                                 ctx.stream));
       ctx.synchronize();
     }
-    if (stats) {
-      const auto& st = solver.stats();
-      stats->iterations = static_cast<size_t>(st.iterations);
-      stats->converged = st.converged ? 1 : 0;
-      stats->max_residual = st.max_residual;
-      stats->seconds = st.seconds;
-      stats->rayleigh_ritz_seconds = st.rr_seconds;
-      stats->h_columns_search = static_cast<size_t>(st.h_columns_search);
-      stats->h_columns_fp64 = static_cast<size_t>(st.h_columns_fp64);
-      stats->s_columns_search = static_cast<size_t>(st.s_columns_search);
-      stats->s_columns_fp64 = static_cast<size_t>(st.s_columns_fp64);
-      stats->rayleigh_ritz_calls = st.rayleigh_ritz;
-      stats->restarts = st.restarts;
-      stats->fp64_refreshes = st.fp64_refreshes;
-      stats->certifications = st.certifications;
-      stats->handoff_iteration = st.handoff_iteration;
-      stats->block_rank_fallbacks = st.block_rank_fallbacks;
+    if (stats) copy_stats(solver.stats(), stats);
+  });
+}
+
+sdft_b200_status sdft_b200_server_create(int device, uint64_t memory_cap, int slots, sdft_b200_server** out) {
+  return guarded([&] {
+    require(out != nullptr, "null server output");
+    auto server = std::make_unique<sdft_b200_server>();
+    server->impl = std::make_unique<sdft_b200::SolveServer>(device, static_cast<std::size_t>(memory_cap), slots);
+    *out = server.release();
+  });
+}
+
+sdft_b200_status sdft_b200_server_destroy(sdft_b200_server* server) {
+  return guarded([&] { delete server; });
+}
+
+sdft_b200_status sdft_b200_server_submit(sdft_b200_server* server, size_t npw, const int32_t* hkl,
+                                         const double* kinetic_ev, size_t potential_count,
+                                         const int32_t* potential_hkl, const double* potential, size_t atoms,
+                                         const uint64_t* projectors, const double* amplitudes, const double* d,
+                                         const double* q, double hartree_to_ev, double regularization,
+                                         const sdft_b200_davidson_options* options, int want_vectors,
+                                         uint64_t* ticket) {
+  return guarded([&] {
+    require(server && ticket && options && hkl && kinetic_ev && npw, "null solve request argument");
+    require(!potential_count || (potential_hkl && potential), "null potential arrays");
+    require(!atoms || (projectors && amplitudes && d && q), "null PAW arrays");
+    require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid matrix-free Davidson problem");
+    auto r = std::make_unique<sdft_b200::SolveRequest>();
+    r->hkl.assign(hkl, hkl + 3 * npw);
+    r->kinetic_ev.assign(kinetic_ev, kinetic_ev + npw);
+    r->potential_hkl.assign(potential_hkl, potential_hkl + 3 * potential_count);
+    r->potential.assign(potential, potential + 2 * potential_count);
+    std::size_t rows = 0, block = 0;
+    if (atoms) {
+      r->projectors.assign(projectors, projectors + atoms);
+      for (auto np : r->projectors) {
+        require(np >= 1 && np <= 256, "invalid PAW low-rank operator dimensions");
+        rows += np;
+        block += np * np;
+      }
+      r->amplitudes.assign(amplitudes, amplitudes + 2 * rows * npw);
+      r->d.assign(d, d + 2 * block);
+      r->q.assign(q, q + 2 * block);
     }
+    r->hartree_to_ev = hartree_to_ev;
+    r->regularization = regularization;
+    r->options.roots = static_cast<int>(options->roots);
+    r->options.max_iterations = static_cast<int>(options->max_iterations);
+    r->options.tolerance = options->tolerance;
+    r->options.precision = precision_of(options->precision);
+    r->options.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
+    r->options.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    r->vectors = want_vectors != 0;
+    *ticket = server->impl->submit(std::move(r));
+  });
+}
+
+sdft_b200_status sdft_b200_server_wait(sdft_b200_server* server, uint64_t ticket, double timeout,
+                                       double* eigenvalues, double* eigenvectors, double* residuals,
+                                       sdft_b200_davidson_stats* stats, sdft_b200_solve_timing* timing) {
+  sdft_b200::SolveResult result;
+  bool finished = false;
+  const sdft_b200_status waited = guarded([&] {
+    require(server != nullptr, "null server");
+    finished = server->impl->wait(ticket, timeout, result);
+  });
+  if (waited != SDFT_B200_OK) return waited;
+  if (!finished) {
+    last_error = "the solve has not finished";
+    return SDFT_B200_NOT_READY;
+  }
+  if (timing) {
+    timing->slot = result.slot;
+    timing->footprint = result.footprint;
+    timing->submitted = result.submitted;
+    timing->started = result.started;
+    timing->finished = result.finished;
+  }
+  if (result.status != SDFT_B200_OK) {
+    last_error = result.error;
+    return static_cast<sdft_b200_status>(result.status);
+  }
+  if (eigenvalues) std::copy(result.eigenvalues.begin(), result.eigenvalues.end(), eigenvalues);
+  if (residuals) std::copy(result.residuals.begin(), result.residuals.end(), residuals);
+  if (eigenvectors && !result.vectors.empty()) std::copy(result.vectors.begin(), result.vectors.end(), eigenvectors);
+  if (stats) copy_stats(result.stats, stats);
+  return SDFT_B200_OK;
+}
+
+sdft_b200_status sdft_b200_server_memory(const sdft_b200_server* server, uint64_t* cap, uint64_t* in_use,
+                                         uint64_t* peak) {
+  return guarded([&] {
+    require(server != nullptr, "null server");
+    if (cap) *cap = server->impl->memory_cap();
+    if (in_use) *in_use = server->impl->in_use();
+    if (peak) *peak = server->impl->peak_in_use();
+  });
+}
+
+sdft_b200_status sdft_b200_solve_footprint(size_t npw, const int32_t* hkl, size_t projectors_total, size_t roots,
+                                           int subspace_factor, uint64_t* bytes) {
+  return guarded([&] {
+    require(bytes != nullptr && roots >= 1 && roots <= npw, "invalid solve footprint arguments");
+    *bytes = sdft_b200::solve_footprint(npw, hkl, projectors_total, static_cast<int>(roots), subspace_factor);
   });
 }
 

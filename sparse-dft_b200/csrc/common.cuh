@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <stdexcept>
@@ -31,6 +32,22 @@ void count_launch();
 unsigned long long launch_count();
 #define SDFT_CUDA(call) ::sdft_b200::check_cuda((call), #call)
 #define SDFT_LAUNCH(what) (::sdft_b200::count_launch(), ::sdft_b200::check_cuda(cudaGetLastError(), what))
+
+// Largest dynamic shared memory a kernel here may take (B200 opt-in limit).
+constexpr std::size_t kMaxDynamicSmem = 227 * 1024;
+
+// Opts a kernel in to all the dynamic shared memory its static shared memory
+// leaves of kMaxDynamicSmem. The attribute is one value per kernel for the
+// whole process, so every call sets the same maximum: solvers on other
+// threads launch the same kernel with other sizes.
+template <typename Kernel>
+void allow_dynamic_smem(Kernel kernel, std::size_t bytes) {
+  cudaFuncAttributes attributes;
+  SDFT_CUDA(cudaFuncGetAttributes(&attributes, kernel));
+  const std::size_t limit = kMaxDynamicSmem - std::min(kMaxDynamicSmem, attributes.sharedSizeBytes);
+  if (bytes > limit) throw InvalidArgument("kernel tile does not fit in shared memory");
+  SDFT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(limit)));
+}
 
 // Interleaved complex in precision T (float2/double2 layout).
 template <typename T>

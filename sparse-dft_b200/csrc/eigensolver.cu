@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "dense.cuh"
@@ -43,10 +44,10 @@ constexpr int kMaxCpc = 10;
 constexpr int kRowsPerThread = 5;  // rows per thread held in registers: m <= 1280
 constexpr int kReflectorBlock = 64;
 constexpr int kInvitThreads = 4;
+constexpr int kMaxShares = 5;  // CTA shares per lane: grid <= 160
 constexpr unsigned long long kWaitNs = 2000000000ULL;
 constexpr double kClusterTolerance = 1e-9;
 
-__device__ unsigned int g_eigen_error;
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -65,48 +66,11 @@ __device__ __forceinline__ Cx<double> cdot1(Cx<double> a, Cx<double> b) {
   return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
 }
 
-// Sum of N complex values over the CTA in a fixed order; result in out[0..N).
-template <int N>
-__device__ void block_sum(Cx<double> (&v)[N], int count, Cx<double>* scratch, Cx<double>* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < N; ++q) {
-    if (q < count) {
-      double re = v[q].re, im = v[q].im;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_xor_sync(0xffffffffu, re, o);
-        im += __shfl_xor_sync(0xffffffffu, im, o);
-      }
-      if (lane == 0) scratch[warp * N + q] = Cx<double>{re, im};
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < count) {
-    Cx<double> s{0.0, 0.0};
-    for (int w = 0; w < kWarps; ++w) s = cadd(s, scratch[w * N + threadIdx.x]);
-    out[threadIdx.x] = s;
-  }
-  __syncthreads();
-}
-
-__device__ double block_sum_real(double v, double* scratch) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) scratch[warp] = v;
-  __syncthreads();
-  double s = 0.0;
-  for (int w = 0; w < kWarps; ++w) s += scratch[w];
-  __syncthreads();
-  return s;
-}
-
 // Counting grid barrier with a time limit. Returns false (and every CTA
 // should return) when the limit expired here or the error word is set. The
 // CTA's writes (ordered before thread 0 by __syncthreads) are released by the
 // arrival; the acquire fence after the wait orders the reads that follow.
-__device__ bool grid_barrier(unsigned int* arrive, unsigned int target, int* ok) {
+__device__ bool grid_barrier(unsigned int* arrive, unsigned int* error, unsigned int target, int* ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(arrive) : "memory");
@@ -116,12 +80,12 @@ __device__ bool grid_barrier(unsigned int* arrive, unsigned int target, int* ok)
       unsigned int cur;
       asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(arrive) : "memory");
       if (cur >= target) break;
-      if (*reinterpret_cast<volatile unsigned int*>(&g_eigen_error) != 0u) {
+      if (*reinterpret_cast<volatile unsigned int*>(error) != 0u) {
         good = 0;
         break;
       }
       if (global_ns() - start > kWaitNs) {
-        atomicOr(&g_eigen_error, 1u);
+        atomicOr(error, 1u);
         good = 0;
         break;
       }
@@ -144,31 +108,54 @@ struct TridiagArgs {
   Cx<double>* pbuf;        // 2 x m
   Cx<double>* dotbuf;      // 2 x grid
   unsigned int* arrive;
+  unsigned int* error;  // set when a barrier wait runs out; every CTA then returns
 };
 
-struct StepScalars {
-  Cx<double> tau, scale, alpha_in;
-  double beta, diag;
-  int trivial;
+// Reflector scalars of one Householder step, formed redundantly by every
+// thread from the same shared inputs (so every thread holds equal values).
+struct Reflector {
+  Cx<double> tau, scale;
+  double beta;
+  bool trivial;
 };
+
+__device__ __forceinline__ Reflector make_reflector(Cx<double> alpha, double xnorm2) {
+  Reflector h;
+  if (xnorm2 == 0.0 && alpha.im == 0.0) {
+    h.trivial = true;
+    h.tau = Cx<double>{0.0, 0.0};
+    h.beta = alpha.re;
+    h.scale = Cx<double>{0.0, 0.0};
+  } else {
+    const double beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + xnorm2), alpha.re);
+    h.trivial = false;
+    h.tau = Cx<double>{(beta - alpha.re) / beta, -alpha.im / beta};
+    h.beta = beta;
+    // 1 / (alpha - beta)
+    const double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
+    h.scale = Cx<double>{dr / den, -di / den};
+  }
+  return h;
+}
 
 // Rows r = tid + kThreads k of the reflector and rank-2 vectors live in
 // registers; own columns c = cta + G s in shared memory. Step j+1's reflector
 // is formed before step j's rank-2 update, so the update of each own column
-// and its product with the next reflector share one pass.
+// and its product with the next reflector share one pass. Per step: one CTA
+// barrier for the next column's norm, one for the column products, and the
+// grid barrier.
 __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int R = kRowsPerThread;
   const int m = t.m, G = t.grid, cpc = t.cpc, cta = blockIdx.x, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   Cx<double>* cols = reinterpret_cast<Cx<double>*>(smem_raw);
-  Cx<double>* red = cols + static_cast<long long>(cpc) * m;  // kWarps * kMaxCpc
-  Cx<double>* res = red + kWarps * kMaxCpc;                   // kMaxCpc
-  Cx<double>* colv = res + kMaxCpc;                           // v at own column indices
-  Cx<double>* colw = colv + kMaxCpc;                          // w at own column indices
-  double* rred = reinterpret_cast<double*>(colw + kMaxCpc);   // kWarps
+  Cx<double>* red = cols + static_cast<long long>(cpc) * m;  // kWarps x kMaxCpc column-product partials
+  Cx<double>* colv = red + kWarps * kMaxCpc;                  // 2 x kMaxCpc: v at own columns, by step parity
+  Cx<double>* colw = colv + 2 * kMaxCpc;                      // kMaxCpc: w at own columns
+  Cx<double>* pick = colw + kMaxCpc;                          // alpha (row jc+1), diagonal (row jc)
+  double* nrm = reinterpret_cast<double*>(pick + 2);          // kWarps norm partials
   __shared__ int ok;
-  __shared__ StepScalars sc;
-  __shared__ Cx<double> head_v, head_w;  // v[j+1], w[j+1]
 
   int slot_of_row[R];
 #pragma unroll
@@ -183,72 +170,85 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
   }
 
   Cx<double> v[R], w[R], vn[R], col[R];
+  Reflector cur, next;
 
   // Reflector of column jc from col[] (rows >= jc): vn[] for rows >= jc+1,
-  // the shared scalars, and CTA 0's outputs.
-  auto reflect = [&](int jc) {
+  // v at own columns into colv[jc & 1], and CTA 0's outputs. Contains the
+  // step's first CTA barrier (after which colw, written before it, is visible).
+  auto reflect = [&](int jc) -> Reflector {
     double part = 0.0;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int r = tid + k * kThreads;
       if (r < m && r >= jc + 2) part += col[k].re * col[k].re + col[k].im * col[k].im;
-      if (r == jc + 1) sc.alpha_in = col[k];
-      if (r == jc) sc.diag = col[k].re;
+      if (r == jc + 1) pick[0] = col[k];
+      if (r == jc) pick[1] = col[k];
     }
-    const double xnorm2 = block_sum_real(part, rred);
-    if (tid == 0) {
-      const Cx<double> alpha = sc.alpha_in;
-      if (xnorm2 == 0.0 && alpha.im == 0.0) {
-        sc.trivial = 1;
-        sc.tau = Cx<double>{0.0, 0.0};
-        sc.beta = alpha.re;
-        sc.scale = Cx<double>{0.0, 0.0};
-      } else {
-        const double beta = -copysign(sqrt(alpha.re * alpha.re + alpha.im * alpha.im + xnorm2), alpha.re);
-        sc.trivial = 0;
-        sc.tau = Cx<double>{(beta - alpha.re) / beta, -alpha.im / beta};
-        sc.beta = beta;
-        // 1 / (alpha - beta)
-        const double dr = alpha.re - beta, di = alpha.im, den = dr * dr + di * di;
-        sc.scale = Cx<double>{dr / den, -di / den};
-      }
-      if (cta == 0) {
-        t.d[jc] = sc.diag;
-        t.e[jc] = sc.beta;
-        t.tau[jc] = sc.tau;
-      }
-    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) nrm[warp] = part;
     __syncthreads();
-    const Cx<double> scale = sc.scale;
-    const int trivial = sc.trivial;
+    double xnorm2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < kWarps; ++q) xnorm2 += nrm[q];
+    const Reflector h = make_reflector(pick[0], xnorm2);
+    if (cta == 0 && tid == 0) {
+      t.d[jc] = pick[1].re;
+      t.e[jc] = h.beta;
+      t.tau[jc] = h.tau;
+    }
+    Cx<double>* cv = colv + (jc & 1) * kMaxCpc;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int r = tid + k * kThreads;
       Cx<double> vr{0.0, 0.0};
       if (r == jc + 1) vr = Cx<double>{1.0, 0.0};
-      else if (r > jc + 1 && r < m && !trivial) vr = cmulz(col[k], scale);
+      else if (r > jc + 1 && r < m && !h.trivial) vr = cmulz(col[k], h.scale);
       vn[k] = vr;
       if (cta == 0 && r > jc && r < m) t.reflectors[r + static_cast<long long>(jc) * m] = vr;
+      if (slot_of_row[k] >= 0) cv[slot_of_row[k]] = vr;
     }
+    return h;
   };
 
-  // p for own columns c > jc and the CTA share of p^H v (v at own columns in colv).
-  auto publish = [&](int jc, Cx<double> (&acc)[kMaxCpc]) {
-    block_sum<kMaxCpc>(acc, cpc, red, res);
-    if (tid < 32) {
+  // Column products conj(A(:,c)) . vn over the CTA (acc), then p = tau A v at
+  // own columns c > jc, the CTA share of p^H v, and column jc+1 published.
+  auto publish = [&](int jc, const Reflector& h, Cx<double> (&acc)[kMaxCpc]) {
+#pragma unroll
+    for (int q = 0; q < kMaxCpc; ++q) {
+      if (q < cpc) {
+        double re = acc[q].re, im = acc[q].im;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          re += __shfl_xor_sync(0xffffffffu, re, o);
+          im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) red[warp * kMaxCpc + q] = Cx<double>{re, im};
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
       Cx<double> dot{0.0, 0.0};
-      const int c = cta + tid * G;
-      if (tid < cpc && c > jc && c < m) {
-        const Cx<double> p = cmulz(sc.tau, res[tid]);
+      const int c = cta + lane * G;
+      if (lane < cpc && c > jc && c < m) {
+        Cx<double> s{0.0, 0.0};
+        for (int q = 0; q < kWarps; ++q) s = cadd(s, red[q * kMaxCpc + lane]);
+        const Cx<double> p = cmulz(h.tau, s);
         t.pbuf[static_cast<long long>(jc & 1) * m + c] = p;
-        dot = cdot1(p, colv[tid]);
+        dot = cdot1(p, colv[(jc & 1) * kMaxCpc + lane]);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         dot.re += __shfl_xor_sync(0xffffffffu, dot.re, o);
         dot.im += __shfl_xor_sync(0xffffffffu, dot.im, o);
       }
-      if (tid == 0) t.dotbuf[static_cast<long long>(jc & 1) * G + cta] = dot;
+      if (lane == 0) t.dotbuf[static_cast<long long>(jc & 1) * G + cta] = dot;
+    }
+    // Column jc+1 (updates 0..jc-1 applied) for step jc+1.
+    if (jc + 1 < m && (jc + 1) % G == cta) {
+      const long long slot = (jc + 1) / G;
+      Cx<double>* dst = t.colbuf + static_cast<long long>((jc + 1) & 1) * m;
+      for (int r = jc + 1 + tid; r < m; r += kThreads) dst[r] = cols[slot * m + r];
     }
   };
 
@@ -258,19 +258,15 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     const int r = tid + k * kThreads;
     col[k] = r < m ? t.a[r] : Cx<double>{0.0, 0.0};
   }
-  __syncthreads();
-  reflect(0);
+  __syncthreads();  // own columns in shared memory
+  cur = reflect(0);
 #pragma unroll
-  for (int k = 0; k < R; ++k) {
-    v[k] = vn[k];
-    if (slot_of_row[k] >= 0) colv[slot_of_row[k]] = v[k];
-  }
+  for (int k = 0; k < R; ++k) v[k] = vn[k];
   {
     Cx<double> acc[kMaxCpc];
 #pragma unroll
-    for (int q = 0; q < kMaxCpc; ++q) acc[q] = Cx<double>{0.0, 0.0};
-#pragma unroll
     for (int q = 0; q < kMaxCpc; ++q) {
+      acc[q] = Cx<double>{0.0, 0.0};
       const int c = cta + q * G;
       if (q >= cpc || c < 1 || c >= m) continue;
       const Cx<double>* a = cols + static_cast<long long>(q) * m;
@@ -280,87 +276,77 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
         if (r >= 1 && r < m) acc[q] = cadd(acc[q], cdot1(a[r], v[k]));
       }
     }
-    __syncthreads();  // colv visible
-    publish(0, acc);
-    if (1 % G == cta)
-      for (int r = 1 + tid; r < m; r += kThreads) t.colbuf[m + r] = cols[static_cast<long long>(1 / G) * m + r];
+    publish(0, cur, acc);
   }
-  if (!grid_barrier(t.arrive, static_cast<unsigned int>(G), &ok)) return;
+  if (!grid_barrier(t.arrive, t.error, static_cast<unsigned int>(G), &ok)) return;
 
   for (int j = 0; j < m - 1; ++j) {
     const bool last = j == m - 2;
-    // w = p - tau/2 (p^H v) v; column j+1 (updates 0..j-1) prefetched.
+    // All of this step's global reads first (one round of L2 latency): p on
+    // own rows, column j+1, p at own columns and at row j+1, the CTA shares
+    // of p^H v (every warp sums them in the same order).
     const double2* pb = reinterpret_cast<const double2*>(t.pbuf + static_cast<long long>(j & 1) * m);
     const double2* cb = reinterpret_cast<const double2*>(t.colbuf + static_cast<long long>((j + 1) & 1) * m);
-    const int trivial = sc.trivial;
-    const Cx<double> tau = sc.tau;
-    Cx<double> pv[R];
+    const double2* db = reinterpret_cast<const double2*>(t.dotbuf + static_cast<long long>(j & 1) * G);
+    const double2 zero2 = make_double2(0.0, 0.0);
+    double2 pq[R], cq[R], shares[kMaxShares];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int r = tid + k * kThreads;
-      pv[k] = Cx<double>{0.0, 0.0};
-      col[k] = Cx<double>{0.0, 0.0};
-      if (r > j && r < m) {
-        if (!trivial) {
-          const double2 q = __ldcg(pb + r);
-          pv[k] = Cx<double>{q.x, q.y};
-        }
-        if (!last) {
-          const double2 q = __ldcg(cb + r);
-          col[k] = Cx<double>{q.x, q.y};
-        }
-      }
+      const bool row = r > j && r < m;
+      pq[k] = (row && !cur.trivial) ? __ldcg(pb + r) : zero2;
+      cq[k] = (row && !last) ? __ldcg(cb + r) : zero2;
     }
-    if (tid < 32) {
-      Cx<double> sum{0.0, 0.0};
-      if (!trivial) {
-        const double2* db = reinterpret_cast<const double2*>(t.dotbuf + static_cast<long long>(j & 1) * G);
-        for (int g = tid; g < G; g += 32) {
-          const double2 q = __ldcg(db + g);
-          sum = cadd(sum, Cx<double>{q.x, q.y});
-        }
+    const int own_c = cta + tid * G;
+    const bool own_w = !cur.trivial && tid < cpc && own_c > j && own_c < m;
+    const double2 pc = own_w ? __ldcg(pb + own_c) : zero2;
+    const double2 ph = cur.trivial ? zero2 : __ldcg(pb + j + 1);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          sum.re += __shfl_xor_sync(0xffffffffu, sum.re, o);
-          sum.im += __shfl_xor_sync(0xffffffffu, sum.im, o);
-        }
-      }
-      if (tid == 0) res[0] = cmulz(Cx<double>{-0.5 * tau.re, -0.5 * tau.im}, sum);
+    for (int i = 0; i < kMaxShares; ++i) {
+      const int g = lane + 32 * i;
+      shares[i] = (!cur.trivial && g < G) ? __ldcg(db + g) : zero2;
     }
-    __syncthreads();
-    const Cx<double> alpha = res[0];
+    Cx<double> sum{0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < kMaxShares; ++i) sum = cadd(sum, Cx<double>{shares[i].x, shares[i].y});
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sum.re += __shfl_xor_sync(0xffffffffu, sum.re, o);
+      sum.im += __shfl_xor_sync(0xffffffffu, sum.im, o);
+    }
+    const Cx<double> alpha = cmulz(Cx<double>{-0.5 * cur.tau.re, -0.5 * cur.tau.im}, sum);
+    // w = p + alpha v on own rows; w at own columns for the update; w[j+1] (v[j+1] = 1).
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int r = tid + k * kThreads;
-      w[k] = (r > j && r < m) ? cadd(pv[k], cmulz(alpha, v[k])) : Cx<double>{0.0, 0.0};
-      if (slot_of_row[k] >= 0) colw[slot_of_row[k]] = w[k];
-      if (r == j + 1) {
-        head_v = v[k];
-        head_w = w[k];
-      }
+      w[k] = (r > j && r < m && !cur.trivial) ? cadd(Cx<double>{pq[k].x, pq[k].y}, cmulz(alpha, v[k]))
+                                               : Cx<double>{0.0, 0.0};
+      col[k] = Cx<double>{cq[k].x, cq[k].y};
     }
-    __syncthreads();
+    const Cx<double> head_w = cur.trivial ? Cx<double>{0.0, 0.0} : cadd(Cx<double>{ph.x, ph.y}, alpha);
+    if (own_w) colw[tid] = cadd(Cx<double>{pc.x, pc.y}, cmulz(alpha, colv[(j & 1) * kMaxCpc + tid]));
 
     // Step j+1's reflector from column j+1 with update j applied.
     if (!last) {
-      const Cx<double> hv = cconj(head_v), hw = cconj(head_w);
+      const Cx<double> hw = cconj(head_w);
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const int r = tid + k * kThreads;
-        if (r > j && r < m) col[k] = csub(col[k], cadd(cmulz(v[k], hw), cmulz(w[k], hv)));
+        if (r > j && r < m) col[k] = csub(col[k], cadd(cmulz(v[k], hw), w[k]));
       }
-      reflect(j + 1);
+      next = reflect(j + 1);
+    } else {
+      __syncthreads();  // colw visible
     }
 
     // Update j on own columns c > j; p_{j+1} partial sums over rows/columns > j+1.
     Cx<double> acc[kMaxCpc];
 #pragma unroll
-    for (int q = 0; q < kMaxCpc; ++q) acc[q] = Cx<double>{0.0, 0.0};
-#pragma unroll
     for (int q = 0; q < kMaxCpc; ++q) {
+      acc[q] = Cx<double>{0.0, 0.0};
       const int c = cta + q * G;
       if (q >= cpc || c <= j || c >= m) continue;
-      const Cx<double> wc = cconj(colw[q]), vc = cconj(colv[q]);
+      const Cx<double> wc = cconj(colw[q]), vc = cconj(colv[(j & 1) * kMaxCpc + q]);
       Cx<double>* a = cols + static_cast<long long>(q) * m;
       const bool dot_column = !last && c > j + 1;
 #pragma unroll
@@ -368,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
         const int r = tid + k * kThreads;
         if (r > j && r < m) {
           Cx<double> x = a[r];
-          if (!trivial) {
+          if (!cur.trivial) {
             x = csub(x, cadd(cmulz(v[k], wc), cmulz(w[k], vc)));
             a[r] = x;
           }
@@ -377,21 +363,12 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
       }
     }
     if (last) break;
-    __syncthreads();  // every thread is done with colv/colw of step j
+    publish(j + 1, next, acc);
+    if (!grid_barrier(t.arrive, t.error, static_cast<unsigned int>(G) * static_cast<unsigned int>(j + 2), &ok))
+      return;
+    cur = next;
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-      v[k] = vn[k];
-      if (slot_of_row[k] >= 0) colv[slot_of_row[k]] = v[k];
-    }
-    __syncthreads();
-    publish(j + 1, acc);
-    // Column j+2 (updates 0..j) for step j+2.
-    if (j + 2 < m && (j + 2) % G == cta) {
-      const long long slot = (j + 2) / G;
-      Cx<double>* dst = t.colbuf + static_cast<long long>((j + 2) & 1) * m;
-      for (int r = j + 2 + tid; r < m; r += kThreads) dst[r] = cols[slot * m + r];
-    }
-    if (!grid_barrier(t.arrive, static_cast<unsigned int>(G) * static_cast<unsigned int>(j + 2), &ok)) return;
+    for (int k = 0; k < R; ++k) v[k] = vn[k];
   }
   __syncthreads();
   if ((m - 1) % G == cta && tid == 0) t.d[m - 1] = cols[static_cast<long long>((m - 1) / G) * m + m - 1].re;
@@ -708,7 +685,7 @@ int sm_count() {
 }
 
 std::size_t tridiag_smem(int m, int cpc) {
-  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc) * m + kWarps * kMaxCpc + 3 * kMaxCpc) +
+  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc) * m + kWarps * kMaxCpc + 3 * kMaxCpc + 2) +
          sizeof(double) * kWarps;
 }
 
@@ -720,11 +697,55 @@ constexpr std::size_t kBlockSmem = sizeof(Cx<double>) * (16 + 2 * kReflectorBloc
 
 }  // namespace
 
+namespace {
+// Cooperative kernels that fill every SM must not run at the same time (two
+// of them could each hold part of the SMs and wait on each other's missing
+// CTAs), so every solver on a device, whatever its stream, launches them in
+// order on one shared stream: the caller's stream hands over with an event
+// and waits for the kernel's completion event.
+struct CooperativeLane {
+  std::mutex mutex;
+  cudaStream_t stream = nullptr;
+};
+
+CooperativeLane& cooperative_lane(int device) {
+  static CooperativeLane lanes[64];
+  if (device < 0 || device >= 64) throw InvalidArgument("device ordinal out of range");
+  return lanes[device];
+}
+
+void cooperative_launch(void* kernel, int grid, int threads, TridiagArgs& args, std::size_t smem, cudaStream_t stream) {
+  int device = 0;
+  SDFT_CUDA(cudaGetDevice(&device));
+  CooperativeLane& lane = cooperative_lane(device);
+  cudaEvent_t ready = nullptr, done = nullptr;
+  SDFT_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  SDFT_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+  try {
+    std::lock_guard<std::mutex> lock(lane.mutex);
+    if (!lane.stream) SDFT_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking));
+    SDFT_CUDA(cudaEventRecord(ready, stream));
+    SDFT_CUDA(cudaStreamWaitEvent(lane.stream, ready, 0));
+    void* params[] = {&args};
+    SDFT_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(threads), params, smem, lane.stream));
+    SDFT_LAUNCH("tridiagonalize_kernel");
+    SDFT_CUDA(cudaEventRecord(done, lane.stream));
+    SDFT_CUDA(cudaStreamWaitEvent(stream, done, 0));
+  } catch (...) {
+    cudaEventDestroy(ready);
+    cudaEventDestroy(done);
+    throw;
+  }
+  cudaEventDestroy(ready);  // released once the recorded work completes
+  cudaEventDestroy(done);
+}
+}  // namespace
+
 int hermitian_eigen_max_order() {
   const int g = sm_count();
   int best = 0;
   for (int m = 2; m <= 4096; ++m) {
-    const int grid = std::min(g, m);
+    const int grid = std::min({g, m, 32 * kMaxShares});
     const int cpc = (m + grid - 1) / grid;
     if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit || m > kRowsPerThread * kThreads ||
         invit_smem(m) > kSmemLimit)
@@ -737,7 +758,7 @@ int hermitian_eigen_max_order() {
 void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors,
                       EigenWorkspace& ws, cudaStream_t stream) {
   if (m < 2 || wanted < 1 || wanted > m) throw InvalidArgument("invalid Hermitian eigenproblem size");
-  const int grid = std::min(sm_count(), m);
+  const int grid = std::min({sm_count(), m, 32 * kMaxShares});
   const int cpc = (m + grid - 1) / grid;
   const std::size_t smem = tridiag_smem(m, cpc);
   if (cpc > kMaxCpc || smem > kSmemLimit) throw InvalidArgument("Hermitian eigenproblem too large for the device solver");
@@ -754,31 +775,35 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   Cx<double>* colbuf = reflectors + mm * mm;
   Cx<double>* pbuf = colbuf + 2 * mm;
   Cx<double>* dotbuf = pbuf + 2 * mm;
-  SDFT_CUDA(cudaMemsetAsync(arrive, 0, sizeof(unsigned int), stream));
+  unsigned int* error_word = arrive + 1;
+  SDFT_CUDA(cudaMemsetAsync(arrive, 0, 2 * sizeof(unsigned int), stream));
   // Entries above each reflector's unit element stay zero for the block products.
   SDFT_CUDA(cudaMemsetAsync(reflectors, 0, sizeof(Cx<double>) * mm * mm, stream));
-  const unsigned int zero = 0;
-  SDFT_CUDA(cudaMemcpyToSymbolAsync(g_eigen_error, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, stream));
 
-  SDFT_CUDA(cudaFuncSetAttribute(tridiagonalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
+  allow_dynamic_smem(tridiagonalize_kernel, smem);
   int per_sm = 0;
   SDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tridiagonalize_kernel, kThreads, smem));
   if (per_sm < 1) throw InvalidArgument("tridiagonalization kernel cannot be resident");
-  TridiagArgs t{a, m, grid, cpc, d, e, tau, reflectors, colbuf, pbuf, dotbuf, arrive};
-  void* args[] = {&t};
-  SDFT_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(tridiagonalize_kernel), dim3(grid), dim3(kThreads),
-                                        args, smem, stream));
-  SDFT_LAUNCH("tridiagonalize_kernel");
+  // SDFT_B200_TRACE: device times of the stages, printed after the final synchronisation.
+  static const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
+  cudaEvent_t marks[6] = {};
+  if (trace)
+    for (auto& ev : marks) SDFT_CUDA(cudaEventCreate(&ev));
+  auto mark = [&](int i) {
+    if (trace) SDFT_CUDA(cudaEventRecord(marks[i], stream));
+  };
+  mark(0);
+  TridiagArgs t{a, m, grid, cpc, d, e, tau, reflectors, colbuf, pbuf, dotbuf, arrive, error_word};
+  cooperative_launch(reinterpret_cast<void*>(tridiagonalize_kernel), grid, kThreads, t, smem, stream);
+  mark(1);
 
   const int warps_per_block = 4;
   const std::size_t bisect_smem = sizeof(double) * 2 * mm;
-  if (bisect_smem > 48 * 1024)
-    SDFT_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(bisect_smem)));
+  allow_dynamic_smem(bisect_kernel, bisect_smem);
   bisect_kernel<<<static_cast<unsigned>(ceil_div(wanted, warps_per_block)), 32 * warps_per_block, bisect_smem,
                   stream>>>(d, e, m, wanted, values);
   SDFT_LAUNCH("bisect_kernel");
+  mark(2);
 
   const int blocks = static_cast<int>(ceil_div(m - 1, kReflectorBlock));
   const std::size_t vbytes =
@@ -790,16 +815,16 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   Cx<double>* wtmp = tfac + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
   Cx<double>* utmp = wtmp + static_cast<std::size_t>(wanted) * kReflectorBlock;
   const std::size_t inv_smem = invit_smem(m);
-  SDFT_CUDA(cudaFuncSetAttribute(inverse_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(inv_smem)));
+  allow_dynamic_smem(inverse_iteration_kernel, inv_smem);
   inverse_iteration_kernel<<<static_cast<unsigned>(ceil_div(wanted, kInvitThreads)), kInvitThreads, inv_smem,
                              stream>>>(d, e, m, wanted, values, zt);
   SDFT_LAUNCH("inverse_iteration_kernel");
+  mark(3);
 
-  SDFT_CUDA(cudaFuncSetAttribute(reflector_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kBlockSmem)));
+  allow_dynamic_smem(reflector_blocks_kernel, kBlockSmem);
   reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, kBlockSmem, stream>>>(reflectors, tau, m, tfac);
   SDFT_LAUNCH("reflector_blocks_kernel");
+  mark(4);
 
   // X = Q Z: blocks from the last to the first, X <- X - V (T (V^H X)) on rows > j0.
   const long long total = static_cast<long long>(m) * wanted;
@@ -817,10 +842,20 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
     zgemm(blas, Op::N, Op::N, nb, wanted, nb, tb, kReflectorBlock, wtmp, kReflectorBlock, utmp, kReflectorBlock, false);
     zgemm(blas, Op::N, Op::N, rows, wanted, nb, vb, m, utmp, kReflectorBlock, xs, m, true, -1.0);
   }
+  mark(5);
 
   unsigned int error = 0;
-  SDFT_CUDA(cudaMemcpyFromSymbolAsync(&error, g_eigen_error, sizeof(error), 0, cudaMemcpyDeviceToHost, stream));
+  SDFT_CUDA(cudaMemcpyAsync(&error, error_word, sizeof(error), cudaMemcpyDeviceToHost, stream));
   SDFT_CUDA(cudaStreamSynchronize(stream));
+  if (trace) {
+    float ms[5];
+    for (int i = 0; i < 5; ++i) SDFT_CUDA(cudaEventElapsedTime(&ms[i], marks[i], marks[i + 1]));
+    std::fprintf(stderr,
+                 "hermitian-lowest m=%d wanted=%d tridiagonalize=%.3fms bisect=%.3fms inverse_iteration=%.3fms "
+                 "reflector_blocks=%.3fms back_transform=%.3fms\n",
+                 m, wanted, ms[0], ms[1], ms[2], ms[3], ms[4]);
+    for (auto& ev : marks) cudaEventDestroy(ev);
+  }
   if (error) throw CudaError("tridiagonalization barrier wait limit exceeded");
 }
 
@@ -871,7 +906,7 @@ void check_solver(cusolverStatus_t status, const char* what) {
 
 void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<double>* h, Cx<double>* s, int m,
                         int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws, RitzSolver mode,
-                        cudaStream_t st, double max_deviation) {
+                        cudaStream_t st, double max_deviation, double first_order_limit) {
   if (m < 1 || wanted < 1 || wanted > m) throw InvalidArgument("invalid Rayleigh-Ritz dimensions");
   const std::size_t mm = static_cast<std::size_t>(m);
   if (mode == RitzSolver::Device && m >= 2 && m <= hermitian_eigen_max_order()) {
@@ -880,9 +915,9 @@ void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<doubl
     static const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
     if (trace)
       std::fprintf(stderr, "rayleigh-ritz m=%d |S-I|max=%.3e path=%s\n", m, deviation,
-                   deviation <= 1e-8 ? "device" : deviation <= max_deviation ? "device-loewdin2" : "cusolver");
-    if (deviation <= 1e-8) {
-      // First order: H' = H - (E H + H E)/2, y -> y - E y / 2 (error O(|E|^2) <= 1e-16).
+                   deviation <= first_order_limit ? "device" : deviation <= max_deviation ? "device-loewdin2" : "cusolver");
+    if (deviation <= first_order_limit) {
+      // First order: H' = H - (E H + H E)/2, y -> y - E y / 2 (error O(|E|^2)).
       const bool correct = deviation > 1e-14;
       Cx<double>* f = nullptr;
       if (correct) {

@@ -45,16 +45,20 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
 // Full), leading dimension m, may alias h, S-orthonormal.
 // Device solver on S = I + E: nothing when max |E| <= 1e-14; the
 // first-order Loewdin transform C = I - E/2 (H' = H - (E H + H E)/2,
-// y -> y - E y/2, error O(|E|^2)) up to 1e-8; the second-order C = I - E/2 +
-// 3/8 E^2 (H' = C H C, y -> C y, error O(|E|^3)) up to max_deviation.
+// y -> y - E y/2, error O(|E|^2)) up to first_order_limit; the second-order
+// C = I - E/2 + 3/8 E^2 (H' = C H C, y -> C y, error O(|E|^3)) up to
+// max_deviation.
 // Beyond that, or when m exceeds hermitian_eigen_max_order(), cuSOLVER
 // zhegvdx solves the pencil.
 void generalized_lowest(cublasHandle_t blas, cusolverDnHandle_t solver, Cx<double>* h, Cx<double>* s, int m,
                         int wanted, double* values, Cx<double>* vectors, EigenWorkspace& ws, RitzSolver mode,
-                        cudaStream_t stream, double max_deviation = 1e-5);
+                        cudaStream_t stream, double max_deviation = 1e-5, double first_order_limit = 1e-8);
 
 // b <- b - I (m x m, leading dimension m); returns max |entry| of the result.
 double identity_deviation(Cx<double>* b, int m, EigenWorkspace& ws, cudaStream_t stream);
+
+// b <- b + I (m x m, leading dimension m).
+void add_identity(Cx<double>* b, int m, cudaStream_t stream);
 
 // a <- a - (f + f^H) / 2 (m x m, leading dimension m).
 void lowdin_combine(Cx<double>* a, const Cx<double>* f, int m, cudaStream_t stream);

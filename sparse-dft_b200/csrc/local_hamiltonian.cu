@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(kThreads) fft_rows_kernel(Cx<T>* __restrict__ 
 
 template <typename Kernel>
 void allow_smem(Kernel kernel, std::size_t bytes) {
-  if (bytes > 227 * 1024) throw InvalidArgument("FFT tile does not fit in shared memory");
-  SDFT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  if (bytes > kMaxDynamicSmem) throw InvalidArgument("FFT tile does not fit in shared memory");
+  allow_dynamic_smem(kernel, bytes);
 }
 
 // Pencil pass with the compile-time kernel for the common axis lengths.

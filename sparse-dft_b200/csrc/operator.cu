@@ -153,6 +153,14 @@ Context::~Context() {
 
 void Context::synchronize() const { SDFT_CUDA(cudaStreamSynchronize(stream)); }
 
+void Context::release_scratch() {
+  synchronize();
+  for (Scratch* s : {&slab32, &slab64, &staging_in, &staging_out, &staging_aux, &projections, &onsite, &tc.a, &tc.b,
+                     &tc.partial, &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
+                     &eigen.solver_work})
+    s->release();
+}
+
 GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
                                 double hartree_to_ev) {
   if (cutoff_ev <= 0.0 || !std::isfinite(cutoff_ev)) throw InvalidArgument("plane-wave cutoff must be finite and positive");

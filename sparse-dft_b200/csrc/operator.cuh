@@ -64,6 +64,8 @@ struct Context {
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
   void synchronize() const;
+  // Frees every scratch buffer (they grow again on demand).
+  void release_scratch();
 };
 
 // Accelerator-style calls on caller host arrays (accelerator.cu).

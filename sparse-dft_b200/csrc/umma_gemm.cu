@@ -427,8 +427,7 @@ void launch(const std::uint16_t* a, long long lda, const std::uint16_t* b, long 
             long long kexp, const EpilogueArgs& ep_in, int splits, int k_blocks, int kpb, cudaStream_t stream) {
   constexpr int S = stages<BN>();
   const std::size_t smem = static_cast<std::size_t>(S) * (BM * BK * 2 + BN * BK * 2) + 1024 + 256;
-  SDFT_CUDA(cudaFuncSetAttribute(umma_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
+  allow_dynamic_smem(umma_gemm_kernel<BN>, smem);
   const CUtensorMap map_a = kmajor_map(a, m, kexp, lda, BM);
   const CUtensorMap map_b = kmajor_map(b, n2, kexp, ldb, BN);
   const dim3 grid(static_cast<unsigned>(ceil_div(m, BM)), static_cast<unsigned>(ceil_div(n2, BN)), splits);
@@ -504,9 +503,20 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
   const bool wide = n2 > 128;
   const int bn = wide ? 256 : 128;
   const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n2, bn));
-  int splits = static_cast<int>(std::min<long long>(std::max<long long>(1, (2 * 148 + tiles - 1) / tiles),
-                                                    std::max(1, k_blocks / 8)));
-  splits = std::min(splits, 128);
+  // Split-K count: one CTA per SM is resident (the ring takes ~190 KB), so the
+  // time goes as waves x K blocks per CTA; take the split that minimises it
+  // (the smallest on ties), with at least 8 K blocks per split.
+  const long long max_splits = std::min<long long>(128, std::max(1, k_blocks / 8));
+  long long best_cost = -1;
+  int splits = 1;
+  for (long long s = 1; s <= max_splits; ++s) {
+    const long long waves = (tiles * s + 147) / 148;
+    const long long cost = waves * ((k_blocks + s - 1) / s);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      splits = static_cast<int>(s);
+    }
+  }
   const int kpb = static_cast<int>(ceil_div(k_blocks, splits));
   splits = static_cast<int>(ceil_div(k_blocks, kpb));
   EpilogueArgs ep{m, n2, nullptr, c, ldc, alpha, add ? 1 : 0};
@@ -569,10 +579,9 @@ void gemm_tc(Op aop, int m, int n, int k, const Cx<double>* a, long long lda, co
   umma_complex_gemm(pa, lda_p, pb, kexp, m, n, kexp, c, ldc, add, alpha, ws.partial, stream);
 }
 
-unsigned int umma_error_flag_read_and_clear() {
-  unsigned int value = 0, zero = 0;
+unsigned int umma_error_flag() {
+  unsigned int value = 0;
   SDFT_CUDA(cudaMemcpyFromSymbol(&value, g_umma_error, sizeof(value)));
-  if (value) SDFT_CUDA(cudaMemcpyToSymbol(g_umma_error, &zero, sizeof(zero)));
   return value;
 }
 

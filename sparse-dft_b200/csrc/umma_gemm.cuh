@@ -84,8 +84,10 @@ void gemm_tc(Op aop, int m, int n, int k, const Cx<double>* a, long long lda, co
              const Cx<double>* b, long long ldb, Cx<double>* c, long long ldc, bool add, double alpha, Split split,
              TensorCoreWorkspace& ws, cudaStream_t stream);
 
-// Reads and clears the device word set when a tensor-core kernel's bounded
-// wait ran out (0 = no failure). Synchronous.
-unsigned int umma_error_flag_read_and_clear();
+// Reads the device word set when a tensor-core kernel's bounded wait ran out
+// (0 = no failure). The word is never cleared: concurrent solvers share it,
+// and after a failure every later tensor-core product winds down and reports
+// it too. Synchronous.
+unsigned int umma_error_flag();
 
 }  // namespace sdft_b200

@@ -12,7 +12,7 @@ import re
 LIBRARY = pathlib.Path(__file__).resolve().parent / "_lib" / "libsdft_b200.so"
 HEADER = pathlib.Path(__file__).resolve().parents[2] / "include" / "sdft_b200.h"
 
-OK, INVALID_ARGUMENT, OVERFLOW, RUNTIME_ERROR, CUDA_ERROR, OUT_OF_MEMORY, NONFINITE = range(7)
+OK, INVALID_ARGUMENT, OVERFLOW, RUNTIME_ERROR, CUDA_ERROR, OUT_OF_MEMORY, NONFINITE, NOT_READY = range(8)
 FP64, MIXED = 0, 1
 HOST, DEVICE = 0, 1
 HAMILTONIAN, OVERLAP = 0, 1
@@ -62,6 +62,14 @@ I32 = ctypes.POINTER(ctypes.c_int32)
 U64 = ctypes.POINTER(ctypes.c_uint64)
 SZ = ctypes.c_size_t
 SZP = ctypes.POINTER(ctypes.c_size_t)
+
+
+class SolveTiming(ctypes.Structure):
+    _fields_ = [("slot", ctypes.c_int), ("footprint", ctypes.c_size_t), ("submitted", ctypes.c_double),
+                ("started", ctypes.c_double), ("finished", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class DavidsonOptions(ctypes.Structure):
@@ -118,6 +126,14 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_project", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_davidson", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
                               ctypes.c_int])
+    fn("sdft_b200_server_create", [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(P)])
+    fn("sdft_b200_server_destroy", [P])
+    fn("sdft_b200_server_submit", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,
+                                   ctypes.POINTER(DavidsonOptions), ctypes.c_int, U64])
+    fn("sdft_b200_server_wait", [P, ctypes.c_uint64, ctypes.c_double, D, P, D, ctypes.POINTER(DavidsonStats),
+                                 ctypes.POINTER(SolveTiming)])
+    fn("sdft_b200_server_memory", [P, U64, U64, U64])
+    fn("sdft_b200_solve_footprint", [SZ, I32, SZ, SZ, ctypes.c_int, U64])
 
 
 def last_error() -> str:

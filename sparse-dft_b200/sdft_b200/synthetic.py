@@ -305,6 +305,14 @@ def gaas_kpoint(index: int, seed: int = 2026, **kw) -> OperatorInputs:
                           **kw)
 
 
+def gaas_small(kpoint=(1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0), seed: int = 2027, ecut_ha: float = 6.0, roots: int = 12,
+               **kw) -> OperatorInputs:
+    """GaAs 8-atom zincblende cell (a = 10.68 bohr, depths -2.2 / -1.8 Ha) at one k-point of the 3x3x3 mesh:
+    the k-point batch's construction at test size."""
+    return build_operator("gaas_small", 10.68, 1, ecut_ha, roots, depths=(-2.2, -1.8), kpoint=kpoint, seed=seed,
+                          **kw)
+
+
 def tiny(seed: int = 7, ecut_ha: float = 4.0, roots: int = 6, a: float = 7.0, **kw) -> OperatorInputs:
     """A small diamond cell for fast parity tests (a few hundred plane waves)."""
     return build_operator("tiny", a, 1, ecut_ha, roots, seed=seed, **kw)

@@ -144,17 +144,32 @@ def compensation_fixture(lib, inputs, name, factor, bands):
     print("compensation", name, "keys", keys.shape[0])
 
 
+KPOINT_MESH = {"gaas_k13": (0.0, 1.0 / 3.0, 1.0 / 3.0), "gaas_k26": (1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)}
+
+
+def kpoint_fixtures(lib):
+    """Reference operator and solve of the 8-atom GaAs cell at two k-points of
+    the 3x3x3 Monkhorst-Pack mesh (complex, off-Gamma pencils, two species)."""
+    for name, kpoint in KPOINT_MESH.items():
+        operator_fixture(lib, synthetic.gaas_small(kpoint), name)
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
+    parser.add_argument("--kpoints", action="store_true", help="only the off-Gamma GaAs fixtures")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
+    if args.kpoints:
+        kpoint_fixtures(lib)
+        return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
     pbe_fixture(lib)
     density_fixture(lib, synthetic.tiny(), "tiny", 4.0, 6)
     density_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     compensation_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
+    kpoint_fixtures(lib)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

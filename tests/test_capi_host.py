@@ -67,3 +67,27 @@ def test_context_without_gpu_reports_cuda_error():
     status = lib.sdft_b200_context_create(0, None, ctypes.byref(handle))
     assert status == C.CUDA_ERROR
     assert "CUDA" in C.last_error()
+
+
+def test_solve_footprint_is_host_arithmetic():
+    """The server's admission budget needs no device: it grows with the roots
+    and the subspace factor and covers at least the three basis blocks."""
+    from sdft_b200 import synthetic
+    from sdft_b200.serving import solve_footprint
+    x = synthetic.si8()
+    small = solve_footprint(x, 8)
+    large = solve_footprint(x, 16)
+    wide = solve_footprint(x, 16, subspace_factor=16)
+    assert 0 < small < large < wide
+    capacity = min(x.npw, max(8 * 16, 64))
+    assert large > 3 * 16 * x.npw * capacity
+
+
+def test_server_without_gpu_reports_cuda_error():
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    lib = C.library()
+    handle = ctypes.c_void_p()
+    assert lib.sdft_b200_server_create(0, 1 << 30, 2, ctypes.byref(handle)) == C.CUDA_ERROR
+    assert "CUDA" in C.last_error()
+    assert lib.sdft_b200_server_create(0, 1 << 30, 0, ctypes.byref(handle)) == C.INVALID_ARGUMENT
