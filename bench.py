@@ -270,6 +270,10 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_density:
         density_rows = density_side(ctx, inputs, stream, roofline["peak"])
 
+    serving_rows = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving_rows = serving_stream(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(inputs)
@@ -288,6 +292,7 @@ def run_b200(args):
             "mixed_over_fp64": statistics.median(fp64_ms) / statistics.median(step_ms),
             "solver_stats": stats, "clocks": clocks.summary(), "gpu_launches": int(launches),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "density_side": density_rows,
+            "serving": serving_rows,
         }
         print(json.dumps(line), flush=True)
     op.close()
@@ -405,6 +410,53 @@ def density_side(ctx, inputs, stream, peak):
     return out
 
 
+def serving_stream(device, requests=24, slots=4, rate_hz=8.0, cap=150e9, seed=4242):
+    """A sample of the seeded serving stream through the solve server: Poisson
+    arrivals (rate_hz) of requests with 2-16 atoms, Ecut 10-15 Ha, 1-2
+    k-points (one solve per k-point), admitted by device footprint under cap
+    with `slots` concurrent solves; the same stream in the mixed and the FP64
+    plain form. Latency = finish - submit of a request's last k-point."""
+    import numpy as np
+    from sdft_b200 import synthetic
+    from sdft_b200.serving import SolveServer
+
+    stream = [synthetic.serving_request(i, seed=seed, atoms=(2, 16), ecut_ha=(10.0, 15.0), kpoints=(1, 2))
+              for i in range(requests)]
+    arrivals = np.cumsum(np.random.Generator(np.random.PCG64(seed)).exponential(1.0 / rate_hz, size=requests))
+
+    def run(precision):
+        with SolveServer(device, cap, slots) as server:
+            t0 = time.perf_counter()
+            tickets = []
+            for when, ops in zip(arrivals, stream):
+                delay = when - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                tickets.append([server.submit(x, precision=precision) for x in ops])
+            results = [[server.wait(t) for t in group] for group in tickets]
+            makespan = time.perf_counter() - t0
+            memory = server.memory()
+        latency = [1e3 * (max(r["timing"]["finished"] for r in group) - min(r["timing"]["submitted"] for r in group))
+                   for group in results]
+        flat = [r for group in results for r in group]
+        pairs = sum(int(np.sum(r["residuals"] <= TOLERANCE)) for r in flat)
+        spans = sorted((r["timing"]["started"], r["timing"]["finished"]) for r in flat)
+        events = sorted([(a, 1) for a, _ in spans] + [(b, -1) for _, b in spans])
+        depth = peak_depth = 0
+        for _, step in events:
+            depth += step
+            peak_depth = max(peak_depth, depth)
+        return {"p50_ms": float(np.percentile(latency, 50)), "p99_ms": float(np.percentile(latency, 99)),
+                "certified_pairs_per_s": pairs / makespan, "certified_pairs": pairs,
+                "solves": len(flat), "all_converged": all(r["converged"] for r in flat),
+                "makespan_s": makespan, "peak_concurrent_solves": peak_depth,
+                "peak_budget_gb": memory["peak"] / 1e9}
+
+    return {"requests": requests, "slots": slots, "arrival_rate_hz": rate_hz, "memory_cap_gb": cap / 1e9,
+            "sample": "seeded stream, 2-16 atoms, Ecut 10-15 Ha, 1-2 k-points, bands 1.25x occupied (min 8)",
+            "mixed": run("mixed"), "fp64_plain": run("fp64")}
+
+
 def end_to_end(ctx, inputs, stream, steps):
     import numpy as np
     import torch
@@ -487,6 +539,7 @@ def main():
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU reference sample")
     parser.add_argument("--no-density", action="store_true", help="skip the density-side measurements")
+    parser.add_argument("--no-serving", action="store_true", help="skip the serving-stream sample")
     parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe"],
                         help="run a few launches of one kernel family for a profiler capture and exit")
     parser.add_argument("--columns", type=int, default=32, help="columns (bands) for --case")

@@ -258,14 +258,16 @@ def _scale_q(amplitudes, q_raw, regularization, floor=0.3):
 def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, depths=(-2.0, -2.0),
                    kpoint=(0.0, 0.0, 0.0), seed: int = 2026, noise: float = 0.05, noise_cut: float = 4.0,
                    width: float = 1.0, tolerance: float = 1e-12, max_iterations: int = 256,
-                   regularization: float = 1e-12) -> OperatorInputs:
-    """One synthetic H~/S~ pencil on an a*reps cubic zincblende/diamond supercell."""
+                   regularization: float = 1e-12, sites=None) -> OperatorInputs:
+    """One synthetic H~/S~ pencil on an a*reps cubic zincblende/diamond supercell
+    (or on the given (fractional positions, species) sites of an a*reps cube)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     cell = a * reps
     lattice = np.eye(3) * cell
     reciprocal = np.eye(3) * (TWO_PI / cell)
     volume = cell ** 3
-    positions, species = zincblende_sites(reps)
+    positions, species = zincblende_sites(reps) if sites is None else (np.asarray(sites[0], dtype=np.float64),
+                                                                        np.asarray(sites[1], dtype=np.int64))
     atom_depths = np.array([depths[s] for s in species], dtype=np.float64)
     hkl, cart, kinetic = enumerate_g_vectors(reciprocal, ecut_ha * HARTREE_TO_EV, kpoint)
     v_hkl, v_values = local_potential(lattice, reciprocal, positions, atom_depths, ecut_ha, noise, noise_cut,
@@ -311,6 +313,30 @@ def gaas_small(kpoint=(1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0), seed: int = 2027, ecut_
     the k-point batch's construction at test size."""
     return build_operator("gaas_small", 10.68, 1, ecut_ha, roots, depths=(-2.2, -1.8), kpoint=kpoint, seed=seed,
                           **kw)
+
+
+SI_VOLUME_PER_ATOM = 10.26 ** 3 / 8.0  # bohr^3, diamond Si
+
+
+def serving_request(index: int, seed: int = 4242, atoms=(2, 128), ecut_ha=(10.0, 25.0), kpoints=(1, 8)):
+    """One request of the seeded serving stream: a cubic cell with a
+    log-uniform atom count (random sites, two species), Ecut uniform in the
+    range, bands = 1.25 x the occupied count (2 per atom) within [8, 320], and
+    1..8 k-points; returns one OperatorInputs per k-point."""
+    rng = np.random.Generator(np.random.PCG64([seed, index]))
+    count = int(round(math.exp(rng.uniform(math.log(atoms[0]), math.log(atoms[1])))))
+    a = (count * SI_VOLUME_PER_ATOM) ** (1.0 / 3.0)
+    positions = rng.uniform(0.0, 1.0, size=(count, 3))
+    species = rng.integers(0, 2, size=count)
+    ecut = float(rng.uniform(ecut_ha[0], ecut_ha[1]))
+    bands = int(min(320, max(8, round(1.25 * 2 * count))))
+    nk = int(rng.integers(kpoints[0], kpoints[1] + 1))
+    out = []
+    for j in range(nk):
+        kpoint = tuple(float(v) for v in rng.uniform(-0.5, 0.5, size=3)) if j else (0.0, 0.0, 0.0)
+        out.append(build_operator(f"request{index}_k{j}", a, 1, ecut, bands, depths=(-2.2, -1.8), kpoint=kpoint,
+                                  seed=seed * 1000 + index, sites=(positions, species)))
+    return out
 
 
 def tiny(seed: int = 7, ecut_ha: float = 4.0, roots: int = 6, a: float = 7.0, **kw) -> OperatorInputs:
