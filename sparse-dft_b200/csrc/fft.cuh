@@ -399,6 +399,53 @@ __device__ __forceinline__ Cx<T>* fft_lines_fixed(Cx<T>* src, Cx<T>* dst, int li
   }
 }
 
+// One stage over `count` listed lines of compile-time length N with
+// contiguous elements: line t starts at rows[t] * line_stride. Work items
+// run butterfly-fastest, so neighbouring threads touch neighbouring words.
+template <typename T, int R, bool INV, int N, int NS, int THREADS>
+__device__ __forceinline__ void pp_stage_fixed_rows(const Cx<T>* src, Cx<T>* dst, int count, const int* rows,
+                                                    int line_stride, const Cx<T>* tw) {
+  constexpr int M = N / R, TWSTRIDE = N / (NS * R);
+  Cx<T> roots[R];
+#pragma unroll
+  for (int p = 1; p < R; ++p) roots[p] = tw[p * M];
+  const int items = count * M;
+  for (int item = static_cast<int>(threadIdx.x); item < items; item += THREADS) {
+    const int t = item / M, j = item - t * M;
+    const int jq = j / NS, jk = j - jq * NS;
+    const int offset = rows[t] * line_stride;
+    const Cx<T>* in = src + offset;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      Cx<T> x = in[j + r * M];
+      if (r > 0 && jk > 0) x = cmul(x, twiddle<T, INV>(tw, r * jk * TWSTRIDE));
+      v[r] = x;
+    }
+    radix_dft_roots<T, R, INV>(v, roots);
+    Cx<T>* out = dst + offset + jq * NS * R + jk;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[r * NS] = v[r];
+  }
+}
+
+// The listed lines of length N (contiguous elements), ping-pong between src
+// and dst; returns the buffer holding the result. Lines not listed are not
+// touched in either buffer.
+template <typename T, bool INV, int N, int THREADS, int S = 0>
+__device__ __forceinline__ Cx<T>* fft_rows_fixed(Cx<T>* src, Cx<T>* dst, int count, const int* rows, int line_stride,
+                                                 const Cx<T>* tw) {
+  static_assert(fixed_stage_count(N) > 0, "line length must be 2/3/5/7-smooth");
+  if constexpr (S == fixed_stage_count(N)) {
+    return src;
+  } else {
+    pp_stage_fixed_rows<T, fixed_radix(N, S), INV, N, fixed_ns(N, S), THREADS>(src, dst, count, rows, line_stride,
+                                                                              tw);
+    __syncthreads();
+    return fft_rows_fixed<T, INV, N, THREADS, S + 1>(dst, src, count, rows, line_stride, tw);
+  }
+}
+
 template <typename T, bool INV>
 __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
                                const int* rows, const LinePlan& plan, const Cx<T>* tw) {

@@ -253,6 +253,121 @@ void allow_smem(Kernel kernel, std::size_t bytes) {
   allow_dynamic_smem(kernel, bytes);
 }
 
+// plane_in_kernel for compile-time axis lengths N1 = N2 = N: backward FFT
+// along i2 on the active i1 rows, then along i1 on every i2 column.
+template <typename T, int N>
+__global__ void __launch_bounds__(kThreads) plane_in_fixed_kernel(const Cx<double>* __restrict__ x, long long ldx,
+                                                                  LocalArgs<T> a, Cx<T>* __restrict__ slab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int np = a.n2p, plane_elems = N * np;
+  Cx<T>* plane_a = tw + N;
+  Cx<T>* plane_b = plane_a + plane_elems;
+  int* rows = reinterpret_cast<int*>(plane_b + plane_elems);
+  const int s = blockIdx.x, c = blockIdx.y;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) tw[i] = a.tw2[i];
+  for (int i = tid; i < a.krows; i += kThreads) rows[i] = a.krow[i];
+  for (int i = tid; i < 2 * plane_elems; i += kThreads) plane_a[i] = Cx<T>{0, 0};
+  __syncthreads();
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  const int p_end = a.point_offset[s + 1];
+  for (int p = a.point_offset[s] + tid; p < p_end; p += kThreads)
+    plane_a[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
+  __syncthreads();
+  Cx<T>* rows_done = fft_rows_fixed<T, true, N, kThreads>(plane_a, plane_b, a.krows, rows, np, tw);
+  Cx<T>* other = rows_done == plane_a ? plane_b : plane_a;
+  Cx<T>* done = fft_lines_fixed<T, true, N, N, kThreads>(rows_done, other, 1, np, tw);
+  Cx<T>* out = slab + (static_cast<long long>(c) * a.slots + s) * (N * N);
+  for (int i = tid; i < N * N; i += kThreads) {
+    const int i1 = i / N, i2 = i - i1 * N;
+    out[i] = done[i1 * np + i2];
+  }
+}
+
+// plane_out_kernel for N1 = N2 = N: forward FFT along i1 on every column,
+// along i2 on the active rows, gather, y = T x + value / count.
+template <typename T, int N>
+__global__ void __launch_bounds__(kThreads) plane_out_fixed_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
+                                                                   const Cx<double>* __restrict__ x, long long ldx,
+                                                                   const double* __restrict__ kinetic, double count,
+                                                                   Cx<double>* __restrict__ y, long long ldy) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int np = a.n2p, plane_elems = N * np;
+  Cx<T>* plane_a = tw + N;
+  Cx<T>* plane_b = plane_a + plane_elems;
+  int* rows = reinterpret_cast<int*>(plane_b + plane_elems);
+  const int s = blockIdx.x, c = blockIdx.y;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) tw[i] = a.tw2[i];
+  for (int i = tid; i < a.krows; i += kThreads) rows[i] = a.krow[i];
+  const Cx<T>* in = slab + (static_cast<long long>(c) * a.slots + s) * (N * N);
+  for (int i = tid; i < N * N; i += kThreads) {
+    const int i1 = i / N, i2 = i - i1 * N;
+    plane_a[i1 * np + i2] = in[i];
+  }
+  __syncthreads();
+  Cx<T>* cols_done = fft_lines_fixed<T, false, N, N, kThreads>(plane_a, plane_b, 1, np, tw);
+  Cx<T>* done = fft_rows_fixed<T, false, N, kThreads>(cols_done, cols_done == plane_a ? plane_b : plane_a, a.krows,
+                                                     rows, np, tw);
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
+  const int p_end = a.point_offset[s + 1];
+  for (int p = a.point_offset[s] + tid; p < p_end; p += kThreads) {
+    const int g = a.point_g[p];
+    const Cx<double> v = cconvert<double>(done[a.point_smem[p]]);
+    const Cx<double> in_g = xc[g];
+    const double t = kinetic[g];
+    yc[g] = Cx<double>{t * in_g.re + v.re / count, t * in_g.im + v.im / count};
+  }
+}
+
+// Plane passes with the compile-time kernels for square planes of the common
+// lengths; false when the plane has another shape.
+template <typename T>
+bool launch_planes_fixed(const LocalArgs<T>& a, bool inward, int columns, const Cx<double>* x, long long ldx,
+                         Cx<T>* slab, const double* kinetic, double count, Cx<double>* y, long long ldy,
+                         cudaStream_t stream) {
+  if (a.n1 != a.n2) return false;
+  const std::size_t smem = sizeof(Cx<T>) * (a.n1 + 2 * static_cast<std::size_t>(a.n1) * a.n2p) +
+                           sizeof(int) * static_cast<std::size_t>(a.krows);
+  const dim3 grid(a.slots, columns);
+  auto go = [&](auto in_kernel, auto out_kernel) {
+    if (inward) {
+      allow_smem(in_kernel, smem);
+      in_kernel<<<grid, kThreads, smem, stream>>>(x, ldx, a, slab);
+      SDFT_LAUNCH("plane_in_fixed_kernel");
+    } else {
+      allow_smem(out_kernel, smem);
+      out_kernel<<<grid, kThreads, smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
+      SDFT_LAUNCH("plane_out_fixed_kernel");
+    }
+    return true;
+  };
+#define SDFT_PLANES(N) \
+  case N:              \
+    return go(plane_in_fixed_kernel<T, N>, plane_out_fixed_kernel<T, N>);
+  switch (a.n1) {
+    SDFT_PLANES(24)
+    SDFT_PLANES(35)
+    SDFT_PLANES(36)
+    SDFT_PLANES(45)
+    SDFT_PLANES(48)
+    SDFT_PLANES(60)
+    SDFT_PLANES(64)
+    SDFT_PLANES(70)
+    SDFT_PLANES(72)
+    SDFT_PLANES(80)
+    SDFT_PLANES(81)
+    SDFT_PLANES(84)
+    SDFT_PLANES(90)
+    SDFT_PLANES(96)
+    default: return false;
+  }
+#undef SDFT_PLANES
+}
+
 // Pencil pass with the compile-time kernel for the common axis lengths.
 template <typename T>
 bool launch_pencil_fixed(const LocalArgs<T>& a, int columns, const T* potential, Cx<T>* slab, cudaStream_t stream) {
@@ -308,29 +423,39 @@ LocalArgs<T> make_args(const SpherePlan& plan) {
   return a;
 }
 
+// The three passes: plane_in, pencil (V(r) multiply) and plane_out, each
+// with its compile-time kernel where the lengths have one.
+template <typename T>
+void run_local_passes(const LocalArgs<T>& a, double count, const Cx<double>* x, long long ldx, int columns,
+                      const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
+                      cudaStream_t stream) {
+  const std::size_t plane_smem = sizeof(Cx<T>) * (a.n1 + a.n2 + 2 * static_cast<std::size_t>(a.n1) * a.n2p);
+  const std::size_t pencil_smem = sizeof(Cx<T>) * (a.n0 + 2 * static_cast<std::size_t>(a.n0) * (kPencilLines + 1));
+  const dim3 planes(a.slots, columns);
+  if (!launch_planes_fixed<T>(a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
+    allow_smem(plane_in_kernel<T>, plane_smem);
+    plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
+    SDFT_LAUNCH("plane_in_kernel");
+  }
+  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
+    const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
+    allow_smem(pencil_kernel<T>, pencil_smem);
+    pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
+    SDFT_LAUNCH("pencil_kernel");
+  }
+  if (!launch_planes_fixed<T>(a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
+    allow_smem(plane_out_kernel<T>, plane_smem);
+    plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
+    SDFT_LAUNCH("plane_out_kernel");
+  }
+}
+
 template <typename T>
 void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long long ldx, int columns,
                             const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
                             cudaStream_t stream) {
   const LocalArgs<T> a = make_args<T>(plan);
-  const std::size_t plane_smem =
-      sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + 2 * static_cast<std::size_t>(plan.n[1]) * plan.n2p);
-  const std::size_t pencil_smem =
-      sizeof(Cx<T>) * (plan.n[0] + 2 * static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
-  allow_smem(plane_in_kernel<T>, plane_smem);
-  allow_smem(pencil_kernel<T>, pencil_smem);
-  allow_smem(plane_out_kernel<T>, plane_smem);
-  const dim3 planes(plan.slots, columns);
-  plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
-  SDFT_LAUNCH("plane_in_kernel");
-  const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
-  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
-    pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
-    SDFT_LAUNCH("pencil_kernel");
-  }
-  plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
-                                                                static_cast<double>(plan.count), y, ldy);
-  SDFT_LAUNCH("plane_out_kernel");
+  run_local_passes<T>(a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
 }
 
 template <typename T, bool INV, int TL>
@@ -487,24 +612,7 @@ void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long 
   a.tw0 = twiddle[0];
   a.tw1 = twiddle[1];
   a.tw2 = twiddle[2];
-  const std::size_t plane_smem =
-      sizeof(Cx<T>) * (plan.n[1] + plan.n[2] + 2 * static_cast<std::size_t>(plan.n[1]) * plan.n2p);
-  const std::size_t pencil_smem =
-      sizeof(Cx<T>) * (plan.n[0] + 2 * static_cast<std::size_t>(plan.n[0]) * (kPencilLines + 1));
-  allow_smem(plane_in_kernel<T>, plane_smem);
-  allow_smem(pencil_kernel<T>, pencil_smem);
-  allow_smem(plane_out_kernel<T>, plane_smem);
-  const dim3 planes(plan.slots, columns);
-  plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
-  SDFT_LAUNCH("plane_in_kernel");
-  const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
-  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
-    pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
-    SDFT_LAUNCH("pencil_kernel");
-  }
-  plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic,
-                                                                static_cast<double>(plan.count), y, ldy);
-  SDFT_LAUNCH("plane_out_kernel");
+  run_local_passes<T>(a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
 }
 
 template void local_hamiltonian_preset<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,
