@@ -446,6 +446,79 @@ __device__ __forceinline__ Cx<T>* fft_rows_fixed(Cx<T>* src, Cx<T>* dst, int cou
   }
 }
 
+// In-place stage over lines of compile-time length N: every thread loads
+// the inputs of all its butterflies into registers, the CTA synchronises,
+// then every thread writes its outputs to the Stockham positions, so one
+// buffer serves both sides of the stage. LISTED: `count` (<= N) lines at
+// rows[t] * line_stride, butterfly index fastest (contiguous elements,
+// es = 1); otherwise N lines at t * line_stride, line index fastest.
+template <typename T, int R, bool INV, int N, int NS, bool LISTED, int THREADS>
+__device__ __forceinline__ void ip_stage_fixed(Cx<T>* buf, int count, const int* rows, int line_stride, int es,
+                                               const Cx<T>* tw) {
+  constexpr int M = N / R, TWSTRIDE = N / (NS * R), MAX_ITEMS = N * M;
+  constexpr int PER = (MAX_ITEMS + THREADS - 1) / THREADS;
+  Cx<T> roots[R];
+#pragma unroll
+  for (int p = 1; p < R; ++p) roots[p] = tw[p * M];
+  const int items = LISTED ? count * M : MAX_ITEMS;
+  Cx<T> v[PER][R];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int item = q * THREADS + static_cast<int>(threadIdx.x);
+    if (item < items) {
+      int t, j;
+      if constexpr (LISTED) {
+        t = item / M;
+        j = item - t * M;
+      } else {
+        j = item / N;
+        t = item - j * N;
+      }
+      const int jk = j % NS;
+      const Cx<T>* in = buf + (LISTED ? rows[t] : t) * line_stride;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        Cx<T> x = in[(j + r * M) * es];
+        if (r > 0 && jk > 0) x = cmul(x, twiddle<T, INV>(tw, r * jk * TWSTRIDE));
+        v[q][r] = x;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int item = q * THREADS + static_cast<int>(threadIdx.x);
+    if (item < items) {
+      int t, j;
+      if constexpr (LISTED) {
+        t = item / M;
+        j = item - t * M;
+      } else {
+        j = item / N;
+        t = item - j * N;
+      }
+      const int jq = j / NS, jk = j - jq * NS;
+      radix_dft_roots<T, R, INV>(v[q], roots);
+      Cx<T>* out = buf + (LISTED ? rows[t] : t) * line_stride + (jq * NS * R + jk) * es;
+#pragma unroll
+      for (int r = 0; r < R; ++r) out[r * NS * es] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+// All stages of ip_stage_fixed (the buffer holds the result).
+template <typename T, bool INV, int N, bool LISTED, int THREADS, int S = 0>
+__device__ __forceinline__ void fft_inplace_fixed(Cx<T>* buf, int count, const int* rows, int line_stride, int es,
+                                                  const Cx<T>* tw) {
+  static_assert(fixed_stage_count(N) > 0, "line length must be 2/3/5/7-smooth");
+  if constexpr (S < fixed_stage_count(N)) {
+    ip_stage_fixed<T, fixed_radix(N, S), INV, N, fixed_ns(N, S), LISTED, THREADS>(buf, count, rows, line_stride, es,
+                                                                                 tw);
+    fft_inplace_fixed<T, INV, N, LISTED, THREADS, S + 1>(buf, count, rows, line_stride, es, tw);
+  }
+}
+
 template <typename T, bool INV>
 __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
                                const int* rows, const LinePlan& plan, const Cx<T>* tw) {

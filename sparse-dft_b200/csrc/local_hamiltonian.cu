@@ -253,40 +253,39 @@ void allow_smem(Kernel kernel, std::size_t bytes) {
   allow_dynamic_smem(kernel, bytes);
 }
 
-// plane_in_kernel for compile-time axis lengths N1 = N2 = N: backward FFT
-// along i2 on the active i1 rows, then along i1 on every i2 column.
+// plane_in_kernel for compile-time axis lengths N1 = N2 = N, one plane
+// buffer (in-place stages): backward FFT along i2 on the active i1 rows, then
+// along i1 on every i2 column.
 template <typename T, int N>
 __global__ void __launch_bounds__(kThreads) plane_in_fixed_kernel(const Cx<double>* __restrict__ x, long long ldx,
                                                                   LocalArgs<T> a, Cx<T>* __restrict__ slab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   const int np = a.n2p, plane_elems = N * np;
-  Cx<T>* plane_a = tw + N;
-  Cx<T>* plane_b = plane_a + plane_elems;
-  int* rows = reinterpret_cast<int*>(plane_b + plane_elems);
+  Cx<T>* plane = tw + N;
+  int* rows = reinterpret_cast<int*>(plane + plane_elems);
   const int s = blockIdx.x, c = blockIdx.y;
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += kThreads) tw[i] = a.tw2[i];
   for (int i = tid; i < a.krows; i += kThreads) rows[i] = a.krow[i];
-  for (int i = tid; i < 2 * plane_elems; i += kThreads) plane_a[i] = Cx<T>{0, 0};
+  for (int i = tid; i < plane_elems; i += kThreads) plane[i] = Cx<T>{0, 0};
   __syncthreads();
   const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
   const int p_end = a.point_offset[s + 1];
   for (int p = a.point_offset[s] + tid; p < p_end; p += kThreads)
-    plane_a[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
+    plane[a.point_smem[p]] = cconvert<T>(xc[a.point_g[p]]);
   __syncthreads();
-  Cx<T>* rows_done = fft_rows_fixed<T, true, N, kThreads>(plane_a, plane_b, a.krows, rows, np, tw);
-  Cx<T>* other = rows_done == plane_a ? plane_b : plane_a;
-  Cx<T>* done = fft_lines_fixed<T, true, N, N, kThreads>(rows_done, other, 1, np, tw);
+  fft_inplace_fixed<T, true, N, true, kThreads>(plane, a.krows, rows, np, 1, tw);
+  fft_inplace_fixed<T, true, N, false, kThreads>(plane, N, nullptr, 1, np, tw);
   Cx<T>* out = slab + (static_cast<long long>(c) * a.slots + s) * (N * N);
   for (int i = tid; i < N * N; i += kThreads) {
     const int i1 = i / N, i2 = i - i1 * N;
-    out[i] = done[i1 * np + i2];
+    out[i] = plane[i1 * np + i2];
   }
 }
 
-// plane_out_kernel for N1 = N2 = N: forward FFT along i1 on every column,
-// along i2 on the active rows, gather, y = T x + value / count.
+// plane_out_kernel for N1 = N2 = N, one plane buffer: forward FFT along i1
+// on every column, along i2 on the active rows, gather, y = T x + value / count.
 template <typename T, int N>
 __global__ void __launch_bounds__(kThreads) plane_out_fixed_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                                    const Cx<double>* __restrict__ x, long long ldx,
@@ -295,9 +294,8 @@ __global__ void __launch_bounds__(kThreads) plane_out_fixed_kernel(const Cx<T>* 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   const int np = a.n2p, plane_elems = N * np;
-  Cx<T>* plane_a = tw + N;
-  Cx<T>* plane_b = plane_a + plane_elems;
-  int* rows = reinterpret_cast<int*>(plane_b + plane_elems);
+  Cx<T>* plane = tw + N;
+  int* rows = reinterpret_cast<int*>(plane + plane_elems);
   const int s = blockIdx.x, c = blockIdx.y;
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += kThreads) tw[i] = a.tw2[i];
@@ -305,18 +303,17 @@ __global__ void __launch_bounds__(kThreads) plane_out_fixed_kernel(const Cx<T>* 
   const Cx<T>* in = slab + (static_cast<long long>(c) * a.slots + s) * (N * N);
   for (int i = tid; i < N * N; i += kThreads) {
     const int i1 = i / N, i2 = i - i1 * N;
-    plane_a[i1 * np + i2] = in[i];
+    plane[i1 * np + i2] = in[i];
   }
   __syncthreads();
-  Cx<T>* cols_done = fft_lines_fixed<T, false, N, N, kThreads>(plane_a, plane_b, 1, np, tw);
-  Cx<T>* done = fft_rows_fixed<T, false, N, kThreads>(cols_done, cols_done == plane_a ? plane_b : plane_a, a.krows,
-                                                     rows, np, tw);
+  fft_inplace_fixed<T, false, N, false, kThreads>(plane, N, nullptr, 1, np, tw);
+  fft_inplace_fixed<T, false, N, true, kThreads>(plane, a.krows, rows, np, 1, tw);
   const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
   Cx<double>* yc = y + static_cast<long long>(c) * ldy;
   const int p_end = a.point_offset[s + 1];
   for (int p = a.point_offset[s] + tid; p < p_end; p += kThreads) {
     const int g = a.point_g[p];
-    const Cx<double> v = cconvert<double>(done[a.point_smem[p]]);
+    const Cx<double> v = cconvert<double>(plane[a.point_smem[p]]);
     const Cx<double> in_g = xc[g];
     const double t = kinetic[g];
     yc[g] = Cx<double>{t * in_g.re + v.re / count, t * in_g.im + v.im / count};
@@ -330,7 +327,7 @@ bool launch_planes_fixed(const LocalArgs<T>& a, bool inward, int columns, const 
                          Cx<T>* slab, const double* kinetic, double count, Cx<double>* y, long long ldy,
                          cudaStream_t stream) {
   if (a.n1 != a.n2) return false;
-  const std::size_t smem = sizeof(Cx<T>) * (a.n1 + 2 * static_cast<std::size_t>(a.n1) * a.n2p) +
+  const std::size_t smem = sizeof(Cx<T>) * (a.n1 + static_cast<std::size_t>(a.n1) * a.n2p) +
                            sizeof(int) * static_cast<std::size_t>(a.krows);
   const dim3 grid(a.slots, columns);
   auto go = [&](auto in_kernel, auto out_kernel) {
