@@ -27,6 +27,13 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPencilLines = 32;
+// Resident CTAs per SM the fixed plane kernels are compiled for: three in
+// FP32 (80 registers, no spills up to N = 70), one in FP64, whose butterfly
+// registers would spill under a tighter bound.
+template <typename T>
+constexpr int plane_blocks() {
+  return sizeof(T) == 4 ? 3 : 1;
+}
 
 template <typename T>
 struct LocalArgs {
@@ -257,7 +264,7 @@ void allow_smem(Kernel kernel, std::size_t bytes) {
 // buffer (in-place stages): backward FFT along i2 on the active i1 rows, then
 // along i1 on every i2 column.
 template <typename T, int N>
-__global__ void __launch_bounds__(kThreads) plane_in_fixed_kernel(const Cx<double>* __restrict__ x, long long ldx,
+__global__ void __launch_bounds__(kThreads, plane_blocks<T>()) plane_in_fixed_kernel(const Cx<double>* __restrict__ x, long long ldx,
                                                                   LocalArgs<T> a, Cx<T>* __restrict__ slab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -287,7 +294,7 @@ __global__ void __launch_bounds__(kThreads) plane_in_fixed_kernel(const Cx<doubl
 // plane_out_kernel for N1 = N2 = N, one plane buffer: forward FFT along i1
 // on every column, along i2 on the active rows, gather, y = T x + value / count.
 template <typename T, int N>
-__global__ void __launch_bounds__(kThreads) plane_out_fixed_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
+__global__ void __launch_bounds__(kThreads, plane_blocks<T>()) plane_out_fixed_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                                    const Cx<double>* __restrict__ x, long long ldx,
                                                                    const double* __restrict__ kinetic, double count,
                                                                    Cx<double>* __restrict__ y, long long ldy) {
