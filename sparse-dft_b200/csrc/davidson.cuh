@@ -4,6 +4,7 @@
 
 #include "eigensolver.cuh"
 #include "operator.cuh"
+#include "umma_gemm.cuh"
 
 namespace sdft_b200 {
 
@@ -46,7 +47,18 @@ class DavidsonSolver {
   void apply_pair(const Cx<double>* x, int cols, Cx<double>* hy, Cx<double>* sy, bool exact);
   bool append_block(Cx<double>* vectors, int k);
   bool append_single(const Cx<double>* v);
-  void update_projected(const Cx<double>* applied, Cx<double>* cached);
+  void update_projected(const Cx<double>* applied, Cx<double>* cached, const std::uint16_t* packed_applied);
+  // Mixed search: BF16-split copies of the basis V and its images HV, SV,
+  // written once per column as the column is formed, in the layouts the
+  // tensor-core products read (A rows for V^H, K entries for V, HV, SV as
+  // left factors, B rows for HV, SV as right factors).
+  bool searching() const { return !exact_mode_ && packs_; }
+  void pack_basis(int first, int count);
+  void pack_images(int first, int count);
+  PackedA basis_rows(int first, int rows) const;                    // V^H rows [first, first+rows), K = n
+  PackedA left_factor(const std::uint16_t* base, int k) const;      // n x k left factor (V, HV or SV)
+  void gemm_left(const std::uint16_t* packed, int n, int k, const Cx<double>* b, long long ldb, Cx<double>* c,
+                 long long ldc, bool add, double alpha);
   void rayleigh_ritz();
   void certify();
   void refresh_images();
@@ -61,6 +73,10 @@ class DavidsonSolver {
   Scratch basis_, hbasis_, sbasis_, cached_h_, cached_s_, rr_a_, rr_b_, rr_w_, rr_work_, info_;
   EigenWorkspace eigen_;
   Scratch xs_, sxs_, hxs_, res_, block_, metric_, original_, projections_, gram_, small_, order_, select_;
+  Scratch pack_vc_, pack_vn_, pack_hn_, pack_sn_, pack_hb_, pack_sb_;
+  bool packs_ = false;
+  Split split_ = Split::BF16x6;
+  long long ld_rows_ = 0, ld_cols_ = 0;  // packed row lengths: K = n (rows of V^H, HV, SV) and K = capacity
   Cx<double>* v_ = nullptr;
   Cx<double>* hv_ = nullptr;
   Cx<double>* sv_ = nullptr;

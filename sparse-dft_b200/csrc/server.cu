@@ -76,6 +76,8 @@ std::size_t solve_footprint(std::size_t npw, const int* hkl, std::size_t project
   // Largest apply (a full basis refresh): FP64 and FP32 grid slabs, PAW
   // projections, packed tensor-core operands and split-K partials.
   bytes += (cx + 8.0) * grid * cap + 3.0 * cx * p * cap + 24.0 * n * cap + 48.0 * n * kmax + 8.0 * cap * kmax * 64.0;
+  // Mixed search: BF16x6 copies of V^H, HV and SV as right factors, V, HV, SV as left factors.
+  bytes += 192.0 * n * cap;
   bytes = bytes * 1.1 + 64.0 * 1024 * 1024;  // allocator rounding and handles
   if (!std::isfinite(bytes) || bytes > 1e18) throw Overflow("solve footprint overflow");
   return static_cast<std::size_t>(bytes);
