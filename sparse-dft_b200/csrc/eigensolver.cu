@@ -379,23 +379,40 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
 // e_{i-2}^2 p_{i-2}, kept in range by exact power-of-two rescaling. A p_i
 // below pivmin |p_{i-1}| counts as a sign change (the q = -pivmin convention
 // of the quotient form q_i = p_i / p_{i-1}).
-__device__ int sturm_count(const double* d, const double* e2, int m, double x, double pivmin) {
-  double p0 = 1.0, p1 = d[0] - x;
-  if (fabs(p1) <= pivmin) p1 = -pivmin;
-  int count = p1 < 0.0;
-  for (int i = 1; i < m; ++i) {
-    double p2 = fma(d[i] - x, p1, -e2[i - 1] * p0);
-    if (fabs(p2) <= pivmin * fabs(p1)) p2 = -pivmin * p1;
-    count += (p2 < 0.0) != (p1 < 0.0);
-    p0 = p1;
-    p1 = p2;
-    // Exact rescaling by 2^-400 / 2^400.
-    const double mag = fabs(p1);
-    const double f = mag > 0x1p+400 ? 0x1p-400 : (mag < 0x1p-400 ? 0x1p+400 : 1.0);
-    p0 *= f;
-    p1 *= f;
+template <int P>
+__device__ void sturm_counts(const double* d, const double* e2, int m, const double (&x)[P], double pivmin,
+                             int (&count)[P]) {
+  double p0[P], p1[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    p0[q] = 1.0;
+    p1[q] = d[0] - x[q];
+    if (fabs(p1[q]) <= pivmin) p1[q] = -pivmin;
+    count[q] = p1[q] < 0.0;
   }
-  return count;
+  for (int i = 1; i < m; ++i) {
+    const double di = d[i], ei = e2[i - 1];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      double p2 = fma(di - x[q], p1[q], -ei * p0[q]);
+      if (fabs(p2) <= pivmin * fabs(p1[q])) p2 = -pivmin * p1[q];
+      count[q] += (p2 < 0.0) != (p1[q] < 0.0);
+      p0[q] = p1[q];
+      p1[q] = p2;
+    }
+    // Exact rescaling by 2^-400 / 2^400 every fourth step: a step grows the
+    // sequence by far less than 2^100 here, so nothing leaves the exponent
+    // range in between, and power-of-two scaling changes no sign or ratio.
+    if ((i & 3) == 0) {
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const double mag = fabs(p1[q]);
+        const double f = mag > 0x1p+400 ? 0x1p-400 : (mag < 0x1p-400 ? 0x1p+400 : 1.0);
+        p0[q] *= f;
+        p1[q] *= f;
+      }
+    }
+  }
 }
 
 // One warp per wanted eigenvalue; 32 x P points per round (P per lane).
@@ -426,19 +443,29 @@ __global__ void bisect_kernel(const double* __restrict__ d, const double* __rest
     emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
   }
   const double pivmin = DBL_MIN * fmax(1.0, emax);
-  const double pad = 4.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin;
+  const double tnorm = fmax(fabs(lo), fabs(hi));  // Gershgorin bound of the spectrum
+  const double pad = 4.0 * DBL_EPSILON * tnorm + pivmin;
   lo -= pad;
   hi += pad;
-  constexpr int P = 2;
+  // Absolute tolerance of the matrix scale (LAPACK dstebz's default abstol,
+  // eps * max(|gl|, |gu|)), beside the relative one: eigenvalues near zero
+  // stop at eps * |T| instead of running every round.
+  const double atol = DBL_EPSILON * tnorm;
+  constexpr int P = 4;
   for (int round = 0; round < 64; ++round) {
     const double width = hi - lo;
-    if (width <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) || width <= pivmin) break;
+    if (width <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) || width <= atol || width <= pivmin) break;
     const double step = width / (32 * P + 1);
-    // point q of lane l is lo + (q * 32 + l + 1) step: increasing over (q, l).
+    // point q of lane l is lo + (q * 32 + l + 1) step: increasing over (q, l);
+    // the lane's P Sturm sequences run interleaved.
+    double x[P];
+    int counts[P];
+#pragma unroll
+    for (int q = 0; q < P; ++q) x[q] = lo + (q * 32 + lane + 1) * step;
+    sturm_counts<P>(sd, se2, m, x, pivmin, counts);
     unsigned masks[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q)
-      masks[q] = __ballot_sync(0xffffffffu, sturm_count(sd, se2, m, lo + (q * 32 + lane + 1) * step, pivmin) > k);
+    for (int q = 0; q < P; ++q) masks[q] = __ballot_sync(0xffffffffu, counts[q] > k);
     int above = -1;  // first point index with count > k
 #pragma unroll
     for (int q = P - 1; q >= 0; --q)

@@ -231,27 +231,35 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
+// C = alpha * sum_s partial[s] (+ C): one thread per (row i = x, column j = y),
+// the splits summed in order with two interleaved accumulators.
 __global__ void reduce_splits_kernel(int m, int n, int splits, const Cx<float>* __restrict__ partial,
                                      Cx<double>* __restrict__ c, long long ldc, bool add, double alpha) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= m) return;
   const long long total = static_cast<long long>(m) * n;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    double re = 0.0, im = 0.0;
-    for (int s = 0; s < splits; ++s) {
-      const Cx<float> v = partial[s * total + idx];
-      re += v.re;
-      im += v.im;
-    }
-    const long long i = idx % m, j = idx / m;
-    Cx<double>& out = c[i + j * ldc];
-    re *= alpha;
-    im *= alpha;
-    if (add) {
-      re += out.re;
-      im += out.im;
-    }
-    out = Cx<double>{re, im};
+  const Cx<float>* p = partial + static_cast<long long>(j) * m + i;
+  double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+  int s = 0;
+  for (; s + 1 < splits; s += 2) {
+    const Cx<float> a = p[s * total], b = p[(s + 1) * total];
+    re0 += a.re;
+    im0 += a.im;
+    re1 += b.re;
+    im1 += b.im;
   }
+  if (s < splits) {
+    const Cx<float> a = p[s * total];
+    re0 += a.re;
+    im0 += a.im;
+  }
+  double re = (re0 + re1) * alpha, im = (im0 + im1) * alpha;
+  Cx<double>& out = c[i + static_cast<long long>(j) * ldc];
+  if (add) {
+    re += out.re;
+    im += out.im;
+  }
+  out = Cx<double>{re, im};
 }
 
 // ---- packing (FP64 complex -> BF16 split terms) ---------------------------
@@ -525,8 +533,9 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
   if (wide) launch<256>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   else launch<128>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   if (splits > 1) {
-    reduce_splits_kernel<<<grid_for(static_cast<long long>(m) * n), 256, 0, stream>>>(m, n, splits, ep.partial, c, ldc,
-                                                                                     add, alpha);
+    if (n > 65535) throw InvalidArgument("split-K reduction has more than 65535 columns");
+    reduce_splits_kernel<<<dim3(static_cast<unsigned>(ceil_div(m, 256)), static_cast<unsigned>(n)), 256, 0, stream>>>(
+        m, n, splits, ep.partial, c, ldc, add, alpha);
     SDFT_LAUNCH("reduce_splits_kernel");
   }
 }
