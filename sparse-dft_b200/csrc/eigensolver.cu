@@ -49,6 +49,11 @@ constexpr unsigned long long kWaitNs = 2000000000ULL;
 constexpr double kClusterTolerance = 1e-9;
 
 
+void check_blas(cublasStatus_t status, const char* what) {
+  if (status != CUBLAS_STATUS_SUCCESS)
+    throw CudaError(std::string("cuBLAS error ") + std::to_string(static_cast<int>(status)) + " in " + what);
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -588,47 +593,24 @@ __global__ void inverse_iteration_kernel(const double* __restrict__ d, const dou
 // H_j0 ... H_j0+nb-1 = I - V T V^H (LAPACK zlarft, forward, columnwise),
 // T upper triangular (column-major, leading dimension kReflectorBlock), from
 // the block's Gram matrix V^H V. One CTA per block.
-__global__ void __launch_bounds__(kThreads) reflector_blocks_kernel(const Cx<double>* __restrict__ reflectors,
+__global__ void __launch_bounds__(kThreads) reflector_blocks_kernel(const Cx<double>* __restrict__ grams,
                                                                     const Cx<double>* __restrict__ tau, int m,
                                                                     Cx<double>* __restrict__ tfac) {
-  constexpr int NB = kReflectorBlock, CH = 16, LD = NB + 1, PAIRS = NB * NB / kThreads;
+  // One CTA per block of NB reflectors: T of I - V T V^H (zlarft) from the
+  // block's Gram matrix G = V^H V (column-major NB x NB, computed by cuBLAS).
+  constexpr int NB = kReflectorBlock, LD = NB + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cx<double>* vs = reinterpret_cast<Cx<double>*>(smem_raw);  // CH x LD
-  Cx<double>* gram = vs + CH * LD;                            // NB x LD
-  Cx<double>* tmat = gram + NB * LD;                          // NB x LD
+  Cx<double>* gram = reinterpret_cast<Cx<double>*>(smem_raw);  // NB x LD, gram[a * LD + b] = G(a, b)
+  Cx<double>* tmat = gram + NB * LD;                            // NB x LD
   const int j0 = blockIdx.x * NB;
   const int nb = min(NB, m - 1 - j0);
   const int tid = threadIdx.x;
-  Cx<double> acc[PAIRS];
-  int pa[PAIRS], pb[PAIRS];
-#pragma unroll
-  for (int q = 0; q < PAIRS; ++q) {
-    acc[q] = Cx<double>{0.0, 0.0};
-    const int idx = tid + q * kThreads;  // over NB*NB
-    pa[q] = idx / NB;
-    pb[q] = idx % NB;
+  const Cx<double>* g = grams + static_cast<long long>(blockIdx.x) * NB * NB;
+  for (int idx = tid; idx < NB * NB; idx += kThreads) {
+    const int col = idx / NB, row = idx % NB;
+    gram[row * LD + col] = g[idx];
+    tmat[(idx / NB) * LD + idx % NB] = Cx<double>{0.0, 0.0};
   }
-  for (int r0 = j0 + 1; r0 < m; r0 += CH) {
-    for (int idx = tid; idx < CH * NB; idx += kThreads) {
-      const int rr = idx % CH, c = idx / CH, r = r0 + rr;
-      Cx<double> val{0.0, 0.0};
-      if (c < nb && r < m && r >= j0 + c + 1) val = reflectors[r + static_cast<long long>(j0 + c) * m];
-      vs[rr * LD + c] = val;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PAIRS; ++q)
-      if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q])
-        for (int rr = 0; rr < CH; ++rr) acc[q] = cadd(acc[q], cdot1(vs[rr * LD + pa[q]], vs[rr * LD + pb[q]]));
-    __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < PAIRS; ++q)
-    if (pa[q] < nb && pb[q] < nb && pa[q] <= pb[q]) {
-      gram[pa[q] * LD + pb[q]] = acc[q];
-      gram[pb[q] * LD + pa[q]] = cconj(acc[q]);
-    }
-  for (int idx = tid; idx < NB * NB; idx += kThreads) tmat[(idx / NB) * LD + idx % NB] = Cx<double>{0.0, 0.0};
   __syncthreads();
   // T(i,i) = tau_i; T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
   for (int i = 0; i < nb; ++i) {
@@ -720,7 +702,7 @@ constexpr std::size_t kSmemLimit = 227 * 1024;
 
 std::size_t invit_smem(int m) { return static_cast<std::size_t>(kInvitThreads) * (5 * sizeof(double) + 1) * m; }
 
-constexpr std::size_t kBlockSmem = sizeof(Cx<double>) * (16 + 2 * kReflectorBlock) * (kReflectorBlock + 1);
+constexpr std::size_t kBlockSmem = sizeof(Cx<double>) * 2 * kReflectorBlock * (kReflectorBlock + 1);
 
 }  // namespace
 
@@ -835,11 +817,12 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   const int blocks = static_cast<int>(ceil_div(m - 1, kReflectorBlock));
   const std::size_t vbytes =
       sizeof(double) * static_cast<std::size_t>(wanted) * mm +
-      sizeof(Cx<double>) * (static_cast<std::size_t>(blocks) + 2 * static_cast<std::size_t>(wanted)) * kReflectorBlock *
-          kReflectorBlock;
+      sizeof(Cx<double>) * (2 * static_cast<std::size_t>(blocks) + 2 * static_cast<std::size_t>(wanted)) *
+          kReflectorBlock * kReflectorBlock;
   auto* zt = static_cast<double*>(ws.vectors.reserve(vbytes));
   auto* tfac = reinterpret_cast<Cx<double>*>(zt + static_cast<std::size_t>(wanted) * mm);
-  Cx<double>* wtmp = tfac + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
+  Cx<double>* grams = tfac + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
+  Cx<double>* wtmp = grams + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
   Cx<double>* utmp = wtmp + static_cast<std::size_t>(wanted) * kReflectorBlock;
   const std::size_t inv_smem = invit_smem(m);
   allow_dynamic_smem(inverse_iteration_kernel, inv_smem);
@@ -848,8 +831,27 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   SDFT_LAUNCH("inverse_iteration_kernel");
   mark(3);
 
+  // Gram blocks V_b^H V_b of the reflector blocks (zeros above each unit
+  // element): one strided-batched ZGEMM over the full blocks, one for the rest.
+  {
+    const cuDoubleComplex one{1.0, 0.0}, zero{0.0, 0.0};
+    const int full = (m - 1) / kReflectorBlock, rest = (m - 1) % kReflectorBlock;
+    const long long block_stride = static_cast<long long>(kReflectorBlock) * m;
+    const long long gram_stride = static_cast<long long>(kReflectorBlock) * kReflectorBlock;
+    auto* v = reinterpret_cast<const cuDoubleComplex*>(reflectors);
+    auto* gz = reinterpret_cast<cuDoubleComplex*>(grams);
+    if (full > 0)
+      check_blas(cublasZgemmStridedBatched(blas, CUBLAS_OP_C, CUBLAS_OP_N, kReflectorBlock, kReflectorBlock, m, &one,
+                                           v, m, block_stride, v, m, block_stride, &zero, gz, kReflectorBlock,
+                                           gram_stride, full),
+                 "zgemmStridedBatched");
+    if (rest > 0)
+      check_blas(cublasZgemm(blas, CUBLAS_OP_C, CUBLAS_OP_N, rest, rest, m, &one, v + full * block_stride, m,
+                             v + full * block_stride, m, &zero, gz + full * gram_stride, kReflectorBlock),
+                 "zgemm");
+  }
   allow_dynamic_smem(reflector_blocks_kernel, kBlockSmem);
-  reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, kBlockSmem, stream>>>(reflectors, tau, m, tfac);
+  reflector_blocks_kernel<<<static_cast<unsigned>(blocks), kThreads, kBlockSmem, stream>>>(grams, tau, m, tfac);
   SDFT_LAUNCH("reflector_blocks_kernel");
   mark(4);
 
