@@ -29,7 +29,16 @@ struct DavidsonStats {
 
 class DavidsonSolver {
  public:
-  explicit DavidsonSolver(DeviceOperator& op) : op_(op) {}
+  // The solver's device state lives in the operator's context (reused by
+  // the solves of later operators on that context).
+  explicit DavidsonSolver(DeviceOperator& op)
+      : op_(op), b_(op.context().davidson), basis_(b_.basis), hbasis_(b_.hbasis), sbasis_(b_.sbasis),
+        cached_h_(b_.cached_h), cached_s_(b_.cached_s), rr_a_(b_.rr_a), rr_b_(b_.rr_b), rr_w_(b_.rr_w),
+        rr_work_(b_.rr_work), info_(b_.info), eigen_(b_.eigen), xs_(b_.xs), sxs_(b_.sxs), hxs_(b_.hxs),
+        res_(b_.res), block_(b_.block), metric_(b_.metric), original_(b_.original), projections_(b_.projections),
+        gram_(b_.gram), small_(b_.small), order_(b_.order), select_(b_.select), pack_vc_(b_.pack_vc),
+        pack_vn_(b_.pack_vn), pack_hn_(b_.pack_hn), pack_sn_(b_.pack_sn), pack_hb_(b_.pack_hb),
+        pack_sb_(b_.pack_sb) {}
   // initial: device n x roots (column-major) warm vectors, or null for a cold start.
   void solve(const DavidsonOptions& options, const Cx<double>* initial);
 
@@ -70,10 +79,12 @@ class DavidsonSolver {
   int size_ = 0, computed_h_ = 0, projected_size_ = 0;
   bool exact_mode_ = true, incremental_ = true, strict_projection_ = false;
   double tolerance_ = 1e-10;
-  Scratch basis_, hbasis_, sbasis_, cached_h_, cached_s_, rr_a_, rr_b_, rr_w_, rr_work_, info_;
-  EigenWorkspace eigen_;
-  Scratch xs_, sxs_, hxs_, res_, block_, metric_, original_, projections_, gram_, small_, order_, select_;
-  Scratch pack_vc_, pack_vn_, pack_hn_, pack_sn_, pack_hb_, pack_sb_;
+  DavidsonBuffers& b_;
+  Scratch &basis_, &hbasis_, &sbasis_, &cached_h_, &cached_s_, &rr_a_, &rr_b_, &rr_w_, &rr_work_, &info_;
+  EigenWorkspace& eigen_;
+  Scratch &xs_, &sxs_, &hxs_, &res_, &block_, &metric_, &original_, &projections_, &gram_, &small_, &order_,
+      &select_;
+  Scratch &pack_vc_, &pack_vn_, &pack_hn_, &pack_sn_, &pack_hb_, &pack_sb_;
   bool packs_ = false;
   Split split_ = Split::BF16x6;
   long long ld_rows_ = 0, ld_cols_ = 0;  // packed row lengths: K = n (rows of V^H, HV, SV) and K = capacity

@@ -159,6 +159,15 @@ void Context::release_scratch() {
                      &tc.partial, &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
                      &eigen.solver_work})
     s->release();
+  davidson.release();
+}
+
+void DavidsonBuffers::release() {
+  for (Scratch* s : {&basis, &hbasis, &sbasis, &cached_h, &cached_s, &rr_a, &rr_b, &rr_w, &rr_work, &info,
+                     &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
+                     &eigen.solver_work, &xs, &sxs, &hxs, &res, &block, &metric, &original, &projections, &gram,
+                     &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb})
+    s->release();
 }
 
 GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],

@@ -48,6 +48,18 @@ struct DensityCache {
 // One CUDA stream with its library handles and grow-only scratch. A context is
 // used by one host thread at a time (the reference keeps one Accelerator per
 // host thread, src/compute_backend.cpp:62-73).
+// Device state of a Davidson solve (basis and images, projected pencil,
+// Rayleigh-Ritz and eigensolver workspace, correction blocks, packed search
+// operands). Owned by the context, so solves of successive operators on one
+// context reuse the allocations.
+struct DavidsonBuffers {
+  Scratch basis, hbasis, sbasis, cached_h, cached_s, rr_a, rr_b, rr_w, rr_work, info;
+  EigenWorkspace eigen;
+  Scratch xs, sxs, hxs, res, block, metric, original, projections, gram, small, order, select;
+  Scratch pack_vc, pack_vn, pack_hn, pack_sn, pack_hb, pack_sb;
+  void release();
+};
+
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -59,6 +71,7 @@ struct Context {
   AcceleratorCache accel;
   DensityCache density;
   EigenWorkspace eigen;
+  DavidsonBuffers davidson;
   explicit Context(int device, cudaStream_t stream);
   ~Context();
   Context(const Context&) = delete;
