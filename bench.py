@@ -264,7 +264,7 @@ def run_b200(args):
 
     # End to end through the public API with host buffers: operator upload from
     # host arrays, solve, eigenvectors read back, every step.
-    e2e = end_to_end(ctx, inputs, stream, steps=max(1, min(args.steps, 2)))
+    e2e = end_to_end(ctx, inputs, stream, steps=max(1, min(args.steps, 3)))
 
     density_rows = None
     if rank == 0 and world == 1 and not args.no_density:
@@ -457,6 +457,20 @@ def serving_stream(device, requests=24, slots=4, rate_hz=8.0, cap=150e9, seed=42
             "mixed": run("mixed"), "fp64_plain": run("fp64")}
 
 
+def pinned_inputs(inputs):
+    """A copy of the operator inputs whose arrays live in pinned host memory."""
+    import dataclasses
+    import torch
+
+    def pin(array):
+        t = torch.from_numpy(array.copy())
+        return t.pin_memory().numpy()
+
+    fields = {f: pin(getattr(inputs, f)) for f in ("hkl", "kinetic_ev", "v_hkl", "v_values", "projectors",
+                                                    "amplitudes", "d", "q")}
+    return dataclasses.replace(inputs, **fields)
+
+
 def end_to_end(ctx, inputs, stream, steps):
     import numpy as np
     import torch
@@ -464,6 +478,7 @@ def end_to_end(ctx, inputs, stream, steps):
     h2d = (inputs.amplitudes.nbytes + inputs.v_values.nbytes + inputs.v_hkl.nbytes + inputs.hkl.nbytes +
            inputs.kinetic_ev.nbytes + inputs.d.nbytes + inputs.q.nbytes)
     d2h = inputs.roots * inputs.npw * 16 + 2 * inputs.roots * 8
+    inputs = pinned_inputs(inputs)
     pairs, seconds = 0, 0.0
     for _ in range(steps):
         torch.cuda.synchronize()
@@ -475,7 +490,7 @@ def end_to_end(ctx, inputs, stream, steps):
         pairs += int(np.sum(result["residuals"] <= TOLERANCE))
         op.close()
     return {"value": pairs / seconds, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "path": "sdft_b200_operator_create (host arrays) + sdft_b200_davidson (host eigenvectors)"}
+            "path": "sdft_b200_operator_create (pinned host arrays) + sdft_b200_davidson (host eigenvectors)"}
 
 
 def cpu_baseline(inputs):
