@@ -143,20 +143,35 @@ __global__ void __launch_bounds__(kThreads) pencil_fixed_kernel(Cx<T>* __restric
   for (int s = tid; s < a.slots; s += kThreads) slot_of_row[a.slot_row[s]] = s;
   __syncthreads();
   Cx<T>* base = slab + static_cast<long long>(c) * a.slots * a.n12 + kl0;
-  for (int idx = tid; idx < N0 * TL; idx += kThreads) {
+  // All of the thread's slab entries and V(r) values are loaded before the
+  // first transform, so the loads are in flight together.
+  constexpr int PER = (N0 * TL + kThreads - 1) / kThreads;
+  Cx<T> entry[PER];
+  T pot[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int idx = tid + q * kThreads;
     const int i = idx / TL, t = idx - i * TL;
-    const int s = slot_of_row[i];
-    tile_a[i * STRIDE + t] =
-        (s >= 0 && t < lines) ? base[static_cast<long long>(s) * a.n12 + t] : Cx<T>{0, 0};
+    entry[q] = Cx<T>{0, 0};
+    pot[q] = T(0);
+    if (idx < N0 * TL && t < lines) {
+      const int s = slot_of_row[i];
+      if (s >= 0) entry[q] = base[static_cast<long long>(s) * a.n12 + t];
+      pot[q] = potential[static_cast<long long>(i) * a.n12 + kl0 + t];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int idx = tid + q * kThreads;
+    if (idx < N0 * TL) tile_a[(idx / TL) * STRIDE + idx % TL] = entry[q];
   }
   __syncthreads();
   Cx<T>* field = fft_lines_fixed<T, true, N0, TL, kThreads>(tile_a, tile_b, 1, STRIDE, tw0);
-  for (int idx = tid; idx < N0 * TL; idx += kThreads) {
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int idx = tid + q * kThreads;
     const int i = idx / TL, t = idx - i * TL;
-    if (t < lines) {
-      const T v = potential[static_cast<long long>(i) * a.n12 + kl0 + t];
-      field[i * STRIDE + t] = cscale(field[i * STRIDE + t], v);
-    }
+    if (idx < N0 * TL && t < lines) field[i * STRIDE + t] = cscale(field[i * STRIDE + t], pot[q]);
   }
   __syncthreads();
   Cx<T>* back = fft_lines_fixed<T, false, N0, TL, kThreads>(field, field == tile_a ? tile_b : tile_a, 1, STRIDE, tw0);
@@ -308,17 +323,49 @@ __global__ void __launch_bounds__(kThreads, plane_blocks<T>()) plane_out_fixed_k
   for (int i = tid; i < N; i += kThreads) tw[i] = a.tw2[i];
   for (int i = tid; i < a.krows; i += kThreads) rows[i] = a.krow[i];
   const Cx<T>* in = slab + (static_cast<long long>(c) * a.slots + s) * (N * N);
-  for (int i = tid; i < N * N; i += kThreads) {
-    const int i1 = i / N, i2 = i - i1 * N;
-    plane[i1 * np + i2] = in[i];
+  // The plane's slab entries and the first points' x and T values are all
+  // requested before the transforms (one round of memory latency).
+  constexpr int PER = (N * N + kThreads - 1) / kThreads, POINTS = 4;
+  {
+    Cx<T> entry[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int i = tid + q * kThreads;
+      entry[q] = i < N * N ? in[i] : Cx<T>{0, 0};
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int i = tid + q * kThreads;
+      if (i < N * N) plane[(i / N) * np + i % N] = entry[q];
+    }
+  }
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
+  const int p_begin = a.point_offset[s], p_end = a.point_offset[s + 1];
+  int pg[POINTS], ps[POINTS];
+  Cx<double> px[POINTS];
+  double pt[POINTS];
+#pragma unroll
+  for (int q = 0; q < POINTS; ++q) {
+    const int p = p_begin + tid + q * kThreads;
+    pg[q] = -1;
+    if (p < p_end) {
+      pg[q] = a.point_g[p];
+      ps[q] = a.point_smem[p];
+      px[q] = xc[pg[q]];
+      pt[q] = kinetic[pg[q]];
+    }
   }
   __syncthreads();
   fft_inplace_fixed<T, false, N, false, kThreads>(plane, N, nullptr, 1, np, tw);
   fft_inplace_fixed<T, false, N, true, kThreads>(plane, a.krows, rows, np, 1, tw);
-  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
-  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
-  const int p_end = a.point_offset[s + 1];
-  for (int p = a.point_offset[s] + tid; p < p_end; p += kThreads) {
+#pragma unroll
+  for (int q = 0; q < POINTS; ++q)
+    if (pg[q] >= 0) {
+      const Cx<double> v = cconvert<double>(plane[ps[q]]);
+      yc[pg[q]] = Cx<double>{pt[q] * px[q].re + v.re / count, pt[q] * px[q].im + v.im / count};
+    }
+  for (int p = p_begin + tid + POINTS * kThreads; p < p_end; p += kThreads) {
     const int g = a.point_g[p];
     const Cx<double> v = cconvert<double>(plane[a.point_smem[p]]);
     const Cx<double> in_g = xc[g];
