@@ -15,10 +15,11 @@
 //    returns.
 // 2. bisect_kernel: one warp per wanted eigenvalue, 64-point multisection on
 //    division-free Sturm counts of the tridiagonal matrix.
-// 3. inverse_iteration_kernel: one thread per cluster of eigenvalues closer
-//    than 1e-9 of the matrix scale, factors in shared memory; LU with partial
-//    pivoting of T - lambda I, two solves, Gram-Schmidt against earlier
-//    members of the cluster.
+// 3. inverse_iteration_kernel: one thread per wanted eigenvalue, factors in
+//    shared memory; LU with partial pivoting of T - lambda I, two solves from
+//    a start vector of its own; then cluster_orthonormalize_kernel, one CTA
+//    per cluster of eigenvalues closer than 1e-9 of the matrix scale, runs
+//    CGS2 over the cluster's vectors in eigenvalue order.
 // 4. reflector_blocks_kernel: the reflectors in blocks of 64 as
 //    I - V T V^H (compact WY); the blocks are applied to the tridiagonal
 //    eigenvectors from the last to the first with three cuBLAS ZGEMMs each.
@@ -494,11 +495,11 @@ __device__ __forceinline__ double start_entry(int k, int i) {
   return static_cast<double>(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
-// One thread per cluster start, kInvitThreads threads per CTA, each with its
-// LU factors and vector in shared memory: reciprocal pivots, the two U
-// superdiagonals, multipliers, z and pivot flags (bytes). Members of a
-// cluster after the first are orthogonalised against the earlier ones
-// (stored in zt) after each solve.
+// One thread per wanted eigenvalue, kInvitThreads threads per CTA, each with
+// its LU factors and vector in shared memory: reciprocal pivots, the two U
+// superdiagonals, multipliers, z and pivot flags (bytes); two solves from a
+// start vector of its own. Clusters are orthonormalised afterwards
+// (cluster_orthonormalize_kernel).
 __global__ void inverse_iteration_kernel(const double* __restrict__ d, const double* __restrict__ e, int m, int wanted,
                                          const double* __restrict__ values, double* __restrict__ zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -515,13 +516,10 @@ __global__ void inverse_iteration_kernel(const double* __restrict__ d, const dou
   if (k >= wanted) return;
   double norm = 0.0;
   for (int i = 0; i < m; ++i) norm = fmax(norm, fabs(d[i]) + (i + 1 < m ? fabs(e[i]) : 0.0));
-  const double cluster = kClusterTolerance * fmax(norm, DBL_MIN);
-  if (k > 0 && values[k] - values[k - 1] <= cluster) return;
-  int end = k;
-  while (end + 1 < wanted && values[end + 1] - values[end] <= cluster) ++end;
   const double tiny = DBL_EPSILON * fmax(norm, DBL_MIN);
   const long long W = wanted;
-  for (int q = k; q <= end; ++q) {
+  {
+    const int q = k;
     const double lam = values[q];
     // LU of T - lam I with partial pivoting (rows i, i+1 swapped when |sub| wins).
     double cur_d = d[0] - lam, cur_u = m > 1 ? e[0] : 0.0;
@@ -575,17 +573,72 @@ __global__ void inverse_iteration_kernel(const double* __restrict__ d, const dou
         z2 = z1;
         z1 = zi;
       }
-      for (int p = k; p < q; ++p) {
-        double dot = 0.0;
-        for (int i = 0; i < m; ++i) dot += zt[i * W + p] * z[i];
-        for (int i = 0; i < m; ++i) z[i] -= dot * zt[i * W + p];
-      }
       double nrm = 0.0;
       for (int i = 0; i < m; ++i) nrm += z[i] * z[i];
       const double inv = 1.0 / sqrt(nrm);
       for (int i = 0; i < m; ++i) z[i] *= inv;
     }
     for (int i = 0; i < m; ++i) zt[i * W + q] = z[i];
+  }
+}
+
+// Orthonormalises the inverse-iteration vectors of each cluster of
+// eigenvalues closer than kClusterTolerance of the matrix scale (chains of
+// such gaps), in eigenvalue order: classical Gram-Schmidt against the earlier
+// members, twice, then normalisation. One CTA per cluster (CTAs whose index
+// does not start a cluster of two or more return at once); the vectors,
+// found independently from distinct start vectors, span the cluster's
+// invariant subspace.
+__global__ void __launch_bounds__(kThreads) cluster_orthonormalize_kernel(const double* __restrict__ d,
+                                                                          const double* __restrict__ e, int m,
+                                                                          int wanted, const double* __restrict__ values,
+                                                                          double* __restrict__ zt) {
+  extern __shared__ double dots[];  // one per earlier cluster member
+  __shared__ double partial[kWarps];
+  const int k = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double norm = 0.0;
+  for (int i = tid; i < m; i += kThreads) norm = fmax(norm, fabs(d[i]) + (i + 1 < m ? fabs(e[i]) : 0.0));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) norm = fmax(norm, __shfl_xor_sync(0xffffffffu, norm, o));
+  if (lane == 0) partial[warp] = norm;
+  __syncthreads();
+  norm = 0.0;
+  for (int w = 0; w < kWarps; ++w) norm = fmax(norm, partial[w]);
+  const double cluster = kClusterTolerance * fmax(norm, DBL_MIN);
+  if (k > 0 && values[k] - values[k - 1] <= cluster) return;
+  int end = k;
+  while (end + 1 < wanted && values[end + 1] - values[end] <= cluster) ++end;
+  if (end == k) return;
+  const long long W = wanted;
+  for (int q = k + 1; q <= end; ++q) {
+    for (int pass = 0; pass < 2; ++pass) {
+      __syncthreads();
+      // dots with the earlier members: warp w takes members k + w, k + w + kWarps, ...
+      for (int p = k + warp; p < q; p += kWarps) {
+        double s = 0.0;
+        for (int i = lane; i < m; i += 32) s += zt[i * W + p] * zt[i * W + q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) dots[p - k] = s;
+      }
+      __syncthreads();
+      for (int i = tid; i < m; i += kThreads) {
+        double v = zt[i * W + q];
+        for (int p = k; p < q; ++p) v -= dots[p - k] * zt[i * W + p];
+        zt[i * W + q] = v;
+      }
+    }
+    __syncthreads();
+    double s = 0.0;
+    for (int i = tid; i < m; i += kThreads) s += zt[i * W + q] * zt[i * W + q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) partial[warp] = s;
+    __syncthreads();
+    double total = 0.0;
+    for (int w = 0; w < kWarps; ++w) total += partial[w];
+    const double inv = 1.0 / sqrt(total);
+    for (int i = tid; i < m; i += kThreads) zt[i * W + q] *= inv;
   }
 }
 
@@ -829,6 +882,11 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   inverse_iteration_kernel<<<static_cast<unsigned>(ceil_div(wanted, kInvitThreads)), kInvitThreads, inv_smem,
                              stream>>>(d, e, m, wanted, values, zt);
   SDFT_LAUNCH("inverse_iteration_kernel");
+  const std::size_t dots_smem = sizeof(double) * static_cast<std::size_t>(wanted);
+  allow_dynamic_smem(cluster_orthonormalize_kernel, dots_smem);
+  cluster_orthonormalize_kernel<<<static_cast<unsigned>(wanted), kThreads, dots_smem, stream>>>(d, e, m, wanted,
+                                                                                                values, zt);
+  SDFT_LAUNCH("cluster_orthonormalize_kernel");
   mark(3);
 
   // Gram blocks V_b^H V_b of the reflector blocks (zeros above each unit

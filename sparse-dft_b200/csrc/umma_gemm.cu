@@ -132,7 +132,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   std::uint32_t* tmem_holder = reinterpret_cast<std::uint32_t*>(accum + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int tile_m = blockIdx.x * BM, tile_n = blockIdx.y * BN;
+  // Column tiles run fastest, so the CTAs sharing an A tile are resident
+  // together and all but the first read it from L2.
+  const int tile_n = blockIdx.x * BN, tile_m = blockIdx.y * BM;
   const int kb0 = blockIdx.z * k_blocks_per_split;
   const int nkb = max(0, min(k_blocks_total, kb0 + k_blocks_per_split) - kb0);
 
@@ -438,7 +440,8 @@ void launch(const std::uint16_t* a, long long lda, const std::uint16_t* b, long 
   allow_dynamic_smem(umma_gemm_kernel<BN>, smem);
   const CUtensorMap map_a = kmajor_map(a, m, kexp, lda, BM);
   const CUtensorMap map_b = kmajor_map(b, n2, kexp, ldb, BN);
-  const dim3 grid(static_cast<unsigned>(ceil_div(m, BM)), static_cast<unsigned>(ceil_div(n2, BN)), splits);
+  if (ceil_div(m, BM) > 65535) throw InvalidArgument("tensor-core GEMM has more than 65535 row tiles");
+  const dim3 grid(static_cast<unsigned>(ceil_div(n2, BN)), static_cast<unsigned>(ceil_div(m, BM)), splits);
   umma_gemm_kernel<BN><<<grid, kThreads, smem, stream>>>(map_a, map_b, k_blocks, kpb, ep_in);
   SDFT_LAUNCH("umma_gemm_kernel");
 }
@@ -508,18 +511,31 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
   if (kexp % BK != 0) throw InvalidArgument("expanded K must be a multiple of 64");
   const int n2 = 2 * n;
   const int k_blocks = static_cast<int>(kexp / BK);
-  const bool wide = n2 > 128;
-  const int bn = wide ? 256 : 128;
+  // Column tile width: the one of 128 / 160 / 256 that pads the 2n real
+  // columns least (the larger on ties).
+  int bn = 256;
+  long long padded = ceil_div(n2, 256) * 256LL;
+  for (int w : {160, 128}) {
+    const long long p = ceil_div(n2, w) * static_cast<long long>(w);
+    if (p < padded) {
+      padded = p;
+      bn = w;
+    }
+  }
   const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n2, bn));
-  // Split-K count: one CTA per SM is resident (the ring takes ~190 KB), so the
-  // time goes as waves x K blocks per CTA; take the split that minimises it
-  // (the smallest on ties), with at least 8 K blocks per split.
+  // Split-K count: one CTA per SM is resident (the ring takes ~200 KB), so the
+  // time goes as waves x K blocks per CTA, plus the FP32 partials that a split
+  // writes and the reduction reads, counted in K blocks' worth of operand
+  // traffic spread over the SMs; the smallest split on ties, at least 8 K
+  // blocks per split.
+  const double kblock_bytes = static_cast<double>(BM + bn) * BK * 2;
   const long long max_splits = std::min<long long>(128, std::max(1, k_blocks / 8));
-  long long best_cost = -1;
+  double best_cost = -1;
   int splits = 1;
   for (long long s = 1; s <= max_splits; ++s) {
     const long long waves = (tiles * s + 147) / 148;
-    const long long cost = waves * ((k_blocks + s - 1) / s);
+    const double partial = s > 1 ? 2.0 * 4.0 * static_cast<double>(m) * n2 * s / (148.0 * kblock_bytes) : 0.0;
+    const double cost = static_cast<double>(waves * ((k_blocks + s - 1) / s)) + partial;
     if (best_cost < 0 || cost < best_cost) {
       best_cost = cost;
       splits = static_cast<int>(s);
@@ -530,7 +546,8 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
   EpilogueArgs ep{m, n2, nullptr, c, ldc, alpha, add ? 1 : 0};
   if (splits > 1)
     ep.partial = static_cast<Cx<float>*>(workspace.reserve(sizeof(Cx<float>) * static_cast<std::size_t>(m) * n * splits));
-  if (wide) launch<256>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
+  if (bn == 256) launch<256>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
+  else if (bn == 160) launch<160>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   else launch<128>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   if (splits > 1) {
     if (n > 65535) throw InvalidArgument("split-K reduction has more than 65535 columns");
