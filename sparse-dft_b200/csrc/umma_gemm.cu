@@ -191,6 +191,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int row = tile_m + warp * 32 + lane;
   const int n_complex_total = ep.n2 / 2;
   for (int c0 = 0; c0 < BN; c0 += 16) {
+    // The chunk's earlier C values (accumulating products) are requested
+    // before the accumulator read, all eight at once.
+    Cx<double> prior[8];
+    const bool accumulate = !ep.partial && ep.add && row < ep.m;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = (tile_n + c0) / 2 + q;
+      prior[q] = (accumulate && j < n_complex_total) ? ep.c[row + static_cast<long long>(j) * ep.ldc]
+                                                     : Cx<double>{0.0, 0.0};
+    }
     std::uint32_t r[16];
     if (have) {
       const std::uint32_t taddr = tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c0);
@@ -213,13 +223,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (ep.partial) {
           ep.partial[(static_cast<long long>(blockIdx.z) * n_complex_total + j) * ep.m + row] = Cx<float>{re, im};
         } else {
-          Cx<double>& out = ep.c[row + static_cast<long long>(j) * ep.ldc];
           double vr = ep.alpha * static_cast<double>(re), vi = ep.alpha * static_cast<double>(im);
           if (ep.add) {
-            vr += out.re;
-            vi += out.im;
+            vr += prior[q].re;
+            vi += prior[q].im;
           }
-          out = Cx<double>{vr, vi};
+          ep.c[row + static_cast<long long>(j) * ep.ldc] = Cx<double>{vr, vi};
         }
       }
     }
