@@ -276,6 +276,26 @@ SDFT_B200_API sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const 
                                                   const double* initial, double* eigenvalues, double* eigenvectors,
                                                   double* residuals, sdft_b200_davidson_stats* stats, int memory);
 
+/* ---- Solver snapshots ------------------------------------------------------
+ * The reference's SDFTPWO3 files (PlaneWaveOperator::save_solver_snapshot,
+ * src/plane_wave_operator.cpp:542-569; replayed by sdft_solver_replay):
+ * the operator's internal arrays and the solve settings. */
+typedef struct {
+  size_t npw, grid_points, projectors, atoms, roots, iterations, initial_values;
+  int32_t shape[3];
+  double regularization, tolerance;
+} sdft_b200_snapshot_info;
+
+/* Header fields after the reference's checks (host only, no device).
+ * Replaces: the header checks of PlaneWaveOperator::load_solver_snapshot,
+ * src/plane_wave_operator.cpp:571-604. */
+SDFT_B200_API sdft_b200_status sdft_b200_snapshot_read_info(const char* path, sdft_b200_snapshot_info* info);
+/* Device operator from a snapshot; initial (band-major roots x npw, host,
+ * may be NULL) receives the snapshot's warm vectors when it has them.
+ * Replaces: PlaneWaveOperator::load_solver_snapshot, src/plane_wave_operator.cpp:571-653. */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_from_snapshot(sdft_b200_context* context, const char* path,
+                                                                sdft_b200_operator** out, double* initial);
+
 /* ---- Solve server: continuous batching of independent solves ------------
  * One request = one operator (one cell, one k-point) and its Davidson solve,
  * copied in at submit. Requests wait in a FIFO queue and start when a worker

@@ -259,6 +259,29 @@ class ReferenceOperator:
         return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),
                 "iterations": int(iters.value)}
 
+    @classmethod
+    def from_snapshot(cls, lib: ReferenceLibrary, path):
+        """The reference's PlaneWaveOperator::load_solver_snapshot; the warm
+        vectors are read from the file (the driver does not return them)."""
+        import pathlib
+        import struct
+        raw = pathlib.Path(path).read_bytes()
+        n, roots_h = struct.unpack_from("<Q", raw, 8)[0], struct.unpack_from("<Q", raw, 56)[0]
+        warm = struct.unpack_from("<Q", raw, 72)[0]
+        roots, iterations, tolerance = ctypes.c_long(), ctypes.c_long(), ctypes.c_double()
+        err = ctypes.create_string_buffer(1024)
+        handle = lib.lib.ref_load_snapshot(str(path).encode(), ctypes.byref(roots), ctypes.byref(iterations),
+                                           ctypes.byref(tolerance), err, 1024)
+        if not handle:
+            raise RuntimeError(err.value.decode(errors="replace"))
+        op = cls(lib, handle=handle)
+        op.n = int(n)
+        initial = None
+        if warm:
+            initial = np.frombuffer(raw, dtype="<c16", count=warm, offset=len(raw) - 16 * warm).reshape(roots_h, n).copy()
+        return {"operator": op, "roots": roots.value, "iterations": iterations.value, "tolerance": tolerance.value,
+                "initial": initial}
+
     def save_snapshot(self, path, roots, iterations, tolerance, initial=None):
         init = np.ascontiguousarray(initial if initial is not None else np.zeros(0), dtype=np.complex128)
         self._call(self.lib.lib.ref_save_snapshot, self.handle, str(path).encode(), roots, iterations, tolerance,

@@ -617,6 +617,36 @@ sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davi
   });
 }
 
+sdft_b200_status sdft_b200_snapshot_read_info(const char* path, sdft_b200_snapshot_info* info) {
+  return guarded([&] {
+    require(path && info, "null snapshot argument");
+    const auto snap = sdft_b200::read_operator_snapshot(path, true);
+    info->npw = snap.npw;
+    info->grid_points = snap.count;
+    info->projectors = snap.projectors;
+    info->atoms = snap.channels.size();
+    info->roots = snap.roots;
+    info->iterations = snap.iterations;
+    info->initial_values = snap.initial_values;
+    for (int a = 0; a < 3; ++a) info->shape[a] = snap.shape[a];
+    info->regularization = snap.regularization;
+    info->tolerance = snap.tolerance;
+  });
+}
+
+sdft_b200_status sdft_b200_operator_from_snapshot(sdft_b200_context* context, const char* path,
+                                                  sdft_b200_operator** out, double* initial) {
+  return guarded([&] {
+    require(context && path && out, "null snapshot argument");
+    const auto snap = sdft_b200::read_operator_snapshot(path, false);
+    auto op = std::make_unique<sdft_b200_operator>();
+    op->impl = std::make_unique<sdft_b200::DeviceOperator>(*context->impl, snap);
+    if (initial && !snap.initial.empty())
+      std::memcpy(initial, snap.initial.data(), sizeof(Cx<double>) * snap.initial.size());
+    *out = op.release();
+  });
+}
+
 sdft_b200_status sdft_b200_server_create(int device, uint64_t memory_cap, int slots, sdft_b200_server** out) {
   return guarded([&] {
     require(out != nullptr, "null server output");

@@ -380,21 +380,8 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     }
   }
   // Device upload.
-  plan_.build(shape, h_indices_);
-  auto upload = [&](auto*& dst, const auto& src) {
-    using E = typename std::remove_reference_t<decltype(src)>::value_type;
-    SDFT_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), sizeof(E) * std::max<std::size_t>(1, src.size())));
-    if (!src.empty()) SDFT_CUDA(cudaMemcpy(dst, src.data(), sizeof(E) * src.size(), cudaMemcpyHostToDevice));
-  };
-  upload(kinetic_, h_kinetic_);
-  upload(v64_, h_local_real_);
-  std::vector<float> v32(h_local_real_.begin(), h_local_real_.end());
-  upload(v32_, v32);
+  upload_common(shape, d_blocks, q_blocks, offsets, storage);
   if (np_) {
-    upload(d_, d_blocks);
-    upload(q_, q_blocks);
-    upload(block_offsets_, offsets);
-    upload(block_storage_, storage);
     // B: the row-major per-atom amplitudes (the input layout) are uploaded as
     // they are, checked and transposed on the device into the column-major
     // Sigma_np x NPW matrix; the diagonals' PAW terms Re(b_g^H D b_g) and
@@ -423,6 +410,70 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     cudaFree(raw);
     cudaFree(diag);
     if (bad) throw InvalidArgument("nonfinite PAW projector/D/Q data");
+    const Split split = search_split();
+    pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
+    pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
+  }
+  SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+namespace {
+template <typename T>
+void upload_array(T*& dst, const std::vector<T>& src) {
+  SDFT_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), sizeof(T) * std::max<std::size_t>(1, src.size())));
+  if (!src.empty()) SDFT_CUDA(cudaMemcpy(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+}
+}  // namespace
+
+void DeviceOperator::upload_common(const int shape[3], const std::vector<Cx<double>>& d_blocks,
+                                   const std::vector<Cx<double>>& q_blocks, const std::vector<int>& offsets,
+                                   const std::vector<long long>& storage) {
+  plan_.build(shape, h_indices_);
+  upload_array(kinetic_, h_kinetic_);
+  upload_array(v64_, h_local_real_);
+  std::vector<float> v32(h_local_real_.begin(), h_local_real_.end());
+  upload_array(v32_, v32);
+  if (np_) {
+    upload_array(d_, d_blocks);
+    upload_array(q_, q_blocks);
+    upload_array(block_offsets_, offsets);
+    upload_array(block_storage_, storage);
+  }
+}
+
+// From a snapshot (the reference's load_solver_snapshot,
+// src/plane_wave_operator.cpp:571-653): the arrays are the operator's own, so
+// nothing is rebuilt; B is already column-major Sigma_np x NPW.
+DeviceOperator::DeviceOperator(Context& ctx, const OperatorSnapshot& snap) : ctx_(ctx) {
+  SDFT_CUDA(cudaSetDevice(ctx.device));
+  if (snap.npw > static_cast<std::size_t>(std::numeric_limits<int>::max()) || snap.projectors > 65536 ||
+      snap.channels.size() > static_cast<std::size_t>(std::numeric_limits<int>::max()))
+    throw Overflow("solver snapshot dimensions exceed the device operator's limits");
+  npw_ = static_cast<int>(snap.npw);
+  regularization_ = snap.regularization;
+  h_indices_ = snap.indices;
+  h_kinetic_ = snap.kinetic;
+  h_diag_ = snap.h_diagonal;
+  s_diag_ = snap.s_diagonal;
+  h_local_real_ = snap.local_real;
+  atoms_ = static_cast<int>(snap.channels.size());
+  std::vector<int> offsets(atoms_ + 1, 0);
+  std::vector<long long> storage(atoms_, 0);
+  std::size_t total = 0, block_total = 0;
+  for (int a = 0; a < atoms_; ++a) {
+    const std::size_t np = snap.channels[a];
+    if (!np || np > 256) throw InvalidArgument("invalid PAW low-rank operator dimensions");
+    offsets[a] = static_cast<int>(total);
+    storage[a] = static_cast<long long>(block_total);
+    total += np;
+    block_total += np * np;
+    max_block_ = std::max<int>(max_block_, static_cast<int>(np));
+  }
+  offsets[atoms_] = static_cast<int>(total);
+  np_ = static_cast<int>(total);
+  upload_common(snap.shape, snap.d, snap.q, offsets, storage);
+  if (np_) {
+    upload_array(b_, snap.all_b);
     const Split split = search_split();
     pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
     pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);

@@ -6,6 +6,7 @@
 #include <array>
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "eigensolver.cuh"
@@ -123,9 +124,32 @@ struct OperatorInput {
   double regularization = 1e-12;
 };
 
+// A solver snapshot in the reference's SDFTPWO3 format (per-atom D/Q
+// blocks): the operator's internal arrays and the solve settings. Little-
+// endian uint64 header; FP64 arrays; complex arrays interleaved, column-major.
+struct OperatorSnapshot {
+  int shape[3] = {0, 0, 0};
+  std::size_t npw = 0, count = 0, projectors = 0, roots = 0, iterations = 0, initial_values = 0;
+  double regularization = 0, tolerance = 0;
+  std::vector<std::uint64_t> channels;  // projectors per atom
+  std::vector<std::uint64_t> indices;   // wrapped row-major grid index per plane wave
+  std::vector<double> kinetic, h_diagonal, s_diagonal, local_real;
+  std::vector<Cx<double>> all_b;        // projectors x npw, column-major
+  std::vector<Cx<double>> d, q;         // per atom channels^2, column-major, concatenated
+  std::vector<Cx<double>> initial;      // roots x npw band-major warm vectors, or empty
+};
+
+// Reads and validates a snapshot (the reference's load_solver_snapshot
+// checks: dimensions, exact file length, unique in-range indices, finite
+// arrays, positive overlap diagonal, Hermitian blocks). header_only skips
+// the arrays after the atom boundaries.
+OperatorSnapshot read_operator_snapshot(const std::string& path, bool header_only = false);
+
 class DeviceOperator {
  public:
   DeviceOperator(Context& ctx, const OperatorInput& input);
+  // From a solver snapshot's internal arrays (no rebuild from G components).
+  DeviceOperator(Context& ctx, const OperatorSnapshot& snapshot);
   ~DeviceOperator();
   DeviceOperator(const DeviceOperator&) = delete;
   DeviceOperator& operator=(const DeviceOperator&) = delete;
@@ -159,6 +183,11 @@ class DeviceOperator {
   std::size_t device_bytes() const;
 
  private:
+  // Device arrays from the host state (plan, kinetic, V(r), D/Q blocks and
+  // boundaries); B and the diagonals are the caller's.
+  void upload_common(const int shape[3], const std::vector<Cx<double>>& d_blocks,
+                     const std::vector<Cx<double>>& q_blocks, const std::vector<int>& offsets,
+                     const std::vector<long long>& storage);
   void local_part(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
   void paw_add(const Cx<double>* p, int columns, bool overlap, Cx<double>* y, Precision precision);
   void backproject(const Cx<double>* dp, int columns, Cx<double>* y, Precision precision);

@@ -64,6 +64,18 @@ SZ = ctypes.c_size_t
 SZP = ctypes.POINTER(ctypes.c_size_t)
 
 
+class SnapshotInfo(ctypes.Structure):
+    _fields_ = [("npw", ctypes.c_size_t), ("grid_points", ctypes.c_size_t), ("projectors", ctypes.c_size_t),
+                ("atoms", ctypes.c_size_t), ("roots", ctypes.c_size_t), ("iterations", ctypes.c_size_t),
+                ("initial_values", ctypes.c_size_t), ("shape", ctypes.c_int32 * 3), ("regularization", ctypes.c_double),
+                ("tolerance", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        out = {name: getattr(self, name) for name, _ in self._fields_}
+        out["shape"] = tuple(int(v) for v in self.shape)
+        return out
+
+
 class SolveTiming(ctypes.Structure):
     _fields_ = [("slot", ctypes.c_int), ("footprint", ctypes.c_size_t), ("submitted", ctypes.c_double),
                 ("started", ctypes.c_double), ("finished", ctypes.c_double)]
@@ -126,6 +138,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_project", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_davidson", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
                               ctypes.c_int])
+    fn("sdft_b200_snapshot_read_info", [ctypes.c_char_p, ctypes.POINTER(SnapshotInfo)])
+    fn("sdft_b200_operator_from_snapshot", [P, ctypes.c_char_p, ctypes.POINTER(P), P])
     fn("sdft_b200_server_create", [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(P)])
     fn("sdft_b200_server_destroy", [P])
     fn("sdft_b200_server_submit", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,

@@ -73,8 +73,33 @@ def enumerate_g_vectors(reciprocal, cutoff_ev: float, kpoint=(0.0, 0.0, 0.0), ha
     return hkl, cart, kin
 
 
+def snapshot_info(path) -> dict:
+    """Header of a solver snapshot (the reference's SDFTPWO3 file), host only."""
+    info = C.SnapshotInfo()
+    C.check(C.library().sdft_b200_snapshot_read_info(str(path).encode(), ctypes.byref(info)))
+    return info.as_dict()
+
+
 class PlaneWaveOperator:
     """Device-resident H~ and S~ built from the reference's constructor arguments."""
+
+    @classmethod
+    def from_snapshot(cls, context: Context, path):
+        """Operator from a solver snapshot (the reference's load_solver_snapshot);
+        returns (operator, settings) with the snapshot's roots, iterations,
+        tolerance and warm vectors (band-major roots x npw, or None)."""
+        info = snapshot_info(path)
+        warm = np.zeros((info["roots"], info["npw"]), dtype=np.complex128) if info["initial_values"] else None
+        self = cls.__new__(cls)
+        self.context = context
+        self._lib = C.library()
+        handle = ctypes.c_void_p()
+        C.check(self._lib.sdft_b200_operator_from_snapshot(context.handle, str(path).encode(), ctypes.byref(handle),
+                                                           ctypes.c_void_p(warm.ctypes.data) if warm is not None else None))
+        self.handle = handle
+        self._read_info()
+        return self, {"roots": info["roots"], "iterations": info["iterations"], "tolerance": info["tolerance"],
+                      "initial": warm}
 
     def __init__(self, context: Context, inputs):
         self.context = context
@@ -95,6 +120,10 @@ class PlaneWaveOperator:
             amp.ctypes.data_as(C.D), d.ctypes.data_as(C.D), q.ctypes.data_as(C.D), x.hartree_to_ev, x.regularization,
             ctypes.byref(handle)))
         self.handle = handle
+        self._read_info()
+
+    def _read_info(self) -> None:
+        handle = self.handle
         shape = np.zeros(3, dtype=np.int32)
         grid = ctypes.c_size_t()
         nproj = ctypes.c_size_t()

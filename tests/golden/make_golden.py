@@ -144,6 +144,32 @@ def compensation_fixture(lib, inputs, name, factor, bands):
     print("compensation", name, "keys", keys.shape[0])
 
 
+def snapshot_fixtures(lib):
+    """Solver snapshots written by the reference (save_solver_snapshot) for
+    the tiny pencil, cold and warm (the reference's eigenvectors with seeded
+    1e-3 perturbations), and the reference's solves of each snapshot as
+    loaded by its own load_solver_snapshot."""
+    inputs = synthetic.tiny()
+    op = ref_oracle.ReferenceOperator(lib, inputs)
+    base = op.davidson(inputs.roots, inputs.max_iterations, inputs.tolerance)
+    rng = np.random.Generator(np.random.PCG64(17))
+    warm = base["eigenvectors"] + 1e-3 * (rng.standard_normal(base["eigenvectors"].shape) +
+                                         1j * rng.standard_normal(base["eigenvectors"].shape))
+    results = {}
+    for name, initial in (("tiny_cold", None), ("tiny_warm", warm)):
+        path = HERE / f"{name}.pwo3"
+        if path.exists():
+            path.unlink()
+        op.save_snapshot(path, inputs.roots, inputs.max_iterations, inputs.tolerance, initial)
+        loaded = ref_oracle.ReferenceOperator.from_snapshot(lib, path)
+        r = loaded["operator"].davidson(loaded["roots"], loaded["iterations"], loaded["tolerance"],
+                                        initial=loaded["initial"])
+        results[f"{name}_eigenvalues"] = r["eigenvalues"]
+        results[f"{name}_iterations"] = np.array(r["iterations"])
+    np.savez_compressed(HERE / "snapshots.npz", **results)
+    print("snapshots", {k: v for k, v in results.items() if "iterations" in k})
+
+
 KPOINT_MESH = {"gaas_k13": (0.0, 1.0 / 3.0, 1.0 / 3.0), "gaas_k26": (1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)}
 
 
@@ -158,10 +184,14 @@ def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
     parser.add_argument("--kpoints", action="store_true", help="only the off-Gamma GaAs fixtures")
+    parser.add_argument("--snapshots", action="store_true", help="only the solver snapshot fixtures")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
         kpoint_fixtures(lib)
+        return
+    if args.snapshots:
+        snapshot_fixtures(lib)
         return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
@@ -170,6 +200,7 @@ def main():
     density_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     compensation_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     kpoint_fixtures(lib)
+    snapshot_fixtures(lib)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

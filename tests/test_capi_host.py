@@ -1,5 +1,6 @@
 """C ABI checks that need no GPU: the library loads, exports its header, host logic is exact."""
 import ctypes
+import pathlib
 import subprocess
 
 import numpy as np
@@ -91,3 +92,25 @@ def test_server_without_gpu_reports_cuda_error():
     assert lib.sdft_b200_server_create(0, 1 << 30, 2, ctypes.byref(handle)) == C.CUDA_ERROR
     assert "CUDA" in C.last_error()
     assert lib.sdft_b200_server_create(0, 1 << 30, 0, ctypes.byref(handle)) == C.INVALID_ARGUMENT
+
+
+def test_snapshot_header_matches_reference_file():
+    """The snapshot reader's header (host only) agrees with the file the
+    reference wrote (tests/golden/tiny_*.pwo3); non-snapshots are refused."""
+    import struct
+    from sdft_b200.operator import snapshot_info
+    golden = pathlib.Path(__file__).resolve().parent / "golden"
+    for name, warm in (("tiny_cold", False), ("tiny_warm", True)):
+        raw = (golden / f"{name}.pwo3").read_bytes()
+        n, count, s0, s1, s2, nproj, roots, iters, ninit = struct.unpack_from("<9Q", raw, 8)
+        reg, tol = struct.unpack_from("<2d", raw, 80)
+        info = snapshot_info(golden / f"{name}.pwo3")
+        assert (info["npw"], info["grid_points"], info["projectors"], info["roots"], info["iterations"]) == (
+            n, count, nproj, roots, iters)
+        assert info["shape"] == (s0, s1, s2) and info["atoms"] == struct.unpack_from("<Q", raw, 96)[0]
+        assert info["regularization"] == reg and info["tolerance"] == tol
+        assert (info["initial_values"] == n * roots) == warm and (info["initial_values"] == 0) != warm
+    with pytest.raises(C.SdftError, match="unsupported solver snapshot format"):
+        snapshot_info(golden / "tiny.npz")
+    with pytest.raises(C.SdftError, match="cannot open solver snapshot"):
+        snapshot_info(golden / "no_such_snapshot.pwo3")
