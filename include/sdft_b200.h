@@ -211,6 +211,12 @@ SDFT_B200_API sdft_b200_status sdft_b200_compensation_create(
 SDFT_B200_API sdft_b200_status sdft_b200_compensation_destroy(sdft_b200_compensation* charge);
 SDFT_B200_API sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensation* charge, const double* onsite,
                                                               double* out, int memory);
+/* The adjoint: potential (V(G) on the charge's support keys, in their order;
+ * a mode absent from the potential is 0), out (atoms x dimension^2 row-major)
+ * = sum_LM [sum_G V(-G) e^{-iG.tau_a} F_LM(G)] T_LM, the (L,M) transform T.
+ * Replaces: PawCompensationOperator::project_potential_batch, src/paw_compensation.cpp:552-629. */
+SDFT_B200_API sdft_b200_status sdft_b200_compensation_project(sdft_b200_compensation* charge, const double* potential,
+                                                              double* out, int memory);
 
 /* Rayleigh-Ritz eigensolve of a projected pencil in FP64: the lowest
  * `requested` (0 = all n) solutions of H y = e S y, H and S n x n Hermitian

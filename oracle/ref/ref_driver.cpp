@@ -360,4 +360,40 @@ int ref_compensation_density(const double* lattice, long atoms, const double* fr
     return 1;
   }
 }
+
+// PawCompensationOperator::project_potential_batch (src/paw_compensation.cpp:552)
+// of a potential given on `potential_count` keys; out: atoms x dim^2 complex.
+int ref_compensation_project(const double* lattice, long atoms, const double* fractional, long count,
+                             const int* keys, long channels, const int* channel_l, int max_l, long radial,
+                             const double* radial_grid, const double* aug_moment, const double* compensation_r2,
+                             long potential_count, const int* potential_keys, const double* potential, double* out,
+                             char* error, long error_length) {
+  try {
+    const auto a = augmentation(channels, channel_l, max_l, radial, radial_grid, aug_moment, compensation_r2);
+    std::array<sdft::Vec3, 3> cell{};
+    for (int r = 0; r < 3; ++r) cell[r] = {lattice[3 * r], lattice[3 * r + 1], lattice[3 * r + 2]};
+    std::vector<std::tuple<int, int, int>> support(static_cast<std::size_t>(count));
+    for (long i = 0; i < count; ++i) support[i] = {keys[3 * i], keys[3 * i + 1], keys[3 * i + 2]};
+    std::size_t dim = 0;
+    for (int l : a.channel_l) dim += 2 * l + 1;
+    std::vector<sdft::PawCompensationOperator> ops;
+    ops.reserve(static_cast<std::size_t>(atoms));
+    for (long i = 0; i < atoms; ++i) {
+      const sdft::Vec3 f{fractional[3 * i], fractional[3 * i + 1], fractional[3 * i + 2]};
+      ops.emplace_back(a, cell, f, support, sdft::AtomicUnitConvention::Codata, i ? &ops.front() : nullptr);
+    }
+    sdft::FourierDensity v;
+    const auto* pv = reinterpret_cast<const C*>(potential);
+    for (long i = 0; i < potential_count; ++i)
+      v[{potential_keys[3 * i], potential_keys[3 * i + 1], potential_keys[3 * i + 2]}] = pv[i];
+    const auto projected = sdft::PawCompensationOperator::project_potential_batch(ops, v);
+    auto* o = reinterpret_cast<C*>(out);
+    for (long i = 0; i < atoms; ++i)
+      for (std::size_t e = 0; e < dim * dim; ++e) o[i * dim * dim + e] = projected[i][e];
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
 }

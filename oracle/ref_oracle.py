@@ -83,6 +83,10 @@ class ReferenceLibrary:
         L.ref_compensation_density.argtypes = [_dbl, ctypes.c_long, _dbl, ctypes.c_long, _int, ctypes.c_long, _int,
                                                ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, _dbl, _dbl,
                                                ctypes.c_char_p, ctypes.c_long]
+        L.ref_compensation_project.restype = ctypes.c_int
+        L.ref_compensation_project.argtypes = [_dbl, ctypes.c_long, _dbl, ctypes.c_long, _int, ctypes.c_long, _int,
+                                               ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, ctypes.c_long, _int,
+                                               _dbl, _dbl, ctypes.c_char_p, ctypes.c_long]
 
     # -- basis ---------------------------------------------------------------
     def enumerate_g_vectors(self, reciprocal, cutoff_ev, kpoint=(0.0, 0.0, 0.0), hartree_to_ev=27.211386245988):
@@ -155,6 +159,25 @@ class ReferenceLibrary:
         rc = self.lib.ref_compensation_density(_ptr(lat), frac.shape[0], _ptr(frac), k.shape[0], _ptr(k, _int),
                                                ch.size, _ptr(ch, _int), max_l, r.size, _ptr(r), _ptr(mom), _ptr(r2),
                                                rho.view(np.float64).ctypes.data_as(_dbl),
+                                               out.view(np.float64).ctypes.data_as(_dbl), err, 512)
+        self._check(rc, err)
+        return out
+
+    def compensation_project(self, lattice, fractional, keys, aug, potential_keys, potential):
+        """PawCompensationOperator::project_potential_batch (src/paw_compensation.cpp:552):
+        (atoms, dim, dim) projections of the potential given on potential_keys."""
+        ch, max_l, r, mom, r2 = self._augmentation(aug)
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        frac = np.ascontiguousarray(fractional, dtype=np.float64).reshape(-1, 3)
+        k = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+        pk = np.ascontiguousarray(potential_keys, dtype=np.int32).reshape(-1, 3)
+        pv = np.ascontiguousarray(potential, dtype=np.complex128)
+        dim = int(np.sum(2 * np.asarray(aug["channel_l"]) + 1))
+        out = np.zeros((frac.shape[0], dim, dim), dtype=np.complex128)
+        err = ctypes.create_string_buffer(512)
+        rc = self.lib.ref_compensation_project(_ptr(lat), frac.shape[0], _ptr(frac), k.shape[0], _ptr(k, _int),
+                                               ch.size, _ptr(ch, _int), max_l, r.size, _ptr(r), _ptr(mom), _ptr(r2),
+                                               pk.shape[0], _ptr(pk, _int), pv.view(np.float64).ctypes.data_as(_dbl),
                                                out.view(np.float64).ctypes.data_as(_dbl), err, 512)
         self._check(rc, err)
         return out

@@ -440,3 +440,30 @@ def compensation_density(lattice, fractional, keys, augmentation, transform, ons
         phase = np.exp(-1j * (q @ positions[atom]))
         total += phase * (moments[atom] @ complex_form) / volume
     return total
+
+
+def compensation_project(lattice, fractional, keys, augmentation, transform, potential) -> np.ndarray:
+    """The adjoint of compensation_density: out_a = sum_LM [sum_G V(-G) exp(-i G.tau_a) F_LM(G)] T_LM,
+    with V given on the support keys (0 for an absent mode); shape (atoms, dim, dim)
+    (src/paw_compensation.cpp:552-629)."""
+    a, b, _ = _reciprocal(lattice)
+    keys = np.asarray(keys).reshape(-1, 3)
+    q = keys.astype(np.float64) @ b
+    form = compensation_form(lattice, keys, augmentation)
+    max_l = int(augmentation["max_l"])
+    imaginary = np.array([L % 2 for L in range(max_l + 1) for _ in range(2 * L + 1)], dtype=bool)
+    complex_form = np.where(imaginary[:, None], 1j * form, form)
+    where = {tuple(k): i for i, k in enumerate(keys.tolist())}
+    v = np.asarray(potential, dtype=np.complex128)
+    opposite = np.array([v[where[(-k[0], -k[1], -k[2])]] if (-k[0], -k[1], -k[2]) in where else 0.0
+                         for k in keys.tolist()], dtype=np.complex128)
+    positions = np.asarray(fractional, dtype=np.float64).reshape(-1, 3) @ a
+    t = np.asarray(transform, dtype=np.complex128)
+    dim = int(round(math.sqrt(t.shape[1])))
+    out = np.zeros((positions.shape[0], dim, dim), dtype=np.complex128)
+    for atom in range(positions.shape[0]):
+        phase = np.exp(-1j * (q @ positions[atom]))
+        responses = complex_form @ (opposite * phase)
+        out[atom] = (responses @ t).reshape(dim, dim)
+    return out
+

@@ -496,6 +496,29 @@ sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensation* charge, 
   });
 }
 
+sdft_b200_status sdft_b200_compensation_project(sdft_b200_compensation* charge, const double* potential,
+                                                double* out, int memory) {
+  return guarded([&] {
+    require(charge && potential && out, "invalid PAW compensation dimensions");
+    auto& c = *charge->impl;
+    auto& ctx = c.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    using C = sdft_b200::Cx<double>;
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      c.project(reinterpret_cast<const C*>(potential), reinterpret_cast<C*>(out));
+      return;
+    }
+    require(memory == SDFT_B200_MEMORY_HOST, "memory must be host or device");
+    const std::size_t out_count = c.atoms() * c.dimension() * c.dimension();
+    auto* din = static_cast<C*>(ctx.staging_in.reserve(sizeof(C) * c.count()));
+    auto* dout = static_cast<C*>(ctx.staging_out.reserve(sizeof(C) * out_count));
+    SDFT_CUDA(cudaMemcpyAsync(din, potential, sizeof(C) * c.count(), cudaMemcpyHostToDevice, ctx.stream));
+    c.project(din, dout);
+    SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * out_count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.synchronize();
+  });
+}
+
 sdft_b200_status sdft_b200_rayleigh_ritz(sdft_b200_context* context, size_t n, size_t requested, const double* h,
                                         const double* s, double* values, double* vectors, int memory) {
   return guarded([&] {

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <unordered_map>
 
 #include "operator.cuh"
 #include "paw_density.cuh"
@@ -197,6 +198,89 @@ __global__ void compensation_kernel(const double* __restrict__ q, const double* 
   }
 }
 
+// Adjoint partial sums: CTA b adds, for every atom in order, V(-G)
+// e^{-iG.tau_a} F_LM(G) over its grid-stride share of G (F imaginary for odd
+// L), reduced over the CTA in a fixed order into partials[(b * atoms + a) * LMS + lm].
+constexpr int kProjectThreads = 256;
+
+template <int LMS>
+__global__ void __launch_bounds__(kProjectThreads) project_partials_kernel(
+    const double* __restrict__ q, const double* __restrict__ form, std::size_t count,
+    const double* __restrict__ positions, int atoms, const int* __restrict__ opposite,
+    const Cx<double>* __restrict__ potential, Cx<double>* __restrict__ partials) {
+  __shared__ Cx<double> red[kProjectThreads / 32][LMS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int a = 0; a < atoms; ++a) {
+    const double tx = __ldg(positions + 3 * a), ty = __ldg(positions + 3 * a + 1), tz = __ldg(positions + 3 * a + 2);
+    Cx<double> acc[LMS];
+#pragma unroll
+    for (int lm = 0; lm < LMS; ++lm) acc[lm] = Cx<double>{0.0, 0.0};
+    for (std::size_t g = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; g < count;
+         g += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+      const int o = opposite[g];
+      if (o < 0) continue;
+      const double theta = dot3(q[3 * g], q[3 * g + 1], q[3 * g + 2], tx, ty, tz);
+      double sn, cs;
+      sincos(-theta, &sn, &cs);
+      const Cx<double> w = mul_rn(potential[o], Cx<double>{cs, sn});
+      int lm = 0;
+#pragma unroll
+      for (int L = 0; L * L < LMS; ++L) {
+#pragma unroll
+        for (int M = 0; M <= 2 * L; ++M, ++lm) {
+          const double fv = form[static_cast<std::size_t>(lm) * count + g];
+          if (L & 1) acc[lm] = {acc[lm].re - w.im * fv, acc[lm].im + w.re * fv};
+          else acc[lm] = {acc[lm].re + w.re * fv, acc[lm].im + w.im * fv};
+        }
+      }
+    }
+#pragma unroll
+    for (int lm = 0; lm < LMS; ++lm) {
+      double re = acc[lm].re, im = acc[lm].im;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, s);
+        im += __shfl_xor_sync(0xffffffffu, im, s);
+      }
+      if (lane == 0) red[warp][lm] = Cx<double>{re, im};
+    }
+    __syncthreads();
+    if (threadIdx.x < LMS) {
+      Cx<double> sum{0.0, 0.0};
+      for (int w = 0; w < kProjectThreads / 32; ++w) sum = {sum.re + red[w][threadIdx.x].re, sum.im + red[w][threadIdx.x].im};
+      partials[(static_cast<std::size_t>(blockIdx.x) * atoms + a) * LMS + threadIdx.x] = sum;
+    }
+    __syncthreads();
+  }
+}
+
+// responses[a][lm] = sum over CTAs in order; then out[a][e] = sum_lm responses * transform.
+__global__ void project_responses_kernel(const Cx<double>* __restrict__ partials, int blocks, int atoms, int lms,
+                                         Cx<double>* __restrict__ responses) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= atoms * lms) return;
+  Cx<double> sum{0.0, 0.0};
+  for (int b = 0; b < blocks; ++b) {
+    const Cx<double> v = partials[static_cast<std::size_t>(b) * atoms * lms + id];
+    sum = {sum.re + v.re, sum.im + v.im};
+  }
+  responses[id] = sum;
+}
+
+__global__ void project_contract_kernel(const Cx<double>* __restrict__ responses,
+                                        const Cx<double>* __restrict__ transform, int atoms, int lms, int entries,
+                                        Cx<double>* __restrict__ out) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= atoms * entries) return;
+  const int a = id / entries, e = id - a * entries;
+  Cx<double> sum{0.0, 0.0};
+  for (int lm = 0; lm < lms; ++lm) {
+    const Cx<double> t = mul_rn(responses[a * lms + lm], transform[static_cast<std::size_t>(lm) * entries + e]);
+    sum = {__dadd_rn(sum.re, t.re), __dadd_rn(sum.im, t.im)};
+  }
+  out[id] = sum;
+}
+
 __global__ void onsite_kernel(const Cx<double>* __restrict__ p, long long stride, int rows, int atoms, int bands,
                               const double* __restrict__ occupations, Cx<double>* __restrict__ out,
                               unsigned int* __restrict__ flags) {
@@ -322,6 +406,23 @@ CompensationCharge::CompensationCharge(Context& ctx, const CompensationInput& in
   SDFT_CUDA(cudaMalloc(&form_, sizeof(double) * lms_ * count_));
   SDFT_CUDA(cudaMalloc(&moments_, sizeof(Cx<double>) * lms_ * atoms_));
   SDFT_CUDA(cudaMalloc(&flags_, sizeof(unsigned int)));
+  {
+    // index of -G in the support (the adjoint samples V(-G)), -1 when absent
+    std::unordered_map<std::uint64_t, int> where;
+    where.reserve(count_ * 2);
+    auto key = [](int h, int k, int l) {
+      const auto b = [](int v) { return static_cast<std::uint64_t>(static_cast<std::int64_t>(v) + (1LL << 20)) & 0x1FFFFF; };
+      return (b(h) << 42) | (b(k) << 21) | b(l);
+    };
+    for (std::size_t g = 0; g < count_; ++g)
+      where[key(in.keys[3 * g], in.keys[3 * g + 1], in.keys[3 * g + 2])] = static_cast<int>(g);
+    std::vector<int> opposite(count_);
+    for (std::size_t g = 0; g < count_; ++g) {
+      const auto found = where.find(key(-in.keys[3 * g], -in.keys[3 * g + 1], -in.keys[3 * g + 2]));
+      opposite[g] = found == where.end() ? -1 : found->second;
+    }
+    opposite_ = upload(opposite.data(), opposite.size());
+  }
   int* d_shell = upload(shell.data(), shell.size());
   double* d_radii = upload(radii.data(), radii.size());
   double* d_r = upload(in.radial_grid, in.radial);
@@ -344,8 +445,40 @@ CompensationCharge::CompensationCharge(Context& ctx, const CompensationInput& in
 
 CompensationCharge::~CompensationCharge() {
   for (void* p : {static_cast<void*>(q_), static_cast<void*>(positions_), static_cast<void*>(form_),
-                  static_cast<void*>(transform_), static_cast<void*>(moments_), static_cast<void*>(flags_)})
+                  static_cast<void*>(transform_), static_cast<void*>(moments_), static_cast<void*>(flags_),
+                  static_cast<void*>(opposite_), static_cast<void*>(partials_), static_cast<void*>(responses_)})
     if (p) cudaFree(p);
+}
+
+void CompensationCharge::project(const Cx<double>* potential, Cx<double>* out) {
+  const int atoms = static_cast<int>(atoms_), entries = static_cast<int>(dim_ * dim_);
+  const int blocks = static_cast<int>(std::min<std::size_t>(std::max<std::size_t>(1, ceil_div(count_, kProjectThreads)),
+                                                            148ULL * 4));
+  if (!partials_) {
+    SDFT_CUDA(cudaMalloc(&partials_, sizeof(Cx<double>) * static_cast<std::size_t>(148 * 4) * atoms_ * lms_));
+    SDFT_CUDA(cudaMalloc(&responses_, sizeof(Cx<double>) * atoms_ * lms_));
+  }
+#define SDFT_PROJECT_CASE(N)                                                                                     \
+  case N:                                                                                                        \
+    project_partials_kernel<N><<<blocks, kProjectThreads, 0, ctx_.stream>>>(q_, form_, count_, positions_, atoms, \
+                                                                          opposite_, potential, partials_);     \
+    break;
+  switch (lms_) {
+    SDFT_PROJECT_CASE(1)
+    SDFT_PROJECT_CASE(4)
+    SDFT_PROJECT_CASE(9)
+    SDFT_PROJECT_CASE(16)
+    default:
+      throw InvalidArgument("compensation potential projection supports L_max <= 3");
+  }
+#undef SDFT_PROJECT_CASE
+  SDFT_LAUNCH("project_partials_kernel");
+  project_responses_kernel<<<static_cast<unsigned>(ceil_div(atoms * lms_, 128)), 128, 0, ctx_.stream>>>(
+      partials_, blocks, atoms, lms_, responses_);
+  SDFT_LAUNCH("project_responses_kernel");
+  project_contract_kernel<<<static_cast<unsigned>(ceil_div(atoms * entries, 128)), 128, 0, ctx_.stream>>>(
+      responses_, transform_, atoms, lms_, entries, out);
+  SDFT_LAUNCH("project_contract_kernel");
 }
 
 void CompensationCharge::density(const Cx<double>* onsite, Cx<double>* out) {

@@ -46,6 +46,12 @@ class CompensationCharge {
 
   // onsite: device, atoms x dimension^2 row-major Hermitian; out: device, count values.
   void density(const Cx<double>* onsite, Cx<double>* out);
+  // The adjoint (the reference's project_potential_batch,
+  // src/paw_compensation.cpp:552-629): potential: device, count values on
+  // the support (V(G) in key order; a mode absent from the potential is 0);
+  // out: device, atoms x dimension^2 row-major,
+  // out_a = sum_LM [sum_G V(-G) e^{-iG.tau_a} F_LM(G)] transform_LM.
+  void project(const Cx<double>* potential, Cx<double>* out);
   std::size_t count() const { return count_; }
   std::size_t atoms() const { return atoms_; }
   std::size_t dimension() const { return dim_; }
@@ -65,6 +71,9 @@ class CompensationCharge {
   Cx<double>* transform_ = nullptr;
   Cx<double>* moments_ = nullptr;  // atoms x lms
   unsigned int* flags_ = nullptr;
+  int* opposite_ = nullptr;         // index of -G in the support, or -1
+  Cx<double>* partials_ = nullptr;  // per-CTA sums of the adjoint
+  Cx<double>* responses_ = nullptr; // atoms x lms
 };
 
 }  // namespace sdft_b200

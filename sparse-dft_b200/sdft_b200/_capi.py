@@ -128,6 +128,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_compensation_create", [P, D, SZ, D, I32, SZ, ctypes.c_int, SZ, D, D, SZ, D, ctypes.POINTER(P)])
     fn("sdft_b200_compensation_destroy", [P])
     fn("sdft_b200_compensation_density", [P, P, P, ctypes.c_int])
+    fn("sdft_b200_compensation_project", [P, P, P, ctypes.c_int])
     fn("sdft_b200_local_hamiltonian", [P, I32, U64, SZ, D, D, P, SZ, P, ctypes.c_int, ctypes.c_uint64])
     fn("sdft_b200_paw_pair", [P, ctypes.c_uint64, SZ, SZ, SZ, P, P, P, P, P, P, ctypes.c_int, ctypes.c_uint64])
     fn("sdft_b200_complex_gemm", [P, ctypes.c_int, ctypes.c_int, SZ, SZ, SZ, P, SZ, P, SZ, P, SZ, ctypes.c_int,

@@ -133,6 +133,26 @@ class CompensationCharge:
                                                          ctypes.c_void_p(out.ctypes.data), C.HOST))
         return out
 
+    def project(self, potential):
+        """The adjoint (the reference's project_potential_batch): potential on the
+        support keys (numpy, host path; or a torch CUDA tensor, device path) ->
+        (atoms, dim, dim) projections."""
+        shape = (self.atoms, self.dimension, self.dimension)
+        if getattr(potential, "is_cuda", False):
+            import torch
+            v = potential.contiguous()
+            out = torch.empty(shape, dtype=torch.complex128, device=v.device)
+            C.check(self._lib.sdft_b200_compensation_project(self.handle, ctypes.c_void_p(v.data_ptr()),
+                                                             ctypes.c_void_p(out.data_ptr()), C.DEVICE))
+            return out
+        v = np.ascontiguousarray(potential, dtype=np.complex128).ravel()
+        if v.size != self.keys.shape[0]:
+            raise ValueError("potential must hold one value per support key")
+        out = np.zeros(shape, dtype=np.complex128)
+        C.check(self._lib.sdft_b200_compensation_project(self.handle, ctypes.c_void_p(v.ctypes.data),
+                                                         ctypes.c_void_p(out.ctypes.data), C.HOST))
+        return out
+
     def close(self):
         if getattr(self, "handle", None):
             self._lib.sdft_b200_compensation_destroy(self.handle)

@@ -144,6 +144,23 @@ def compensation_fixture(lib, inputs, name, factor, bands):
     print("compensation", name, "keys", keys.shape[0])
 
 
+def compensation_project_fixture(lib, inputs, name, factor):
+    """Reference project_potential_batch (src/paw_compensation.cpp:552) of a
+    seeded potential given on the support minus a few modes plus keys
+    outside it (those never enter)."""
+    aug = synthetic.augmentation()
+    keys = synthetic.density_support(inputs, factor)
+    rng = np.random.Generator(np.random.PCG64(71))
+    keep = rng.uniform(size=keys.shape[0]) > 0.02
+    extra = keys[:5] * 0 + np.array([[40, 0, 0], [0, 41, 0], [0, 0, 42], [43, 1, 0], [-44, 0, 2]])
+    pkeys = np.concatenate([keys[keep], extra]).astype(np.int32)
+    potential = rng.standard_normal(pkeys.shape[0]) + 1j * rng.standard_normal(pkeys.shape[0])
+    out = lib.compensation_project(inputs.lattice, inputs.positions, keys, aug, pkeys, potential)
+    np.savez_compressed(HERE / f"compensation_project_{name}.npz", factor=np.array(factor), potential_keys=pkeys,
+                        potential=potential, projection=out)
+    print("compensation projection", name, "keys", keys.shape[0], "potential keys", pkeys.shape[0])
+
+
 def snapshot_fixtures(lib):
     """Solver snapshots written by the reference (save_solver_snapshot) for
     the tiny pencil, cold and warm (the reference's eigenvectors with seeded
@@ -185,6 +202,7 @@ def main():
     parser.add_argument("--si64", action="store_true", help="also solve the Si64 pencil (long)")
     parser.add_argument("--kpoints", action="store_true", help="only the off-Gamma GaAs fixtures")
     parser.add_argument("--snapshots", action="store_true", help="only the solver snapshot fixtures")
+    parser.add_argument("--projection", action="store_true", help="only the compensation projection fixture")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
@@ -192,6 +210,9 @@ def main():
         return
     if args.snapshots:
         snapshot_fixtures(lib)
+        return
+    if args.projection:
+        compensation_project_fixture(lib, synthetic.si8(), "si8", 2.0)
         return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
@@ -201,6 +222,7 @@ def main():
     compensation_fixture(lib, synthetic.si8(), "si8", 2.0, 16)
     kpoint_fixtures(lib)
     snapshot_fixtures(lib)
+    compensation_project_fixture(lib, synthetic.si8(), "si8", 2.0)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

@@ -262,3 +262,42 @@ def test_onsite_and_compensation_reject_invalid_inputs(context):
     with pytest.raises(_capi.InvalidArgument, match="radial mesh"):
         bad_aug = dict(aug, radial_grid=aug["radial_grid"][::-1].copy())
         density.CompensationCharge(context, x.lattice, x.positions, keys, bad_aug, transform)
+
+
+def test_compensation_projection_matches_reference_fixture(context, golden):
+    """The adjoint against the reference's project_potential_batch (host and device paths)."""
+    import torch
+    from conftest import relative_error
+    from test_oracle_pins import _potential_on_support
+    from sdft_b200 import density, synthetic
+    g = golden("compensation_project_si8")
+    x = synthetic.si8()
+    aug = synthetic.augmentation()
+    keys = synthetic.density_support(x, float(g["factor"]))
+    charge = density.CompensationCharge(context, x.lattice, x.positions, keys, aug, synthetic.lm_transform(aug))
+    v = _potential_on_support(keys, g["potential_keys"], g["potential"])
+    out = charge.project(v)
+    assert relative_error(out, g["projection"]) < 1e-12
+    device = charge.project(torch.from_numpy(v).cuda())
+    assert np.array_equal(device.cpu().numpy(), out)
+    charge.close()
+
+
+def test_compensation_projection_is_the_adjoint_at_si64_f16(context):
+    """sum_a,e P_a[e] rho_a[e] = Omega sum_G V(-G) n(G) on the config-size support
+    (Si64, f = 16, ~1.5 M keys, 64 atoms), for a seeded potential and occupations."""
+    from sdft_b200 import density, synthetic
+    x = synthetic.si64()
+    aug, rows, amplitudes, keys = _compensation_inputs(x, 128, 16.0)
+    onsite = density.onsite_density(context, amplitudes, rows, np.full(128, 2.0))
+    charge = density.CompensationCharge(context, x.lattice, x.positions, keys, aug, synthetic.lm_transform(aug))
+    n = charge.density(onsite)
+    rng = np.random.Generator(np.random.PCG64(5))
+    v = rng.standard_normal(keys.shape[0]) + 1j * rng.standard_normal(keys.shape[0])
+    projection = charge.project(v)
+    position = {tuple(k): i for i, k in enumerate(keys.tolist())}
+    v_opposite = np.array([v[position[(-h, -k, -l)]] for h, k, l in keys.tolist()])
+    left = np.sum(projection * onsite)
+    right = x.volume * np.sum(v_opposite * n)
+    assert abs(left - right) < 1e-10 * max(abs(left), 1.0)
+    charge.close()

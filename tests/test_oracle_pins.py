@@ -153,3 +153,21 @@ def test_compensation_restatement_matches_live_reference_off_gamma_lattice(refer
     expected = reference.compensation_density(lattice, fractional, keys, aug, onsite)
     charge = sdft_oracle.compensation_density(lattice, fractional, keys, aug, synthetic.lm_transform(aug), onsite)
     assert relative_error(charge, expected) < 1e-13
+
+
+def _potential_on_support(keys, potential_keys, potential):
+    """V on the support keys in their order, 0 where the potential has no mode."""
+    where = {tuple(k): v for k, v in zip(np.asarray(potential_keys).tolist(), potential)}
+    return np.array([where.get(tuple(k), 0.0) for k in np.asarray(keys).tolist()], dtype=np.complex128)
+
+
+def test_compensation_projection_restatement_matches_golden(golden):
+    """The adjoint (project_potential_batch) against the reference's fixture:
+    a potential missing 2 % of the support's modes and carrying modes outside it."""
+    g = golden("compensation_project_si8")
+    x = synthetic.si8()
+    aug = synthetic.augmentation()
+    keys = synthetic.density_support(x, float(g["factor"]))
+    v = _potential_on_support(keys, g["potential_keys"], g["potential"])
+    out = sdft_oracle.compensation_project(x.lattice, x.positions, keys, aug, synthetic.lm_transform(aug), v)
+    assert relative_error(out, g["projection"]) < 1e-12
