@@ -78,6 +78,23 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_create(sdft_b200_context* cont
                                            const double* q, double hartree_to_ev, double regularization,
                                            sdft_b200_operator** out);
 SDFT_B200_API sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op);
+/* SCF refresh of a live operator: replaces V(G) (potential_count keys, as in
+ * sdft_b200_operator_create) and the per-atom D_a, Q_a (row-major, the
+ * operator's projector counts), recomputing V(r) and the H/S diagonals, while
+ * the basis maps, FFT plan, B and B's tensor-core packing stay resident. Same
+ * checks and arithmetic as sdft_b200_operator_create: the operator afterwards
+ * equals one created from the same basis and amplitudes with the new V(G), D
+ * and Q, bit for bit (the grid depends on the basis extent alone, since only
+ * keys inside it are retained). INVALID_ARGUMENT, with the operator
+ * unchanged, when a check fails, when SDFT_FFT_GRID changed since creation so
+ * that the grid would differ, or for an operator read from a snapshot (no G
+ * components). Synchronous.
+ * Replaces: the per-iteration PlaneWaveOperator rebuild that keeps B resident
+ * through an immutable projector identity, src/scf_core.cpp:2312-2313
+ * (src/plane_wave_operator.cpp:395-397, src/compute_backend.hpp:32-39). */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_update(sdft_b200_operator* op, size_t potential_count,
+                                                         const int32_t* potential_hkl, const double* potential,
+                                                         const double* d, const double* q);
 
 /* Grid shape, grid points, total projector rows, plane waves, and the number
  * of grid rows i0 that hold sphere points (the rows the fused FFT keeps).

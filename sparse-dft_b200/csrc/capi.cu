@@ -216,6 +216,15 @@ sdft_b200_status sdft_b200_operator_create(sdft_b200_context* context, size_t np
   });
 }
 
+sdft_b200_status sdft_b200_operator_update(sdft_b200_operator* op, size_t potential_count,
+                                           const int32_t* potential_hkl, const double* potential, const double* d,
+                                           const double* q) {
+  return guarded([&] {
+    require(op != nullptr, "null operator");
+    op->impl->update(potential_count, potential_hkl, potential, d, q);
+  });
+}
+
 sdft_b200_status sdft_b200_operator_destroy(sdft_b200_operator* op) {
   return guarded([&] { delete op; });
 }

@@ -75,8 +75,11 @@ __global__ void paw_transpose_kernel(const Cx<double>* __restrict__ raw, int row
 // (atoms, rows i, columns j: db_i = sum_j D(i,j) b_j, hd = sum_i conj(b_i) db_i)
 // each rounded on its own, so the diagonals equal the host arithmetic's. The
 // symmetrised blocks are column-major (D(i,j) at i + j*np) and uniform over
-// the block's threads; the amplitudes are read row-major (coalesced).
-__global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ raw, int npw, int atoms,
+// the block's threads. The amplitudes are strided: the row-major input at
+// construction (coalesced), or the resident column-major B when D and Q are
+// replaced (each thread's column then stays in L1 across the block products).
+__global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ amplitudes, std::size_t row_stride,
+                                    std::size_t column_stride, int npw, int atoms,
                                     const int* __restrict__ offsets, const long long* __restrict__ storage,
                                     const Cx<double>* __restrict__ d, const Cx<double>* __restrict__ q,
                                     double* __restrict__ h_diag, double* __restrict__ s_diag) {
@@ -87,12 +90,12 @@ __global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ raw, int npw,
     const int base = offsets[a], np = offsets[a + 1] - offsets[a];
     const Cx<double>* da = d + storage[a];
     const Cx<double>* qa = q + storage[a];
-    const Cx<double>* col = raw + static_cast<std::size_t>(base) * npw + g;
+    const Cx<double>* col = amplitudes + static_cast<std::size_t>(base) * row_stride + static_cast<std::size_t>(g) * column_stride;
     double hr = 0, hi = 0, sr = 0, si = 0;
     for (int i = 0; i < np; ++i) {
       double dr = 0, di = 0, qr = 0, qi = 0;
       for (int j = 0; j < np; ++j) {
-        const Cx<double> bj = col[static_cast<std::size_t>(j) * npw];
+        const Cx<double> bj = col[static_cast<std::size_t>(j) * row_stride];
         const Cx<double> dij = da[i + static_cast<std::size_t>(j) * np], qij = qa[i + static_cast<std::size_t>(j) * np];
         dr = __dadd_rn(dr, __dsub_rn(__dmul_rn(dij.re, bj.re), __dmul_rn(dij.im, bj.im)));
         di = __dadd_rn(di, __dadd_rn(__dmul_rn(dij.re, bj.im), __dmul_rn(dij.im, bj.re)));
@@ -102,7 +105,7 @@ __global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ raw, int npw,
       // conj(b_i) * db: real part b.re*db.re - (-b.im)*db.im, imaginary part
       // b.re*db.im + (-b.im)*db.re (only the real part reaches the diagonal,
       // the imaginary part is summed as on the host for the same operation count).
-      const Cx<double> bi = col[static_cast<std::size_t>(i) * npw];
+      const Cx<double> bi = col[static_cast<std::size_t>(i) * row_stride];
       hr = __dadd_rn(hr, __dsub_rn(__dmul_rn(bi.re, dr), __dmul_rn(-bi.im, di)));
       hi = __dadd_rn(hi, __dadd_rn(__dmul_rn(bi.re, di), __dmul_rn(-bi.im, dr)));
       sr = __dadd_rn(sr, __dsub_rn(__dmul_rn(bi.re, qr), __dmul_rn(-bi.im, qi)));
@@ -117,6 +120,16 @@ __global__ void paw_diagonal_kernel(const Cx<double>* __restrict__ raw, int npw,
   s_diag[g] = sdiag;
 }
 
+// Adds the PAW terms to the diagonals; amplitude (row r, plane wave g) sits at
+// amplitudes[r * row_stride + g * column_stride].
+void paw_diagonals(const Cx<double>* amplitudes, std::size_t row_stride, std::size_t column_stride, int npw, int atoms,
+                   const int* offsets, const long long* storage, const Cx<double>* d, const Cx<double>* q,
+                   double* h_diag, double* s_diag, cudaStream_t stream) {
+  paw_diagonal_kernel<<<(npw + 127) / 128, 128, 0, stream>>>(amplitudes, row_stride, column_stride, npw, atoms, offsets,
+                                                             storage, d, q, h_diag, s_diag);
+  SDFT_LAUNCH("paw_diagonal_kernel");
+}
+
 void paw_prepare(const Cx<double>* raw, int rows, int npw, int atoms, const int* offsets, const long long* storage,
                  const Cx<double>* d, const Cx<double>* q, Cx<double>* b, double* h_diag, double* s_diag,
                  unsigned int* bad, cudaStream_t stream) {
@@ -124,8 +137,7 @@ void paw_prepare(const Cx<double>* raw, int rows, int npw, int atoms, const int*
   if (tiles.y > 65535u) throw Overflow("PAW projector tiles exceed the grid limit");
   paw_transpose_kernel<<<tiles, dim3(32, 8), 0, stream>>>(raw, rows, npw, b, bad);
   SDFT_LAUNCH("paw_transpose_kernel");
-  paw_diagonal_kernel<<<(npw + 127) / 128, 128, 0, stream>>>(raw, npw, atoms, offsets, storage, d, q, h_diag, s_diag);
-  SDFT_LAUNCH("paw_diagonal_kernel");
+  paw_diagonals(raw, npw, 1, npw, atoms, offsets, storage, d, q, h_diag, s_diag, stream);
 }
 }  // namespace
 
@@ -214,42 +226,44 @@ GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, co
   return out;
 }
 
-DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx) {
-  SDFT_CUDA(cudaSetDevice(ctx.device));
-  if (!in.npw || !std::isfinite(in.hartree_to_ev) || in.hartree_to_ev <= 0 || !std::isfinite(in.regularization) ||
-      in.regularization < 0)
-    throw InvalidArgument("invalid plane-wave operator dimensions or units");
-  if (in.npw > static_cast<std::size_t>(std::numeric_limits<int>::max())) throw Overflow("plane-wave count exceeds int32");
-  npw_ = static_cast<int>(in.npw);
-  regularization_ = in.regularization;
-  // Bounding box of the basis and the retained potential radius (:400-415).
-  int low[3], high[3], radius[3] = {0, 0, 0};
-  for (int a = 0; a < 3; ++a) low[a] = high[a] = in.hkl[a];
-  for (std::size_t g = 0; g < in.npw; ++g)
-    for (int a = 0; a < 3; ++a) {
-      low[a] = std::min(low[a], in.hkl[3 * g + a]);
-      high[a] = std::max(high[a], in.hkl[3 * g + a]);
-    }
+namespace {
+
+// The retained local potential of an operator whose basis spans span[a] =
+// high_a - low_a along each axis: its grid and V(r).
+struct LocalPotential {
+  int shape[3];
+  double v0;                  // V(G = 0), added to the H diagonal
+  std::vector<double> real;   // V(r), row-major grid
+};
+
+// Validation, grid rule and V(r) of the reference constructor
+// (src/plane_wave_operator.cpp:400-475): finite and Hermitian V(G), the
+// retained keys (|k_a| <= span_a) set the potential radius, the grid is the
+// alias-free minimum rounded to a smooth length, and V(r) is one backward FFT
+// of the retained keys on the device in FP64.
+LocalPotential local_potential(Context& ctx, const int span[3], std::size_t potential_count, const int* potential_hkl,
+                               const double* potential) {
+  int radius[3] = {0, 0, 0};
   double max_potential = 0;
   std::unordered_map<std::uint64_t, std::size_t> keys;
-  keys.reserve(in.potential_count * 2 + 1);
-  for (std::size_t i = 0; i < in.potential_count; ++i) {
-    const C v(in.potential[2 * i], in.potential[2 * i + 1]);
+  keys.reserve(potential_count * 2 + 1);
+  for (std::size_t i = 0; i < potential_count; ++i) {
+    const C v(potential[2 * i], potential[2 * i + 1]);
     if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) throw InvalidArgument("nonfinite local potential");
-    const int* k = in.potential_hkl + 3 * i;
+    const int* k = potential_hkl + 3 * i;
     bool retained = true;
-    for (int a = 0; a < 3; ++a) retained &= std::abs(k[a]) <= high[a] - low[a];
+    for (int a = 0; a < 3; ++a) retained &= std::abs(k[a]) <= span[a];
     if (retained)
       for (int a = 0; a < 3; ++a) radius[a] = std::max(radius[a], std::abs(k[a]));
     max_potential = std::max(max_potential, std::abs(v));
     keys[pack_key(k[0], k[1], k[2])] = i;
   }
   // Hermitian V(G) (:438-444).
-  for (std::size_t i = 0; i < in.potential_count; ++i) {
-    const int* k = in.potential_hkl + 3 * i;
-    const C v(in.potential[2 * i], in.potential[2 * i + 1]);
+  for (std::size_t i = 0; i < potential_count; ++i) {
+    const int* k = potential_hkl + 3 * i;
+    const C v(potential[2 * i], potential[2 * i + 1]);
     const auto other = keys.find(pack_key(-k[0], -k[1], -k[2]));
-    const C partner = other == keys.end() ? C{} : C(in.potential[2 * other->second], in.potential[2 * other->second + 1]);
+    const C partner = other == keys.end() ? C{} : C(potential[2 * other->second], potential[2 * other->second + 1]);
     if (std::abs(v - std::conj(partner)) > 1e-10 * std::max(1., max_potential))
       throw InvalidArgument("local Fourier potential is not Hermitian");
   }
@@ -259,15 +273,16 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
   const char* mode = std::getenv("SDFT_FFT_GRID");
   if (mode && std::string(mode) != "minimal" && std::string(mode) != "fast")
     throw InvalidArgument("SDFT_FFT_GRID must be minimal or fast");
-  int shape[3];
+  LocalPotential out;
   std::size_t count = 1;
   for (int a = 0; a < 3; ++a) {
-    const int minimum = std::max(3, 2 * std::max(radius[a], high[a] - low[a]) + 1);
-    shape[a] = (mode && std::string(mode) == "minimal" && fft_length_supported(minimum)) ? minimum
-                                                                                          : fast_fft_length(minimum);
-    if (count > std::numeric_limits<std::size_t>::max() / shape[a]) throw Overflow("plane-wave FFT grid overflow");
-    count *= shape[a];
+    const int minimum = std::max(3, 2 * std::max(radius[a], span[a]) + 1);
+    out.shape[a] = (mode && std::string(mode) == "minimal" && fft_length_supported(minimum)) ? minimum
+                                                                                              : fast_fft_length(minimum);
+    if (count > std::numeric_limits<std::size_t>::max() / out.shape[a]) throw Overflow("plane-wave FFT grid overflow");
+    count *= out.shape[a];
   }
+  const int* shape = out.shape;
   auto wrap = [](int x, int size) {
     int r = x % size;
     return r < 0 ? r + size : r;
@@ -276,37 +291,113 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     return (static_cast<std::uint64_t>(wrap(h, shape[0])) * shape[1] + wrap(k, shape[1])) * shape[2] + wrap(l, shape[2]);
   };
   // V(r) by one backward FFT of the retained keys, on the device in FP64 (:464-475).
-  {
-    std::vector<Cx<double>> grid(count, Cx<double>{0, 0});
-    for (std::size_t i = 0; i < in.potential_count; ++i) {
-      const int* k = in.potential_hkl + 3 * i;
-      bool retained = true;
-      for (int a = 0; a < 3; ++a) retained &= std::abs(k[a]) <= high[a] - low[a];
-      if (!retained) continue;
-      grid[index(k[0], k[1], k[2])] = Cx<double>{in.potential[2 * i], in.potential[2 * i + 1]};
-    }
-    Cx<double>* dgrid = nullptr;
-    SDFT_CUDA(cudaMalloc(&dgrid, sizeof(Cx<double>) * count));
-    try {
-      SDFT_CUDA(cudaMemcpyAsync(dgrid, grid.data(), sizeof(Cx<double>) * count, cudaMemcpyHostToDevice, ctx.stream));
-      fft3d<double>(dgrid, shape, 1, true, ctx.stream);
-      SDFT_CUDA(cudaMemcpyAsync(grid.data(), dgrid, sizeof(Cx<double>) * count, cudaMemcpyDeviceToHost, ctx.stream));
-      SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
-    } catch (...) {
-      cudaFree(dgrid);
-      throw;
-    }
-    cudaFree(dgrid);
-    h_local_real_.resize(count);
-    for (std::size_t i = 0; i < count; ++i) {
-      if (std::abs(grid[i].im) > 1e-9 * std::max(1., std::abs(grid[i].re)))
-        throw std::runtime_error("complex real-space local potential");
-      h_local_real_[i] = grid[i].re;
-    }
+  std::vector<Cx<double>> grid(count, Cx<double>{0, 0});
+  for (std::size_t i = 0; i < potential_count; ++i) {
+    const int* k = potential_hkl + 3 * i;
+    bool retained = true;
+    for (int a = 0; a < 3; ++a) retained &= std::abs(k[a]) <= span[a];
+    if (!retained) continue;
+    grid[index(k[0], k[1], k[2])] = Cx<double>{potential[2 * i], potential[2 * i + 1]};
   }
-  // Basis maps and diagonals (:476-483).
+  Cx<double>* dgrid = nullptr;
+  SDFT_CUDA(cudaMalloc(&dgrid, sizeof(Cx<double>) * count));
+  try {
+    SDFT_CUDA(cudaMemcpyAsync(dgrid, grid.data(), sizeof(Cx<double>) * count, cudaMemcpyHostToDevice, ctx.stream));
+    fft3d<double>(dgrid, out.shape, 1, true, ctx.stream);
+    SDFT_CUDA(cudaMemcpyAsync(grid.data(), dgrid, sizeof(Cx<double>) * count, cudaMemcpyDeviceToHost, ctx.stream));
+    SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
+  } catch (...) {
+    cudaFree(dgrid);
+    throw;
+  }
+  cudaFree(dgrid);
+  out.real.resize(count);
+  for (std::size_t i = 0; i < count; ++i) {
+    if (std::abs(grid[i].im) > 1e-9 * std::max(1., std::abs(grid[i].re)))
+      throw std::runtime_error("complex real-space local potential");
+    out.real[i] = grid[i].re;
+  }
   const auto zero = keys.find(pack_key(0, 0, 0));
-  const double v0 = zero == keys.end() ? 0.0 : in.potential[2 * zero->second];
+  out.v0 = zero == keys.end() ? 0.0 : potential[2 * zero->second];
+  return out;
+}
+
+// Per-atom D and Q (row-major np_a x np_a input) checked for finiteness and
+// Hermiticity and stored symmetrised, column-major and concatenated
+// (src/plane_wave_operator.cpp:484-509).
+void symmetrised_blocks(const std::vector<std::uint64_t>& channels, const double* in_d, const double* in_q,
+                        std::vector<Cx<double>>& d_blocks, std::vector<Cx<double>>& q_blocks) {
+  std::size_t block_total = 0;
+  for (auto np : channels) block_total += np * np;
+  d_blocks.assign(block_total, Cx<double>{0, 0});
+  q_blocks.assign(block_total, Cx<double>{0, 0});
+  std::size_t blk_offset = 0;
+  for (std::size_t a = 0; a < channels.size(); ++a) {
+    const std::size_t np = channels[a];
+    std::vector<C> d(np * np), q(np * np);
+    for (std::size_t i = 0; i < np * np; ++i) {
+      d[i] = C(in_d[2 * (blk_offset + i)], in_d[2 * (blk_offset + i) + 1]);
+      q[i] = C(in_q[2 * (blk_offset + i)], in_q[2 * (blk_offset + i) + 1]);
+    }
+    for (const auto* m : {&d, &q})
+      for (const auto& v : *m)
+        if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) throw InvalidArgument("nonfinite PAW projector/D/Q data");
+    // row-major d[i*np + j] = D(i,j); Hermitian check and symmetrisation.
+    std::vector<C> dd(np * np), qd(np * np);
+    for (std::size_t i = 0; i < np; ++i)
+      for (std::size_t j = 0; j < np; ++j) {
+        dd[i * np + j] = d[i * np + j] - std::conj(d[j * np + i]);
+        qd[i * np + j] = q[i * np + j] - std::conj(q[j * np + i]);
+      }
+    const double de = frobenius(dd), qe = frobenius(qd);
+    if (de > 1e-10 * std::max(1., frobenius(d)) || qe > 1e-10 * std::max(1., frobenius(q))) {
+      std::ostringstream reason;
+      reason << "invalid Hermitian PAW blocks: atom=" << a << " D_norm=" << frobenius(d) << " D_asymmetry=" << de
+             << " Q_norm=" << frobenius(q) << " Q_asymmetry=" << qe;
+      throw InvalidArgument(reason.str());
+    }
+    // symmetrised, column-major device storage M(i,j) at i + j*np
+    for (std::size_t i = 0; i < np; ++i)
+      for (std::size_t j = 0; j < np; ++j) {
+        const C ds = .5 * (d[i * np + j] + std::conj(d[j * np + i]));
+        const C qs = .5 * (q[i * np + j] + std::conj(q[j * np + i]));
+        d_blocks[blk_offset + i + j * np] = Cx<double>{ds.real(), ds.imag()};
+        q_blocks[blk_offset + i + j * np] = Cx<double>{qs.real(), qs.imag()};
+      }
+    blk_offset += np * np;
+  }
+}
+
+}  // namespace
+
+DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx) {
+  SDFT_CUDA(cudaSetDevice(ctx.device));
+  if (!in.npw || !std::isfinite(in.hartree_to_ev) || in.hartree_to_ev <= 0 || !std::isfinite(in.regularization) ||
+      in.regularization < 0)
+    throw InvalidArgument("invalid plane-wave operator dimensions or units");
+  if (in.npw > static_cast<std::size_t>(std::numeric_limits<int>::max())) throw Overflow("plane-wave count exceeds int32");
+  npw_ = static_cast<int>(in.npw);
+  regularization_ = in.regularization;
+  // Bounding box of the basis (:400-415).
+  int low[3], high[3];
+  for (int a = 0; a < 3; ++a) low[a] = high[a] = in.hkl[a];
+  for (std::size_t g = 0; g < in.npw; ++g)
+    for (int a = 0; a < 3; ++a) {
+      low[a] = std::min(low[a], in.hkl[3 * g + a]);
+      high[a] = std::max(high[a], in.hkl[3 * g + a]);
+    }
+  for (int a = 0; a < 3; ++a) span_[a] = high[a] - low[a];
+  LocalPotential local = local_potential(ctx, span_, in.potential_count, in.potential_hkl, in.potential);
+  const int* shape = local.shape;
+  h_local_real_ = std::move(local.real);
+  auto wrap = [](int x, int size) {
+    int r = x % size;
+    return r < 0 ? r + size : r;
+  };
+  auto index = [&](int h, int k, int l) {
+    return (static_cast<std::uint64_t>(wrap(h, shape[0])) * shape[1] + wrap(k, shape[1])) * shape[2] + wrap(l, shape[2]);
+  };
+  // Basis maps and diagonals (:476-483).
   h_indices_.resize(in.npw);
   h_kinetic_.resize(in.npw);
   h_diag_.resize(in.npw);
@@ -315,7 +406,7 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     if (!std::isfinite(in.kinetic_ev[g])) throw InvalidArgument("nonfinite kinetic energy");
     h_indices_[g] = index(in.hkl[3 * g], in.hkl[3 * g + 1], in.hkl[3 * g + 2]);
     h_kinetic_[g] = in.kinetic_ev[g] / in.hartree_to_ev;
-    h_diag_[g] = in.kinetic_ev[g] / in.hartree_to_ev + v0;
+    h_diag_[g] = in.kinetic_ev[g] / in.hartree_to_ev + local.v0;
   }
   {
     auto sorted = h_indices_;
@@ -341,44 +432,9 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
   offsets[atoms_] = static_cast<int>(total);
   if (total > 65536) throw InvalidArgument("too many PAW projectors");
   np_ = static_cast<int>(total);
-  std::vector<Cx<double>> d_blocks(block_total), q_blocks(block_total);
-  {
-    std::size_t blk_offset = 0;
-    for (int a = 0; a < atoms_; ++a) {
-      const std::size_t np = in.projectors[a];
-      std::vector<C> d(np * np), q(np * np);
-      for (std::size_t i = 0; i < np * np; ++i) {
-        d[i] = C(in.d[2 * (blk_offset + i)], in.d[2 * (blk_offset + i) + 1]);
-        q[i] = C(in.q[2 * (blk_offset + i)], in.q[2 * (blk_offset + i) + 1]);
-      }
-      for (const auto* m : {&d, &q})
-        for (const auto& v : *m)
-          if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) throw InvalidArgument("nonfinite PAW projector/D/Q data");
-      // row-major d[i*np + j] = D(i,j); Hermitian check and symmetrisation.
-      std::vector<C> dd(np * np), qd(np * np);
-      for (std::size_t i = 0; i < np; ++i)
-        for (std::size_t j = 0; j < np; ++j) {
-          dd[i * np + j] = d[i * np + j] - std::conj(d[j * np + i]);
-          qd[i * np + j] = q[i * np + j] - std::conj(q[j * np + i]);
-        }
-      const double de = frobenius(dd), qe = frobenius(qd);
-      if (de > 1e-10 * std::max(1., frobenius(d)) || qe > 1e-10 * std::max(1., frobenius(q))) {
-        std::ostringstream reason;
-        reason << "invalid Hermitian PAW blocks: atom=" << a << " D_norm=" << frobenius(d) << " D_asymmetry=" << de
-               << " Q_norm=" << frobenius(q) << " Q_asymmetry=" << qe;
-        throw InvalidArgument(reason.str());
-      }
-      // symmetrised, column-major device storage M(i,j) at i + j*np
-      for (std::size_t i = 0; i < np; ++i)
-        for (std::size_t j = 0; j < np; ++j) {
-          const C ds = .5 * (d[i * np + j] + std::conj(d[j * np + i]));
-          const C qs = .5 * (q[i * np + j] + std::conj(q[j * np + i]));
-          d_blocks[blk_offset + i + j * np] = Cx<double>{ds.real(), ds.imag()};
-          q_blocks[blk_offset + i + j * np] = Cx<double>{qs.real(), qs.imag()};
-        }
-      blk_offset += np * np;
-    }
-  }
+  h_channels_.assign(in.projectors, in.projectors + in.atoms);
+  std::vector<Cx<double>> d_blocks, q_blocks;
+  symmetrised_blocks(h_channels_, in.d, in.q, d_blocks, q_blocks);
   // Device upload.
   upload_common(shape, d_blocks, q_blocks, offsets, storage);
   if (np_) {
@@ -479,6 +535,52 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorSnapshot& snap) : ctx
     pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
   }
   SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// SCF refresh: new V(G) and per-atom D/Q on the resident basis maps, plan,
+// B and its tensor-core packing. The reference rebuilds the operator each SCF
+// iteration and keeps only B's device copy through an immutable projector
+// identity (src/scf_core.cpp:2312-2313, src/plane_wave_operator.cpp:395-397);
+// here everything that depends on the basis and B stays, and the potential,
+// blocks and diagonals are recomputed with the constructor's own checks and
+// arithmetic. All validation happens before any state changes.
+void DeviceOperator::update(std::size_t potential_count, const int* potential_hkl, const double* potential,
+                            const double* d, const double* q) {
+  if (span_[0] < 0)
+    throw InvalidArgument("operator built from a solver snapshot has no G components; create a new operator");
+  if (potential_count && (!potential_hkl || !potential)) throw InvalidArgument("null potential arrays");
+  if (atoms_ && (!d || !q)) throw InvalidArgument("null PAW arrays");
+  SDFT_CUDA(cudaSetDevice(ctx_.device));
+  SDFT_CUDA(cudaStreamSynchronize(ctx_.stream));
+  LocalPotential local = local_potential(ctx_, span_, potential_count, potential_hkl, potential);
+  for (int a = 0; a < 3; ++a)
+    if (local.shape[a] != plan_.n[a])
+      throw InvalidArgument("SDFT_FFT_GRID changed the FFT grid since the operator was created; create a new operator");
+  std::vector<Cx<double>> d_blocks, q_blocks;
+  symmetrised_blocks(h_channels_, d, q, d_blocks, q_blocks);
+  std::vector<double> h_diag(npw_), s_diag(npw_, 1 + regularization_);
+  for (int g = 0; g < npw_; ++g) h_diag[g] = h_kinetic_[g] + local.v0;
+  std::vector<float> v32(local.real.begin(), local.real.end());
+  SDFT_CUDA(cudaMemcpyAsync(v64_, local.real.data(), sizeof(double) * local.real.size(), cudaMemcpyHostToDevice,
+                            ctx_.stream));
+  SDFT_CUDA(cudaMemcpyAsync(v32_, v32.data(), sizeof(float) * v32.size(), cudaMemcpyHostToDevice, ctx_.stream));
+  if (np_) {
+    SDFT_CUDA(cudaMemcpyAsync(d_, d_blocks.data(), sizeof(Cx<double>) * d_blocks.size(), cudaMemcpyHostToDevice,
+                              ctx_.stream));
+    SDFT_CUDA(cudaMemcpyAsync(q_, q_blocks.data(), sizeof(Cx<double>) * q_blocks.size(), cudaMemcpyHostToDevice,
+                              ctx_.stream));
+    auto* diag = static_cast<double*>(ctx_.staging_aux.reserve(sizeof(double) * 2 * npw_));
+    SDFT_CUDA(cudaMemcpyAsync(diag, h_diag.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice, ctx_.stream));
+    SDFT_CUDA(cudaMemcpyAsync(diag + npw_, s_diag.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice, ctx_.stream));
+    paw_diagonals(b_, 1, static_cast<std::size_t>(np_), npw_, atoms_, block_offsets_, block_storage_, d_, q_, diag,
+                  diag + npw_, ctx_.stream);
+    SDFT_CUDA(cudaMemcpyAsync(h_diag.data(), diag, sizeof(double) * npw_, cudaMemcpyDeviceToHost, ctx_.stream));
+    SDFT_CUDA(cudaMemcpyAsync(s_diag.data(), diag + npw_, sizeof(double) * npw_, cudaMemcpyDeviceToHost, ctx_.stream));
+  }
+  SDFT_CUDA(cudaStreamSynchronize(ctx_.stream));
+  h_local_real_ = std::move(local.real);
+  h_diag_ = std::move(h_diag);
+  s_diag_ = std::move(s_diag);
 }
 
 DeviceOperator::~DeviceOperator() {

@@ -179,6 +179,15 @@ class DeviceOperator {
   }
   // P = B x (np x columns, ld np)
   void project(const Cx<double>* x, int columns, Cx<double>* p, Precision precision);
+  // SCF refresh: replaces V(G) and the per-atom D/Q (the constructor's input
+  // layouts) and recomputes V(r) and the diagonals; the basis maps, FFT plan,
+  // B and its tensor-core packing stay resident. The result equals a new
+  // operator built from the same basis, B and the new V(G), D, Q (the grid
+  // depends on the basis extent alone: only keys inside it are retained).
+  // Rejected (operator unchanged) when a check fails, when SDFT_FFT_GRID
+  // changed so that the grid would differ, or for a snapshot operator.
+  void update(std::size_t potential_count, const int* potential_hkl, const double* potential, const double* d,
+              const double* q);
 
   std::size_t device_bytes() const;
 
@@ -199,6 +208,8 @@ class DeviceOperator {
   std::vector<double> h_kinetic_, h_diag_, h_local_real_;
   std::vector<double> s_diag_;
   std::vector<std::uint64_t> h_indices_;
+  std::vector<std::uint64_t> h_channels_;  // projectors per atom
+  int span_[3] = {-1, -1, -1};             // basis extent high - low per axis; -1 for a snapshot operator
   double* kinetic_ = nullptr;
   double* v64_ = nullptr;
   float* v32_ = nullptr;

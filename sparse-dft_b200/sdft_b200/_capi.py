@@ -118,6 +118,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_operator_create", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,
                                      ctypes.POINTER(P)])
     fn("sdft_b200_operator_destroy", [P])
+    fn("sdft_b200_operator_update", [P, SZ, I32, D, D, D])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])

@@ -113,6 +113,7 @@ class PlaneWaveOperator:
         amp = np.ascontiguousarray(x.amplitudes, dtype=np.complex128)
         d = np.ascontiguousarray(x.d, dtype=np.complex128)
         q = np.ascontiguousarray(x.q, dtype=np.complex128)
+        self._block_entries = int(np.sum(proj.astype(np.int64) ** 2))
         handle = ctypes.c_void_p()
         C.check(self._lib.sdft_b200_operator_create(
             context.handle, hkl.shape[0], hkl.ctypes.data_as(C.I32), _dptr(kin), vh.shape[0],
@@ -121,6 +122,26 @@ class PlaneWaveOperator:
             ctypes.byref(handle)))
         self.handle = handle
         self._read_info()
+
+    def update(self, v_hkl, v_values, d, q) -> None:
+        """SCF refresh: new V(G) and per-atom D/Q (the constructor's layouts) on
+        the resident basis, FFT plan and B; afterwards the operator equals one
+        built from the same basis and amplitudes with these values. Raises
+        (operator unchanged) when a check fails."""
+        vh = np.ascontiguousarray(v_hkl, dtype=np.int32).reshape(-1, 3)
+        vv = np.ascontiguousarray(v_values, dtype=np.complex128).reshape(-1)
+        if vv.shape[0] != vh.shape[0]:
+            raise ValueError("potential keys and values disagree")
+        dd = np.ascontiguousarray(d, dtype=np.complex128).reshape(-1)
+        qq = np.ascontiguousarray(q, dtype=np.complex128).reshape(-1)
+        entries = getattr(self, "_block_entries", None)
+        if entries is None:
+            raise ValueError("an operator read from a snapshot cannot be updated")
+        if dd.shape[0] != entries or qq.shape[0] != entries:
+            raise ValueError(f"D and Q must hold {entries} entries (sum of projectors per atom squared)")
+        C.check(self._lib.sdft_b200_operator_update(self.handle, vh.shape[0], vh.ctypes.data_as(C.I32),
+                                                    vv.ctypes.data_as(C.D), dd.ctypes.data_as(C.D),
+                                                    qq.ctypes.data_as(C.D)))
 
     def _read_info(self) -> None:
         handle = self.handle

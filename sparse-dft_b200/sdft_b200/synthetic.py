@@ -315,6 +315,43 @@ def gaas_small(kpoint=(1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0), seed: int = 2027, ecut_
                           **kw)
 
 
+def scf_step(inputs: OperatorInputs, step: int, seed: int = 91, keep: float = 1.0) -> OperatorInputs:
+    """Inputs of one SCF-like iteration on the same basis and projectors: V(G)
+    scaled by (1 + 0.05 step) plus Hermitian noise of 0.01 Ha on its keys, D
+    plus Hermitian noise of 0.02 Ha per atom; B and Q unchanged (the
+    reference's SCF rebuilds its operator each iteration with new V and D and
+    the same projectors). keep < 1 retains that fraction of the nonzero key
+    pairs (k, -k), so the key set changes as well; G = 0 is always kept."""
+    rng = np.random.Generator(np.random.PCG64([seed, step]))
+    keys = [tuple(int(v) for v in k) for k in inputs.v_hkl]
+    where = {k: i for i, k in enumerate(keys)}
+    noise = 0.01 * (rng.standard_normal(len(keys)) + 1j * rng.standard_normal(len(keys)))
+    values = inputs.v_values * (1.0 + 0.05 * step)
+    selected = []
+    for i, k in enumerate(keys):
+        j = where.get((-k[0], -k[1], -k[2]))
+        if j is None:  # an unpaired key must stay as it is (its partner is an implicit zero)
+            selected.append(i)
+            continue
+        if j < i:
+            continue
+        if i == j:
+            values[i] = values[i] + noise[i].real
+            selected.append(i)
+        elif keep >= 1.0 or rng.uniform() < keep:
+            w = 0.5 * (noise[i] + np.conj(noise[j]))
+            values[i] = values[i] + w
+            values[j] = values[j] + np.conj(w)
+            selected += [i, j]
+    order = np.sort(np.asarray(selected, dtype=np.int64))
+    d = inputs.d.copy()
+    for a in range(d.shape[0]):
+        e = rng.standard_normal(d.shape[1:]) + 1j * rng.standard_normal(d.shape[1:])
+        d[a] = d[a] + 0.01 * (e + e.conj().T)
+    return dataclasses.replace(inputs, name=f"{inputs.name}_scf{step}", v_hkl=np.ascontiguousarray(inputs.v_hkl[order]),
+                               v_values=np.ascontiguousarray(values[order]), d=d)
+
+
 SI_VOLUME_PER_ATOM = 10.26 ** 3 / 8.0  # bohr^3, diamond Si
 
 

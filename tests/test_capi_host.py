@@ -94,6 +94,28 @@ def test_server_without_gpu_reports_cuda_error():
     assert lib.sdft_b200_server_create(0, 1 << 30, 0, ctypes.byref(handle)) == C.INVALID_ARGUMENT
 
 
+def test_operator_update_null_operator_is_invalid_argument():
+    """The SCF refresh checks its handle before any device work."""
+    lib = C.library()
+    assert lib.sdft_b200_operator_update(None, 0, None, None, None, None) == C.INVALID_ARGUMENT
+    assert "null operator" in C.last_error()
+
+
+def test_scf_step_keeps_potential_and_blocks_hermitian():
+    """The seeded SCF sequence (test input of the operator refresh) keeps V(G)
+    Hermitian on its keys, G = 0 present, and every D block Hermitian."""
+    from sdft_b200 import synthetic
+    x = synthetic.tiny()
+    for step, keep in ((1, 1.0), (2, 0.5)):
+        y = synthetic.scf_step(x, step, keep=keep)
+        values = {tuple(k): v for k, v in zip(y.v_hkl.tolist(), y.v_values)}
+        assert (0, 0, 0) in values
+        assert max(abs(v - np.conj(values.get((-k[0], -k[1], -k[2]), 0.0))) for k, v in values.items()) == 0.0
+        assert np.array_equal(y.d, np.conj(np.transpose(y.d, (0, 2, 1))))
+        assert np.array_equal(y.amplitudes, x.amplitudes) and np.array_equal(y.q, x.q)
+        assert (y.v_hkl.shape[0] == x.v_hkl.shape[0]) == (keep == 1.0)
+
+
 def test_snapshot_header_matches_reference_file():
     """The snapshot reader's header (host only) agrees with the file the
     reference wrote (tests/golden/tiny_*.pwo3); non-snapshots are refused."""
