@@ -235,6 +235,36 @@ SDFT_B200_API sdft_b200_status sdft_b200_compensation_density(sdft_b200_compensa
 SDFT_B200_API sdft_b200_status sdft_b200_compensation_project(sdft_b200_compensation* charge, const double* potential,
                                                               double* out, int memory);
 
+/* Hartree + PBE exchange-correlation functional of a Fourier density
+ * n(r) = sum_G n_G exp(+iG.r) on one device, with the reference's default
+ * packing (paired real transforms, fused PBE tiles, fixed-tile reductions).
+ * lattice: rows a1, a2, a3 (bohr). density: `count` keys hkl (x3) and values
+ * (interleaved complex), unique, any order; core: the optional frozen
+ * pseudo-core (core_count 0 for none), added for XC only. quadrature_padding
+ * 0 takes SDFT_FFT_OVERSAMPLING or 2; the XC grid is padding * max(3, 2m+1)
+ * per axis (any length up to 512; SDFT_FAST_DENSITY_GRID=1 rounds it up to a
+ * 2/3/5/7-smooth length). Outputs on the union support of density and core
+ * in the reference's map order (lexicographic h, k, l): support_hkl (x3),
+ * potential = Hartree (density keys, 0 at G = 0) + v_xc, and xc_potential =
+ * v_xc (interleaved complex). Call with capacity 0 to get *support_count
+ * (host only: context may be NULL, and the host checks run); capacity below
+ * it is INVALID_ARGUMENT. The
+ * scalars agree with the reference to rounding (double-double sums where it
+ * sums long double). Host pointers, synchronous.
+ * Replaces: evaluate_density_functionals, src/density_functionals.hpp:45-47
+ * (src/density_functionals.cpp:462-729). */
+typedef struct {
+  double hartree_energy, xc_energy, vxc_density;
+  double hartree_stress[9], xc_stress[9]; /* row-major 3 x 3 */
+  double sampled_electrons, minimum_density;
+  uint64_t clipped_density_points, grid_points;
+  int32_t grid[3];
+} sdft_b200_functionals;
+SDFT_B200_API sdft_b200_status sdft_b200_density_functionals(
+    sdft_b200_context* context, const double lattice[9], size_t count, const int32_t* hkl, const double* density,
+    size_t core_count, const int32_t* core_hkl, const double* core, int quadrature_padding, int32_t* support_hkl,
+    double* potential, double* xc_potential, size_t capacity, size_t* support_count, sdft_b200_functionals* result);
+
 /* Rayleigh-Ritz eigensolve of a projected pencil in FP64: the lowest
  * `requested` (0 = all n) solutions of H y = e S y, H and S n x n Hermitian
  * (lower triangles referenced, column-major), S positive definite. values:

@@ -14,6 +14,7 @@
 //   onsite_density_from_amplitudes      src/onsite_density.hpp:10-36
 //   paw_lm_moments_from_density         src/paw_augmentation.cpp:490-525
 //   PawCompensationOperator ctor/density_sum src/paw_compensation.cpp:185-342,465-524
+//   evaluate_density_functionals        src/density_functionals.cpp:462-729
 // Complex arrays are interleaved (re, im) doubles, column-major blocks.
 #include "plane_wave_operator.hpp"
 #include "pw_core.hpp"
@@ -26,6 +27,7 @@
 #include "paw_compensation.hpp"
 
 #include <algorithm>
+#include <array>
 #include <complex>
 #include <cstring>
 #include <exception>
@@ -394,6 +396,68 @@ int ref_compensation_project(const double* lattice, long atoms, const double* fr
   } catch (const std::exception& e) {
     set_error(error, error_length, e);
     return 1;
+  }
+}
+}
+
+extern "C" {
+
+// evaluate_density_functionals on a density (and optional frozen core) given
+// as key/value arrays. Returns the support size (the potential's keys, in map
+// order) or -1 with the error text. With capacity >= that size it writes the
+// keys, potential, xc_potential and scalars = [hartree_energy, xc_energy,
+// vxc_density, sampled_electrons, minimum_density, clipped_density_points,
+// grid_points, hartree_stress (9, row-major), xc_stress (9)].
+long ref_density_functionals(const double* lattice, long count, const int* keys, const double* values,
+                             long core_count, const int* core_keys, const double* core, int padding, long capacity,
+                             int* out_keys, double* potential, double* xc_potential, double* scalars, char* error,
+                             long error_length) {
+  try {
+    std::array<sdft::Vec3, 3> cell{};
+    for (int r = 0; r < 3; ++r) cell[r] = {lattice[3 * r], lattice[3 * r + 1], lattice[3 * r + 2]};
+    sdft::FourierDensity density, frozen;
+    const auto* pv = reinterpret_cast<const C*>(values);
+    for (long i = 0; i < count; ++i) density[{keys[3 * i], keys[3 * i + 1], keys[3 * i + 2]}] = pv[i];
+    const auto* pc = reinterpret_cast<const C*>(core);
+    for (long i = 0; i < core_count; ++i)
+      frozen[{core_keys[3 * i], core_keys[3 * i + 1], core_keys[3 * i + 2]}] = pc[i];
+    const auto result = sdft::evaluate_density_functionals(density, cell, core_count ? &frozen : nullptr, padding,
+                                                           false);
+    const long size = static_cast<long>(result.potential.size());
+    if (capacity < size) return size;
+    long i = 0;
+    auto* po = reinterpret_cast<C*>(potential);
+    auto* xo = reinterpret_cast<C*>(xc_potential);
+    for (const auto& [key, value] : result.potential) {
+      out_keys[3 * i] = std::get<0>(key);
+      out_keys[3 * i + 1] = std::get<1>(key);
+      out_keys[3 * i + 2] = std::get<2>(key);
+      po[i] = value;
+      const auto found = result.xc_potential.find(key);
+      xo[i] = found == result.xc_potential.end() ? C{} : found->second;
+      ++i;
+    }
+    scalars[0] = result.hartree_energy;
+    scalars[1] = result.xc_energy;
+    scalars[2] = result.vxc_density;
+    scalars[3] = result.sampled_electrons;
+    scalars[4] = result.minimum_density;
+    scalars[5] = static_cast<double>(result.clipped_density_points);
+    scalars[6] = static_cast<double>(result.grid_points);
+    for (int a = 0; a < 3; ++a) {
+      const auto& h = result.hartree_stress[a];
+      const auto& x = result.xc_stress[a];
+      scalars[7 + 3 * a] = h.x;
+      scalars[8 + 3 * a] = h.y;
+      scalars[9 + 3 * a] = h.z;
+      scalars[16 + 3 * a] = x.x;
+      scalars[17 + 3 * a] = x.y;
+      scalars[18 + 3 * a] = x.z;
+    }
+    return size;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return -1;
   }
 }
 }

@@ -87,6 +87,10 @@ class ReferenceLibrary:
         L.ref_compensation_project.argtypes = [_dbl, ctypes.c_long, _dbl, ctypes.c_long, _int, ctypes.c_long, _int,
                                                ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, ctypes.c_long, _int,
                                                _dbl, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_density_functionals.restype = ctypes.c_long
+        L.ref_density_functionals.argtypes = [_dbl, ctypes.c_long, _int, _dbl, ctypes.c_long, _int, _dbl,
+                                              ctypes.c_int, ctypes.c_long, _int, _dbl, _dbl, _dbl, ctypes.c_char_p,
+                                              ctypes.c_long]
 
     # -- basis ---------------------------------------------------------------
     def enumerate_g_vectors(self, reciprocal, cutoff_ev, kpoint=(0.0, 0.0, 0.0), hartree_to_ev=27.211386245988):
@@ -180,6 +184,42 @@ class ReferenceLibrary:
                                                pk.shape[0], _ptr(pk, _int), pv.view(np.float64).ctypes.data_as(_dbl),
                                                out.view(np.float64).ctypes.data_as(_dbl), err, 512)
         self._check(rc, err)
+        return out
+
+    def density_functionals(self, lattice, keys, values, core_keys=None, core_values=None, padding: int = 0):
+        """evaluate_density_functionals (src/density_functionals.cpp:696-729): the
+        potential's keys in map order, potential, xc_potential and the scalars."""
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        k = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+        v = np.ascontiguousarray(values, dtype=np.complex128).reshape(-1)
+        if core_keys is None:
+            ck, cv = np.zeros((0, 3), dtype=np.int32), np.zeros(0, dtype=np.complex128)
+        else:
+            ck = np.ascontiguousarray(core_keys, dtype=np.int32).reshape(-1, 3)
+            cv = np.ascontiguousarray(core_values, dtype=np.complex128).reshape(-1)
+        err = ctypes.create_string_buffer(512)
+        scalars = np.zeros(25)
+        args = (_ptr(lat), k.shape[0], _ptr(k, _int), v.view(np.float64).ctypes.data_as(_dbl), ck.shape[0],
+                _ptr(ck, _int), cv.view(np.float64).ctypes.data_as(_dbl), int(padding))
+        size = self.lib.ref_density_functionals(*args, 0, None, None, None, _ptr(scalars), err, 512)
+        if size < 0:
+            raise ValueError(err.value.decode(errors="replace"))
+        out_keys = np.zeros((size, 3), dtype=np.int32)
+        potential = np.zeros(size, dtype=np.complex128)
+        xc = np.zeros(size, dtype=np.complex128)
+        size = self.lib.ref_density_functionals(*args, size, _ptr(out_keys, _int),
+                                                potential.view(np.float64).ctypes.data_as(_dbl),
+                                                xc.view(np.float64).ctypes.data_as(_dbl), _ptr(scalars), err, 512)
+        if size < 0:
+            raise ValueError(err.value.decode(errors="replace"))
+        names = ("hartree_energy", "xc_energy", "vxc_density", "sampled_electrons", "minimum_density",
+                 "clipped_density_points", "grid_points")
+        out = {name: float(scalars[i]) for i, name in enumerate(names)}
+        out["clipped_density_points"] = int(out["clipped_density_points"])
+        out["grid_points"] = int(out["grid_points"])
+        out["hartree_stress"] = scalars[7:16].reshape(3, 3).copy()
+        out["xc_stress"] = scalars[16:25].reshape(3, 3).copy()
+        out.update({"hkl": out_keys, "potential": potential, "xc_potential": xc})
         return out
 
     def density(self, hkl, coefficients, occupations, volume, support_hkl):

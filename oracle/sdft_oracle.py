@@ -467,3 +467,105 @@ def compensation_project(lattice, fractional, keys, augmentation, transform, pot
         out[atom] = (responses @ t).reshape(dim, dim)
     return out
 
+
+
+# --- Hartree + PBE functional (src/density_functionals.cpp:462-729) ----------
+
+def density_functionals(lattice, keys, values, core_keys=None, core_values=None, padding: int = 2,
+                        fast: bool = False) -> dict:
+    """The reference's evaluate_density_functionals with its default packing, in
+    numpy. The support (density keys, plus frozen-core keys for XC) is taken in
+    map order (lexicographic h, k, l). Hartree per density key (:476-497):
+    V_H = 4 pi n / q^2 and E_H = sum 2 pi Omega |n|^2 / q^2 for q^2 > 1e-12,
+    stress 4 pi |n|^2 q_a q_c / q^4 minus E_H / Omega on the diagonal (:693).
+    XC on the grid padding * max(3, 2m+1) per axis (:498-519; `fast` rounds
+    each axis up to a 2/3/5/7-smooth length): n, grad n by backward FFTs of n_G
+    and i q n_G (valence and core transformed separately and summed, :527-559),
+    PBE at max(1e-10, n) per point, tile sums of electrons, energy and stress
+    (:600-641, summed exactly here), forward FFTs of the local potential and
+    the gradient responses, v_xc(G) = l(G) - i q.d(G) (:665-683), and
+    <n, v_xc> = Omega sum Re n(G) v_xc(-G) (:684-691)."""
+    a = np.asarray(lattice, dtype=np.float64).reshape(3, 3)
+    det = float(np.dot(a[0], np.cross(a[1], a[2])))
+    volume = abs(det)
+    if volume < 1e-12 or not math.isfinite(volume):
+        raise ValueError("singular density-grid lattice")
+    b = 2.0 * math.pi / det * np.array([np.cross(a[1], a[2]), np.cross(a[2], a[0]), np.cross(a[0], a[1])])
+    density = {tuple(int(v) for v in k): complex(x) for k, x in zip(np.asarray(keys).reshape(-1, 3), np.asarray(values).ravel())}
+    if not density:
+        raise ValueError("density Fourier support is empty")
+    core = {}
+    if core_keys is not None:
+        core = {tuple(int(v) for v in k): complex(x)
+                for k, x in zip(np.asarray(core_keys).reshape(-1, 3), np.asarray(core_values).ravel())}
+    support = sorted(set(density) | set(core))
+    sk = np.array(support, dtype=np.int64).reshape(-1, 3)
+    q = sk[:, 0:1] * b[0] + sk[:, 1:2] * b[1] + sk[:, 2:3] * b[2]
+    q2 = (q * q).sum(axis=1)
+    in_density = np.array([k in density for k in support])
+    rho = np.array([density.get(k, 0.0) for k in support], dtype=np.complex128)
+    rho_core = np.array([core.get(k, 0.0) for k in support], dtype=np.complex128)
+    # Hartree (density keys only).
+    coulomb = in_density & (q2 > 1e-12)
+    norm = (rho.real ** 2 + rho.imag ** 2)
+    hartree = np.where(coulomb, 4.0 * math.pi * rho / np.where(coulomb, q2, 1.0), 0.0)
+    e_h = math.fsum((2.0 * math.pi * volume * norm[coulomb] / q2[coulomb]).tolist())
+    stress_h = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            stress_h[i, j] = math.fsum((4.0 * math.pi * norm[coulomb] * q[coulomb, i] * q[coulomb, j]
+                                        / (q2[coulomb] * q2[coulomb])).tolist())
+    # XC grid.
+    m = np.abs(sk).max(axis=0)
+    shape = tuple(padding * max(3, 2 * int(v) + 1) for v in m)
+    if fast:
+        shape = tuple(fast_fft_length(v) for v in shape)
+    if max(shape) > 512:
+        raise ValueError("XC grid axis above 512 points")
+    idx = tuple(np.mod(sk[:, a_], shape[a_]) for a_ in range(3))
+
+    def fields(coefficients):
+        grids = np.zeros((4,) + shape, dtype=np.complex128)
+        grids[0][idx] = coefficients
+        for axis in range(3):
+            grids[axis + 1][idx] = 1j * q[:, axis] * coefficients
+        return [backward_fft(g).real for g in grids]
+
+    if core:
+        valence_fields = fields(np.where(in_density, rho, 0.0))
+        core_fields = fields(rho_core)
+        total = [v + c for v, c in zip(valence_fields, core_fields)]
+        valence = valence_fields[0]
+    else:
+        total = fields(rho)
+        valence = total[0]
+    raw, gx, gy, gz = total
+    n = np.maximum(1e-10, raw)
+    grad = np.sqrt(gx * gx + gy * gy + gz * gz)
+    xc = pbe_unpolarized(n.ravel(), grad.ravel())
+    energy = xc[:, 0].reshape(shape)
+    local = (xc[:, 4] + xc[:, 5]).reshape(shape)
+    coefficient = xc[:, 6].reshape(shape)
+    d = [coefficient * gx, coefficient * gy, coefficient * gz]
+    g = [gx, gy, gz]
+    points = int(np.prod(shape))
+    weight = volume / points
+    pressure = energy - local * raw - d[0] * gx - d[1] * gy - d[2] * gz
+    stress_xc = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            term = (pressure if i == j else 0.0) - d[i] * g[j]
+            stress_xc[i, j] = math.fsum(np.ravel(term).tolist()) / points
+    # Forward transforms and v_xc on the support.
+    transforms = [forward_fft(f)[idx] / points for f in (local, d[0], d[1], d[2])]
+    vxc = transforms[0] - 1j * (q[:, 0] * transforms[1] + q[:, 1] * transforms[2] + q[:, 2] * transforms[3])
+    where = {k: i for i, k in enumerate(support)}
+    vxc_density = math.fsum(volume * (rho[i] * vxc[where[(-k[0], -k[1], -k[2])]]).real
+                            for i, k in enumerate(support) if in_density[i] and (-k[0], -k[1], -k[2]) in where)
+    stress_h -= np.eye(3) * (e_h / volume)
+    return {"hkl": sk.astype(np.int32), "potential": np.where(in_density, hartree, 0.0) + vxc, "xc_potential": vxc,
+            "hartree_energy": e_h, "xc_energy": math.fsum(energy.ravel().tolist()) * weight,
+            "vxc_density": vxc_density, "hartree_stress": stress_h, "xc_stress": stress_xc,
+            "sampled_electrons": math.fsum(valence.ravel().tolist()) * weight,
+            "minimum_density": float(raw.min()), "clipped_density_points": int((raw < 1e-10).sum()),
+            "grid_points": points, "grid": shape}

@@ -13,6 +13,7 @@
 #include "paw_density.cuh"
 #include "operator.cuh"
 #include "server.cuh"
+#include "xc_functional.cuh"
 
 struct sdft_b200_context {
   std::unique_ptr<sdft_b200::Context> impl;
@@ -525,6 +526,43 @@ sdft_b200_status sdft_b200_compensation_project(sdft_b200_compensation* charge, 
     c.project(din, dout);
     SDFT_CUDA(cudaMemcpyAsync(out, dout, sizeof(C) * out_count, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.synchronize();
+  });
+}
+
+sdft_b200_status sdft_b200_density_functionals(sdft_b200_context* context, const double lattice[9], size_t count,
+                                               const int32_t* hkl, const double* density, size_t core_count,
+                                               const int32_t* core_hkl, const double* core, int quadrature_padding,
+                                               int32_t* support_hkl, double* potential, double* xc_potential,
+                                               size_t capacity, size_t* support_count,
+                                               sdft_b200_functionals* result) {
+  return guarded([&] {
+    require(lattice && support_count, "null density functional argument");
+    require(!count || (hkl && density), "null density arrays");
+    require(!core_count || (core_hkl && core), "null core arrays");
+    const auto support = sdft_b200::functional_support(lattice, count, hkl, density, core_count, core_hkl, core,
+                                                       quadrature_padding);
+    const std::size_t n = support.keys.size();
+    *support_count = n;
+    if (!capacity) return;
+    require(capacity >= n, "density functional output capacity below the support size");
+    require(context && support_hkl && potential && xc_potential && result, "null density functional outputs");
+    for (std::size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) support_hkl[3 * i + a] = support.keys[i][a];
+    sdft_b200::FunctionalResult r;
+    sdft_b200::density_functionals(*context->impl, support, reinterpret_cast<sdft_b200::Cx<double>*>(potential),
+                                   reinterpret_cast<sdft_b200::Cx<double>*>(xc_potential), r);
+    result->hartree_energy = r.hartree_energy;
+    result->xc_energy = r.xc_energy;
+    result->vxc_density = r.vxc_density;
+    for (int k = 0; k < 9; ++k) {
+      result->hartree_stress[k] = r.hartree_stress[k];
+      result->xc_stress[k] = r.xc_stress[k];
+    }
+    result->sampled_electrons = r.sampled_electrons;
+    result->minimum_density = r.minimum_density;
+    result->clipped_density_points = r.clipped_density_points;
+    result->grid_points = r.grid_points;
+    for (int a = 0; a < 3; ++a) result->grid[a] = r.grid[a];
   });
 }
 

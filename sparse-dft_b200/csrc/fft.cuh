@@ -24,8 +24,10 @@ struct LinePlan {
   int radix[kMaxStages] = {};
 };
 
-// Host: factor n into supported radices (4 first, then 2, 3, 5, 7).
-LinePlan make_line_plan(int n);
+// Host: factor n into supported radices (4 first, then 2, 3, 5, 7). With
+// general = true the rest of n is factored into odd primes above 7, which
+// only the general-length drivers (fft_lines_pp_general) execute.
+LinePlan make_line_plan(int n, bool general = false);
 bool fft_length_supported(int n);
 // Smallest 2/3/5/7-smooth length >= minimum (the reference's fast_fft_length,
 // src/fft_planning.hpp:16-23).
@@ -537,6 +539,100 @@ __device__ Cx<T>* fft_lines_pp(Cx<T>* src, Cx<T>* dst, int count, int line_strid
     Cx<T>* swap = src;
     src = dst;
     dst = swap;
+    ns *= r;
+  }
+  return src;
+}
+
+// Radix-R stage for a runtime odd prime R > 7 (a general length's large
+// factors), in two passes so that no thread holds R values. Pass 1 (src ->
+// dst), one butterfly (j, line) per item: applies the stage twiddles and
+// stores x0, the pair sums a_r = x_r + x_{R-r} and differences
+// b_r = x_r - x_{R-r} (r = 1..H, H = (R-1)/2) in the butterfly's R output
+// slots. Pass 2 (dst -> src), one output q per item: y_0 = x0 + sum_r a_r and
+// y_q = x0 + sum_r a_r cos(2 pi rq/R) -/+ i sum_r b_r sin(2 pi rq/R), the
+// arithmetic of radix_dft for the compiled odd radices, with the roots read
+// from the length-n table. The result is left in src.
+template <typename T, bool INV>
+__device__ void pp_stage_prime(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int es, const int* rows, int n,
+                               int ns, int R, const Cx<T>* tw) {
+  const int m = n / R, twstride = n / (ns * R), unit = n / R, H = (R - 1) / 2;
+  for (int item = threadIdx.x; item < count * m; item += blockDim.x) {
+    const int j = item / count, t = item - j * count;
+    const int k = j % ns;
+    const int offset = (rows ? rows[t] : t) * line_stride;
+    const Cx<T>* in = src + offset;
+    Cx<T>* out = dst + offset + ((j / ns) * ns * R + k) * es;
+    out[0] = in[j * es];
+    for (int r = 1; r <= H; ++r) {
+      Cx<T> x = in[(j + r * m) * es], y = in[(j + (R - r) * m) * es];
+      if (k > 0) {
+        x = cmul(x, twiddle<T, INV>(tw, r * k * twstride));
+        y = cmul(y, twiddle<T, INV>(tw, (R - r) * k * twstride));
+      }
+      out[r * ns * es] = x + y;
+      out[(H + r) * ns * es] = x - y;
+    }
+  }
+  __syncthreads();
+  for (int item = threadIdx.x; item < count * n; item += blockDim.x) {
+    const int o = item / count, t = item - o * count;
+    const int j = o / R, q = o - j * R;
+    const int k = j % ns;
+    const int offset = (rows ? rows[t] : t) * line_stride;
+    const Cx<T>* packed = dst + offset + ((j / ns) * ns * R + k) * es;
+    const Cx<T> x0 = packed[0];
+    Cx<T> y;
+    if (q == 0) {
+      y = x0;
+      for (int r = 1; r <= H; ++r) y = y + packed[r * ns * es];
+    } else {
+      const int qq = q <= H ? q : R - q;
+      T cre = x0.re, cim = x0.im, sre = 0, sim = 0;
+      int root = 0;
+      for (int r = 1; r <= H; ++r) {
+        root += qq;
+        if (root >= R) root -= R;
+        const Cx<T> w = tw[root * unit];  // cos, -sin (forward)
+        const Cx<T> a = packed[r * ns * es], b = packed[(H + r) * ns * es];
+        cre += a.re * w.re;
+        cim += a.im * w.re;
+        const T s = INV ? -w.im : w.im;
+        sre -= b.im * s;
+        sim += b.re * s;
+      }
+      y = q <= H ? Cx<T>{cre + sre, cim + sim} : Cx<T>{cre - sre, cim - sim};
+    }
+    src[offset + ((j / ns) * ns * R + k + q * ns) * es] = y;
+  }
+}
+
+// fft_lines_pp for plans that may hold odd prime radices above 7 (general
+// lengths); the compiled radices run the same ping-pong stages.
+template <typename T, bool INV>
+__device__ Cx<T>* fft_lines_pp_general(Cx<T>* src, Cx<T>* dst, int count, int line_stride, int elem_stride,
+                                       const int* rows, const LinePlan& plan, const Cx<T>* tw) {
+  int ns = 1;
+  for (int s = 0; s < plan.stages; ++s) {
+    const int r = plan.radix[s];
+    bool swapped = true;
+    switch (r) {
+      case 2: pp_stage_flat<T, 2, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 3: pp_stage_flat<T, 3, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 4: pp_stage_flat<T, 4, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 5: pp_stage_flat<T, 5, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      case 7: pp_stage_flat<T, 7, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, tw); break;
+      default:
+        pp_stage_prime<T, INV>(src, dst, count, line_stride, elem_stride, rows, plan.n, ns, r, tw);
+        swapped = false;
+        break;
+    }
+    __syncthreads();
+    if (swapped) {
+      Cx<T>* swap = src;
+      src = dst;
+      dst = swap;
+    }
     ns *= r;
   }
   return src;

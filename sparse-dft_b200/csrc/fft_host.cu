@@ -18,7 +18,7 @@ std::atomic<unsigned long long> launches{0};
 void count_launch() { launches.fetch_add(1, std::memory_order_relaxed); }
 unsigned long long launch_count() { return launches.load(std::memory_order_relaxed); }
 
-LinePlan make_line_plan(int n) {
+LinePlan make_line_plan(int n, bool general) {
   if (n < 1 || n > kMaxLine) throw InvalidArgument("FFT length out of the supported range [1, 512]");
   LinePlan plan;
   plan.n = n;
@@ -31,6 +31,9 @@ LinePlan make_line_plan(int n) {
   while (rest % 4 == 0) push(4);
   for (int p : {2, 3, 5, 7})
     while (rest % p == 0) push(p);
+  if (general)
+    for (int p = 11; rest > 1; p += 2)
+      while (rest % p == 0) push(p);
   if (rest != 1) throw InvalidArgument("FFT length must be 2/3/5/7-smooth: " + std::to_string(n));
   return plan;
 }

@@ -218,7 +218,8 @@ __global__ void __launch_bounds__(kThreads) plane_out_kernel(const Cx<T>* __rest
 }
 
 // Lines along a strided axis: element e of line i at base + e*stride + i.
-template <typename T, bool INV, int TL>
+// GENERAL plans may hold prime radices above 7 (general lengths).
+template <typename T, bool INV, int TL, bool GENERAL>
 __global__ void __launch_bounds__(kThreads) fft_strided_kernel(Cx<T>* __restrict__ data, int n, long long stride,
                                                                long long inner, long long outer_stride, LinePlan p,
                                                                const Cx<T>* __restrict__ tw_global) {
@@ -237,7 +238,8 @@ __global__ void __launch_bounds__(kThreads) fft_strided_kernel(Cx<T>* __restrict
     if (t < lines) tile_a[e * STRIDE + t] = base[e * stride + t];
   }
   __syncthreads();
-  const Cx<T>* done = fft_lines_pp<T, INV>(tile_a, tile_b, lines, 1, STRIDE, nullptr, p, tw);
+  const Cx<T>* done = GENERAL ? fft_lines_pp_general<T, INV>(tile_a, tile_b, lines, 1, STRIDE, nullptr, p, tw)
+                              : fft_lines_pp<T, INV>(tile_a, tile_b, lines, 1, STRIDE, nullptr, p, tw);
   for (int idx = tid; idx < n * TL; idx += blockDim.x) {
     const int e = idx / TL, t = idx - e * TL;
     if (t < lines) base[e * stride + t] = done[e * STRIDE + t];
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kThreads) fft_strided_kernel(Cx<T>* __restrict
 }
 
 // Contiguous rows of length n (the innermost axis).
-template <typename T, bool INV, int TR>
+template <typename T, bool INV, int TR, bool GENERAL>
 __global__ void __launch_bounds__(kThreads) fft_rows_kernel(Cx<T>* __restrict__ data, int n, int np, long long rows,
                                                             LinePlan p, const Cx<T>* __restrict__ tw_global) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -262,7 +264,8 @@ __global__ void __launch_bounds__(kThreads) fft_rows_kernel(Cx<T>* __restrict__ 
     tile_a[r * np + e] = base[idx];
   }
   __syncthreads();
-  const Cx<T>* done = fft_lines_pp<T, INV>(tile_a, tile_b, count, np, 1, nullptr, p, tw);
+  const Cx<T>* done = GENERAL ? fft_lines_pp_general<T, INV>(tile_a, tile_b, count, np, 1, nullptr, p, tw)
+                              : fft_lines_pp<T, INV>(tile_a, tile_b, count, np, 1, nullptr, p, tw);
   for (int idx = tid; idx < count * n; idx += blockDim.x) {
     const int r = idx / n, e = idx - r * n;
     base[idx] = done[r * np + e];
@@ -509,51 +512,51 @@ void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long lo
   run_local_passes<T>(a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
 }
 
-template <typename T, bool INV, int TL>
+template <typename T, bool INV, int TL, bool GENERAL>
 void fft3d_tiles(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
   const long long n12 = static_cast<long long>(n[1]) * n[2];
   const long long count = n12 * n[0];
   // axis 2: contiguous rows
   {
-    const LinePlan p = make_line_plan(n[2]);
+    const LinePlan p = make_line_plan(n[2], GENERAL);
     const int np = n[2] | 1;
     const std::size_t smem = sizeof(Cx<T>) * (n[2] + 2 * static_cast<std::size_t>(TL) * np);
-    allow_smem(fft_rows_kernel<T, INV, TL>, smem);
+    allow_smem(fft_rows_kernel<T, INV, TL, GENERAL>, smem);
     const long long rows = count / n[2] * batch;
-    fft_rows_kernel<T, INV, TL><<<static_cast<unsigned>(ceil_div(rows, TL)), kThreads, smem, stream>>>(
+    fft_rows_kernel<T, INV, TL, GENERAL><<<static_cast<unsigned>(ceil_div(rows, TL)), kThreads, smem, stream>>>(
         grid, n[2], np, rows, p, device_twiddles<T>(n[2]));
     SDFT_LAUNCH("fft_rows_kernel");
   }
   // axis 1: stride n2, n0*batch outer blocks
   {
-    const LinePlan p = make_line_plan(n[1]);
+    const LinePlan p = make_line_plan(n[1], GENERAL);
     const std::size_t smem = sizeof(Cx<T>) * (n[1] + 2 * static_cast<std::size_t>(n[1]) * (TL + 1));
-    allow_smem(fft_strided_kernel<T, INV, TL>, smem);
+    allow_smem(fft_strided_kernel<T, INV, TL, GENERAL>, smem);
     const dim3 blocks(static_cast<unsigned>(ceil_div(n[2], TL)), static_cast<unsigned>(n[0] * batch));
-    fft_strided_kernel<T, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[1], n[2], n[2], n12, p,
+    fft_strided_kernel<T, INV, TL, GENERAL><<<blocks, kThreads, smem, stream>>>(grid, n[1], n[2], n[2], n12, p,
                                                                             device_twiddles<T>(n[1]));
     SDFT_LAUNCH("fft_strided_kernel axis1");
   }
   // axis 0: stride n1*n2
   {
-    const LinePlan p = make_line_plan(n[0]);
+    const LinePlan p = make_line_plan(n[0], GENERAL);
     const std::size_t smem = sizeof(Cx<T>) * (n[0] + 2 * static_cast<std::size_t>(n[0]) * (TL + 1));
-    allow_smem(fft_strided_kernel<T, INV, TL>, smem);
+    allow_smem(fft_strided_kernel<T, INV, TL, GENERAL>, smem);
     const dim3 blocks(static_cast<unsigned>(ceil_div(n12, TL)), static_cast<unsigned>(batch));
-    fft_strided_kernel<T, INV, TL><<<blocks, kThreads, smem, stream>>>(grid, n[0], n12, n12, count, p,
+    fft_strided_kernel<T, INV, TL, GENERAL><<<blocks, kThreads, smem, stream>>>(grid, n[0], n12, n12, count, p,
                                                                             device_twiddles<T>(n[0]));
     SDFT_LAUNCH("fft_strided_kernel axis0");
   }
 }
 
 // Tile width: 32 lines when the widest axis fits in shared memory, else 16 or 8.
-template <typename T, bool INV>
+template <typename T, bool INV, bool GENERAL>
 void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
   const std::size_t nmax = std::max({n[0], n[1], n[2]});
   auto fits = [&](std::size_t tl) { return sizeof(Cx<T>) * (nmax + 2 * nmax * (tl + 1)) <= 227 * 1024; };
-  if (fits(32)) fft3d_tiles<T, INV, 32>(grid, n, batch, stream);
-  else if (fits(16)) fft3d_tiles<T, INV, 16>(grid, n, batch, stream);
-  else fft3d_tiles<T, INV, 8>(grid, n, batch, stream);
+  if (fits(32)) fft3d_tiles<T, INV, 32, GENERAL>(grid, n, batch, stream);
+  else if (fits(16)) fft3d_tiles<T, INV, 16, GENERAL>(grid, n, batch, stream);
+  else fft3d_tiles<T, INV, 8, GENERAL>(grid, n, batch, stream);
 }
 
 }  // namespace
@@ -630,11 +633,18 @@ void local_hamiltonian(const SpherePlan& plan, const Cx<double>* x, long long ld
 }
 
 template <typename T>
-void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream) {
+void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream, bool general) {
   const int nmax = std::max({n[0], n[1], n[2]});
   if (nmax > kMaxLine) throw InvalidArgument("3D FFT axes above 512 points are not supported");
-  if (backward) fft3d_impl<T, true>(grid, n, batch, stream);
-  else fft3d_impl<T, false>(grid, n, batch, stream);
+  // Smooth lengths keep the compiled-radix kernels even when general lengths are allowed.
+  general = general && !(fft_length_supported(n[0]) && fft_length_supported(n[1]) && fft_length_supported(n[2]));
+  if (general) {
+    if (backward) fft3d_impl<T, true, true>(grid, n, batch, stream);
+    else fft3d_impl<T, false, true>(grid, n, batch, stream);
+  } else {
+    if (backward) fft3d_impl<T, true, false>(grid, n, batch, stream);
+    else fft3d_impl<T, false, false>(grid, n, batch, stream);
+  }
 }
 
 template <typename T>
@@ -676,7 +686,7 @@ template void local_hamiltonian<float>(const SpherePlan&, const Cx<double>*, lon
                                        const double*, Cx<double>*, long long, Cx<float>*, cudaStream_t);
 template void local_hamiltonian<double>(const SpherePlan&, const Cx<double>*, long long, int, const double*,
                                         const double*, Cx<double>*, long long, Cx<double>*, cudaStream_t);
-template void fft3d<float>(Cx<float>*, const int[3], int, bool, cudaStream_t);
-template void fft3d<double>(Cx<double>*, const int[3], int, bool, cudaStream_t);
+template void fft3d<float>(Cx<float>*, const int[3], int, bool, cudaStream_t, bool);
+template void fft3d<double>(Cx<double>*, const int[3], int, bool, cudaStream_t, bool);
 
 }  // namespace sdft_b200

@@ -49,8 +49,10 @@ void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long 
                               const T* potential, const double* kinetic, Cx<double>* y, long long ldy,
                               Cx<T>* slab, const Cx<T>* const twiddle[3], cudaStream_t stream);
 
-// In-place unnormalised 3D FFT of `batch` contiguous row-major grids.
+// In-place unnormalised 3D FFT of `batch` contiguous row-major grids. Axis
+// lengths up to 512; with general = true any length (odd prime factors above
+// 7 run the two-pass prime stage), else 2/3/5/7-smooth lengths only.
 template <typename T>
-void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream);
+void fft3d(Cx<T>* grid, const int n[3], int batch, bool backward, cudaStream_t stream, bool general = false);
 
 }  // namespace sdft_b200

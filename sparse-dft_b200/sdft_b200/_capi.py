@@ -9,6 +9,8 @@ import ctypes
 import pathlib
 import re
 
+import numpy as np
+
 LIBRARY = pathlib.Path(__file__).resolve().parent / "_lib" / "libsdft_b200.so"
 HEADER = pathlib.Path(__file__).resolve().parents[2] / "include" / "sdft_b200.h"
 
@@ -76,6 +78,25 @@ class SnapshotInfo(ctypes.Structure):
         return out
 
 
+class Functionals(ctypes.Structure):
+    _fields_ = [("hartree_energy", ctypes.c_double), ("xc_energy", ctypes.c_double), ("vxc_density", ctypes.c_double),
+                ("hartree_stress", ctypes.c_double * 9), ("xc_stress", ctypes.c_double * 9),
+                ("sampled_electrons", ctypes.c_double), ("minimum_density", ctypes.c_double),
+                ("clipped_density_points", ctypes.c_uint64), ("grid_points", ctypes.c_uint64),
+                ("grid", ctypes.c_int32 * 3)]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            value = getattr(self, name)
+            if name.endswith("stress"):
+                value = np.array(list(value)).reshape(3, 3)
+            elif name == "grid":
+                value = tuple(int(v) for v in value)
+            out[name] = value
+        return out
+
+
 class SolveTiming(ctypes.Structure):
     _fields_ = [("slot", ctypes.c_int), ("footprint", ctypes.c_size_t), ("submitted", ctypes.c_double),
                 ("started", ctypes.c_double), ("finished", ctypes.c_double)]
@@ -119,6 +140,8 @@ def _declare(lib: ctypes.CDLL) -> None:
                                      ctypes.POINTER(P)])
     fn("sdft_b200_operator_destroy", [P])
     fn("sdft_b200_operator_update", [P, SZ, I32, D, D, D])
+    fn("sdft_b200_density_functionals", [P, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, SZ, SZP,
+                                         ctypes.POINTER(Functionals)])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])

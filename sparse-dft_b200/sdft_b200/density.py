@@ -52,6 +52,54 @@ def pbe_points(context: Context, density, gradient):
     return out
 
 
+def density_functionals(context: Context | None, lattice, hkl, density, core_hkl=None, core=None,
+                        quadrature_padding: int = 0, support_only: bool = False):
+    """Hartree + PBE XC functional of a Fourier density on the device (the
+    reference's evaluate_density_functionals). Returns a dict with the union
+    support keys `hkl` (lexicographic order), `potential` (Hartree + v_xc),
+    `xc_potential` and the DensityFunctionals scalars; with support_only the
+    keys alone (host only, context may be None)."""
+    lib = C.library()
+    lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+    keys = np.ascontiguousarray(hkl, dtype=np.int32).reshape(-1, 3)
+    values = np.ascontiguousarray(density, dtype=np.complex128).reshape(-1)
+    if values.shape[0] != keys.shape[0]:
+        raise ValueError("density keys and values disagree")
+    if core_hkl is not None:
+        ckeys = np.ascontiguousarray(core_hkl, dtype=np.int32).reshape(-1, 3)
+        cvalues = np.ascontiguousarray(core, dtype=np.complex128).reshape(-1)
+        if cvalues.shape[0] != ckeys.shape[0]:
+            raise ValueError("core keys and values disagree")
+    else:
+        ckeys = np.zeros((0, 3), dtype=np.int32)
+        cvalues = np.zeros(0, dtype=np.complex128)
+    handle = context.handle if context is not None else None
+    count = ctypes.c_size_t()
+    result = C.Functionals()
+    args = (lat.ctypes.data_as(C.D), keys.shape[0], keys.ctypes.data_as(C.I32), values.ctypes.data_as(C.D),
+            ckeys.shape[0], ckeys.ctypes.data_as(C.I32), cvalues.ctypes.data_as(C.D), int(quadrature_padding))
+    C.check(lib.sdft_b200_density_functionals(handle, *args, None, None, None, 0, ctypes.byref(count),
+                                              ctypes.byref(result)))
+    n = count.value
+    if support_only:
+        return _support_keys(keys, ckeys)
+    support = np.zeros((n, 3), dtype=np.int32)
+    potential = np.zeros(n, dtype=np.complex128)
+    xc = np.zeros(n, dtype=np.complex128)
+    C.check(lib.sdft_b200_density_functionals(handle, *args, support.ctypes.data_as(C.I32),
+                                              potential.ctypes.data_as(C.D), xc.ctypes.data_as(C.D), n,
+                                              ctypes.byref(count), ctypes.byref(result)))
+    out = result.as_dict()
+    out.update({"hkl": support, "potential": potential, "xc_potential": xc})
+    return out
+
+
+def _support_keys(keys, core_keys) -> np.ndarray:
+    """Union of the key sets in lexicographic order (the library's support order)."""
+    union = {tuple(int(v) for v in k) for k in keys} | {tuple(int(v) for v in k) for k in core_keys}
+    return np.array(sorted(union), dtype=np.int32).reshape(-1, 3)
+
+
 def band_density(context: Context, hkl, coefficients, occupations, volume: float, support):
     """n(G) at the support keys from band-major coefficients (bands, npw), the
     reference's plane_wave_density_fft arithmetic on the device. A torch CUDA

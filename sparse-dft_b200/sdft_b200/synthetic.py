@@ -387,6 +387,47 @@ def density_support(inputs: OperatorInputs, factor: float) -> np.ndarray:
     return np.ascontiguousarray(hkl, dtype=np.int32)
 
 
+def gaussian_density(lattice, positions, keys, charge: float = 4.0, width: float = 1.2) -> np.ndarray:
+    """n_G = sum_sites (charge / Omega) exp(-|G|^2 width^2 / 4) exp(-i G.tau) on the keys: normalised
+    Gaussian charges at the fractional positions (a smooth stand-in for a valence or pseudo-core
+    density; the truncated support leaves small negative regions, as real densities have)."""
+    a = np.asarray(lattice, dtype=np.float64).reshape(3, 3)
+    volume = abs(float(np.dot(a[0], np.cross(a[1], a[2]))))
+    b = 2.0 * math.pi * np.linalg.inv(a).T
+    k = np.asarray(keys, dtype=np.float64).reshape(-1, 3)
+    q = k @ b
+    g2 = (q * q).sum(axis=1)
+    taus = np.asarray(positions, dtype=np.float64).reshape(-1, 3) @ a
+    phases = np.exp(-1j * (q @ taus.T)).sum(axis=1)
+    return (charge / volume) * np.exp(-g2 * width * width / 4.0) * phases
+
+
+def functional_case(name: str) -> dict:
+    """Seeded inputs of the Hartree + XC functional: lattice (rows, bohr), density keys and values
+    (Gaussian valence charges on {1/2|G|^2 <= f Ecut}) and a frozen core (narrower Gaussians on a
+    smaller support). si8: diamond Si8 (a = 10.26), f Ecut = 15 Ha, grid 34^3 (2 x 17);
+    triclinic: a skewed 2-site cell on a box of keys, grid 18 x 22 x 14 (2 x 11, 2 x 7), with the
+    core on a box that reaches past it (22 x 22 x 18 with the core);
+    si64: Si64 (a = 20.52), f Ecut = 60 Ha (f = 4 of the 15 Ha basis), grid 142^3 (2 x 71)."""
+    if name == "triclinic":
+        lattice = np.array([[6.0, 0.0, 0.0], [0.3, 6.0, 0.0], [0.1, 0.2, 6.6]])
+        positions = np.array([[0.0, 0.0, 0.0], [0.25, 0.25, 0.3]])
+        keys = np.array([(h, k, l) for h in range(-4, 5) for k in range(-5, 6) for l in range(-3, 4)], dtype=np.int32)
+        core_keys = np.array([(h, k, l) for h in range(-5, 6) for k in range(-3, 4) for l in range(-4, 5)],
+                             dtype=np.int32)  # reaches past the density box: core-only keys
+    else:
+        reps, cut_ha = {"si8": (1, 15.0), "si64": (2, 60.0)}[name]
+        lattice = np.eye(3) * 10.26 * reps
+        positions, _ = zincblende_sites(reps)
+        reciprocal = 2.0 * math.pi * np.linalg.inv(lattice).T
+        keys, _, _ = enumerate_g_vectors(reciprocal, cut_ha * HARTREE_TO_EV)
+        core_keys, _, _ = enumerate_g_vectors(reciprocal, 0.5 * cut_ha * HARTREE_TO_EV)
+    keys = np.ascontiguousarray(keys, dtype=np.int32)
+    core_keys = np.ascontiguousarray(core_keys, dtype=np.int32)
+    return {"lattice": lattice, "keys": keys, "values": gaussian_density(lattice, positions, keys, 4.0, 1.2),
+            "core_keys": core_keys, "core_values": gaussian_density(lattice, positions, core_keys, 2.0, 0.8)}
+
+
 def band_coefficients(inputs: OperatorInputs, bands: int, seed: int = 31) -> np.ndarray:
     """Seeded normalised band-major plane-wave coefficients, (bands, npw) complex128,
     with a kinetic decay so that the bands look like smooth valence states."""

@@ -187,6 +187,22 @@ def snapshot_fixtures(lib):
     print("snapshots", {k: v for k, v in results.items() if "iterations" in k})
 
 
+def functional_fixtures(lib):
+    """Reference evaluate_density_functionals (src/density_functionals.cpp:696-729)
+    of the seeded Gaussian densities of synthetic.functional_case, without and
+    with the frozen core: support keys, potential, xc_potential and scalars."""
+    for name in ("si8", "triclinic"):
+        case = synthetic.functional_case(name)
+        fields = {}
+        for label, core in (("plain", False), ("core", True)):
+            kw = {"core_keys": case["core_keys"], "core_values": case["core_values"]} if core else {}
+            out = lib.density_functionals(case["lattice"], case["keys"], case["values"], **kw)
+            for key, value in out.items():
+                fields[f"{label}_{key}"] = np.asarray(value)
+        np.savez_compressed(HERE / f"functional_{name}.npz", **fields)
+        print("functional", name, "support", fields["core_hkl"].shape[0], "grid points", int(fields["plain_grid_points"]))
+
+
 KPOINT_MESH = {"gaas_k13": (0.0, 1.0 / 3.0, 1.0 / 3.0), "gaas_k26": (1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)}
 
 
@@ -203,6 +219,7 @@ def main():
     parser.add_argument("--kpoints", action="store_true", help="only the off-Gamma GaAs fixtures")
     parser.add_argument("--snapshots", action="store_true", help="only the solver snapshot fixtures")
     parser.add_argument("--projection", action="store_true", help="only the compensation projection fixture")
+    parser.add_argument("--functional", action="store_true", help="only the Hartree + XC functional fixtures")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
@@ -214,6 +231,9 @@ def main():
     if args.projection:
         compensation_project_fixture(lib, synthetic.si8(), "si8", 2.0)
         return
+    if args.functional:
+        functional_fixtures(lib)
+        return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
     pbe_fixture(lib)
@@ -223,6 +243,7 @@ def main():
     kpoint_fixtures(lib)
     snapshot_fixtures(lib)
     compensation_project_fixture(lib, synthetic.si8(), "si8", 2.0)
+    functional_fixtures(lib)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)

@@ -136,3 +136,38 @@ def test_snapshot_header_matches_reference_file():
         snapshot_info(golden / "tiny.npz")
     with pytest.raises(C.SdftError, match="cannot open solver snapshot"):
         snapshot_info(golden / "no_such_snapshot.pwo3")
+
+
+def test_functional_support_query_and_checks_are_host_only(golden):
+    """The functional's support query (capacity 0) runs on the host with no
+    context, and the reference's input checks fail before any device work."""
+    from sdft_b200 import density
+    case = synthetic.functional_case("triclinic")
+    lib = C.library()
+    lat = np.ascontiguousarray(case["lattice"], dtype=np.float64).reshape(9)
+    keys = np.ascontiguousarray(case["keys"], dtype=np.int32)
+    values = np.ascontiguousarray(case["values"], dtype=np.complex128)
+    core_keys = np.ascontiguousarray(case["core_keys"], dtype=np.int32)
+    core = np.ascontiguousarray(case["core_values"], dtype=np.complex128)
+    count = ctypes.c_size_t()
+    assert lib.sdft_b200_density_functionals(None, lat.ctypes.data_as(C.D), keys.shape[0], keys.ctypes.data_as(C.I32),
+                                             values.ctypes.data_as(C.D), core_keys.shape[0],
+                                             core_keys.ctypes.data_as(C.I32), core.ctypes.data_as(C.D), 0, None,
+                                             None, None, 0, ctypes.byref(count), None) == C.OK
+    assert count.value == golden("functional_triclinic")["core_hkl"].shape[0]
+
+    def fails(match, lattice=case["lattice"], k=case["keys"], v=case["values"], ck=None, cv=None, padding=0):
+        with pytest.raises(C.InvalidArgument, match=match):
+            density.density_functionals(None, lattice, k, v, ck, cv, padding, support_only=True)
+
+    fails("singular", lattice=np.zeros((3, 3)))
+    fails("empty", k=np.zeros((0, 3)), v=np.zeros(0))
+    fails("duplicate", k=np.concatenate([keys, keys[:1]]), v=np.concatenate([values, values[:1]]))
+    bad = values.copy()
+    bad[3] = np.nan
+    fails("non-finite valence density", v=bad)
+    bad_core = core.copy()
+    bad_core[0] = np.inf
+    fails("pseudo-core", ck=core_keys, cv=bad_core)
+    fails("quadrature", padding=9)
+    fails("above 512", k=np.array([[300, 0, 0], [0, 0, 0]]), v=np.array([0.1, 1.0]))

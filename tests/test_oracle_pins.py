@@ -171,3 +171,53 @@ def test_compensation_projection_restatement_matches_golden(golden):
     v = _potential_on_support(keys, g["potential_keys"], g["potential"])
     out = sdft_oracle.compensation_project(x.lattice, x.positions, keys, aug, synthetic.lm_transform(aug), v)
     assert relative_error(out, g["projection"]) < 1e-12
+
+
+FUNCTIONAL_SCALARS = ("hartree_energy", "xc_energy", "vxc_density", "sampled_electrons")
+
+
+def functional_inputs(name, label):
+    case = synthetic.functional_case(name)
+    core = {"core_keys": case["core_keys"], "core_values": case["core_values"]} if label == "core" else {}
+    return case, core
+
+
+def check_functional(result, golden, label, scalar_tol, potential_tol):
+    """Shared bars for the functional: keys in the same order, scalars and
+    stresses relative, the minimum density relative, the clipped count exact,
+    potentials relative in norm."""
+    assert np.array_equal(np.asarray(result["hkl"]), golden[f"{label}_hkl"])
+    assert int(result["grid_points"]) == int(golden[f"{label}_grid_points"])
+    for name in FUNCTIONAL_SCALARS:
+        expected = float(golden[f"{label}_{name}"])
+        assert abs(result[name] - expected) <= scalar_tol * abs(expected), name
+    for name in ("hartree_stress", "xc_stress"):
+        expected = golden[f"{label}_{name}"]
+        assert np.max(np.abs(np.asarray(result[name]) - expected)) <= 10 * scalar_tol * np.max(np.abs(expected)), name
+    expected_min = float(golden[f"{label}_minimum_density"])
+    assert abs(result["minimum_density"] - expected_min) <= 1e-10 * abs(expected_min)
+    assert int(result["clipped_density_points"]) == int(golden[f"{label}_clipped_density_points"])
+    for name in ("potential", "xc_potential"):
+        assert relative_error(result[name], golden[f"{label}_{name}"]) < potential_tol, name
+
+
+@pytest.mark.parametrize("name", ["si8", "triclinic"])
+@pytest.mark.parametrize("label", ["plain", "core"])
+def test_functional_restatement_matches_golden(golden, name, label):
+    """The numpy restatement of evaluate_density_functionals against the
+    reference's outputs (tests/golden/functional_*.npz): 1e-12 relative on
+    energies, electrons and <n, v_xc>, 1e-12 on the potentials."""
+    case, core = functional_inputs(name, label)
+    result = sdft_oracle.density_functionals(case["lattice"], case["keys"], case["values"], **core)
+    check_functional(result, golden(f"functional_{name}"), label, 1e-12, 1e-12)
+
+
+def test_functional_restatement_matches_live_reference_padding(reference):
+    """Quadrature padding 1 and 3 (the reference's override), against the live reference."""
+    case = synthetic.functional_case("triclinic")
+    for padding in (1, 3):
+        r = reference.density_functionals(case["lattice"], case["keys"], case["values"], padding=padding)
+        o = sdft_oracle.density_functionals(case["lattice"], case["keys"], case["values"], padding=padding)
+        assert r["grid_points"] == o["grid_points"]
+        assert abs(r["xc_energy"] - o["xc_energy"]) <= 1e-12 * abs(r["xc_energy"])
+        assert relative_error(o["potential"], r["potential"]) < 1e-12
