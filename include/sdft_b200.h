@@ -329,6 +329,25 @@ SDFT_B200_API sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const 
                                                   const double* initial, double* eigenvalues, double* eigenvectors,
                                                   double* residuals, sdft_b200_davidson_stats* stats, int memory);
 
+/* Residual-minimisation trial for SCF warm solves: at most
+ * min(16, max_iterations/2) steps of global rotation, preconditioned
+ * directions and a per-band 2 x 2 residual minimisation from the warm block
+ * `initial` (band-major roots x npw, required); tolerance must be coarse
+ * (> 1e-9). A block whose fresh FP64 residuals meet the tolerance and is
+ * S-orthonormal within 1e-10 returns with *trial_manifold = 1 and
+ * stats->converged = 0 (a residual-checked trial, explicitly not a converged
+ * lowest spectrum); otherwise the Davidson solve continues from the trial's
+ * block with the remaining iterations (*trial_manifold = 0) and its result is
+ * returned, iterations counted in total. Directions are applied in FP64 for
+ * tolerances below 1e-6, in the mixed form otherwise.
+ * Replaces: solve_generalized_hermitian_rmm_trial, src/pw_core.hpp:170-178
+ * (src/rmm_trial.cpp:128-206; selected by SDFT_SCF_RMM_TRIAL=1 for SCF warm
+ * requests, src/pw_core.cpp:558-563). */
+SDFT_B200_API sdft_b200_status sdft_b200_rmm_trial(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                                   const double* initial, double* eigenvalues, double* eigenvectors,
+                                                   double* residuals, sdft_b200_davidson_stats* stats,
+                                                   int* trial_manifold, int memory);
+
 /* ---- Solver snapshots ------------------------------------------------------
  * The reference's SDFTPWO3 files (PlaneWaveOperator::save_solver_snapshot,
  * src/plane_wave_operator.cpp:542-569; replayed by sdft_solver_replay):

@@ -60,6 +60,10 @@ class ReferenceLibrary:
         L.ref_davidson.restype = ctypes.c_int
         L.ref_davidson.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl, _dbl,
                                    _dbl, _int, _long, ctypes.c_char_p, ctypes.c_long]
+        L.ref_rmm_trial.restype = ctypes.c_int
+        L.ref_rmm_trial.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl, _dbl,
+                                    _dbl, ctypes.POINTER(ctypes.c_int), _long, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.c_char_p, ctypes.c_long]
         L.ref_kinetic_preconditioner.restype = ctypes.c_double
         L.ref_kinetic_preconditioner.argtypes = [ctypes.c_double, ctypes.c_double]
         L.ref_save_snapshot.restype = ctypes.c_int
@@ -321,6 +325,19 @@ class ReferenceOperator:
                    _ptr(res), ctypes.byref(conv), ctypes.byref(iters))
         return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),
                 "iterations": int(iters.value)}
+
+    def rmm_trial(self, roots, initial, max_iterations=256, tolerance=1e-6):
+        """solve_generalized_hermitian_rmm_trial as an SCF warm request."""
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        vec = np.zeros((roots, self.n), dtype=np.complex128)
+        conv, manifold, iters = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_long(0)
+        init = np.ascontiguousarray(initial, dtype=np.complex128)
+        self._call(self.lib.lib.ref_rmm_trial, self.handle, roots, max_iterations, tolerance,
+                   init.ctypes.data_as(_dbl), _ptr(eig), vec.ctypes.data_as(_dbl), _ptr(res), ctypes.byref(conv),
+                   ctypes.byref(iters), ctypes.byref(manifold))
+        return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),
+                "iterations": int(iters.value), "trial_manifold": bool(manifold.value)}
 
     @classmethod
     def from_snapshot(cls, lib: ReferenceLibrary, path):

@@ -12,6 +12,7 @@
 #include "band_density.cuh"
 #include "paw_density.cuh"
 #include "operator.cuh"
+#include "rmm_trial.cuh"
 #include "server.cuh"
 #include "xc_functional.cuh"
 
@@ -21,6 +22,7 @@ struct sdft_b200_context {
 struct sdft_b200_operator {
   std::unique_ptr<sdft_b200::DeviceOperator> impl;
   std::unique_ptr<sdft_b200::DavidsonSolver> solver;  // workspace reused across solves
+  std::unique_ptr<sdft_b200::RmmTrial> rmm;
 };
 
 struct sdft_b200_compensation {
@@ -684,6 +686,51 @@ sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davi
       ctx.synchronize();
     }
     if (stats) copy_stats(solver.stats(), stats);
+  });
+}
+
+sdft_b200_status sdft_b200_rmm_trial(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                     const double* initial, double* eigenvalues, double* eigenvectors,
+                                     double* residuals, sdft_b200_davidson_stats* stats, int* trial_manifold,
+                                     int memory) {
+  return guarded([&] {
+    require(op && options && initial && eigenvalues && residuals, "invalid RMM trial problem");
+    require(memory == SDFT_B200_MEMORY_HOST || memory == SDFT_B200_MEMORY_DEVICE, "memory must be host or device");
+    auto& o = *op->impl;
+    auto& ctx = o.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid RMM trial problem");
+    require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid RMM trial problem");
+    sdft_b200::DavidsonOptions d;
+    d.roots = static_cast<int>(options->roots);
+    d.max_iterations = static_cast<int>(options->max_iterations);
+    d.tolerance = options->tolerance;
+    d.precision = precision_of(options->precision);
+    d.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
+    d.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    const std::size_t block = static_cast<std::size_t>(o.npw()) * d.roots;
+    Staged stage(ctx, memory);
+    const Cx<double>* warm = stage.in(initial, block, ctx.staging_in);
+    if (!op->solver) op->solver = std::make_unique<sdft_b200::DavidsonSolver>(o);
+    if (!op->rmm) op->rmm = std::make_unique<sdft_b200::RmmTrial>(o, *op->solver);
+    const auto result = op->rmm->solve(d, warm);
+    std::copy(result.eigenvalues.begin(), result.eigenvalues.end(), eigenvalues);
+    std::copy(result.residuals.begin(), result.residuals.end(), residuals);
+    if (eigenvectors) {
+      SDFT_CUDA(cudaMemcpyAsync(eigenvectors, op->rmm->vectors(), sizeof(Cx<double>) * block,
+                                memory == SDFT_B200_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                ctx.stream));
+      ctx.synchronize();
+    }
+    if (trial_manifold) *trial_manifold = result.trial_manifold ? 1 : 0;
+    if (stats) {
+      sdft_b200::DavidsonStats st = result.fell_back ? result.fallback_stats : sdft_b200::DavidsonStats{};
+      st.iterations = result.iterations;
+      st.converged = result.converged;
+      st.max_residual = result.residuals.empty() ? 0.0
+                                                 : *std::max_element(result.residuals.begin(), result.residuals.end());
+      copy_stats(st, stats);
+    }
   });
 }
 

@@ -140,6 +140,8 @@ def _declare(lib: ctypes.CDLL) -> None:
                                      ctypes.POINTER(P)])
     fn("sdft_b200_operator_destroy", [P])
     fn("sdft_b200_operator_update", [P, SZ, I32, D, D, D])
+    fn("sdft_b200_rmm_trial", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
+                               ctypes.POINTER(ctypes.c_int), ctypes.c_int])
     fn("sdft_b200_density_functionals", [P, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, SZ, SZP,
                                          ctypes.POINTER(Functionals)])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])

@@ -273,6 +273,26 @@ class PlaneWaveOperator:
         return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
                 "iterations": int(info["iterations"]), "stats": info}
 
+    def rmm_trial(self, roots: int, initial, max_iterations: int = 256, tolerance: float = 1e-6,
+                  precision="mixed", subspace_factor: int = 8, handoff: float = 1e-8):
+        """Residual-minimisation trial for an SCF warm solve (the reference's
+        solve_generalized_hermitian_rmm_trial): the Davidson result dict plus
+        `trial_manifold` (a residual-checked, explicitly not converged block)."""
+        opts = C.DavidsonOptions(roots=roots, max_iterations=max_iterations, tolerance=tolerance,
+                                 precision=_precision(precision), subspace_factor=subspace_factor, handoff=handoff)
+        stats = C.DavidsonStats()
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        keep = np.ascontiguousarray(initial, dtype=np.complex128).reshape(roots, self.npw)
+        vec = np.zeros((roots, self.npw), dtype=np.complex128)
+        manifold = ctypes.c_int(0)
+        C.check(self._lib.sdft_b200_rmm_trial(self.handle, ctypes.byref(opts), ctypes.c_void_p(keep.ctypes.data),
+                                              _dptr(eig), ctypes.c_void_p(vec.ctypes.data), _dptr(res),
+                                              ctypes.byref(stats), ctypes.byref(manifold), C.HOST))
+        info = stats.as_dict()
+        return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
+                "iterations": int(info["iterations"]), "trial_manifold": bool(manifold.value), "stats": info}
+
 
 def complex_gemm(context: Context, a, b, adjoint_a: bool = False, precision="fp64", c=None):
     """C = op(A) B (+ c when given), the reference's complex_gemm (host arrays).
