@@ -27,12 +27,13 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPencilLines = 32;
-// Resident CTAs per SM the fixed plane kernels are compiled for: three in
-// FP32 (80 registers, no spills up to N = 70), one in FP64, whose butterfly
-// registers would spill under a tighter bound.
+// Resident CTAs per SM the fixed plane and pencil kernels are compiled for:
+// four in FP32 (64 registers; at N = 70 plane_out spills 144 B and still
+// runs faster than at three CTAs: the passes are latency-bound), one in FP64,
+// whose butterfly registers would spill under a tighter bound.
 template <typename T>
 constexpr int plane_blocks() {
-  return sizeof(T) == 4 ? 3 : 1;
+  return sizeof(T) == 4 ? 4 : 1;
 }
 
 template <typename T>
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(kThreads) pencil_kernel(Cx<T>* __restrict__ sl
 // written once (slab value or zero), and the stages unroll with constant
 // index arithmetic.
 template <typename T, int N0>
-__global__ void __launch_bounds__(kThreads) pencil_fixed_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
+__global__ void __launch_bounds__(kThreads, plane_blocks<T>()) pencil_fixed_kernel(Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                                 const T* __restrict__ potential) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int TL = kPencilLines, STRIDE = TL + 1;
