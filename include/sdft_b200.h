@@ -265,6 +265,25 @@ SDFT_B200_API sdft_b200_status sdft_b200_density_functionals(
     size_t core_count, const int32_t* core_hkl, const double* core, int quadrature_padding, int32_t* support_hkl,
     double* potential, double* xc_potential, size_t capacity, size_t* support_count, sdft_b200_functionals* result);
 
+/* Collinear spin form on one device: up and down channel densities (each
+ * `count` keys and values, unique), the optional frozen core (each channel
+ * receives half of it for XC), padding 0 = SDFT_FFT_OVERSAMPLING or 2. Per
+ * channel: potential = Hartree of the total density + that channel's v_xc,
+ * xc_potential = v_xc (collinear PBE with PW92 spin interpolation), and
+ * result[c] with the Hartree and XC energies and stresses split equally,
+ * <n_c, v_xc,c>, electrons Omega Re n_c(0), the channel's minimum and its
+ * count of negative samples (clipped_density_points). Outputs on the union
+ * support of both channels and the core in map order; capacity 0 queries
+ * *support_count on the host (context may be NULL).
+ * Replaces: evaluate_collinear_density_functionals, src/density_functionals.hpp:52-56
+ * (src/density_functionals.cpp:732-806; pbe_collinear, src/spin_pbe_xc.cpp:54-107). */
+SDFT_B200_API sdft_b200_status sdft_b200_collinear_functionals(
+    sdft_b200_context* context, const double lattice[9], size_t count_up, const int32_t* hkl_up, const double* up,
+    size_t count_down, const int32_t* hkl_down, const double* down, size_t core_count, const int32_t* core_hkl,
+    const double* core, int padding, int32_t* support_hkl, double* potential_up, double* potential_down,
+    double* xc_potential_up, double* xc_potential_down, size_t capacity, size_t* support_count,
+    sdft_b200_functionals result[2]);
+
 /* Rayleigh-Ritz eigensolve of a projected pencil in FP64: the lowest
  * `requested` (0 = all n) solutions of H y = e S y, H and S n x n Hermitian
  * (lower triangles referenced, column-major), S positive definite. values:

@@ -16,6 +16,7 @@
 //   paw_lm_moments_from_density         src/paw_augmentation.cpp:490-525
 //   PawCompensationOperator ctor/density_sum src/paw_compensation.cpp:185-342,465-524
 //   evaluate_density_functionals        src/density_functionals.cpp:462-729
+//   evaluate_collinear_density_functionals src/density_functionals.cpp:732-806
 // Complex arrays are interleaved (re, im) doubles, column-major blocks.
 #include "plane_wave_operator.hpp"
 #include "pw_core.hpp"
@@ -481,6 +482,75 @@ long ref_density_functionals(const double* lattice, long count, const int* keys,
       scalars[16 + 3 * a] = x.x;
       scalars[17 + 3 * a] = x.y;
       scalars[18 + 3 * a] = x.z;
+    }
+    return size;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return -1;
+  }
+}
+}
+
+extern "C" {
+
+// evaluate_collinear_density_functionals on up/down densities and an
+// optional frozen core. Returns the support size (map order) or -1 with the
+// error text; with capacity >= that size it writes the keys, per channel the
+// potential and xc_potential (up then down, capacity entries each) and
+// scalars[25 * channel + ...] in ref_density_functionals' order.
+long ref_collinear_functionals(const double* lattice, long count_up, const int* keys_up, const double* up,
+                               long count_down, const int* keys_down, const double* down, long core_count,
+                               const int* core_keys, const double* core, int padding, long capacity, int* out_keys,
+                               double* potential, double* xc_potential, double* scalars, char* error,
+                               long error_length) {
+  try {
+    std::array<sdft::Vec3, 3> cell{};
+    for (int r = 0; r < 3; ++r) cell[r] = {lattice[3 * r], lattice[3 * r + 1], lattice[3 * r + 2]};
+    std::array<sdft::FourierDensity, 2> density;
+    sdft::FourierDensity frozen;
+    const auto fill = [](sdft::FourierDensity& map, long count, const int* keys, const double* values) {
+      const auto* v = reinterpret_cast<const C*>(values);
+      for (long i = 0; i < count; ++i) map[{keys[3 * i], keys[3 * i + 1], keys[3 * i + 2]}] = v[i];
+    };
+    fill(density[0], count_up, keys_up, up);
+    fill(density[1], count_down, keys_down, down);
+    fill(frozen, core_count, core_keys, core);
+    const auto result = sdft::evaluate_collinear_density_functionals(density, cell, core_count ? &frozen : nullptr,
+                                                                      padding);
+    const long size = static_cast<long>(result[0].potential.size());
+    if (capacity < size) return size;
+    for (int s = 0; s < 2; ++s) {
+      long i = 0;
+      auto* po = reinterpret_cast<C*>(potential) + s * capacity;
+      auto* xo = reinterpret_cast<C*>(xc_potential) + s * capacity;
+      for (const auto& [key, value] : result[s].potential) {
+        if (s == 0) {
+          out_keys[3 * i] = std::get<0>(key);
+          out_keys[3 * i + 1] = std::get<1>(key);
+          out_keys[3 * i + 2] = std::get<2>(key);
+        }
+        po[i] = value;
+        const auto found = result[s].xc_potential.find(key);
+        xo[i] = found == result[s].xc_potential.end() ? C{} : found->second;
+        ++i;
+      }
+      double* o = scalars + 25 * s;
+      const auto& r = result[s];
+      o[0] = r.hartree_energy;
+      o[1] = r.xc_energy;
+      o[2] = r.vxc_density;
+      o[3] = r.sampled_electrons;
+      o[4] = r.minimum_density;
+      o[5] = static_cast<double>(r.clipped_density_points);
+      o[6] = static_cast<double>(r.grid_points);
+      for (int a = 0; a < 3; ++a) {
+        o[7 + 3 * a] = r.hartree_stress[a].x;
+        o[8 + 3 * a] = r.hartree_stress[a].y;
+        o[9 + 3 * a] = r.hartree_stress[a].z;
+        o[16 + 3 * a] = r.xc_stress[a].x;
+        o[17 + 3 * a] = r.xc_stress[a].y;
+        o[18 + 3 * a] = r.xc_stress[a].z;
+      }
     }
     return size;
   } catch (const std::exception& e) {

@@ -91,6 +91,10 @@ class ReferenceLibrary:
         L.ref_compensation_project.argtypes = [_dbl, ctypes.c_long, _dbl, ctypes.c_long, _int, ctypes.c_long, _int,
                                                ctypes.c_int, ctypes.c_long, _dbl, _dbl, _dbl, ctypes.c_long, _int,
                                                _dbl, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_collinear_functionals.restype = ctypes.c_long
+        L.ref_collinear_functionals.argtypes = [_dbl, ctypes.c_long, _int, _dbl, ctypes.c_long, _int, _dbl,
+                                                ctypes.c_long, _int, _dbl, ctypes.c_int, ctypes.c_long, _int, _dbl,
+                                                _dbl, _dbl, ctypes.c_char_p, ctypes.c_long]
         L.ref_density_functionals.restype = ctypes.c_long
         L.ref_density_functionals.argtypes = [_dbl, ctypes.c_long, _int, _dbl, ctypes.c_long, _int, _dbl,
                                               ctypes.c_int, ctypes.c_long, _int, _dbl, _dbl, _dbl, ctypes.c_char_p,
@@ -224,6 +228,49 @@ class ReferenceLibrary:
         out["hartree_stress"] = scalars[7:16].reshape(3, 3).copy()
         out["xc_stress"] = scalars[16:25].reshape(3, 3).copy()
         out.update({"hkl": out_keys, "potential": potential, "xc_potential": xc})
+        return out
+
+    def collinear_functionals(self, lattice, up_keys, up, down_keys, down, core_keys=None, core=None,
+                              padding: int = 0):
+        """evaluate_collinear_density_functionals (src/density_functionals.cpp:732-806):
+        {"hkl", "up": {...}, "down": {...}} with each channel's potential, xc_potential and scalars."""
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        arrays = []
+        for keys, values in ((up_keys, up), (down_keys, down),
+                             (core_keys if core_keys is not None else np.zeros((0, 3)),
+                              core if core is not None else np.zeros(0))):
+            arrays.append((np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3),
+                           np.ascontiguousarray(values, dtype=np.complex128).reshape(-1)))
+        args = [_ptr(lat)]
+        for k, v in arrays:
+            args += [k.shape[0], _ptr(k, _int), v.view(np.float64).ctypes.data_as(_dbl)]
+        args.append(int(padding))
+        err = ctypes.create_string_buffer(512)
+        scalars = np.zeros(50)
+        size = self.lib.ref_collinear_functionals(*args, 0, None, None, None, _ptr(scalars), err, 512)
+        if size < 0:
+            raise ValueError(err.value.decode(errors="replace"))
+        keys = np.zeros((size, 3), dtype=np.int32)
+        potential = np.zeros(2 * size, dtype=np.complex128)
+        xc = np.zeros(2 * size, dtype=np.complex128)
+        size = self.lib.ref_collinear_functionals(*args, size, _ptr(keys, _int),
+                                                  potential.view(np.float64).ctypes.data_as(_dbl),
+                                                  xc.view(np.float64).ctypes.data_as(_dbl), _ptr(scalars), err, 512)
+        if size < 0:
+            raise ValueError(err.value.decode(errors="replace"))
+        names = ("hartree_energy", "xc_energy", "vxc_density", "sampled_electrons", "minimum_density",
+                 "clipped_density_points", "grid_points")
+        out = {"hkl": keys}
+        for s, channel in enumerate(("up", "down")):
+            o = scalars[25 * s:25 * (s + 1)]
+            r = {name: float(o[i]) for i, name in enumerate(names)}
+            r["clipped_density_points"] = int(r["clipped_density_points"])
+            r["grid_points"] = int(r["grid_points"])
+            r["hartree_stress"] = o[7:16].reshape(3, 3).copy()
+            r["xc_stress"] = o[16:25].reshape(3, 3).copy()
+            r.update({"hkl": keys, "potential": potential[s * size:(s + 1) * size],
+                      "xc_potential": xc[s * size:(s + 1) * size]})
+            out[channel] = r
         return out
 
     def density(self, hkl, coefficients, occupations, volume, support_hkl):

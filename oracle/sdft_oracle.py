@@ -569,3 +569,216 @@ def density_functionals(lattice, keys, values, core_keys=None, core_values=None,
             "sampled_electrons": math.fsum(valence.ravel().tolist()) * weight,
             "minimum_density": float(raw.min()), "clipped_density_points": int((raw < 1e-10).sum()),
             "grid_points": points, "grid": shape}
+
+
+# --- Collinear spin PBE and functional (src/spin_pbe_xc.cpp:54-107,
+#     src/density_functionals.cpp:732-806) ------------------------------------
+
+class _D5:
+    """Value and derivatives in five variables (n_up, n_down, sigma_uu, sigma_ud, sigma_dd), per point."""
+
+    def __init__(self, v, g=None):
+        self.v = np.asarray(v, dtype=np.float64)
+        self.g = np.zeros(self.v.shape + (5,)) if g is None else g
+
+    @staticmethod
+    def variable(x, k):
+        d = _D5(x)
+        d.g[..., k] = 1.0
+        return d
+
+    @staticmethod
+    def lift(x):
+        return x if isinstance(x, _D5) else _D5(np.broadcast_to(np.asarray(x, dtype=np.float64), ()).copy())
+
+    def __add__(self, o):
+        o = _D5.lift(o)
+        return _D5(self.v + o.v, self.g + o.g)
+
+    __radd__ = __add__
+
+    def __sub__(self, o):
+        o = _D5.lift(o)
+        return _D5(self.v - o.v, self.g - o.g)
+
+    def __rsub__(self, o):
+        return _D5.lift(o) - self
+
+    def __neg__(self):
+        return _D5(0.0) - self
+
+    def __mul__(self, o):
+        o = _D5.lift(o)
+        return _D5(self.v * o.v, self.g * o.v[..., None] + self.v[..., None] * o.g)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        o = _D5.lift(o)
+        r = self.v / o.v
+        return _D5(r, (self.g - r[..., None] * o.g) / o.v[..., None])
+
+    def __rtruediv__(self, o):
+        return _D5.lift(o) / self
+
+    def pow(self, p):
+        r = np.power(self.v, p)
+        return _D5(r, (p * r / self.v)[..., None] * self.g)
+
+    def log1p(self):
+        return _D5(np.log1p(self.v), self.g / (1.0 + self.v)[..., None])
+
+    def expm1(self):
+        r = np.expm1(self.v)
+        return _D5(r, (1.0 + r)[..., None] * self.g)
+
+
+def _pw_spin(rs, a, alpha, b1, b2, b3, b4):
+    root = rs.pow(0.5)
+    poly = b1 * root + b2 * rs + b3 * rs * root + b4 * rs * rs
+    return -2 * a * (1 + alpha * rs) * (1 / (2 * a * poly)).log1p()
+
+
+def _spin_exchange(n, sigma):
+    doubled = 2 * n
+    root = doubled.pow(1.0 / 3.0)
+    kf = np.cbrt(3 * math.pi * math.pi) * root
+    denominator = 4 * kf * kf * doubled * doubled
+    numerator = 4 * (_PBE_MU / _PBE_KAPPA) * sigma
+    fx = 1 + _PBE_KAPPA * numerator / (denominator + numerator)
+    return -.375 * np.cbrt(3 / math.pi) * doubled * root * fx
+
+
+def pbe_collinear(up, down, gu, gd):
+    """(energy density, (v_up, v_down), gradient responses (2, N, 3)) of collinear PBE with
+    PW92 spin interpolation for densities up, down > 0 and gradients gu, gd (N, 3)
+    (src/spin_pbe_xc.cpp:54-107)."""
+    up = np.asarray(up, dtype=np.float64)
+    down = np.asarray(down, dtype=np.float64)
+    uu = gu[:, 0] * gu[:, 0] + gu[:, 1] * gu[:, 1] + gu[:, 2] * gu[:, 2]
+    ud = gu[:, 0] * gd[:, 0] + gu[:, 1] * gd[:, 1] + gu[:, 2] * gd[:, 2]
+    dd = gd[:, 0] * gd[:, 0] + gd[:, 1] * gd[:, 1] + gd[:, 2] * gd[:, 2]
+    nu, nd = _D5.variable(np.maximum(up, 1e-99), 0), _D5.variable(np.maximum(down, 1e-99), 1)
+    su, sud, sd = _D5.variable(uu, 2), _D5.variable(ud, 3), _D5.variable(dd, 4)
+    n = nu + nd
+    root = n.pow(1.0 / 3.0)
+    rs = np.cbrt(3 / (4 * math.pi)) / root
+    z = (nu - nd) / n
+    z.v = np.clip(z.v, -.9999999999999, .9999999999999)
+    z2 = z * z
+    z4 = z2 * z2
+    pu, pd = 1 + z, 1 - z
+    denominator = 0.5198420997897463295
+    fzz = 8 / (9 * denominator)
+    f = (pu.pow(4.0 / 3.0) + pd.pow(4.0 / 3.0) - 2) / denominator
+    eu = _pw_spin(rs, .0310907, .21370, 7.5957, 3.5876, 1.6382, .49294)
+    ep = _pw_spin(rs, .01554535, .20548, 14.1189, 6.1977, 3.3662, .62517)
+    alpha = -_pw_spin(rs, .0168869, .11125, 10.357, 3.6231, .88026, .49671)
+    ec = eu + alpha * f / fzz * (1 - z4) + (ep - eu) * f * z4
+    phi = .5 * (pu.pow(2.0 / 3.0) + pd.pow(2.0 / 3.0))
+    eta = 1e-12
+    gz = (np.power(pu.v * pu.v + eta, -1.0 / 6.0) - np.power(pd.v * pd.v + eta, -1.0 / 6.0)) / 3.0
+    phi.g = gz[..., None] * z.g
+    phi3 = phi * phi * phi
+    sigma = su + 2 * sud + sd
+    kf = np.cbrt(3 * math.pi * math.pi) * root
+    ks2 = 4 * kf / math.pi
+    t2 = sigma / (4 * phi * phi * ks2 * n * n)
+    a = (_PBE_BETA / _PBE_GAMMA) / (-ec / (_PBE_GAMMA * phi3)).expm1()
+    at = a * t2
+    h = _PBE_GAMMA * phi3 * ((_PBE_BETA / _PBE_GAMMA) * t2 * (1 + at) / (1 + at + at * at)).log1p()
+    ex = _spin_exchange(nu, su) + _spin_exchange(nd, sd)
+    total = ex + n * (ec + h)
+    g = total.g
+    response = np.stack([2 * g[:, 2:3] * gu + g[:, 3:4] * gd, 2 * g[:, 4:5] * gd + g[:, 3:4] * gu])
+    return total.v, (g[:, 0], g[:, 1]), response
+
+
+def collinear_functionals(lattice, up_keys, up_values, down_keys, down_values, core_keys=None, core_values=None,
+                          padding: int = 2, fast: bool = False) -> dict:
+    """The reference's evaluate_collinear_density_functionals in numpy: Hartree of the total
+    density split equally, per channel the XC fields of n_s + core/2 on the padded grid,
+    collinear PBE with the floors max(5e-11, n_s) (both raised to 5e-11 when n_up + n_down
+    < 1e-10), tile sums summed exactly, per channel v_xc,s = l_s - i q.d_s on the union
+    support and <n_s, v_xc,s>; returns {"hkl", "up": {...}, "down": {...}}."""
+    a = np.asarray(lattice, dtype=np.float64).reshape(3, 3)
+    det = float(np.dot(a[0], np.cross(a[1], a[2])))
+    volume = abs(det)
+    if not math.isfinite(volume) or volume < 1e-12 or len(up_keys) == 0 or len(down_keys) == 0:
+        raise ValueError("invalid collinear density/lattice")
+    b = 2.0 * math.pi / det * np.array([np.cross(a[1], a[2]), np.cross(a[2], a[0]), np.cross(a[0], a[1])])
+
+    def as_map(keys, values):
+        return {tuple(int(v) for v in k): complex(x) for k, x in zip(np.asarray(keys).reshape(-1, 3),
+                                                                      np.asarray(values).ravel())}
+
+    channels = [as_map(up_keys, up_values), as_map(down_keys, down_values)]
+    core = as_map(core_keys, core_values) if core_keys is not None else {}
+    total = dict(channels[0])
+    for k, v in channels[1].items():
+        total[k] = total.get(k, 0.0) + v
+    support = sorted(set(channels[0]) | set(channels[1]) | set(core))
+    sk = np.array(support, dtype=np.int64).reshape(-1, 3)
+    q = sk[:, 0:1] * b[0] + sk[:, 1:2] * b[1] + sk[:, 2:3] * b[2]
+    q2 = (q * q).sum(axis=1)
+    in_total = np.array([k in total for k in support])
+    rho_total = np.array([total.get(k, 0.0) for k in support], dtype=np.complex128)
+    coulomb = in_total & ~(q2 < 1e-12)
+    norm = rho_total.real ** 2 + rho_total.imag ** 2
+    hartree = np.where(coulomb, 4 * math.pi * rho_total / np.where(coulomb, q2, 1.0), 0.0)
+    eh = math.fsum((2 * math.pi * volume * norm[coulomb] / q2[coulomb]).tolist())
+    sh = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            sh[i, j] = math.fsum((4 * math.pi * norm[coulomb] * q[coulomb, i] * q[coulomb, j]
+                                  / (q2[coulomb] * q2[coulomb])).tolist())
+    sh -= np.eye(3) * (eh / volume)
+    m = np.abs(sk).max(axis=0)
+    shape = tuple(padding * max(3, 2 * int(v) + 1) for v in m)
+    if fast:
+        shape = tuple(fast_fft_length(v) for v in shape)
+    idx = tuple(np.mod(sk[:, a_], shape[a_]) for a_ in range(3))
+    fields = []
+    for s in range(2):
+        xc = np.array([channels[s].get(k, 0.0) + (0.5 * core[k] if k in core else 0.0) for k in support],
+                      dtype=np.complex128)
+        grids = np.zeros((4,) + shape, dtype=np.complex128)
+        grids[0][idx] = xc
+        for axis in range(3):
+            grids[axis + 1][idx] = 1j * q[:, axis] * xc
+        fields.append([backward_fft(g).real for g in grids])
+    raw = [fields[s][0].ravel() for s in range(2)]
+    grad = [np.stack([fields[s][1].ravel(), fields[s][2].ravel(), fields[s][3].ravel()], axis=1) for s in range(2)]
+    n = [raw[0].copy(), raw[1].copy()]
+    low = n[0] + n[1] < 1e-10
+    n[0] = np.where(low, np.maximum(n[0], 5e-11), n[0])
+    n[1] = np.where(low, np.maximum(n[1], 5e-11), n[1])
+    energy, potentials, response = pbe_collinear(np.maximum(5e-11, n[0]), np.maximum(5e-11, n[1]), grad[0], grad[1])
+    points = int(np.prod(shape))
+    pressure = energy.copy()
+    for s in range(2):
+        pressure = pressure - potentials[s] * raw[s]
+        for ax in range(3):
+            pressure = pressure - response[s][:, ax] * grad[s][:, ax]
+    stress = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            term = (pressure if i == j else 0.0) - response[0][:, i] * grad[0][:, j] - response[1][:, i] * grad[1][:, j]
+            stress[i, j] = math.fsum(np.ravel(term).tolist())
+    e_sum = math.fsum(energy.tolist())
+    where = {k: i for i, k in enumerate(support)}
+    out = {"hkl": sk.astype(np.int32)}
+    for s, name in enumerate(("up", "down")):
+        transforms = [forward_fft(f.reshape(shape))[idx] / points
+                      for f in (potentials[s], response[s][:, 0], response[s][:, 1], response[s][:, 2])]
+        vxc = transforms[0] - 1j * (q[:, 0] * transforms[1] + q[:, 1] * transforms[2] + q[:, 2] * transforms[3])
+        rho = channels[s]
+        vxc_density = math.fsum(volume * (rho[k] * vxc[where[(-k[0], -k[1], -k[2])]]).real
+                                for k in support if k in rho and (-k[0], -k[1], -k[2]) in where)
+        out[name] = {"hkl": sk.astype(np.int32), "potential": hartree + vxc, "xc_potential": vxc,
+                     "hartree_energy": .5 * eh, "hartree_stress": .5 * sh, "xc_energy": .5 * e_sum * volume / points,
+                     "xc_stress": .5 * stress / points, "vxc_density": vxc_density,
+                     "sampled_electrons": volume * rho[(0, 0, 0)].real if (0, 0, 0) in rho else 0.0,
+                     "minimum_density": float(raw[s].min()), "clipped_density_points": int((raw[s] < 0).sum()),
+                     "grid_points": points, "grid": shape}
+    return out

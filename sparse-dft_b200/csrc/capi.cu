@@ -568,6 +568,52 @@ sdft_b200_status sdft_b200_density_functionals(sdft_b200_context* context, const
   });
 }
 
+sdft_b200_status sdft_b200_collinear_functionals(
+    sdft_b200_context* context, const double lattice[9], size_t count_up, const int32_t* hkl_up, const double* up,
+    size_t count_down, const int32_t* hkl_down, const double* down, size_t core_count, const int32_t* core_hkl,
+    const double* core, int padding, int32_t* support_hkl, double* potential_up, double* potential_down,
+    double* xc_potential_up, double* xc_potential_down, size_t capacity, size_t* support_count,
+    sdft_b200_functionals result[2]) {
+  return guarded([&] {
+    require(lattice && support_count, "null density functional argument");
+    require((!count_up || (hkl_up && up)) && (!count_down || (hkl_down && down)), "null spin density arrays");
+    require(!core_count || (core_hkl && core), "null core arrays");
+    const std::size_t counts[2] = {count_up, count_down};
+    const int* const keys[2] = {hkl_up, hkl_down};
+    const double* const values[2] = {up, down};
+    const auto support =
+        sdft_b200::collinear_support(lattice, counts, keys, values, core_count, core_hkl, core, padding);
+    const std::size_t n = support.keys.size();
+    *support_count = n;
+    if (!capacity) return;
+    require(capacity >= n, "density functional output capacity below the support size");
+    require(context && support_hkl && potential_up && potential_down && xc_potential_up && xc_potential_down &&
+                result,
+            "null density functional outputs");
+    for (std::size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) support_hkl[3 * i + a] = support.keys[i][a];
+    using C = sdft_b200::Cx<double>;
+    C* const potential[2] = {reinterpret_cast<C*>(potential_up), reinterpret_cast<C*>(potential_down)};
+    C* const xc[2] = {reinterpret_cast<C*>(xc_potential_up), reinterpret_cast<C*>(xc_potential_down)};
+    sdft_b200::FunctionalResult r[2];
+    sdft_b200::collinear_functionals(*context->impl, support, potential, xc, r);
+    for (int c = 0; c < 2; ++c) {
+      result[c].hartree_energy = r[c].hartree_energy;
+      result[c].xc_energy = r[c].xc_energy;
+      result[c].vxc_density = r[c].vxc_density;
+      for (int k = 0; k < 9; ++k) {
+        result[c].hartree_stress[k] = r[c].hartree_stress[k];
+        result[c].xc_stress[k] = r[c].xc_stress[k];
+      }
+      result[c].sampled_electrons = r[c].sampled_electrons;
+      result[c].minimum_density = r[c].minimum_density;
+      result[c].clipped_density_points = r[c].clipped_density_points;
+      result[c].grid_points = r[c].grid_points;
+      for (int a = 0; a < 3; ++a) result[c].grid[a] = r[c].grid[a];
+    }
+  });
+}
+
 sdft_b200_status sdft_b200_rayleigh_ritz(sdft_b200_context* context, size_t n, size_t requested, const double* h,
                                         const double* s, double* values, double* vectors, int memory) {
   return guarded([&] {

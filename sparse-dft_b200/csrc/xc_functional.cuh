@@ -17,9 +17,10 @@ struct FunctionalSupport {
   bool with_core = false;
   int shape[3] = {0, 0, 0};
   long long points = 0;
+  bool collinear = false;                // two spin channels: valence = up, down = down
   std::vector<std::array<int, 3>> keys;  // sorted lexicographically
-  std::vector<Cx<double>> valence, core; // 0 where the key is absent
-  std::vector<unsigned char> flags;      // bit 0: density key, bit 1: core key
+  std::vector<Cx<double>> valence, core, down;  // 0 where the key is absent
+  std::vector<unsigned char> flags;      // bit 0: density (up) key, bit 1: core key, bit 2: down key
   std::vector<long long> index, opposite;  // wrapped grid index of +G, -G
   std::vector<int> opposite_key;           // union position of -G, or -1
   std::vector<double> q;                   // G per key, 3 values
@@ -47,5 +48,18 @@ FunctionalSupport functional_support(const double lattice[9], std::size_t count,
 // its order, into host arrays; the scalars into result.
 void density_functionals(Context& ctx, const FunctionalSupport& support, Cx<double>* potential,
                          Cx<double>* xc_potential, FunctionalResult& result);
+
+// Collinear spin form (the reference's evaluate_collinear_density_functionals,
+// src/density_functionals.hpp:52-56, src/density_functionals.cpp:732-806):
+// host checks and support (union of both channels and the core, which each
+// channel receives with weight 1/2), then per channel the potential
+// (Hartree of the total density + the channel's v_xc), v_xc and the scalars
+// (Hartree and XC energies and stresses split equally, <n_s, v_xc,s>,
+// electrons Omega Re n_s(0), minimum and count of negative samples).
+FunctionalSupport collinear_support(const double lattice[9], const std::size_t count[2], const int* const hkl[2],
+                                    const double* const density[2], std::size_t core_count, const int* core_hkl,
+                                    const double* core, int padding);
+void collinear_functionals(Context& ctx, const FunctionalSupport& support, Cx<double>* const potential[2],
+                           Cx<double>* const xc_potential[2], FunctionalResult result[2]);
 
 }  // namespace sdft_b200

@@ -144,6 +144,8 @@ def _declare(lib: ctypes.CDLL) -> None:
                                ctypes.POINTER(ctypes.c_int), ctypes.c_int])
     fn("sdft_b200_density_functionals", [P, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, SZ, SZP,
                                          ctypes.POINTER(Functionals)])
+    fn("sdft_b200_collinear_functionals", [P, D, SZ, I32, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, D, D,
+                                           SZ, SZP, ctypes.POINTER(Functionals)])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])

@@ -94,6 +94,51 @@ def density_functionals(context: Context | None, lattice, hkl, density, core_hkl
     return out
 
 
+def collinear_functionals(context: Context | None, lattice, up_hkl, up, down_hkl, down, core_hkl=None, core=None,
+                          padding: int = 0, support_only: bool = False):
+    """Collinear spin form of the functional on the device (the reference's
+    evaluate_collinear_density_functionals): the union support keys `hkl` and
+    per channel ("up", "down") a dict with `potential`, `xc_potential` and the
+    scalars; with support_only the keys alone (host only, context may be None)."""
+    lib = C.library()
+    lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+    channels = []
+    for keys, values in ((up_hkl, up), (down_hkl, down)):
+        k = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1, 3)
+        v = np.ascontiguousarray(values, dtype=np.complex128).reshape(-1)
+        if v.shape[0] != k.shape[0]:
+            raise ValueError("spin density keys and values disagree")
+        channels.append((k, v))
+    if core_hkl is not None:
+        ck = np.ascontiguousarray(core_hkl, dtype=np.int32).reshape(-1, 3)
+        cv = np.ascontiguousarray(core, dtype=np.complex128).reshape(-1)
+    else:
+        ck, cv = np.zeros((0, 3), dtype=np.int32), np.zeros(0, dtype=np.complex128)
+    handle = context.handle if context is not None else None
+    args = [lat.ctypes.data_as(C.D)]
+    for k, v in channels:
+        args += [k.shape[0], k.ctypes.data_as(C.I32), v.ctypes.data_as(C.D)]
+    args += [ck.shape[0], ck.ctypes.data_as(C.I32), cv.ctypes.data_as(C.D), int(padding)]
+    count = ctypes.c_size_t()
+    results = (C.Functionals * 2)()
+    C.check(lib.sdft_b200_collinear_functionals(handle, *args, None, None, None, None, None, 0, ctypes.byref(count),
+                                                results))
+    if support_only:
+        return _support_keys(np.concatenate([channels[0][0], channels[1][0]]), ck)
+    n = count.value
+    support = np.zeros((n, 3), dtype=np.int32)
+    arrays = [np.zeros(n, dtype=np.complex128) for _ in range(4)]
+    C.check(lib.sdft_b200_collinear_functionals(handle, *args, support.ctypes.data_as(C.I32),
+                                                *[a.ctypes.data_as(C.D) for a in arrays], n, ctypes.byref(count),
+                                                results))
+    out = {"hkl": support}
+    for c, name in enumerate(("up", "down")):
+        channel = results[c].as_dict()
+        channel.update({"hkl": support, "potential": arrays[c], "xc_potential": arrays[2 + c]})
+        out[name] = channel
+    return out
+
+
 def _support_keys(keys, core_keys) -> np.ndarray:
     """Union of the key sets in lexicographic order (the library's support order)."""
     union = {tuple(int(v) for v in k) for k in keys} | {tuple(int(v) for v in k) for k in core_keys}

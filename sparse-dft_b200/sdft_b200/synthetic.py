@@ -428,6 +428,22 @@ def functional_case(name: str) -> dict:
             "core_keys": core_keys, "core_values": gaussian_density(lattice, positions, core_keys, 2.0, 0.8)}
 
 
+def collinear_case(name: str) -> dict:
+    """Spin-polarised inputs of the collinear functional on functional_case's cells: the up
+    channel carries 2.4 electrons per site (width 1.2), the down channel 1.6 on keys one
+    shell narrower in h (width 1.4), the frozen core as in functional_case."""
+    case = functional_case(name)
+    lattice, keys = case["lattice"], case["keys"]
+    if name == "triclinic":
+        positions = np.array([[0.0, 0.0, 0.0], [0.25, 0.25, 0.3]])
+    else:
+        positions, _ = zincblende_sites({"si8": 1, "si64": 2}[name])
+    down_keys = np.ascontiguousarray(keys[np.abs(keys[:, 0]) < np.abs(keys[:, 0]).max()], dtype=np.int32)
+    return {"lattice": lattice, "up_keys": keys, "up": gaussian_density(lattice, positions, keys, 2.4, 1.2),
+            "down_keys": down_keys, "down": gaussian_density(lattice, positions, down_keys, 1.6, 1.4),
+            "core_keys": case["core_keys"], "core_values": case["core_values"]}
+
+
 def band_coefficients(inputs: OperatorInputs, bands: int, seed: int = 31) -> np.ndarray:
     """Seeded normalised band-major plane-wave coefficients, (bands, npw) complex128,
     with a kinetic decay so that the bands look like smooth valence states."""

@@ -203,6 +203,26 @@ def functional_fixtures(lib):
         print("functional", name, "support", fields["core_hkl"].shape[0], "grid points", int(fields["plain_grid_points"]))
 
 
+def collinear_fixtures(lib):
+    """Reference evaluate_collinear_density_functionals (src/density_functionals.cpp:732-806)
+    of synthetic.collinear_case, without and with the frozen core: support keys
+    and per channel the potential, xc_potential and scalars."""
+    for name in ("si8", "triclinic"):
+        case = synthetic.collinear_case(name)
+        fields = {}
+        for label, core in (("plain", False), ("core", True)):
+            kw = {"core_keys": case["core_keys"], "core": case["core_values"]} if core else {}
+            out = lib.collinear_functionals(case["lattice"], case["up_keys"], case["up"], case["down_keys"],
+                                            case["down"], **kw)
+            fields[f"{label}_hkl"] = out["hkl"]
+            for channel in ("up", "down"):
+                for key, value in out[channel].items():
+                    if key != "hkl":
+                        fields[f"{label}_{channel}_{key}"] = np.asarray(value)
+        np.savez_compressed(HERE / f"collinear_{name}.npz", **fields)
+        print("collinear", name, "support", fields["core_hkl"].shape[0])
+
+
 KPOINT_MESH = {"gaas_k13": (0.0, 1.0 / 3.0, 1.0 / 3.0), "gaas_k26": (1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)}
 
 
@@ -220,6 +240,7 @@ def main():
     parser.add_argument("--snapshots", action="store_true", help="only the solver snapshot fixtures")
     parser.add_argument("--projection", action="store_true", help="only the compensation projection fixture")
     parser.add_argument("--functional", action="store_true", help="only the Hartree + XC functional fixtures")
+    parser.add_argument("--collinear", action="store_true", help="only the collinear spin functional fixtures")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
@@ -234,6 +255,9 @@ def main():
     if args.functional:
         functional_fixtures(lib)
         return
+    if args.collinear:
+        collinear_fixtures(lib)
+        return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)
     pbe_fixture(lib)
@@ -244,6 +268,7 @@ def main():
     snapshot_fixtures(lib)
     compensation_project_fixture(lib, synthetic.si8(), "si8", 2.0)
     functional_fixtures(lib)
+    collinear_fixtures(lib)
     if args.si64:
         inputs = synthetic.si64()
         op = ref_oracle.ReferenceOperator(lib, inputs)
