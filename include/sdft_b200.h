@@ -367,6 +367,20 @@ SDFT_B200_API sdft_b200_status sdft_b200_rmm_trial(sdft_b200_operator* op, const
                                                    double* residuals, sdft_b200_davidson_stats* stats,
                                                    int* trial_manifold, int memory);
 
+/* Band-group solve: groups of SDFT_BAND_GROUP_SIZE (default 8) bands solved
+ * in turn by local Davidson solves (capacity 5 x group size) deflated
+ * against the S-orthonormalised completed bands, then a roots x roots
+ * Rayleigh-Ritz rotation of the whole block and fresh FP64 residuals; two
+ * sweeps, or with SDFT_BAND_GROUP_SWEEP=1 3-iteration local searches within
+ * half the budget and a global Davidson solve for the rest. initial: band-major
+ * roots x npw warm vectors or NULL. Returns OK with stats->converged = 0 when
+ * the sweeps end uncertified, as the reference does.
+ * Replaces: solve_generalized_hermitian_band_groups, src/pw_core.hpp:179-182
+ * (src/band_group_solver.cpp:55-212; SDFT_BAND_GROUP_SOLVER=1, src/pw_core.cpp:564-567). */
+SDFT_B200_API sdft_b200_status sdft_b200_band_groups(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                                     const double* initial, double* eigenvalues, double* eigenvectors,
+                                                     double* residuals, sdft_b200_davidson_stats* stats, int memory);
+
 /* ---- Solver snapshots ------------------------------------------------------
  * The reference's SDFTPWO3 files (PlaneWaveOperator::save_solver_snapshot,
  * src/plane_wave_operator.cpp:542-569; replayed by sdft_solver_replay):

@@ -8,6 +8,7 @@
 //   hamiltonian()/overlap() callbacks   src/plane_wave_operator.cpp:672-719
 //   solve_generalized_hermitian_davidson src/pw_core.cpp:532-1437
 //   solve_generalized_hermitian_rmm_trial src/rmm_trial.cpp:128-206
+//   solve_generalized_hermitian_band_groups src/band_group_solver.cpp:55-212
 //   kinetic_preconditioner              src/pw_core.cpp:33-47
 //   save/load_solver_snapshot           src/plane_wave_operator.cpp:542-653
 //   plane_wave_density_fft              src/density_functionals.cpp:407-460
@@ -208,6 +209,31 @@ int ref_rmm_trial(void* handle, long roots, long max_iterations, double toleranc
     *converged = result.converged ? 1 : 0;
     *iterations = static_cast<long>(result.iterations);
     *trial_manifold = result.trial_manifold ? 1 : 0;
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
+// solve_generalized_hermitian_band_groups (src/band_group_solver.cpp:55-212).
+int ref_band_groups(void* handle, long roots, long max_iterations, double tolerance, const double* initial,
+                    double* eigenvalues, double* vectors, double* residuals, int* converged, long* iterations,
+                    char* error, long error_length) {
+  try {
+    auto* h = static_cast<Handle*>(handle);
+    auto ham = h->op->hamiltonian();
+    auto ovl = h->op->overlap();
+    std::vector<C> warm;
+    if (initial) warm.assign(reinterpret_cast<const C*>(initial), reinterpret_cast<const C*>(initial) + roots * ham.dimension);
+    const auto result = sdft::solve_generalized_hermitian_band_groups(ham, ovl, static_cast<std::size_t>(roots),
+                                                                      static_cast<std::size_t>(max_iterations),
+                                                                      tolerance, warm);
+    std::copy(result.eigenvalues.begin(), result.eigenvalues.end(), eigenvalues);
+    std::copy(result.residual_norms.begin(), result.residual_norms.end(), residuals);
+    std::memcpy(vectors, result.eigenvectors.data(), result.eigenvectors.size() * sizeof(C));
+    *converged = result.converged ? 1 : 0;
+    *iterations = static_cast<long>(result.iterations);
     return 0;
   } catch (const std::exception& e) {
     set_error(error, error_length, e);

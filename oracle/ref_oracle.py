@@ -64,6 +64,10 @@ class ReferenceLibrary:
         L.ref_rmm_trial.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl, _dbl,
                                     _dbl, ctypes.POINTER(ctypes.c_int), _long, ctypes.POINTER(ctypes.c_int),
                                     ctypes.c_char_p, ctypes.c_long]
+        L.ref_band_groups.restype = ctypes.c_int
+        L.ref_band_groups.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl,
+                                      _dbl, _dbl, ctypes.POINTER(ctypes.c_int), _long, ctypes.c_char_p,
+                                      ctypes.c_long]
         L.ref_kinetic_preconditioner.restype = ctypes.c_double
         L.ref_kinetic_preconditioner.argtypes = [ctypes.c_double, ctypes.c_double]
         L.ref_save_snapshot.restype = ctypes.c_int
@@ -368,6 +372,19 @@ class ReferenceOperator:
         if initial is not None:
             init = np.ascontiguousarray(initial, dtype=np.complex128)
         self._call(self.lib.lib.ref_davidson, self.handle, roots, max_iterations, tolerance,
+                   init.ctypes.data_as(_dbl) if init is not None else None, _ptr(eig), vec.ctypes.data_as(_dbl),
+                   _ptr(res), ctypes.byref(conv), ctypes.byref(iters))
+        return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),
+                "iterations": int(iters.value)}
+
+    def band_groups(self, roots, max_iterations=256, tolerance=1e-10, initial=None):
+        """solve_generalized_hermitian_band_groups (src/band_group_solver.cpp:55-212)."""
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        vec = np.zeros((roots, self.n), dtype=np.complex128)
+        conv, iters = ctypes.c_int(0), ctypes.c_long(0)
+        init = None if initial is None else np.ascontiguousarray(initial, dtype=np.complex128)
+        self._call(self.lib.lib.ref_band_groups, self.handle, roots, max_iterations, tolerance,
                    init.ctypes.data_as(_dbl) if init is not None else None, _ptr(eig), vec.ctypes.data_as(_dbl),
                    _ptr(res), ctypes.byref(conv), ctypes.byref(iters))
         return {"eigenvalues": eig, "eigenvectors": vec, "residuals": res, "converged": bool(conv.value),

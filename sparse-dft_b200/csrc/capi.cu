@@ -10,6 +10,7 @@
 #include "dense.cuh"
 #include "eigensolver.cuh"
 #include "band_density.cuh"
+#include "band_groups.cuh"
 #include "paw_density.cuh"
 #include "operator.cuh"
 #include "rmm_trial.cuh"
@@ -23,6 +24,7 @@ struct sdft_b200_operator {
   std::unique_ptr<sdft_b200::DeviceOperator> impl;
   std::unique_ptr<sdft_b200::DavidsonSolver> solver;  // workspace reused across solves
   std::unique_ptr<sdft_b200::RmmTrial> rmm;
+  std::unique_ptr<sdft_b200::BandGroupSolver> groups;
 };
 
 struct sdft_b200_compensation {
@@ -771,6 +773,52 @@ sdft_b200_status sdft_b200_rmm_trial(sdft_b200_operator* op, const sdft_b200_dav
     if (trial_manifold) *trial_manifold = result.trial_manifold ? 1 : 0;
     if (stats) {
       sdft_b200::DavidsonStats st = result.fell_back ? result.fallback_stats : sdft_b200::DavidsonStats{};
+      st.iterations = result.iterations;
+      st.converged = result.converged;
+      st.max_residual = result.residuals.empty() ? 0.0
+                                                 : *std::max_element(result.residuals.begin(), result.residuals.end());
+      copy_stats(st, stats);
+    }
+  });
+}
+
+sdft_b200_status sdft_b200_band_groups(sdft_b200_operator* op, const sdft_b200_davidson_options* options,
+                                       const double* initial, double* eigenvalues, double* eigenvectors,
+                                       double* residuals, sdft_b200_davidson_stats* stats, int memory) {
+  return guarded([&] {
+    require(op && options && eigenvalues && residuals, "invalid bounded band-group problem");
+    require(memory == SDFT_B200_MEMORY_HOST || memory == SDFT_B200_MEMORY_DEVICE, "memory must be host or device");
+    auto& o = *op->impl;
+    auto& ctx = o.context();
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid bounded band-group problem");
+    require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid bounded band-group problem");
+    sdft_b200::DavidsonOptions d;
+    d.roots = static_cast<int>(options->roots);
+    d.max_iterations = static_cast<int>(options->max_iterations);
+    d.tolerance = options->tolerance;
+    d.precision = precision_of(options->precision);
+    d.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
+    d.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    const std::size_t block = static_cast<std::size_t>(o.npw()) * d.roots;
+    const Cx<double>* warm = nullptr;
+    if (initial) {
+      Staged stage(ctx, memory);
+      warm = stage.in(initial, block, ctx.staging_in);
+    }
+    if (!op->solver) op->solver = std::make_unique<sdft_b200::DavidsonSolver>(o);
+    if (!op->groups) op->groups = std::make_unique<sdft_b200::BandGroupSolver>(o, *op->solver);
+    const auto result = op->groups->solve(d, warm);
+    std::copy(result.eigenvalues.begin(), result.eigenvalues.end(), eigenvalues);
+    std::copy(result.residuals.begin(), result.residuals.end(), residuals);
+    if (eigenvectors) {
+      SDFT_CUDA(cudaMemcpyAsync(eigenvectors, op->groups->vectors(), sizeof(Cx<double>) * block,
+                                memory == SDFT_B200_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                ctx.stream));
+      ctx.synchronize();
+    }
+    if (stats) {
+      sdft_b200::DavidsonStats st;
       st.iterations = result.iterations;
       st.converged = result.converged;
       st.max_residual = result.residuals.empty() ? 0.0

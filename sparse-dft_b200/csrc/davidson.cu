@@ -122,6 +122,17 @@ void DavidsonSolver::apply_pair(const Cx<double>* x, int cols, Cx<double>* hy, C
   (exact ? stats_.s_columns_fp64 : stats_.s_columns_search) += cols;
 }
 
+// vectors -= E (SE^H vectors) for the completed bands E of a band-group local
+// solve, FP64 (the reference's remove_excluded, src/pw_core.cpp:701-712).
+// The coefficients use the region after the S images that solve() reserved
+// (excluded_count x max(excluded_count, kmax) entries; cols <= kmax).
+void DavidsonSolver::remove_excluded(Cx<double>* vectors, int cols) {
+  if (cols > std::max(excluded_count_, kmax_)) throw InvalidArgument("completed-band projection block too wide");
+  Cx<double>* coefficients = excluded_s_ + static_cast<std::size_t>(n_) * excluded_count_;
+  gemm(Op::C, excluded_count_, cols, n_, excluded_s_, n_, vectors, n_, coefficients, excluded_count_, false, 1.0, true);
+  gemm(Op::N, n_, cols, excluded_count_, excluded_, n_, coefficients, excluded_count_, vectors, n_, true, -1.0, true);
+}
+
 // One direction at a time (src/pw_core.cpp:796-853): CGS2 in the S metric with
 // FP64 operators, reject norm^2 < 1e-24.
 bool DavidsonSolver::append_single(const Cx<double>* source) {
@@ -137,7 +148,9 @@ bool DavidsonSolver::append_single(const Cx<double>* source) {
   if (!std::isfinite(norm)) throw std::runtime_error("nonfinite Davidson direction");
   if (norm == 0) return false;
   unit_columns(v, n_, n_, 1, dsmall_, st);
-  for (int pass = 0; pass < 2 && size_; ++pass) {
+  for (int pass = 0; pass < 2 && (size_ || excluded_count_); ++pass) {
+    if (excluded_count_) remove_excluded(v, 1);
+    if (!size_) continue;
     apply_s(v, 1, sv, true);
     gemm(Op::C, size_, 1, n_, v_, n_, sv, n_, proj, size_, false, 1.0, true);
     gemm(Op::N, n_, 1, size_, v_, n_, proj, size_, v, n_, true, -1.0, true);
@@ -180,7 +193,15 @@ bool DavidsonSolver::append_block(Cx<double>* vectors, int k) {
   Cx<double>* proj = as<Cx<double>>(projections_, static_cast<std::size_t>(capacity_) * kmax_);
   copy_block(vectors, n_, original, n_, n_, k, st);
   apply_s(vectors, k, metric, exact);
-  for (int pass = 0; size_ && pass < 2; ++pass) {
+  for (int pass = 0; (size_ || excluded_count_) && pass < 2; ++pass) {
+    if (excluded_count_) {
+      remove_excluded(vectors, k);
+      if (!size_) {
+        apply_s(vectors, k, metric, exact);
+        continue;
+      }
+      apply_s(vectors, k, metric, exact);
+    }
     if (!exact && searching()) {
       const PackedA vh = basis_rows(0, size_);
       gemm_tc(Op::C, size_, k, n_, nullptr, 0, &vh, metric, n_, proj, size_, false, 1.0, split_, ctx.tc, st);
@@ -371,7 +392,10 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
     if (!std::isfinite(op_.h_diagonal()[i]) || !std::isfinite(op_.s_diagonal()[i]) || op_.s_diagonal()[i] <= 0)
       throw InvalidArgument("invalid Davidson operator diagonal");
   tolerance_ = o.tolerance;
-  capacity_ = std::min(n_, std::max(o.subspace_factor * roots_, 64));
+  capacity_ = o.capacity > 0 ? std::min(n_, o.capacity) : std::min(n_, std::max(o.subspace_factor * roots_, 64));
+  if (o.excluded_count < 0 || (o.excluded_count && !o.excluded) || o.excluded_count + roots_ > n_ ||
+      capacity_ < roots_)
+    throw InvalidArgument("invalid matrix-free Davidson problem");
   const bool warm = initial != nullptr && 2 * roots_ < n_;
   const int guard_count = std::min(n_, 2 * roots_);
   kmax_ = std::min(capacity_, std::max(3 * roots_, 2));
@@ -380,7 +404,7 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
   if (packs_) {
     split_ = search_split();
     ld_rows_ = expanded_k(n_, split_);
-    ld_cols_ = expanded_k(std::min(n_, std::max(o.subspace_factor * o.roots, 64)), split_);
+    ld_cols_ = expanded_k(capacity_, split_);
   }
   incremental_ = o.tolerance >= 1e-12;
   strict_projection_ = false;
@@ -410,6 +434,21 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
     for (Scratch* s : {&pack_vn_, &pack_hn_, &pack_sn_}) SDFT_CUDA(cudaMemsetAsync(s->reserve(cols_bytes), 0, cols_bytes, st));
   }
   int* dselect = as<int>(select_, static_cast<std::size_t>(std::max(n_, roots_)));
+  // Completed bands of a band-group local solve: their S images (FP64) and
+  // the S-orthonormality the reference requires (src/pw_core.cpp:675-700).
+  excluded_count_ = o.excluded_count;
+  excluded_ = o.excluded;
+  if (excluded_count_) {
+    const std::size_t ne = static_cast<std::size_t>(n_) * excluded_count_;
+    excluded_s_ = as<Cx<double>>(b_.excluded, ne + static_cast<std::size_t>(excluded_count_) *
+                                                       std::max(excluded_count_, kmax_));
+    op_.apply_overlap(excluded_, excluded_count_, excluded_s_, Precision::FP64);
+    Cx<double>* gram = excluded_s_ + ne;
+    zgemm(ctx.blas, Op::C, Op::N, excluded_count_, excluded_count_, n_, excluded_, n_, excluded_s_, n_, gram,
+          excluded_count_, false);
+    if (identity_deviation(gram, excluded_count_, eigen_, st) > 1e-10)
+      throw InvalidArgument("completed bands must be S orthonormal");
+  }
 
   // Seeds (src/pw_core.cpp:1016-1112): warm vectors (perturbed) + 2*roots
   // canonical guards on the lowest H/S diagonal ratios, each with full support.

@@ -15,6 +15,13 @@ struct DavidsonOptions {
   Precision precision = Precision::FP64;  // search precision; certification is always FP64
   int subspace_factor = 8;                // capacity = min(n, max(factor*roots, 64)), in [4,16]
   double handoff = 1e-8;                  // search residual that hands the basis to FP64
+  // Band-group local solves (src/band_group_solver.cpp:95-107): an explicit
+  // subspace capacity (0 = the factor rule) and completed lower bands, device
+  // n x excluded_count, S-orthonormal, projected out of every search
+  // direction (the reference's excluded_vectors, src/pw_core.cpp:675-712).
+  int capacity = 0;
+  const Cx<double>* excluded = nullptr;
+  int excluded_count = 0;
 };
 
 struct DavidsonStats {
@@ -68,6 +75,7 @@ class DavidsonSolver {
   PackedA left_factor(const std::uint16_t* base, int k) const;      // n x k left factor (V, HV or SV)
   void gemm_left(const std::uint16_t* packed, int n, int k, const Cx<double>* b, long long ldb, Cx<double>* c,
                  long long ldc, bool add, double alpha);
+  void remove_excluded(Cx<double>* vectors, int cols);
   void rayleigh_ritz();
   void certify();
   void refresh_images();
@@ -77,6 +85,9 @@ class DavidsonSolver {
   DavidsonStats stats_;
   int n_ = 0, roots_ = 0, capacity_ = 0, kmax_ = 0;
   int size_ = 0, computed_h_ = 0, projected_size_ = 0;
+  const Cx<double>* excluded_ = nullptr;  // completed bands of a band-group local solve
+  Cx<double>* excluded_s_ = nullptr;      // their S images
+  int excluded_count_ = 0;
   bool exact_mode_ = true, incremental_ = true, strict_projection_ = false;
   double tolerance_ = 1e-10;
   DavidsonBuffers& b_;

@@ -178,7 +178,8 @@ void DavidsonBuffers::release() {
   for (Scratch* s : {&basis, &hbasis, &sbasis, &cached_h, &cached_s, &rr_a, &rr_b, &rr_w, &rr_work, &info,
                      &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
                      &eigen.solver_work, &xs, &sxs, &hxs, &res, &block, &metric, &original, &projections, &gram,
-                     &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb})
+                     &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb,
+                     &excluded})
     s->release();
 }
 

@@ -58,6 +58,7 @@ struct DavidsonBuffers {
   EigenWorkspace eigen;
   Scratch xs, sxs, hxs, res, block, metric, original, projections, gram, small, order, select;
   Scratch pack_vc, pack_vn, pack_hn, pack_sn, pack_hb, pack_sb;
+  Scratch excluded;  // S images and projections of a band-group solve's completed bands
   void release();
 };
 

@@ -142,6 +142,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_operator_update", [P, SZ, I32, D, D, D])
     fn("sdft_b200_rmm_trial", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
                                ctypes.POINTER(ctypes.c_int), ctypes.c_int])
+    fn("sdft_b200_band_groups", [P, ctypes.POINTER(DavidsonOptions), P, D, P, D, ctypes.POINTER(DavidsonStats),
+                                 ctypes.c_int])
     fn("sdft_b200_density_functionals", [P, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, SZ, SZP,
                                          ctypes.POINTER(Functionals)])
     fn("sdft_b200_collinear_functionals", [P, D, SZ, I32, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, D, D,

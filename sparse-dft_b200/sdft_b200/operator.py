@@ -293,6 +293,25 @@ class PlaneWaveOperator:
         return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
                 "iterations": int(info["iterations"]), "trial_manifold": bool(manifold.value), "stats": info}
 
+    def band_groups(self, roots: int, max_iterations: int = 256, tolerance: float = 1e-10, precision="fp64",
+                    initial=None, subspace_factor: int = 8, handoff: float = 1e-8):
+        """Band-group solve (the reference's solve_generalized_hermitian_band_groups):
+        the Davidson result dict."""
+        opts = C.DavidsonOptions(roots=roots, max_iterations=max_iterations, tolerance=tolerance,
+                                 precision=_precision(precision), subspace_factor=subspace_factor, handoff=handoff)
+        stats = C.DavidsonStats()
+        eig = np.zeros(roots)
+        res = np.zeros(roots)
+        keep = None if initial is None else np.ascontiguousarray(initial, dtype=np.complex128).reshape(roots, self.npw)
+        vec = np.zeros((roots, self.npw), dtype=np.complex128)
+        C.check(self._lib.sdft_b200_band_groups(self.handle, ctypes.byref(opts),
+                                                None if keep is None else ctypes.c_void_p(keep.ctypes.data),
+                                                _dptr(eig), ctypes.c_void_p(vec.ctypes.data), _dptr(res),
+                                                ctypes.byref(stats), C.HOST))
+        info = stats.as_dict()
+        return {"eigenvalues": eig, "residuals": res, "eigenvectors": vec, "converged": bool(info["converged"]),
+                "iterations": int(info["iterations"]), "stats": info}
+
 
 def complex_gemm(context: Context, a, b, adjoint_a: bool = False, precision="fp64", c=None):
     """C = op(A) B (+ c when given), the reference's complex_gemm (host arrays).
