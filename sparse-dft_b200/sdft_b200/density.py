@@ -1,6 +1,10 @@
 """Density-side entry points of the C ABI: PBE per point, band density,
-one-centre occupations. Host numpy arrays in, numpy out; all arithmetic on
-the device."""
+one-centre occupations, compensation charge and its adjoint, the Hartree +
+XC functionals. Host numpy arrays in, numpy out; all arithmetic on the
+device. With torch CUDA tensors the calls are ordered on the context's
+stream only: a caller whose tensors come from another stream synchronises
+that stream before the call and the context after it (or builds the context
+on its torch stream)."""
 from __future__ import annotations
 
 import ctypes

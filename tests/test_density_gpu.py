@@ -123,7 +123,10 @@ def test_band_density_config_size_properties(context):
     position = {tuple(k): i for i, k in enumerate(support.tolist())}
     mirror = np.array([position[(-h, -k, -l)] for h, k, l in support.tolist()])
     assert np.max(np.abs(out[mirror] - np.conj(out))) < 1e-15 * np.max(np.abs(out)) * 1e3
-    device = density.band_density(context, x.hkl, torch.from_numpy(coefficients).cuda(), occ, x.volume, support)
+    coefficients_device = torch.from_numpy(coefficients).cuda()
+    torch.cuda.synchronize()  # the context runs on its own stream: inputs ready before the call
+    device = density.band_density(context, x.hkl, coefficients_device, occ, x.volume, support)
+    context.synchronize()     # and the result complete before torch reads it
     assert np.array_equal(device.cpu().numpy(), out)
 
 
@@ -229,7 +232,10 @@ def test_compensation_si64_f16_matches_oracle_and_device_path(context):
     sub = slice(0, None, 97)  # oracle on a strided subset of the keys
     expected = sdft_oracle.compensation_density(x.lattice, x.positions, keys[sub], aug, transform, onsite)
     assert relative_error(out[sub], expected) < 1e-12
-    device = charge.density(torch.from_numpy(onsite).cuda())
+    onsite_device = torch.from_numpy(onsite).cuda()
+    torch.cuda.synchronize()
+    device = charge.density(onsite_device)
+    context.synchronize()
     assert np.array_equal(device.cpu().numpy(), out)
     # n(-G) = conj n(G) for a Hermitian occupation.
     position = {tuple(k): i for i, k in enumerate(keys.tolist())}
@@ -278,7 +284,10 @@ def test_compensation_projection_matches_reference_fixture(context, golden):
     v = _potential_on_support(keys, g["potential_keys"], g["potential"])
     out = charge.project(v)
     assert relative_error(out, g["projection"]) < 1e-12
-    device = charge.project(torch.from_numpy(v).cuda())
+    v_device = torch.from_numpy(v).cuda()
+    torch.cuda.synchronize()
+    device = charge.project(v_device)
+    context.synchronize()
     assert np.array_equal(device.cpu().numpy(), out)
     charge.close()
 

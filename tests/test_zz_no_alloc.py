@@ -30,7 +30,9 @@ def si8_operator():
 def _device_block(npw, columns, seed):
     import torch
     x = probe_block(npw, columns, seed)
-    return torch.from_numpy(x.T.copy()).cuda().T  # column-major, ld npw
+    block = torch.from_numpy(x.T.copy()).cuda().T  # column-major, ld npw
+    torch.cuda.synchronize()  # the context runs on its own stream
+    return block
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -68,6 +70,7 @@ def test_noalloc_rejects_blocks_beyond_the_static_array(si8_operator):
     columns = 1000  # ~1 GB of FP64 slab for Si8, far above 32 MiB
     x = torch.zeros((columns, op.npw), dtype=torch.complex128, device="cuda").T
     y = torch.empty_like(x.T).T
+    torch.cuda.synchronize()
     with pytest.raises(_capi.InvalidArgument, match="static scratch; at most [0-9]+ columns"):
         op.local_apply_noalloc(x, y, precision="fp64")
     small = _device_block(op.npw, 2, 6)
