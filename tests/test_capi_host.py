@@ -171,3 +171,37 @@ def test_functional_support_query_and_checks_are_host_only(golden):
     fails("pseudo-core", ck=core_keys, cv=bad_core)
     fails("quadrature", padding=9)
     fails("above 512", k=np.array([[300, 0, 0], [0, 0, 0]]), v=np.array([0.1, 1.0]))
+
+
+def test_solver_routes_check_handles_without_a_gpu():
+    """The RMM trial and the band-group solve reject a null operator before
+    any device work."""
+    lib = C.library()
+    opts = C.DavidsonOptions(roots=4, max_iterations=8, tolerance=1e-6, precision=C.FP64, subspace_factor=8,
+                             handoff=1e-8)
+    values = np.zeros(4)
+    residuals = np.zeros(4)
+    assert lib.sdft_b200_rmm_trial(None, ctypes.byref(opts), None, values.ctypes.data_as(C.D), None,
+                                   residuals.ctypes.data_as(C.D), None, None, C.HOST) == C.INVALID_ARGUMENT
+    assert "RMM" in C.last_error()
+    assert lib.sdft_b200_band_groups(None, ctypes.byref(opts), None, values.ctypes.data_as(C.D), None,
+                                     residuals.ctypes.data_as(C.D), None, C.HOST) == C.INVALID_ARGUMENT
+    assert "band-group" in C.last_error()
+
+
+def test_collinear_support_query_and_checks_are_host_only(golden):
+    """The collinear form's support query runs on the host with no context and
+    equals the reference's support; its input checks fail before device work."""
+    from sdft_b200 import density
+    case = synthetic.collinear_case("triclinic")
+    args = (case["lattice"], case["up_keys"], case["up"], case["down_keys"], case["down"], case["core_keys"],
+            case["core_values"])
+    keys = density.collinear_functionals(None, *args, support_only=True)
+    assert np.array_equal(keys, golden("collinear_triclinic")["core_hkl"])
+    with pytest.raises(C.InvalidArgument, match="invalid collinear density/lattice"):
+        density.collinear_functionals(None, np.zeros((3, 3)), *args[1:], support_only=True)
+    with pytest.raises(C.InvalidArgument, match="invalid collinear density/lattice"):
+        density.collinear_functionals(None, case["lattice"], case["up_keys"], case["up"], np.zeros((0, 3)),
+                                      np.zeros(0), support_only=True)
+    with pytest.raises(C.InvalidArgument, match="invalid collinear XC padding"):
+        density.collinear_functionals(None, *args, padding=9, support_only=True)
