@@ -349,8 +349,9 @@ def density_side(ctx, inputs, stream, peak):
     timed call each after a warm-up call (CUDA events on the library's stream):
     band density of 128 occupied bands (f_n = 2) on the supports f = 4, 8, 16;
     the compensation charge of 64 atoms on the f = 16 support from the one-centre
-    occupations of 128 bands; PBE on every point of the f = 16 density grid.
-    GB/s use the scope table's algorithmic bytes."""
+    occupations of 128 bands; PBE on every point of the f = 16 density grid;
+    the Hartree + PBE functionals (spin-unpolarised and collinear) of the
+    f = 4 densities, wall clock. GB/s use the scope table's algorithmic bytes."""
     import numpy as np
     import torch
     from sdft_b200 import density, synthetic
@@ -407,6 +408,24 @@ def density_side(ctx, inputs, stream, peak):
     ms, _ = timed(lambda: density.pbe_points(ctx, nval, gval))
     out["pbe"] = {"points": points, "ms": ms, "points_per_s": points / (ms * 1e-3),
                   "achieved_gbs": points * 64 / (ms * 1e-3) / 1e9}
+    # Hartree + PBE functional, spin-unpolarised and collinear, of the Si64
+    # f = 4 Gaussian densities with a frozen core (142^3 grid, prime-71 axes):
+    # wall time of the host call, the host key sort and union included.
+    case = synthetic.functional_case("si64")
+    args = (case["lattice"], case["keys"], case["values"], case["core_keys"], case["core_values"])
+    spin = synthetic.collinear_case("si64")
+    spin_args = (spin["lattice"], spin["up_keys"], spin["up"], spin["down_keys"], spin["down"], spin["core_keys"],
+                 spin["core_values"])
+    density.density_functionals(ctx, *args)
+    density.collinear_functionals(ctx, *spin_args)
+    start = time.perf_counter()
+    result = density.density_functionals(ctx, *args)
+    middle = time.perf_counter()
+    density.collinear_functionals(ctx, *spin_args)
+    end = time.perf_counter()
+    out["functional"] = {"grid": list(result["grid"]), "keys": int(result["hkl"].shape[0]),
+                         "ms": (middle - start) * 1e3, "collinear_ms": (end - middle) * 1e3,
+                         "timing": "wall clock of the host call (host key sort and union included)"}
     return out
 
 
