@@ -13,6 +13,7 @@
 //   save/load_solver_snapshot           src/plane_wave_operator.cpp:542-653
 //   plane_wave_density_fft              src/density_functionals.cpp:407-460
 //   pbe_unpolarized                     src/pbe_xc.cpp:116-140
+//   pbe_collinear                       src/spin_pbe_xc.cpp:54-107
 //   onsite_density_from_amplitudes      src/onsite_density.hpp:10-36
 //   paw_lm_moments_from_density         src/paw_augmentation.cpp:490-525
 //   PawCompensationOperator ctor/density_sum src/paw_compensation.cpp:185-342,465-524
@@ -24,6 +25,7 @@
 #include "compute_backend.hpp"
 #include "density_functionals.hpp"
 #include "pbe_xc.hpp"
+#include "spin_pbe_xc.hpp"
 #include "env_cache.hpp"
 #include "onsite_density.hpp"
 #include "paw_augmentation.hpp"
@@ -315,6 +317,31 @@ void ref_pbe_unpolarized(long count, const double* density, const double* gradie
     o[4] = p.exchange_potential;
     o[5] = p.correlation_potential;
     o[6] = p.gradient_squared_coefficient;
+  }
+}
+
+// pbe_collinear (src/spin_pbe_xc.cpp:54-107) per point: out[9 i ..] =
+// energy density, v_up, v_down, gradient responses up (3) and down (3).
+int ref_pbe_collinear(long count, const double* up, const double* down, const double* gradient_up,
+                      const double* gradient_down, double* out, char* error, long error_length) {
+  try {
+    for (long i = 0; i < count; ++i) {
+      const std::array<double, 3> gu{gradient_up[3 * i], gradient_up[3 * i + 1], gradient_up[3 * i + 2]};
+      const std::array<double, 3> gd{gradient_down[3 * i], gradient_down[3 * i + 1], gradient_down[3 * i + 2]};
+      const auto p = sdft::pbe_collinear(up[i], down[i], gu, gd);
+      double* o = out + 9 * i;
+      o[0] = p.energy_density;
+      o[1] = p.density_potential[0];
+      o[2] = p.density_potential[1];
+      for (int a = 0; a < 3; ++a) {
+        o[3 + a] = p.gradient_response[0][a];
+        o[6 + a] = p.gradient_response[1][a];
+      }
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
   }
 }
 

@@ -78,6 +78,8 @@ class ReferenceLibrary:
         L.ref_plane_wave_density_fft.restype = ctypes.c_int
         L.ref_plane_wave_density_fft.argtypes = [ctypes.c_long, _int, ctypes.c_long, _dbl, _dbl, ctypes.c_double,
                                                  ctypes.c_long, _int, _dbl, ctypes.c_char_p, ctypes.c_long]
+        L.ref_pbe_collinear.restype = ctypes.c_int
+        L.ref_pbe_collinear.argtypes = [ctypes.c_long, _dbl, _dbl, _dbl, _dbl, _dbl, ctypes.c_char_p, ctypes.c_long]
         L.ref_pbe_unpolarized.restype = None
         L.ref_pbe_unpolarized.argtypes = [ctypes.c_long, _dbl, _dbl, _dbl]
         L.ref_refresh_environment.restype = None
@@ -127,6 +129,18 @@ class ReferenceLibrary:
         g = np.ascontiguousarray(gradient, dtype=np.float64)
         out = np.zeros((n.size, 7))
         self.lib.ref_pbe_unpolarized(n.size, _ptr(n), _ptr(g), _ptr(out))
+        return out
+
+    def pbe_collinear(self, up, down, gradient_up, gradient_down):
+        """(count, 9): energy density, v_up, v_down, gradient responses up (3) and down (3)."""
+        u = np.ascontiguousarray(up, dtype=np.float64)
+        d = np.ascontiguousarray(down, dtype=np.float64)
+        gu = np.ascontiguousarray(gradient_up, dtype=np.float64).reshape(-1, 3)
+        gd = np.ascontiguousarray(gradient_down, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((u.size, 9))
+        err = ctypes.create_string_buffer(512)
+        self._check(self.lib.ref_pbe_collinear(u.size, _ptr(u), _ptr(d), _ptr(gu), _ptr(gd), _ptr(out), err, 512),
+                    err)
         return out
 
     @staticmethod
