@@ -9,7 +9,13 @@ from their seeds by the tests, so only reference OUTPUTS are stored). Values
 come from the unmodified reference: the PWO3 solver snapshot it writes
 (src/plane_wave_operator.cpp:542-569) for its internal arrays, its
 apply_block_into / apply_pair_into callbacks for H~x, S~x, and
-solve_generalized_hermitian_davidson for eigenpairs.
+solve_generalized_hermitian_davidson for eigenpairs; the density side from
+plane_wave_density_fft, pbe_unpolarized, onsite_density_from_amplitudes, the
+PawCompensationOperator (density and project_potential_batch) and
+evaluate_density_functionals / evaluate_collinear_density_functionals
+(functional_*.npz, collinear_*.npz, on synthetic.functional_case /
+collinear_case). Single groups: --kpoints, --snapshots, --projection,
+--functional, --collinear.
 """
 from __future__ import annotations
 
