@@ -152,10 +152,38 @@ def reference_cpu_sample(inputs, iterations: int):
     return seconds, result
 
 
-def cpu_full_solve_iterations() -> int:
-    """Iterations the reference needs for this pencil (recorded with its solution in tests/golden)."""
-    import numpy as np
-    return int(np.load(ROOT / "tests" / "golden" / "si64_solution.npz")["iterations"])
+CALIBRATION = ROOT / "tests" / "golden" / "si64_reference_timing.json"
+SAMPLE_ITERATIONS = 2
+
+
+def reference_calibration():
+    """Full-solve time over the time of its first SAMPLE_ITERATIONS
+    iterations, both measured for the reference on one host by
+    `bench.py --calibrate-reference` (the first iterations apply the
+    operator to all 2*roots guard columns and so cost more than the average
+    one; the ratio carries that shape to another host's sample)."""
+    data = json.loads(CALIBRATION.read_text())
+    return data
+
+
+def calibrate_reference(args):
+    """One full reference solve of the pencil and three SAMPLE_ITERATIONS
+    samples on all host threads; writes the ratio to tests/golden."""
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    inputs = load_inputs()
+    samples = [reference_cpu_sample(inputs, SAMPLE_ITERATIONS)[0] for _ in range(3)]
+    full, result = reference_cpu_sample(inputs, 256)
+    data = {"workload": WORKLOAD, "threads": threads, "full_solve_seconds": full,
+            "full_solve_iterations": int(result["iterations"]), "converged": bool(result["converged"]),
+            "sample_iterations": SAMPLE_ITERATIONS, "sample_seconds": samples,
+            "ratio": full / statistics.median(samples), "host": os.uname().nodename,
+            "how": "python bench.py --calibrate-reference (oracle/_ref, unmodified reference sources)"}
+    text = json.dumps(data, indent=1)
+    print(text, flush=True)
+    if args.write_calibration:
+        CALIBRATION.write_text(text + "\n")
 
 
 def run_reference(args):
@@ -166,19 +194,19 @@ def run_reference(args):
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     inputs = load_inputs()
-    full_iterations = cpu_full_solve_iterations()
-    sample_iterations = 2
+    calibration = reference_calibration()
     for _ in range(args.warmup):
         pass  # the reference has no device state to warm; its setup is outside the timed region
     times = []
     for _ in range(args.steps):
-        seconds, _ = reference_cpu_sample(inputs, sample_iterations)
+        seconds, _ = reference_cpu_sample(inputs, SAMPLE_ITERATIONS)
         times.append(seconds)
-    per_iteration = statistics.median(times) / sample_iterations
-    solve = per_iteration * full_iterations
+    solve = statistics.median(times) * calibration["ratio"]
     value = inputs.roots / solve
-    sample = (f"reference Davidson (oracle/_ref, unmodified src/ + FFTW-API shim) for {sample_iterations} iterations "
-              f"per step, extrapolated to the {full_iterations} iterations the reference needs for this pencil")
+    sample = (f"reference Davidson (oracle/_ref, unmodified src/ + FFTW-API shim): its first {SAMPLE_ITERATIONS} "
+              f"iterations per step, scaled to its full {calibration['full_solve_iterations']}-iteration solve by "
+              f"the measured full/sample time ratio {calibration['ratio']:.2f} "
+              f"({calibration['full_solve_seconds']:.0f} s full solve on {calibration['threads']} threads)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3, "higher_is_better": True,
@@ -217,12 +245,17 @@ def run_b200(args):
     def certified(result):
         return int(np.sum(result["residuals"] <= TOLERANCE))
 
+    reference_values = reference_eigenvalues()
+
+    def eigenvalue_error(result):
+        return float(np.max(np.abs(result["eigenvalues"] - reference_values)))
+
     for _ in range(max(args.warmup, 0)):
         solve("mixed")
     torch.cuda.synchronize()
     barrier(world)
     launches0 = lib.sdft_b200_kernel_launches()
-    step_ms, pairs, iters, stats = [], 0, [], None
+    step_ms, pairs, iters, stats, errors = [], 0, [], None, []
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         start_all = torch.cuda.Event(enable_timing=True)
@@ -238,6 +271,7 @@ def run_b200(args):
             step_ms.append(e0.elapsed_time(e1))
             pairs += certified(result)
             iters.append(result["iterations"])
+            errors.append(eigenvalue_error(result))
             stats = result["stats"]
         end_all.record(stream)
         torch.cuda.synchronize()
@@ -247,7 +281,7 @@ def run_b200(args):
     value = pairs * world / (total_ms / 1e3)
 
     # FP64 plain form on the same GPU (after the timed region).
-    fp64_ms, fp64_pairs = [], 0
+    fp64_ms, fp64_pairs, fp64_errors = [], 0, []
     for _ in range(max(1, min(args.steps, 2))):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -257,10 +291,12 @@ def run_b200(args):
         torch.cuda.synchronize()
         fp64_ms.append(e0.elapsed_time(e1))
         fp64_pairs += certified(r64)
+        fp64_errors.append(eigenvalue_error(r64))
     fp64_value = fp64_pairs / (sum(fp64_ms) / 1e3)
 
     # Roofline of the fused local H~psi (FP32 slab FFT) on a 160-column block.
     roofline = fused_local_roofline(op, inputs, stream)
+    apply_errors = operator_apply_errors(op, stream)
 
     # End to end through the public API with host buffers: operator upload from
     # host arrays, solve, eigenvectors read back, every step.
@@ -287,8 +323,14 @@ def run_b200(args):
             "config": config(args, {"parallelism": f"replicas{world}", "precision": "mixed"}),
             "p50_solve_ms": statistics.median(step_ms), "p99_solve_ms": float(np.percentile(step_ms, 99)),
             "iterations": iters, "certified_pairs_per_solve": pairs / args.steps,
+            "max_eigenvalue_error_vs_reference": max(errors),
+            "eigenvalue_error_per_solve": errors,
+            "max_apply_error_fp64": max(apply_errors["fp64"].values()),
+            "max_apply_error_mixed": max(apply_errors["mixed"].values()),
+            "apply_errors": apply_errors,
             "fp64_plain": {"value": fp64_value, "unit": UNIT, "p50_solve_ms": statistics.median(fp64_ms),
-                           "certified_pairs_per_solve": fp64_pairs / len(fp64_ms)},
+                           "certified_pairs_per_solve": fp64_pairs / len(fp64_ms),
+                           "max_eigenvalue_error_vs_reference": max(fp64_errors)},
             "mixed_over_fp64": statistics.median(fp64_ms) / statistics.median(step_ms),
             "solver_stats": stats, "clocks": clocks.summary(), "gpu_launches": int(launches),
             "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "density_side": density_rows,
@@ -300,6 +342,42 @@ def run_b200(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def reference_eigenvalues():
+    """The reference's own 160 eigenvalues of this pencil (its FP64 solve)."""
+    import numpy as np
+    return np.load(ROOT / "tests" / "golden" / "si64_solution.npz")["eigenvalues"]
+
+
+def operator_apply_errors(op, stream):
+    """Relative error of H~x and S~x against the reference's on a seeded
+    160-column block (one call each, device pointers): the two columns the
+    reference fixture holds in full, and every column through its norm and
+    its inner product with a seeded probe vector. Per precision and operator."""
+    import numpy as np
+    import torch
+    g = np.load(ROOT / "tests" / "golden" / "si64_apply.npz")
+
+    def probe(columns, seed):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        return rng.standard_normal((op.npw, columns)) + 1j * rng.standard_normal((op.npw, columns))
+
+    x = probe(160, int(g["probe_seed"]))
+    u = probe(1, int(g["checksum_seed"]))[:, 0]
+    xd = torch.from_numpy(np.ascontiguousarray(x.T)).cuda().T
+    out = {}
+    for precision in ("fp64", "mixed"):
+        out[precision] = {}
+        for overlap, key in ((False, "hx"), (True, "sx")):
+            y = op.apply(xd, overlap=overlap, precision=precision)
+            torch.cuda.synchronize()
+            y = y.T.cpu().numpy().T
+            full = np.linalg.norm(y[:, g["columns"]] - g[key]) / np.linalg.norm(g[key])
+            norms = np.max(np.abs(np.linalg.norm(y, axis=0) - g[f"{key}_norms"]) / g[f"{key}_norms"])
+            dots = np.max(np.abs(u.conj() @ y - g[f"{key}_dots"]) / (np.linalg.norm(u) * g[f"{key}_norms"]))
+            out[precision]["H" if key == "hx" else "S"] = float(max(full, norms, dots))
+    return out
 
 
 def fused_local_roofline(op, inputs, stream):
@@ -518,13 +596,13 @@ def cpu_baseline(inputs):
         return None
     threads = os.cpu_count() or 1
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    iterations = 2
-    seconds, _ = reference_cpu_sample(inputs, iterations)
-    full = cpu_full_solve_iterations()
-    solve = seconds / iterations * full
+    calibration = reference_calibration()
+    seconds, _ = reference_cpu_sample(inputs, SAMPLE_ITERATIONS)
+    solve = seconds * calibration["ratio"]
     return {"value": inputs.roots / solve, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"reference Davidson for {iterations} iterations on the host cores "
-                      f"({seconds:.1f} s), extrapolated to its {full}-iteration solve of this pencil"}
+            "sample": f"reference Davidson, its first {SAMPLE_ITERATIONS} iterations on the host cores "
+                      f"({seconds:.1f} s), scaled to its full {calibration['full_solve_iterations']}-iteration solve "
+                      f"by the measured full/sample ratio {calibration['ratio']:.2f}"}
 
 
 def run_case(args):
@@ -580,8 +658,14 @@ def main():
     parser.add_argument("--repeat", type=int, default=2, help="repetitions for --case")
     parser.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="precision for --case")
     parser.add_argument("--factor", type=float, default=16.0, help="density support factor f for --case density")
+    parser.add_argument("--calibrate-reference", action="store_true",
+                        help="time one full reference solve and its first-iterations sample on the host cores")
+    parser.add_argument("--write-calibration", action="store_true",
+                        help="with --calibrate-reference: write tests/golden/si64_reference_timing.json")
     args = parser.parse_args()
-    if args.case:
+    if args.calibrate_reference:
+        calibrate_reference(args)
+    elif args.case:
         run_case(args)
     elif args.impl == "reference":
         run_reference(args)

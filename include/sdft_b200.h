@@ -32,7 +32,9 @@ typedef enum {
   SDFT_B200_CUDA_ERROR = 4,       /* runtime_error("CUDA: ...") / cuBLAS / cuSOLVER */
   SDFT_B200_OUT_OF_MEMORY = 5,    /* std::bad_alloc */
   SDFT_B200_NONFINITE = 6,        /* runtime_error on a nonfinite operator result */
-  SDFT_B200_NOT_READY = 7         /* a served solve has not finished within the wait */
+  SDFT_B200_NOT_READY = 7,        /* a served solve has not finished within the wait */
+  SDFT_B200_UNSUPPORTED = 8       /* the reference routes this case to a solver not provided here
+                                     (indefinite PAW overlap: the caller keeps the reference's route) */
 } sdft_b200_status;
 
 enum { SDFT_B200_PRECISION_FP64 = 0, SDFT_B200_PRECISION_MIXED = 1 };
@@ -101,6 +103,19 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_update(sdft_b200_operator* op,
  * Replaces: PlaneWaveOperator::fft_grid_points, src/plane_wave_operator.hpp:38. */
 SDFT_B200_API sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t shape[3], size_t* grid_points,
                                          size_t* projectors, size_t* npw, size_t* active_rows);
+/* Signature of S~ from its projector block: *minimum = min(1+reg, lowest
+ * eigenvalue of (1+reg) I + R Q R) with R = (B B^H)^(1/2), *indefinite =
+ * (minimum < -1e-10); RUNTIME_ERROR "original PAW overlap is numerically
+ * singular" when |minimum| <= 1e-10 (the outputs are still written). FP64 on
+ * the device, computed once per operator (again after an update). The
+ * Davidson entry points make the same checks first: singular is that
+ * RUNTIME_ERROR, indefinite is UNSUPPORTED (the reference hands such a pencil
+ * to its indefinite-metric solver, src/pw_core.cpp:556-557).
+ * Replaces: the signature block of PlaneWaveOperator::overlap() and
+ * HermitianOperator::indefinite_metric, src/plane_wave_operator.cpp:702-717,
+ * src/pw_core.hpp:167. */
+SDFT_B200_API sdft_b200_status sdft_b200_operator_metric_signature(sdft_b200_operator* op, double* minimum,
+                                                                   int* indefinite);
 /* Local part of H~ (y = T o x + (1/N) FFT_fwd(V(r) . FFT_bwd(scatter x))) on
  * DEVICE pointers x, y (npw x columns, ld npw), with no allocation of any
  * kind: the FFT slab and twiddle tables live in a fixed 32 MiB static device
@@ -113,8 +128,10 @@ SDFT_B200_API sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator*
  * threads or contexts race; calls on one stream are ordered. Same results as
  * sdft_b200_apply_local. For callers that must not allocate (memory reserved
  * up front, or no room for the device-wide synchronisation of cudaFree).
- * No reference counterpart: the reference allocates its FFT work arrays per
- * call (src/compute_cuda.cu:141-177). */
+ * x and y must be memory of the operator's device (INVALID_ARGUMENT before
+ * any launch otherwise). The array's address belongs to the device's primary
+ * context, which the library assumes for the life of the process.
+ * No reference counterpart. */
 SDFT_B200_API sdft_b200_status sdft_b200_apply_local_noalloc(sdft_b200_operator* op, const double* x,
                                                              size_t columns, double* y, int precision);
 /* Sphere-to-grid index map (npw values), T (Hartree), H and S diagonals
@@ -316,7 +333,15 @@ SDFT_B200_API sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context
  * plain form throughout); Rayleigh-Ritz, the FP64 refresh and the final
  * certificate are FP64 on the device in both. subspace_factor in [4,16]
  * (capacity = min(npw, max(factor*roots, 64)); 0 selects 8). handoff: search
- * residual below which the basis is re-applied in FP64 (0 selects 1e-8). */
+ * residual below which the basis is re-applied in FP64 (0 selects 1e-8).
+ * correction_steps (MIXED only): how the basis is expanded. The reference
+ * expands with the kinetic preconditioner applied once to each residual
+ * (src/pw_core.cpp:1384-1401); a positive value runs that many steps of
+ * preconditioned CG on each unconverged root's Jacobi-Davidson correction
+ * equation instead (mixed-form applies, tensor-core projections), which
+ * needs far fewer outer iterations; 0 selects the library's default for
+ * MIXED (SDFT_B200_CORRECTION_STEPS, else 6); -1 keeps the reference's
+ * single preconditioner step. FP64 solves take 0 (the reference's step). */
 typedef struct {
   size_t roots;
   size_t max_iterations;
@@ -324,6 +349,7 @@ typedef struct {
   int precision;
   int subspace_factor;
   double handoff;
+  int correction_steps;
 } sdft_b200_davidson_options;
 
 typedef struct {
@@ -334,6 +360,7 @@ typedef struct {
   double rayleigh_ritz_seconds;
   size_t h_columns_search, h_columns_fp64, s_columns_search, s_columns_fp64;
   int rayleigh_ritz_calls, restarts, fp64_refreshes, certifications, handoff_iteration, block_rank_fallbacks;
+  size_t correction_columns; /* mixed-form pair applies spent on Jacobi-Davidson corrections, in columns */
 } sdft_b200_davidson_stats;
 
 /* Lowest `roots` eigenpairs of H~ x = e S~ x. initial: band-major roots x npw

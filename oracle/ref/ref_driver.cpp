@@ -191,6 +191,21 @@ int ref_davidson(void* handle, long roots, long max_iterations, double tolerance
   }
 }
 
+// The signature PlaneWaveOperator::overlap() determines
+// (src/plane_wave_operator.cpp:702-717): *indefinite = indefinite_metric;
+// a numerically singular S~ is its runtime_error (returns 1 with the message).
+int ref_overlap_signature(void* handle, int* indefinite, char* error, long error_length) {
+  try {
+    auto* h = static_cast<Handle*>(handle);
+    const auto ovl = h->op->overlap();
+    *indefinite = ovl.indefinite_metric ? 1 : 0;
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(error, error_length, e);
+    return 1;
+  }
+}
+
 // solve_generalized_hermitian_rmm_trial (src/rmm_trial.cpp:128-206) on the
 // operator's callbacks marked as an SCF warm request (scf_trial_update).
 int ref_rmm_trial(void* handle, long roots, long max_iterations, double tolerance, const double* initial,

@@ -57,6 +57,9 @@ class ReferenceLibrary:
         L.ref_project.argtypes = [ctypes.c_void_p, _dbl, ctypes.c_long, _dbl, ctypes.c_char_p, ctypes.c_long]
         L.ref_projector_rows.restype = ctypes.c_long
         L.ref_projector_rows.argtypes = [ctypes.c_void_p]
+        L.ref_overlap_signature.restype = ctypes.c_int
+        L.ref_overlap_signature.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                            ctypes.c_long]
         L.ref_davidson.restype = ctypes.c_int
         L.ref_davidson.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_double, _dbl, _dbl, _dbl,
                                    _dbl, _int, _long, ctypes.c_char_p, ctypes.c_long]
@@ -375,6 +378,13 @@ class ReferenceOperator:
         p = np.zeros((rows, xf.shape[1]), dtype=np.complex128, order="F")
         self._call(self.lib.lib.ref_project, self.handle, xf.ctypes.data_as(_dbl), xf.shape[1], p.ctypes.data_as(_dbl))
         return p
+
+    def overlap_signature(self):
+        """overlap()'s signature decision: {'indefinite': bool}; a numerically
+        singular S~ raises RuntimeError with the reference's message."""
+        flag = ctypes.c_int(0)
+        self._call(self.lib.lib.ref_overlap_signature, self.handle, ctypes.byref(flag))
+        return {"indefinite": bool(flag.value)}
 
     def davidson(self, roots, max_iterations=256, tolerance=1e-12, initial=None):
         eig = np.zeros(roots)

@@ -151,6 +151,24 @@ class Operator:
         return self.apply_h(eye), self.apply_s(eye)
 
 
+def metric_signature(op: Operator):
+    """Lowest eigenvalue of S~'s nontrivial block, capped at 1+reg, as the
+    reference's overlap() computes it (src/plane_wave_operator.cpp:702-717):
+    R = (B B^H)^(1/2) with the Gram eigenvalues clamped at 0, then
+    (1+reg) I + R Q R. Returns (minimum, indefinite, singular)."""
+    reg = op.regularization
+    if op.b.shape[0] == 0:
+        minimum = 1.0 + reg
+    else:
+        gram = op.b @ op.b.conj().T
+        w, u = np.linalg.eigh(0.5 * (gram + gram.conj().T))
+        root = (u * np.sqrt(np.maximum(w, 0.0))) @ u.conj().T
+        q = op._onsite(np.eye(op.b.shape[0], dtype=np.complex128), op.q)
+        small = (1.0 + reg) * np.eye(op.b.shape[0]) + root @ q @ root
+        minimum = min(1.0 + reg, float(np.linalg.eigvalsh(0.5 * (small + small.conj().T))[0]))
+    return minimum, minimum < -1e-10, abs(minimum) <= 1e-10
+
+
 def generalized_eigenvalues(h: np.ndarray, s: np.ndarray, roots: int) -> np.ndarray:
     """Lowest roots of H v = e S v by Cholesky reduction (dense oracle, small n)."""
     hh = 0.5 * (h + h.conj().T)

@@ -1,6 +1,7 @@
 // extern "C" boundary (include/sdft_b200.h): converts exceptions into status
 // codes and a thread-local message, and host pointers into staged device copies.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -37,6 +38,30 @@ struct sdft_b200_server {
 namespace {
 thread_local std::string last_error;
 
+// Jacobi-Davidson CG steps for a Davidson request: MIXED takes the caller's
+// positive count, 0 = SDFT_B200_CORRECTION_STEPS or 6, -1 = the reference's
+// single preconditioner step; FP64 keeps the reference's step.
+int correction_steps_of(const sdft_b200_davidson_options& o) {
+  if (o.correction_steps < -1) throw sdft_b200::InvalidArgument("correction_steps must be -1, 0 or positive");
+  if (o.precision != SDFT_B200_PRECISION_MIXED) {
+    if (o.correction_steps > 0)
+      throw sdft_b200::InvalidArgument("Jacobi-Davidson correction steps apply to the mixed form only");
+    return 0;
+  }
+  if (o.correction_steps < 0) return 0;
+  if (o.correction_steps > 0) return std::min(o.correction_steps, 64);
+  static const int fallback = [] {
+    const char* v = std::getenv("SDFT_B200_CORRECTION_STEPS");
+    if (!v) return 6;
+    char* end = nullptr;
+    const long steps = std::strtol(v, &end, 10);
+    if (end == v || *end || steps < 0 || steps > 64)
+      throw sdft_b200::InvalidArgument("SDFT_B200_CORRECTION_STEPS must be an integer in [0, 64]");
+    return static_cast<int>(steps);
+  }();
+  return fallback;
+}
+
 void copy_stats(const sdft_b200::DavidsonStats& st, sdft_b200_davidson_stats* stats) {
   stats->iterations = static_cast<size_t>(st.iterations);
   stats->converged = st.converged ? 1 : 0;
@@ -53,6 +78,7 @@ void copy_stats(const sdft_b200::DavidsonStats& st, sdft_b200_davidson_stats* st
   stats->certifications = st.certifications;
   stats->handoff_iteration = st.handoff_iteration;
   stats->block_rank_fallbacks = st.block_rank_fallbacks;
+  stats->correction_columns = static_cast<size_t>(st.correction_columns);
 }
 
 template <typename F>
@@ -72,6 +98,9 @@ sdft_b200_status guarded(F&& body) {
   } catch (const sdft_b200::NonFinite& e) {
     last_error = e.what();
     return SDFT_B200_NONFINITE;
+  } catch (const sdft_b200::Unsupported& e) {
+    last_error = e.what();
+    return SDFT_B200_UNSUPPORTED;
   } catch (const sdft_b200::CudaError& e) {
     last_error = e.what();
     return SDFT_B200_CUDA_ERROR;
@@ -101,6 +130,22 @@ void require(bool condition, const char* message) {
 }
 
 // Stage host data into context scratch (device), or pass device pointers through.
+// A pointer the caller declares as device memory must be memory of the
+// context's device (device or managed), checked before any launch: a host
+// pointer, or another GPU's memory without peer access, would fault a kernel.
+void require_device_memory(const void* p, int device, const char* what) {
+  cudaPointerAttributes attributes{};
+  const cudaError_t code = cudaPointerGetAttributes(&attributes, p);
+  if (code != cudaSuccess) {
+    cudaGetLastError();  // clear the error the failed query recorded
+    throw sdft_b200::InvalidArgument(std::string(what) + " is not a CUDA device pointer");
+  }
+  const bool on_device = attributes.type == cudaMemoryTypeDevice || attributes.type == cudaMemoryTypeManaged;
+  if (!on_device || attributes.device != device)
+    throw sdft_b200::InvalidArgument(std::string(what) + " must be device memory of the context's device " +
+                                     std::to_string(device));
+}
+
 struct Staged {
   sdft_b200::Context& ctx;
   int memory;
@@ -108,13 +153,19 @@ struct Staged {
     require(m == SDFT_B200_MEMORY_HOST || m == SDFT_B200_MEMORY_DEVICE, "memory must be host or device");
   }
   const Cx<double>* in(const double* host, std::size_t complex_count, sdft_b200::Scratch& slot) {
-    if (memory == SDFT_B200_MEMORY_DEVICE) return reinterpret_cast<const Cx<double>*>(host);
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      require_device_memory(host, ctx.device, "input");
+      return reinterpret_cast<const Cx<double>*>(host);
+    }
     auto* dst = static_cast<Cx<double>*>(slot.reserve(sizeof(Cx<double>) * complex_count));
     SDFT_CUDA(cudaMemcpyAsync(dst, host, sizeof(Cx<double>) * complex_count, cudaMemcpyHostToDevice, ctx.stream));
     return dst;
   }
   Cx<double>* out(double* host, std::size_t complex_count, sdft_b200::Scratch& slot) {
-    if (memory == SDFT_B200_MEMORY_DEVICE) return reinterpret_cast<Cx<double>*>(host);
+    if (memory == SDFT_B200_MEMORY_DEVICE) {
+      require_device_memory(host, ctx.device, "output");
+      return reinterpret_cast<Cx<double>*>(host);
+    }
     return static_cast<Cx<double>*>(slot.reserve(sizeof(Cx<double>) * complex_count));
   }
   void back(double* host, const Cx<double>* dev, std::size_t complex_count) {
@@ -248,6 +299,16 @@ sdft_b200_status sdft_b200_operator_info(const sdft_b200_operator* op, int32_t s
   });
 }
 
+sdft_b200_status sdft_b200_operator_metric_signature(sdft_b200_operator* op, double* minimum, int* indefinite) {
+  return guarded([&] {
+    require(op != nullptr, "null operator");
+    const auto& sig = op->impl->metric_signature();
+    if (minimum) *minimum = sig.minimum;
+    if (indefinite) *indefinite = sig.indefinite ? 1 : 0;
+    if (sig.singular) throw std::runtime_error("original PAW overlap is numerically singular");
+  });
+}
+
 sdft_b200_status sdft_b200_apply_local(sdft_b200_operator* op, const double* x, size_t columns, double* y,
                                        int precision, int memory) {
   return guarded([&] {
@@ -273,6 +334,8 @@ sdft_b200_status sdft_b200_apply_local_noalloc(sdft_b200_operator* op, const dou
     require(columns <= static_cast<size_t>(INT32_MAX), "too many columns");
     auto& o = *op->impl;
     SDFT_CUDA(cudaSetDevice(o.context().device));
+    require_device_memory(x, o.context().device, "x");
+    require_device_memory(y, o.context().device, "y");
     sdft_b200::apply_local_noalloc(o, reinterpret_cast<const Cx<double>*>(x), static_cast<int>(columns),
                                    reinterpret_cast<Cx<double>*>(y), precision_of(precision));
   });
@@ -706,6 +769,7 @@ sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davi
     SDFT_CUDA(cudaSetDevice(ctx.device));
     require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid matrix-free Davidson problem");
     require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid matrix-free Davidson problem");
+    o.require_positive_metric();  // the overlap() signature checks, src/plane_wave_operator.cpp:702-717
     sdft_b200::DavidsonOptions d;
     d.roots = static_cast<int>(options->roots);
     d.max_iterations = static_cast<int>(options->max_iterations);
@@ -713,6 +777,7 @@ sdft_b200_status sdft_b200_davidson(sdft_b200_operator* op, const sdft_b200_davi
     d.precision = precision_of(options->precision);
     d.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
     d.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    d.correction_steps = correction_steps_of(*options);
     const std::size_t block = static_cast<std::size_t>(o.npw()) * d.roots;
     const Cx<double>* warm = nullptr;
     if (initial) {
@@ -749,6 +814,7 @@ sdft_b200_status sdft_b200_rmm_trial(sdft_b200_operator* op, const sdft_b200_dav
     SDFT_CUDA(cudaSetDevice(ctx.device));
     require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid RMM trial problem");
     require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid RMM trial problem");
+    o.require_positive_metric();  // the overlap() signature checks, src/plane_wave_operator.cpp:702-717
     sdft_b200::DavidsonOptions d;
     d.roots = static_cast<int>(options->roots);
     d.max_iterations = static_cast<int>(options->max_iterations);
@@ -793,6 +859,7 @@ sdft_b200_status sdft_b200_band_groups(sdft_b200_operator* op, const sdft_b200_d
     SDFT_CUDA(cudaSetDevice(ctx.device));
     require(options->roots >= 1 && options->roots <= static_cast<size_t>(o.npw()), "invalid bounded band-group problem");
     require(options->max_iterations >= 1 && options->max_iterations <= 1000000, "invalid bounded band-group problem");
+    o.require_positive_metric();  // the overlap() signature checks, src/plane_wave_operator.cpp:702-717
     sdft_b200::DavidsonOptions d;
     d.roots = static_cast<int>(options->roots);
     d.max_iterations = static_cast<int>(options->max_iterations);
@@ -908,6 +975,7 @@ sdft_b200_status sdft_b200_server_submit(sdft_b200_server* server, size_t npw, c
     r->options.precision = precision_of(options->precision);
     r->options.subspace_factor = options->subspace_factor ? options->subspace_factor : 8;
     r->options.handoff = options->handoff > 0 ? options->handoff : 1e-8;
+    r->options.correction_steps = correction_steps_of(*options);
     r->vectors = want_vectors != 0;
     *ticket = server->impl->submit(std::move(r));
   });

@@ -23,6 +23,11 @@ struct CudaError : std::runtime_error {
 struct NonFinite : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+// A case the reference routes to a solver this library does not provide (the
+// caller keeps the reference's own route for it).
+struct Unsupported : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 inline void check_cuda(cudaError_t code, const char* what) {
   if (code != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(code));

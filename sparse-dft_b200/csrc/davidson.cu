@@ -17,6 +17,7 @@
 #include <numeric>
 #include <string>
 
+#include "correction.cuh"
 #include "davidson.cuh"
 #include "dense.cuh"
 #include "umma_gemm.cuh"
@@ -401,6 +402,9 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
   kmax_ = std::min(capacity_, std::max(3 * roots_, 2));
   exact_mode_ = o.precision == Precision::FP64;
   packs_ = !exact_mode_;
+  if (o.correction_steps < 0 || (exact_mode_ && o.correction_steps > 0))
+    throw InvalidArgument("Jacobi-Davidson correction steps apply to the mixed form only");
+  correction_steps_ = exact_mode_ ? 0 : o.correction_steps;
   if (packs_) {
     split_ = search_split();
     ld_rows_ = expanded_k(n_, split_);
@@ -543,9 +547,20 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
         stalled = recent > 0.5 * earlier;
       }
       if (max_res < o.handoff || stalled || iteration + 1 == o.max_iterations) {
+        // The Jacobi-Davidson-steered form hands over its 2*roots lowest Ritz
+        // vectors only (they carry the search), so the FP64 re-application
+        // covers that block rather than the whole basis.
+        const bool compact = correction_steps_ > 0 && size_ > 2 * roots_;
+        if (compact) gemm_left(static_cast<std::uint16_t*>(pack_vn_.ptr), 2 * roots_, size_, rotation, size_, block,
+                               n_, false, 1.0);
         exact_mode_ = true;
         ++stats_.fp64_refreshes;
         stats_.handoff_iteration = iteration;
+        if (compact) {
+          size_ = computed_h_ = projected_size_ = 0;
+          ++stats_.restarts;
+          append_block(block, 2 * roots_);
+        }
         refresh_images();
         continue;
       }
@@ -605,12 +620,22 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
     for (int r = 0; r < roots_ && size_ + static_cast<int>(selected.size()) < capacity_; ++r)
       if (residual_norms_[r] > 0.5 * tolerance_) selected.push_back(r);
     if (!selected.empty()) {
-      Cx<double>* corrections = static_cast<Cx<double>*>(res_.ptr);  // precondition in place into r_
-      kinetic_precondition(r_, x_, n_, n_, roots_, op_.device_kinetic(), corrections, n_, st);
-      SDFT_CUDA(cudaMemcpyAsync(dselect, selected.data(), sizeof(int) * selected.size(), cudaMemcpyHostToDevice, st));
-      gather_columns(corrections, n_, n_, dselect, static_cast<int>(selected.size()), block, n_, st);
-      append_block(block, static_cast<int>(selected.size()));
+      const int count = static_cast<int>(selected.size());
+      if (correction_steps_ > 0) {
+        jacobi_davidson_corrections(op_, b_.corrections, x_, sx_, r_, w_, roots_, selected.data(), count,
+                                    correction_steps_, block);
+        stats_.correction_columns += static_cast<long long>(count) * correction_steps_;
+        stats_.h_columns_search += static_cast<long long>(count) * correction_steps_;
+        stats_.s_columns_search += static_cast<long long>(count) * correction_steps_;
+      } else {
+        Cx<double>* corrections = static_cast<Cx<double>*>(res_.ptr);  // precondition in place into r_
+        kinetic_precondition(r_, x_, n_, n_, roots_, op_.device_kinetic(), corrections, n_, st);
+        SDFT_CUDA(cudaMemcpyAsync(dselect, selected.data(), sizeof(int) * selected.size(), cudaMemcpyHostToDevice, st));
+        gather_columns(corrections, n_, n_, dselect, count, block, n_, st);
+      }
       phase("corrections");
+      append_block(block, count);
+      phase("append");
     }
     if (size_ == previous) {
       bool added = false;

@@ -15,6 +15,10 @@ struct DavidsonOptions {
   Precision precision = Precision::FP64;  // search precision; certification is always FP64
   int subspace_factor = 8;                // capacity = min(n, max(factor*roots, 64)), in [4,16]
   double handoff = 1e-8;                  // search residual that hands the basis to FP64
+  // Mixed form: CG steps on each unconverged root's Jacobi-Davidson
+  // correction equation (correction.cuh) in place of the reference's single
+  // kinetic-preconditioner step; 0 keeps the reference's step.
+  int correction_steps = 0;
   // Band-group local solves (src/band_group_solver.cpp:95-107): an explicit
   // subspace capacity (0 = the factor rule) and completed lower bands, device
   // n x excluded_count, S-orthonormal, projected out of every search
@@ -31,6 +35,7 @@ struct DavidsonStats {
   long long h_columns_search = 0, h_columns_fp64 = 0, s_columns_search = 0, s_columns_fp64 = 0;
   int rayleigh_ritz = 0, restarts = 0, fp64_refreshes = 0, certifications = 0, handoff_iteration = -1;
   int block_rank_fallbacks = 0;
+  long long correction_columns = 0;
   double seconds = 0.0, rr_seconds = 0.0;
 };
 
@@ -83,7 +88,7 @@ class DavidsonSolver {
 
   DeviceOperator& op_;
   DavidsonStats stats_;
-  int n_ = 0, roots_ = 0, capacity_ = 0, kmax_ = 0;
+  int n_ = 0, roots_ = 0, capacity_ = 0, kmax_ = 0, correction_steps_ = 0;
   int size_ = 0, computed_h_ = 0, projected_size_ = 0;
   const Cx<double>* excluded_ = nullptr;  // completed bands of a band-group local solve
   Cx<double>* excluded_s_ = nullptr;      // their S images

@@ -2,6 +2,7 @@
 #include <algorithm>
 
 #include "dense.cuh"
+#include "preconditioner.cuh"
 
 namespace sdft_b200 {
 
@@ -168,17 +169,6 @@ __global__ void unit_columns_kernel(Cx<double>* __restrict__ x, long long ld, in
   }
 }
 
-__device__ double kinetic_preconditioner(double kinetic, double wavefunction_kinetic) {
-  const double scale = 1.5 * fmax(wavefunction_kinetic, 2.0 / 27.211386245988);
-  const double x = kinetic / scale;
-  if (x > 1.0) {
-    const double inv = 1.0 / x;
-    const double p = inv * (8.0 + inv * (12.0 + inv * (18.0 + 27.0 * inv)));
-    return (2.0 / scale) * p / (p + 16.0);
-  }
-  const double p = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
-  return (2.0 / scale) * p / (p + 16.0 * x * x * x * x);
-}
 
 __global__ void kinetic_precondition_kernel(const Cx<double>* __restrict__ r, const Cx<double>* __restrict__ x,
                                             long long ld, int rows, const double* __restrict__ kinetic,

@@ -12,8 +12,9 @@
 //   - capacity kNoAllocScratchBytes (32 MiB) per device; the twiddle tables
 //     take the first kTwiddleBytes, the slab the rest. A call whose slab
 //     (slots * n1 * n2 * columns complex values) does not fit is rejected.
-//   - nothing in it has to start at zero: each call writes the tables, and
-//     the plane pass writes every slab entry before the pencil pass reads it.
+//   - nothing in it has to start at zero: each call writes the tables (from a
+//     kernel parameter, so no host buffer is read by the device), and the
+//     plane pass writes every slab entry before the pencil pass reads it.
 //   - all calls on one device share it: two calls whose work overlaps in time
 //     (different streams, threads or contexts on the same device) race on it.
 //     Calls issued on one stream are ordered and safe.
@@ -37,6 +38,10 @@ void* g_scratch_address[kMaxDevices] = {};
 
 // Once per device, with that device current. The first call on a device does
 // this look-up, so it must come before any stream capture on that device.
+// The address belongs to the device's primary context, the one the CUDA
+// runtime makes current: the cache assumes that context for the life of the
+// process (a cudaDeviceReset, or a caller that switches to a context of its
+// own through the driver API, would need a new look-up).
 unsigned char* scratch_for(int device) {
   if (device < 0 || device >= kMaxDevices) throw InvalidArgument("device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -46,6 +51,24 @@ unsigned char* scratch_for(int device) {
     g_scratch_address[device] = address;
   }
   return static_cast<unsigned char*>(g_scratch_address[device]);
+}
+
+// The three axes' twiddle tables, packed in the layout the scratch array
+// holds them in, travel as one kernel parameter (24 KiB at most; parameters
+// above 4 KiB need CUDA 12.1 and sm_70 or newer), so the device never reads a
+// host buffer: each table starts at a kMaxLine boundary.
+struct TwiddleTables {
+  // Storage for three tables of Cx<T> entries, table a from entry a * kMaxLine
+  // (Cx<float> tables fill the first half of the bytes).
+  Cx<double> values[3 * kMaxLine];
+};
+static_assert(sizeof(TwiddleTables) <= 24 * 1024, "twiddle tables exceed the parameter budget");
+static_assert(sizeof(TwiddleTables) <= kTwiddleBytes, "twiddle tables exceed their part of the scratch");
+
+__global__ void write_twiddles_kernel(const TwiddleTables tables, int bytes, unsigned char* __restrict__ dst) {
+  const auto* src = reinterpret_cast<const unsigned char*>(tables.values);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bytes / 16; i += gridDim.x * blockDim.x)
+    reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
 }
 
 template <typename T>
@@ -61,17 +84,16 @@ void run(DeviceOperator& op, const Cx<double>* x, int columns, Cx<double>* y, co
                           std::to_string(capacity / per_column) + " columns per call for this operator");
   unsigned char* scratch = scratch_for(ctx.device);
   // Same table values as the cached tables of the regular path.
-  Cx<T> host[3][kMaxLine];
-  std::size_t offset = 0;
+  TwiddleTables tables{};
+  auto* packed = reinterpret_cast<Cx<T>*>(tables.values);
   const Cx<T>* twiddle[3];
   for (int a = 0; a < 3; ++a) {
-    const int n = plan.n[a];
-    host_twiddles<T>(n, host[a]);
-    auto* dst = reinterpret_cast<Cx<T>*>(scratch + offset);
-    SDFT_CUDA(cudaMemcpyAsync(dst, host[a], sizeof(Cx<T>) * n, cudaMemcpyHostToDevice, ctx.stream));
-    twiddle[a] = dst;
-    offset += sizeof(Cx<T>) * kMaxLine;
+    host_twiddles<T>(plan.n[a], packed + static_cast<std::size_t>(a) * kMaxLine);
+    twiddle[a] = reinterpret_cast<const Cx<T>*>(scratch) + static_cast<std::size_t>(a) * kMaxLine;
   }
+  const int bytes = static_cast<int>(sizeof(Cx<T>) * 3 * kMaxLine);
+  write_twiddles_kernel<<<8, 256, 0, ctx.stream>>>(tables, bytes, scratch);
+  SDFT_LAUNCH("write_twiddles_kernel");
   auto* slab = reinterpret_cast<Cx<T>*>(scratch + kTwiddleBytes);
   local_hamiltonian_preset<T>(plan, x, op.npw(), columns, potential, op.device_kinetic(), y, op.npw(), slab, twiddle,
                               ctx.stream);

@@ -11,6 +11,7 @@
 #include <string>
 #include <unordered_map>
 
+#include "dense.cuh"
 #include "operator.cuh"
 
 namespace sdft_b200 {
@@ -181,6 +182,11 @@ void DavidsonBuffers::release() {
                      &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb,
                      &excluded})
     s->release();
+  corrections.release();
+}
+
+void CorrectionBuffers::release() {
+  for (Scratch* s : {&res, &z, &p, &hp, &sp, &xh, &sxh, &xl, &sxl, &coefficients, &scalars, &index}) s->release();
 }
 
 GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
@@ -582,6 +588,107 @@ void DeviceOperator::update(std::size_t potential_count, const int* potential_hk
   h_local_real_ = std::move(local.real);
   h_diag_ = std::move(h_diag);
   s_diag_ = std::move(s_diag);
+  signature_ready_ = false;  // Q changed
+}
+
+namespace {
+__global__ void clamped_root_columns_kernel(Cx<double>* __restrict__ v, int m, const double* __restrict__ lambda) {
+  const long long total = static_cast<long long>(m) * m;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const double s = sqrt(fmax(lambda[i / m], 0.0));
+    v[i] = Cx<double>{v[i].re * s, v[i].im * s};
+  }
+}
+
+__global__ void shift_diagonal_kernel(Cx<double>* __restrict__ a, int m, double shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) a[i + static_cast<long long>(i) * m].re += shift;
+}
+
+// Ascending eigenvalues and eigenvectors (the lowest `wanted` of each) of
+// the Hermitian m x m matrix a (lower triangle, ld m; overwritten) by cuSOLVER
+// zheevd: a once-per-operator set-up step whose matrices (the projector Gram
+// of a symmetric cell) carry large, nearly degenerate clusters.
+void hermitian_eigen(Context& ctx, Cx<double>* a, int m, int wanted, double* values, Cx<double>* vectors) {
+  int lwork = 0;
+  auto* az = reinterpret_cast<cuDoubleComplex*>(a);
+  auto* w = static_cast<double*>(ctx.eigen.product2.reserve(sizeof(double) * m));
+  if (cusolverDnZheevd_bufferSize(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, az, m, w, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    throw CudaError("cuSOLVER error in zheevd_bufferSize");
+  auto* work = static_cast<cuDoubleComplex*>(
+      ctx.eigen.solver_work.reserve(sizeof(cuDoubleComplex) * std::max(1, lwork) + sizeof(int)));
+  int* info = reinterpret_cast<int*>(work + std::max(1, lwork));
+  if (cusolverDnZheevd(ctx.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, az, m, w, work, lwork, info) !=
+      CUSOLVER_STATUS_SUCCESS)
+    throw CudaError("cuSOLVER error in zheevd");
+  int host_info = 0;
+  SDFT_CUDA(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
+  if (host_info) throw std::runtime_error("original PAW Gram decomposition failed");
+  SDFT_CUDA(cudaMemcpyAsync(values, w, sizeof(double) * wanted, cudaMemcpyDeviceToDevice, ctx.stream));
+  if (vectors != a) copy_block(a, m, vectors, m, m, wanted, ctx.stream);
+}
+}  // namespace
+
+// The reference's overlap() signature (src/plane_wave_operator.cpp:702-717),
+// FP64 on the device: Gram = B B^H; its eigendecomposition U diag(l) U^H;
+// R = W U^H with W = U diag(sqrt(max(l, 0))); the lowest eigenvalue of
+// (1+reg) I + R (Q R), the per-atom Q product compensated as in the applies.
+const MetricSignature& DeviceOperator::metric_signature() {
+  if (signature_ready_) return signature_;
+  MetricSignature sig;
+  sig.minimum = 1.0 + regularization_;
+  if (np_ > 0) {
+    SDFT_CUDA(cudaSetDevice(ctx_.device));
+    const cudaStream_t st = ctx_.stream;
+    const std::size_t pp = static_cast<std::size_t>(np_) * np_;
+    auto* gram = static_cast<Cx<double>*>(ctx_.davidson.rr_a.reserve(sizeof(Cx<double>) * pp * 2));
+    Cx<double>* herm = gram + pp;
+    auto* root = static_cast<Cx<double>*>(ctx_.davidson.rr_b.reserve(sizeof(Cx<double>) * pp * 2));
+    Cx<double>* qroot = root + pp;
+    auto* values = static_cast<double*>(ctx_.davidson.rr_w.reserve(sizeof(double) * np_));
+    zgemm(ctx_.blas, Op::N, Op::C, np_, np_, npw_, b_, np_, b_, np_, gram, np_, false);
+    hermitian_part(gram, np_, herm, np_, np_, st);
+    hermitian_eigen(ctx_, herm, np_, np_, values, gram);
+    const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>(ceil_div(pp, 256), 148 * 8));
+    clamped_root_columns_kernel<<<blocks, 256, 0, st>>>(gram, np_, values);
+    SDFT_LAUNCH("clamped_root_columns_kernel");
+    zgemm(ctx_.blas, Op::N, Op::C, np_, np_, np_, gram, np_, herm, np_, root, np_, false);  // W U^H
+    block_product(atoms_, block_offsets_, block_storage_, max_block_, q_, root, np_, np_, qroot, np_, st);
+    zgemm(ctx_.blas, Op::N, Op::N, np_, np_, np_, root, np_, qroot, np_, gram, np_, false);
+    shift_diagonal_kernel<<<static_cast<unsigned>(ceil_div(np_, 256)), 256, 0, st>>>(gram, np_,
+                                                                                     1.0 + regularization_);
+    SDFT_LAUNCH("shift_diagonal_kernel");
+    hermitian_part(gram, np_, herm, np_, np_, st);
+    double lowest = 0.0;
+    if (np_ == 1) {
+      Cx<double> one;
+      SDFT_CUDA(cudaMemcpyAsync(&one, herm, sizeof(one), cudaMemcpyDeviceToHost, st));
+      SDFT_CUDA(cudaStreamSynchronize(st));
+      lowest = one.re;
+    } else {
+      hermitian_eigen(ctx_, herm, np_, 1, values, root);
+      SDFT_CUDA(cudaMemcpyAsync(&lowest, values, sizeof(double), cudaMemcpyDeviceToHost, st));
+      SDFT_CUDA(cudaStreamSynchronize(st));
+    }
+    if (!std::isfinite(lowest)) throw std::runtime_error("original PAW overlap signature failed");
+    sig.minimum = std::min(sig.minimum, lowest);
+  }
+  sig.indefinite = sig.minimum < -1e-10;
+  sig.singular = std::abs(sig.minimum) <= 1e-10;
+  signature_ = sig;
+  signature_ready_ = true;
+  return signature_;
+}
+
+void DeviceOperator::require_positive_metric() {
+  const MetricSignature& sig = metric_signature();
+  if (sig.singular) throw std::runtime_error("original PAW overlap is numerically singular");
+  if (sig.indefinite)
+    throw Unsupported("original PAW overlap is indefinite: the reference solves this pencil with its "
+                      "indefinite-metric Davidson, which this library does not provide");
 }
 
 DeviceOperator::~DeviceOperator() {

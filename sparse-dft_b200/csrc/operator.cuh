@@ -53,12 +53,23 @@ struct DensityCache {
 // Rayleigh-Ritz and eigensolver workspace, correction blocks, packed search
 // operands). Owned by the context, so solves of successive operators on one
 // context reuse the allocations.
+// Device state of the Jacobi-Davidson corrections (correction.cu).
+struct CorrectionBuffers {
+  Scratch res, z, p, hp, sp;   // n x count blocks (the corrections themselves go to the caller's block)
+  Scratch xh, sxh, xl, sxl;    // packed X^H, (SX)^H (rows) and X, SX (left factors)
+  Scratch coefficients;        // roots x count projections
+  Scratch scalars;             // per column: theta, kinetic energy, two (res, z) slots, (p, q)
+  Scratch index;               // selected roots
+  void release();
+};
+
 struct DavidsonBuffers {
   Scratch basis, hbasis, sbasis, cached_h, cached_s, rr_a, rr_b, rr_w, rr_work, info;
   EigenWorkspace eigen;
   Scratch xs, sxs, hxs, res, block, metric, original, projections, gram, small, order, select;
   Scratch pack_vc, pack_vn, pack_hn, pack_sn, pack_hb, pack_sb;
   Scratch excluded;  // S images and projections of a band-group solve's completed bands
+  CorrectionBuffers corrections;
   void release();
 };
 
@@ -146,6 +157,17 @@ struct OperatorSnapshot {
 // the arrays after the atom boundaries.
 OperatorSnapshot read_operator_snapshot(const std::string& path, bool header_only = false);
 
+// Signature of S~ from its nontrivial projector block, as the reference's
+// overlap() determines it (src/plane_wave_operator.cpp:702-717): with
+// R = (B B^H)^(1/2) (eigenvalues clamped at 0), S~ restricted to span(B^H)
+// is similar to (1+reg) I + R Q R, and every other direction has the norm
+// 1+reg.
+struct MetricSignature {
+  double minimum = 1.0;     // min(1+reg, lowest eigenvalue of (1+reg) I + R Q R)
+  bool indefinite = false;  // minimum < -1e-10
+  bool singular = false;    // |minimum| <= 1e-10
+};
+
 class DeviceOperator {
  public:
   DeviceOperator(Context& ctx, const OperatorInput& input);
@@ -192,6 +214,14 @@ class DeviceOperator {
 
   std::size_t device_bytes() const;
 
+  // FP64 on the device, computed at the first call and kept until update().
+  const MetricSignature& metric_signature();
+  // The checks a Davidson solve of this pencil makes first: a numerically
+  // singular S~ is the reference's runtime_error; an indefinite one, which
+  // the reference hands to its indefinite-pencil solver
+  // (src/pw_core.cpp:556-557), throws Unsupported.
+  void require_positive_metric();
+
  private:
   // Device arrays from the host state (plan, kinetic, V(r), D/Q blocks and
   // boundaries); B and the diagonals are the caller's.
@@ -221,6 +251,8 @@ class DeviceOperator {
   Cx<double>* q_ = nullptr;
   int* block_offsets_ = nullptr;         // [atoms+1]
   long long* block_storage_ = nullptr;   // [atoms]
+  MetricSignature signature_;
+  bool signature_ready_ = false;
 };
 
 }  // namespace sdft_b200

@@ -230,6 +230,7 @@ void SolveServer::worker(int slot) {
         in.regularization = q.regularization;
         {
           DeviceOperator op(*ctx, in);
+          op.require_positive_metric();
           DavidsonSolver solver(op);
           solver.solve(q.options, nullptr);
           result.eigenvalues = solver.eigenvalues();

@@ -7,8 +7,7 @@
 // SDFT_COMPUTE_BACKEND=cuda, SDFT_GPU_FFT=1 and SDFT_GPU_PAW_CHAIN=1 route the
 // reference's exact=false work to the hand-written sm_100a kernels. Statuses
 // map back to the reference's exception classes. The device-resident solver
-// (sdft_b200_davidson) is reached through the same library; see
-// INTEGRATION.md.
+// (sdft_b200_davidson) is reached through the same library.
 //
 // SDFT_B200_ACCELERATOR_PRECISION=fp64 (default, the arithmetic the
 // reference's CUDA accelerator promises) or mixed (FP32 FFT, BF16-split

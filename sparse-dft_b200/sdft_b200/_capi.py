@@ -14,7 +14,7 @@ import numpy as np
 LIBRARY = pathlib.Path(__file__).resolve().parent / "_lib" / "libsdft_b200.so"
 HEADER = pathlib.Path(__file__).resolve().parents[2] / "include" / "sdft_b200.h"
 
-OK, INVALID_ARGUMENT, OVERFLOW, RUNTIME_ERROR, CUDA_ERROR, OUT_OF_MEMORY, NONFINITE, NOT_READY = range(8)
+OK, INVALID_ARGUMENT, OVERFLOW, RUNTIME_ERROR, CUDA_ERROR, OUT_OF_MEMORY, NONFINITE, NOT_READY, UNSUPPORTED = range(9)
 FP64, MIXED = 0, 1
 HOST, DEVICE = 0, 1
 HAMILTONIAN, OVERLAP = 0, 1
@@ -36,7 +36,11 @@ class OverflowFailure(SdftError, OverflowError):
     pass
 
 
-_ERRORS = {INVALID_ARGUMENT: InvalidArgument, OVERFLOW: OverflowFailure}
+class Unsupported(SdftError):
+    """The reference routes this case to a solver the library does not provide."""
+
+
+_ERRORS = {INVALID_ARGUMENT: InvalidArgument, OVERFLOW: OverflowFailure, UNSUPPORTED: Unsupported}
 
 _lib = None
 
@@ -107,7 +111,8 @@ class SolveTiming(ctypes.Structure):
 
 class DavidsonOptions(ctypes.Structure):
     _fields_ = [("roots", ctypes.c_size_t), ("max_iterations", ctypes.c_size_t), ("tolerance", ctypes.c_double),
-                ("precision", ctypes.c_int), ("subspace_factor", ctypes.c_int), ("handoff", ctypes.c_double)]
+                ("precision", ctypes.c_int), ("subspace_factor", ctypes.c_int), ("handoff", ctypes.c_double),
+                ("correction_steps", ctypes.c_int)]
 
 
 class DavidsonStats(ctypes.Structure):
@@ -117,7 +122,7 @@ class DavidsonStats(ctypes.Structure):
                 ("s_columns_search", ctypes.c_size_t), ("s_columns_fp64", ctypes.c_size_t),
                 ("rayleigh_ritz_calls", ctypes.c_int), ("restarts", ctypes.c_int), ("fp64_refreshes", ctypes.c_int),
                 ("certifications", ctypes.c_int), ("handoff_iteration", ctypes.c_int),
-                ("block_rank_fallbacks", ctypes.c_int)]
+                ("block_rank_fallbacks", ctypes.c_int), ("correction_columns", ctypes.c_size_t)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -149,6 +154,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_collinear_functionals", [P, D, SZ, I32, D, SZ, I32, D, SZ, I32, D, ctypes.c_int, I32, D, D, D, D,
                                            SZ, SZP, ctypes.POINTER(Functionals)])
     fn("sdft_b200_operator_info", [P, I32, SZP, SZP, SZP, SZP])
+    fn("sdft_b200_operator_metric_signature", [P, D, ctypes.POINTER(ctypes.c_int)])
     fn("sdft_b200_apply_local", [P, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_local_noalloc", [P, P, SZ, P, ctypes.c_int])
     fn("sdft_b200_pbe_points", [P, P, P, SZ, P, ctypes.c_int])

@@ -169,6 +169,17 @@ class PlaneWaveOperator:
         except Exception:
             pass
 
+    def metric_signature(self) -> dict:
+        """Signature of S~ as the reference's overlap() determines it: the lowest
+        eigenvalue of (1+reg) I + R Q R (R = (B B^H)^(1/2)), capped at 1+reg,
+        and whether S~ is indefinite. Raises SdftError (RUNTIME_ERROR) for a
+        numerically singular S~."""
+        minimum = ctypes.c_double()
+        indefinite = ctypes.c_int()
+        C.check(self._lib.sdft_b200_operator_metric_signature(self.handle, ctypes.byref(minimum),
+                                                              ctypes.byref(indefinite)))
+        return {"minimum": minimum.value, "indefinite": bool(indefinite.value)}
+
     def arrays(self) -> dict:
         n, count = self.npw, self.grid_points
         out = {"indices": np.zeros(n, dtype=np.uint64), "kinetic": np.zeros(n), "h_diagonal": np.zeros(n),
@@ -229,6 +240,8 @@ class PlaneWaveOperator:
         optr, ocols, omem, _ = self._block(out)
         if mem != C.DEVICE or omem != C.DEVICE or ocols != cols:
             raise ValueError("x and out must be device blocks with the same column count")
+        if x.device.index != self.context.device or out.device.index != self.context.device:
+            raise ValueError(f"x and out must live on the context's device cuda:{self.context.device}")
         C.check(self._lib.sdft_b200_apply_local_noalloc(self.handle, ptr, cols, optr, _precision(precision)))
         return out
 
@@ -249,14 +262,18 @@ class PlaneWaveOperator:
 
     # -- eigensolver ---------------------------------------------------------
     def davidson(self, roots: int, max_iterations: int = 256, tolerance: float = 1e-10, precision="fp64",
-                 initial=None, subspace_factor: int = 8, handoff: float = 1e-8, vectors: bool = True):
+                 initial=None, subspace_factor: int = 8, handoff: float = 1e-8, vectors: bool = True,
+                 correction_steps: int = 0):
         """Lowest eigenpairs of H~x = e S~x (the reference's solve_generalized_hermitian_davidson).
 
+        correction_steps (mixed only): Jacobi-Davidson CG steps per expansion,
+        0 = the library default, -1 = the reference's single preconditioner step.
         Returns a dict with eigenvalues, residuals (fresh FP64), eigenvectors
         (band-major roots x npw, or None), converged, iterations and stats.
         """
         opts = C.DavidsonOptions(roots=roots, max_iterations=max_iterations, tolerance=tolerance,
-                                 precision=_precision(precision), subspace_factor=subspace_factor, handoff=handoff)
+                                 precision=_precision(precision), subspace_factor=subspace_factor, handoff=handoff,
+                                 correction_steps=correction_steps)
         stats = C.DavidsonStats()
         eig = np.zeros(roots)
         res = np.zeros(roots)

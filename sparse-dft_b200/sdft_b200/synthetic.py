@@ -289,6 +289,20 @@ def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, d
                           q_scale=scale)
 
 
+def scaled_overlap(inputs: OperatorInputs, factor: float) -> OperatorInputs:
+    """The same pencil with every Q_a multiplied by factor. The lowest
+    eigenvalue of (1+reg) I + R Q R moves linearly, from its value m at
+    factor 1 to (1+reg) + factor (m - (1+reg)): zero (a singular S~) at
+    factor (1+reg) / (1+reg-m), negative (an indefinite S~) beyond."""
+    import dataclasses
+    return dataclasses.replace(inputs, q=np.asarray(inputs.q) * factor, q_scale=inputs.q_scale * factor)
+
+
+def singular_overlap_factor(minimum: float, regularization: float) -> float:
+    """The Q factor of scaled_overlap at which S~'s lowest eigenvalue reaches 0."""
+    return (1.0 + regularization) / (1.0 + regularization - minimum)
+
+
 def si8(seed: int = 2026, **kw) -> OperatorInputs:
     """Diamond-cubic Si8, a = 10.26 bohr, Gamma, Ecut 15 Ha, 16 bands."""
     return build_operator("si8", 10.26, 1, 15.0, 16, seed=seed, **kw)

@@ -15,7 +15,8 @@ PawCompensationOperator (density and project_potential_batch) and
 evaluate_density_functionals / evaluate_collinear_density_functionals
 (functional_*.npz, collinear_*.npz, on synthetic.functional_case /
 collinear_case). Single groups: --kpoints, --snapshots, --projection,
---functional, --collinear.
+--functional, --collinear, --si64-apply (si64_apply.npz: the
+headline pencil's operator arrays and a 160-column H~x/S~x probe).
 """
 from __future__ import annotations
 
@@ -232,6 +233,41 @@ def collinear_fixtures(lib):
 KPOINT_MESH = {"gaas_k13": (0.0, 1.0 / 3.0, 1.0 / 3.0), "gaas_k26": (1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)}
 
 
+SI64_APPLY_COLUMNS = 160
+SI64_FULL_COLUMNS = (0, 159)
+SI64_SAMPLE_POINTS = 4096
+
+
+def si64_apply_fixture(lib):
+    """The Si64 pencil at the headline size: the reference's H~x and S~x of a
+    seeded 160-column probe (two columns in full, and for every column its
+    norm and its inner product with a seeded probe vector u), the operator's
+    index map, kinetic energies and diagonals in full, and V(r) at seeded grid
+    points plus its sum and sum of squares."""
+    inputs = synthetic.si64()
+    op = ref_oracle.ReferenceOperator(lib, inputs)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = pathlib.Path(tmp) / "op.pwop"
+        op.save_snapshot(path, inputs.roots, inputs.max_iterations, inputs.tolerance)
+        snap = read_pwo3(path)
+    seed = 11
+    x = probe_block(inputs.npw, SI64_APPLY_COLUMNS, seed)
+    hx, sx = op.apply(x, overlap=False, exact=True), op.apply(x, overlap=True, exact=True)
+    u = probe_block(inputs.npw, 1, 12)[:, 0]
+    rng = np.random.Generator(np.random.PCG64(13))
+    local = snap["local_real"]
+    points = rng.choice(local.size, SI64_SAMPLE_POINTS, replace=False)
+    cols = np.array(SI64_FULL_COLUMNS)
+    np.savez_compressed(
+        HERE / "si64_apply.npz", shape=np.array(snap["shape"]), indices=snap["indices"], kinetic=snap["kinetic"],
+        h_diagonal=snap["h_diagonal"], s_diagonal=snap["s_diagonal"], local_points=points,
+        local_values=local[points], local_sum=np.array(local.sum()), local_sum2=np.array(np.dot(local, local)),
+        probe_seed=np.array(seed), checksum_seed=np.array(12), columns=cols, hx=hx[:, cols], sx=sx[:, cols],
+        hx_dots=u.conj() @ hx, sx_dots=u.conj() @ sx, hx_norms=np.linalg.norm(hx, axis=0),
+        sx_norms=np.linalg.norm(sx, axis=0))
+    print("si64_apply npw", inputs.npw, "grid", snap["shape"])
+
+
 def kpoint_fixtures(lib):
     """Reference operator and solve of the 8-atom GaAs cell at two k-points of
     the 3x3x3 Monkhorst-Pack mesh (complex, off-Gamma pencils, two species)."""
@@ -247,6 +283,7 @@ def main():
     parser.add_argument("--projection", action="store_true", help="only the compensation projection fixture")
     parser.add_argument("--functional", action="store_true", help="only the Hartree + XC functional fixtures")
     parser.add_argument("--collinear", action="store_true", help="only the collinear spin functional fixtures")
+    parser.add_argument("--si64-apply", action="store_true", help="only the Si64 operator and 160-column apply fixture")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
@@ -263,6 +300,9 @@ def main():
         return
     if args.collinear:
         collinear_fixtures(lib)
+        return
+    if args.si64_apply:
+        si64_apply_fixture(lib)
         return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)

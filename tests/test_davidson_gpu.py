@@ -76,3 +76,28 @@ def test_invalid_davidson_arguments(tiny_op):
         tiny_op.davidson(4, tolerance=-1.0)
     with pytest.raises(C.InvalidArgument):
         tiny_op.davidson(4, subspace_factor=3)
+
+
+@pytest.mark.parametrize("steps", [-1, 0, 3])
+def test_mixed_correction_steps_converge_to_reference(si8_op, si8_inputs, golden, steps):
+    """The mixed form with the reference's single preconditioner step (-1), the
+    default Jacobi-Davidson CG steps (0) and three steps: same certified pairs."""
+    result = si8_op.davidson(si8_inputs.roots, 256, 1e-12, precision="mixed", correction_steps=steps)
+    check_solution(result, si8_inputs, golden("si8")["eigenvalues"])
+    assert (result["stats"]["correction_columns"] > 0) == (steps != -1)
+
+
+def test_correction_steps_cut_outer_iterations(si8_op, si8_inputs):
+    plain = si8_op.davidson(si8_inputs.roots, 256, 1e-12, precision="mixed", correction_steps=-1, vectors=False)
+    steered = si8_op.davidson(si8_inputs.roots, 256, 1e-12, precision="mixed", correction_steps=6, vectors=False)
+    assert plain["converged"] and steered["converged"]
+    assert steered["iterations"] < plain["iterations"]
+    assert steered["stats"]["rayleigh_ritz_calls"] < plain["stats"]["rayleigh_ritz_calls"]
+
+
+def test_correction_steps_are_mixed_only(tiny_op, tiny_inputs):
+    from sdft_b200 import _capi as C
+    with pytest.raises(C.InvalidArgument, match="mixed form only"):
+        tiny_op.davidson(tiny_inputs.roots, 50, 1e-10, precision="fp64", correction_steps=3)
+    with pytest.raises(C.InvalidArgument):
+        tiny_op.davidson(tiny_inputs.roots, 50, 1e-10, precision="mixed", correction_steps=-2)

@@ -27,6 +27,26 @@ def test_reference_smoke_tests_pass_with_shims(binary, marker, tmp_path):
 
 
 @pytest.mark.parametrize("name,factory", [("tiny", synthetic.tiny), ("si8", synthetic.si8)])
+def test_metric_signature_decisions_match_reference(reference, name, factory):
+    """The numpy restatement of overlap()'s signature block reaches the
+    reference's decision on a definite, a singular and an indefinite S~
+    (src/plane_wave_operator.cpp:702-717)."""
+    x = factory()
+    minimum, indefinite, singular = sdft_oracle.metric_signature(sdft_oracle.Operator(x))
+    assert abs(minimum - 0.3) < 1e-12 and not indefinite and not singular  # the generator's lambda_min(S~) = 0.3
+    assert not ref_oracle.ReferenceOperator(reference, x).overlap_signature()["indefinite"]
+    pencil = synthetic.scaled_overlap(x, synthetic.singular_overlap_factor(minimum, x.regularization))
+    m, indefinite, singular = sdft_oracle.metric_signature(sdft_oracle.Operator(pencil))
+    assert singular and not indefinite and abs(m) < 1e-13
+    with pytest.raises(RuntimeError, match="original PAW overlap is numerically singular"):
+        ref_oracle.ReferenceOperator(reference, pencil).overlap_signature()
+    pencil = synthetic.scaled_overlap(x, 1.5)
+    m, indefinite, singular = sdft_oracle.metric_signature(sdft_oracle.Operator(pencil))
+    assert indefinite and not singular and m < -0.01
+    assert ref_oracle.ReferenceOperator(reference, pencil).overlap_signature()["indefinite"]
+
+
+@pytest.mark.parametrize("name,factory", [("tiny", synthetic.tiny), ("si8", synthetic.si8)])
 def test_enumeration_bit_exact_against_golden(golden, name, factory):
     g = golden(name)
     x = factory()
