@@ -53,6 +53,16 @@ SDFT_B200_API const char* sdft_b200_version(void);
  * backs the benchmark's launch accounting. */
 SDFT_B200_API unsigned long long sdft_b200_kernel_launches(void);
 
+/* The tensor-core GEMM tile autotuner's table so far (process-wide): per
+ * shape class five values -- rows rounded up to 128, real columns (twice the
+ * complex columns) rounded up to 32, K blocks of 64, the chosen column tile
+ * width and split-K count -- into rows[0 .. 5*capacity). *count receives the
+ * number of classes. The first product of a class times each candidate
+ * (three tile widths x split counts around the cost model's) on its stream
+ * and keeps the fastest; SDFT_B200_GEMM_AUTOTUNE=0 uses the cost model only.
+ * No reference counterpart (the reference calls a library ZGEMM). */
+SDFT_B200_API sdft_b200_status sdft_b200_gemm_tuned_classes(size_t capacity, int32_t* rows, size_t* count);
+
 /* One CUDA stream + library handles on `device`. `stream` may be NULL (a
  * private non-blocking stream is created) or a cudaStream_t to share.
  * Replaces: make_cuda_accelerator() / class Accelerator, src/compute_backend.hpp:64-91. */
@@ -319,14 +329,42 @@ enum { SDFT_B200_OP_NORMAL = 0, SDFT_B200_OP_ADJOINT = 1 };
 
 /* C(m x n, ldc) = op(A) op(B) (+ C when add), column-major complex with
  * explicit leading dimensions. FP64: FP64 arithmetic (cuBLAS ZGEMM). MIXED:
- * BF16 split products on the tcgen05 tensor cores with FP32 accumulation
- * (op(B) must be NORMAL). memory applies to a, b and c.
+ * BF16 split products on the tcgen05 tensor cores with FP32 accumulation (an
+ * ADJOINT right operand is formed as B^H on the device first). memory applies
+ * to a, b and c.
  * Replaces: complex_gemm(MatrixOp, MatrixOp, m, n, k, a, lda, b, ldb, c, ldc, exact, add),
  * src/compute_backend.hpp:23-26 (exact=true -> FP64, exact=false -> MIXED). */
 SDFT_B200_API sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int bop, size_t m,
                                                       size_t n, size_t k, const double* a, size_t lda,
                                                       const double* b, size_t ldb, double* c, size_t ldc,
                                                       int precision, int add, int memory);
+
+/* C(m x n, ldc) = op(A) B (+ C when add) for a left operand A that the caller
+ * promises immutable for `identity` (nonzero, e.g. from the reference's
+ * new_immutable_matrix_identity()): A (op(A) m x k; stored rows x cols with
+ * leading dimension lda) is copied to the device on the first call for that
+ * identity and operation and reused afterwards (MIXED also keeps its
+ * tensor-core packing); B (k x n, ldb) and C are dynamic. Four operands stay
+ * cached per context, least recently used replaced. A changed A must come
+ * with a new identity: the cache never re-reads it.
+ * Replaces: Accelerator::gemm_immutable_left / complex_gemm_immutable_left,
+ * src/compute_backend.hpp:32-41,68-71 (src/compute_backend.cpp:87-100). */
+SDFT_B200_API sdft_b200_status sdft_b200_complex_gemm_immutable_left(sdft_b200_context* context, uint64_t identity,
+                                                                     int aop, size_t m, size_t n, size_t k,
+                                                                     const double* a, size_t lda, const double* b,
+                                                                     size_t ldb, double* c, size_t ldc, int precision,
+                                                                     int add, int memory);
+
+/* C_i(m x n, ldc) = A_i B for i = 0, 1, 2 (A_i m x k with leading dimension
+ * lda, B k x n with ldb shared: staged once). Outputs must not overlap B, the
+ * A_i or each other (INVALID_ARGUMENT, as the reference checks). FP64, or the
+ * tensor-core split products for MIXED.
+ * Replaces: Accelerator::gemm_triple_right / complex_gemm_triple_right,
+ * src/compute_backend.hpp:72-77, src/compute_backend.cpp:255-332. */
+SDFT_B200_API sdft_b200_status sdft_b200_complex_gemm_triple_right(sdft_b200_context* context, size_t m, size_t n,
+                                                                   size_t k, const double* const a[3], size_t lda,
+                                                                   const double* b, size_t ldb, double* const c[3],
+                                                                   size_t ldc, int precision, int memory);
 
 /* Davidson controls. precision selects the search arithmetic (MIXED: FP32
  * FFT/V_loc and FP32-accumulated projector and subspace products; FP64: the
@@ -361,6 +399,9 @@ typedef struct {
   size_t h_columns_search, h_columns_fp64, s_columns_search, s_columns_fp64;
   int rayleigh_ritz_calls, restarts, fp64_refreshes, certifications, handoff_iteration, block_rank_fallbacks;
   size_t correction_columns; /* mixed-form pair applies spent on Jacobi-Davidson corrections, in columns */
+  /* strict FP64 refinements (src/strict_residual_polish.hpp): tangent polish
+   * steps tried / accepted, root-manifold steps tried / accepted */
+  int polish_steps, polish_accepted, manifold_steps, manifold_accepted;
 } sdft_b200_davidson_stats;
 
 /* Lowest `roots` eigenpairs of H~ x = e S~ x. initial: band-major roots x npw

@@ -79,6 +79,10 @@ void copy_stats(const sdft_b200::DavidsonStats& st, sdft_b200_davidson_stats* st
   stats->handoff_iteration = st.handoff_iteration;
   stats->block_rank_fallbacks = st.block_rank_fallbacks;
   stats->correction_columns = static_cast<size_t>(st.correction_columns);
+  stats->polish_steps = st.polish_steps;
+  stats->polish_accepted = st.polish_accepted;
+  stats->manifold_steps = st.manifold_steps;
+  stats->manifold_accepted = st.manifold_accepted;
 }
 
 template <typename F>
@@ -733,12 +737,20 @@ sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int
     if (std::max({m, n, k, lda, ldb, ldc}) > static_cast<size_t>(INT32_MAX))
       throw std::overflow_error("BLAS dimension overflow");
     const Precision p = precision_of(precision);
-    require(p == Precision::FP64 || bop == SDFT_B200_OP_NORMAL, "mixed complex GEMM needs a normal right operand");
     auto& ctx = *context->impl;
     SDFT_CUDA(cudaSetDevice(ctx.device));
     Staged stage(ctx, memory);
     const auto* da = stage.in(a, lda * (ac - 1) + ar, ctx.staging_in);
     const auto* db = stage.in(b, ldb * (bc - 1) + br, ctx.staging_aux);
+    if (p == Precision::Mixed && bop == SDFT_B200_OP_ADJOINT) {
+      // The tensor cores take a normal right operand: form B^H (k x n) first.
+      auto* adjoint = static_cast<Cx<double>*>(ctx.tc.adjoint.reserve(sizeof(Cx<double>) * k * n));
+      sdft_b200::adjoint_block(db, static_cast<long long>(ldb), static_cast<int>(n), static_cast<int>(k), adjoint,
+                               static_cast<long long>(k), ctx.stream);
+      db = adjoint;
+      ldb = k;
+      bop = SDFT_B200_OP_NORMAL;
+    }
     const std::size_t csize = ldc * (n - 1) + m;
     Cx<double>* dc = stage.out(c, csize, ctx.staging_out);
     if (add) stage.matrix_in(dc, c, m, n, ldc);
@@ -753,6 +765,123 @@ sdft_b200_status sdft_b200_complex_gemm(sdft_b200_context* context, int aop, int
                          static_cast<long long>(lda), nullptr, db, static_cast<long long>(ldb), dc,
                          static_cast<long long>(ldc), add != 0, 1.0, sdft_b200::search_split(), ctx.tc, ctx.stream);
     stage.matrix_back(c, dc, m, n, ldc);
+    ctx.synchronize();
+    if (sdft_b200::umma_error_flag()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
+  });
+}
+
+sdft_b200_status sdft_b200_gemm_tuned_classes(size_t capacity, int32_t* rows, size_t* count) {
+  return guarded([&] {
+    require(count != nullptr && (rows != nullptr || capacity == 0), "invalid tuning table buffer");
+    *count = sdft_b200::gemm_tuned_classes(capacity, rows);
+  });
+}
+
+sdft_b200_status sdft_b200_complex_gemm_immutable_left(sdft_b200_context* context, uint64_t identity, int aop,
+                                                       size_t m, size_t n, size_t k, const double* a, size_t lda,
+                                                       const double* b, size_t ldb, double* c, size_t ldc,
+                                                       int precision, int add, int memory) {
+  return guarded([&] {
+    require(context && identity && m && n && k && a && b && c && ldb >= k && ldc >= m &&
+                (aop == SDFT_B200_OP_NORMAL || aop == SDFT_B200_OP_ADJOINT) &&
+                lda >= (aop == SDFT_B200_OP_NORMAL ? m : k),
+            "invalid immutable GEMM operand");
+    if (std::max({m, n, k, lda, ldb, ldc}) > static_cast<size_t>(INT32_MAX))
+      throw std::overflow_error("immutable BLAS dimension overflow");
+    const Precision p = precision_of(precision);
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    Staged stage(ctx, memory);
+    const std::size_t ar = aop == SDFT_B200_OP_NORMAL ? m : k, ac = aop == SDFT_B200_OP_NORMAL ? k : m;
+    const sdft_b200::Op ao = aop == SDFT_B200_OP_NORMAL ? sdft_b200::Op::N : sdft_b200::Op::C;
+    auto& cache = ctx.immutable;
+    sdft_b200::ImmutableLeft* entry = nullptr;
+    for (auto& e : cache.entries)
+      if (e.identity == identity && e.aop == aop && e.rows == ar && e.cols == ac) entry = &e;
+    if (!entry) {
+      entry = &cache.entries[0];
+      for (auto& e : cache.entries)
+        if (e.used < entry->used) entry = &e;
+      entry->identity = 0;  // not valid until the copy below is queued
+      sdft_b200::release(entry->packed);
+      auto* dst = static_cast<Cx<double>*>(entry->fp64.reserve(sizeof(Cx<double>) * ar * ac));
+      if (memory == SDFT_B200_MEMORY_DEVICE) require_device_memory(a, ctx.device, "a");
+      SDFT_CUDA(cudaMemcpy2DAsync(dst, sizeof(Cx<double>) * ar, a, sizeof(Cx<double>) * lda, sizeof(Cx<double>) * ar,
+                                  ac, memory == SDFT_B200_MEMORY_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  ctx.stream));
+      entry->identity = identity;
+      entry->aop = aop;
+      entry->rows = ar;
+      entry->cols = ac;
+    }
+    entry->used = ++cache.clock;
+    const auto* da = static_cast<const Cx<double>*>(entry->fp64.ptr);
+    const auto* db = stage.in(b, ldb * (n - 1) + k, ctx.staging_aux);
+    Cx<double>* dc = stage.out(c, ldc * (n - 1) + m, ctx.staging_out);
+    if (add) stage.matrix_in(dc, c, m, n, ldc);
+    if (p == Precision::FP64) {
+      sdft_b200::zgemm(ctx.blas, ao, sdft_b200::Op::N, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k),
+                       da, static_cast<long long>(ar), db, static_cast<long long>(ldb), dc,
+                       static_cast<long long>(ldc), add != 0);
+    } else {
+      const sdft_b200::Split split = sdft_b200::search_split();
+      if (!entry->packed.data || entry->packed.split != split)
+        sdft_b200::pack_persistent(ao, da, static_cast<long long>(ar), static_cast<int>(m), static_cast<int>(k),
+                                   split, entry->packed, ctx.stream);
+      sdft_b200::gemm_tc(ao, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), da,
+                         static_cast<long long>(ar), &entry->packed, db, static_cast<long long>(ldb), dc,
+                         static_cast<long long>(ldc), add != 0, 1.0, split, ctx.tc, ctx.stream);
+    }
+    stage.matrix_back(c, dc, m, n, ldc);
+    ctx.synchronize();
+    if (sdft_b200::umma_error_flag()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
+  });
+}
+
+sdft_b200_status sdft_b200_complex_gemm_triple_right(sdft_b200_context* context, size_t m, size_t n, size_t k,
+                                                     const double* const a[3], size_t lda, const double* b,
+                                                     size_t ldb, double* const c[3], size_t ldc, int precision,
+                                                     int memory) {
+  return guarded([&] {
+    require(context && a && c && b && m && n && k && lda >= m && ldb >= k && ldc >= m,
+            "invalid joint Ritz rotation dimensions");
+    for (int i = 0; i < 3; ++i) require(a[i] && c[i], "invalid joint Ritz rotation dimensions");
+    if (std::max({m, n, k, lda, ldb, ldc}) > static_cast<size_t>(INT32_MAX))
+      throw std::overflow_error("joint Ritz rotation BLAS dimensions overflow");
+    // Address intervals of the operands, as the reference checks them
+    // (src/compute_backend.cpp:262-282).
+    auto interval = [](const void* p, std::size_t rows, std::size_t columns, std::size_t ld) {
+      const auto first = reinterpret_cast<std::uintptr_t>(p);
+      return std::make_pair(first, first + ((columns - 1) * ld + rows) * sizeof(Cx<double>));
+    };
+    auto overlaps = [](auto x, auto y) { return x.first < y.second && y.first < x.second; };
+    const auto right = interval(b, k, n, ldb);
+    for (int i = 0; i < 3; ++i) {
+      const auto out = interval(c[i], m, n, ldc);
+      require(!overlaps(out, right), "joint Ritz output aliases right operand");
+      for (int j = 0; j < 3; ++j)
+        require(!overlaps(out, interval(a[j], m, k, lda)) && (i == j || !overlaps(out, interval(c[j], m, n, ldc))),
+                "joint Ritz outputs/inputs must be disjoint");
+    }
+    const Precision p = precision_of(precision);
+    auto& ctx = *context->impl;
+    SDFT_CUDA(cudaSetDevice(ctx.device));
+    Staged stage(ctx, memory);
+    const auto* db = stage.in(b, ldb * (n - 1) + k, ctx.staging_aux);
+    const sdft_b200::Split split = sdft_b200::search_split();
+    for (int i = 0; i < 3; ++i) {
+      const auto* da = stage.in(a[i], lda * (k - 1) + m, ctx.staging_in);
+      Cx<double>* dc = stage.out(c[i], ldc * (n - 1) + m, ctx.staging_out);
+      if (p == Precision::FP64)
+        sdft_b200::zgemm(ctx.blas, sdft_b200::Op::N, sdft_b200::Op::N, static_cast<int>(m), static_cast<int>(n),
+                         static_cast<int>(k), da, static_cast<long long>(lda), db, static_cast<long long>(ldb), dc,
+                         static_cast<long long>(ldc), false);
+      else
+        sdft_b200::gemm_tc(sdft_b200::Op::N, static_cast<int>(m), static_cast<int>(n), static_cast<int>(k), da,
+                           static_cast<long long>(lda), nullptr, db, static_cast<long long>(ldb), dc,
+                           static_cast<long long>(ldc), false, 1.0, split, ctx.tc, ctx.stream);
+      stage.matrix_back(c[i], dc, m, n, ldc);
+    }
     ctx.synchronize();
     if (sdft_b200::umma_error_flag()) throw sdft_b200::CudaError("tensor-core GEMM wait limit exceeded");
   });

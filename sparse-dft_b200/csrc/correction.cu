@@ -1,8 +1,8 @@
 // Jacobi-Davidson corrections with preconditioned CG (the mixed form's
 // expansion step; see correction.cuh).
 //
-// Per CG step, for all selected columns at once: one mixed-form (H p, S p)
-// pair apply, the shifted product q = H p - theta S p, the left projection
+// Per CG step, for all selected columns at once: the mixed-form shifted
+// product q = (H - theta S) p (one projection and back-projection), the left projection
 // q <- q - S X (X^H q), the step length alpha = (res, z) / (p, q) per column,
 // t += alpha p, res -= alpha q, then z = P res, the right projection
 // z <- z - X ((S X)^H z) and the next direction p = z + beta p. Every scalar
@@ -19,6 +19,7 @@ namespace sdft_b200 {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kDotThreads = 1024;  // one CTA per column: the column's NPW terms over 1024 threads
 
 __device__ double block_sum(double value, double* shared) {
   const int tid = threadIdx.x;
@@ -73,9 +74,10 @@ __global__ void precondition_kernel(const Cx<double>* __restrict__ res, int rows
 }
 
 // out[j] = Re sum_i conj(a(i, j)) b(i, j).
-__global__ void column_dots_kernel(const Cx<double>* __restrict__ a, const Cx<double>* __restrict__ b, int rows,
-                                   double* __restrict__ out) {
-  __shared__ double shared[kThreads];
+__global__ void __launch_bounds__(kDotThreads) column_dots_kernel(const Cx<double>* __restrict__ a,
+                                                                  const Cx<double>* __restrict__ b, int rows,
+                                                                  double* __restrict__ out) {
+  __shared__ double shared[kDotThreads];
   const long long base = static_cast<long long>(blockIdx.x) * rows;
   double s = 0.0;
   for (int i = threadIdx.x; i < rows; i += blockDim.x) s += a[base + i].re * b[base + i].re + a[base + i].im * b[base + i].im;
@@ -83,34 +85,32 @@ __global__ void column_dots_kernel(const Cx<double>* __restrict__ a, const Cx<do
   if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
-// hp(:, j) -= theta[j] sp(:, j).
-__global__ void shift_kernel(Cx<double>* __restrict__ hp, const Cx<double>* __restrict__ sp, int rows,
-                             const double* __restrict__ theta) {
-  const int j = blockIdx.y;
-  const double s = theta[j];
-  const long long base = static_cast<long long>(j) * rows;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const Cx<double> h = hp[base + i], v = sp[base + i];
-    hp[base + i] = Cx<double>{h.re - s * v.re, h.im - s * v.im};
-  }
-}
-
 __device__ __forceinline__ double step_length(double rz, double pq) {
   return (pq > 0.0 && isfinite(pq) && isfinite(rz)) ? rz / pq : 0.0;
 }
 
-// t += alpha p, res -= alpha q with alpha = rz / pq per column.
+// t += alpha p, res -= alpha q with alpha = rz / pq per column; with z given,
+// also z = P(T, energy[j]) res for the next direction (one pass over res).
 __global__ void cg_step_kernel(Cx<double>* __restrict__ t, Cx<double>* __restrict__ res, const Cx<double>* __restrict__ p,
                                const Cx<double>* __restrict__ q, int rows, const double* __restrict__ rz,
-                               const double* __restrict__ pq) {
+                               const double* __restrict__ pq, const double* __restrict__ kinetic,
+                               const double* __restrict__ energy, Cx<double>* __restrict__ z) {
   const int j = blockIdx.y;
   const double alpha = step_length(rz[j], pq[j]);
-  if (alpha == 0.0) return;
+  const double e = z ? energy[j] : 0.0;
   const long long base = static_cast<long long>(j) * rows;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const Cx<double> pv = p[base + i], qv = q[base + i], tv = t[base + i], rv = res[base + i];
-    t[base + i] = Cx<double>{tv.re + alpha * pv.re, tv.im + alpha * pv.im};
-    res[base + i] = Cx<double>{rv.re - alpha * qv.re, rv.im - alpha * qv.im};
+    Cx<double> rv = res[base + i];
+    if (alpha != 0.0) {
+      const Cx<double> pv = p[base + i], qv = q[base + i], tv = t[base + i];
+      t[base + i] = Cx<double>{tv.re + alpha * pv.re, tv.im + alpha * pv.im};
+      rv = Cx<double>{rv.re - alpha * qv.re, rv.im - alpha * qv.im};
+      res[base + i] = rv;
+    }
+    if (z) {
+      const double scale = kinetic_preconditioner(kinetic[i], e);
+      z[base + i] = Cx<double>{rv.re * scale, rv.im * scale};
+    }
   }
 }
 
@@ -163,7 +163,6 @@ void jacobi_davidson_corrections(DeviceOperator& op, CorrectionBuffers& buf, con
   Cx<double>* z = as<Cx<double>>(buf.z, block);
   Cx<double>* p = as<Cx<double>>(buf.p, block);
   Cx<double>* hp = as<Cx<double>>(buf.hp, block);
-  Cx<double>* sp = as<Cx<double>>(buf.sp, block);
   Cx<double>* coef = as<Cx<double>>(buf.coefficients, static_cast<std::size_t>(roots) * count);
   double* scalars = as<double>(buf.scalars, 5 * static_cast<std::size_t>(count));
   double* theta = scalars;
@@ -189,7 +188,7 @@ void jacobi_davidson_corrections(DeviceOperator& op, CorrectionBuffers& buf, con
     project_right(z);
   };
   auto dots = [&](const Cx<double>* a, const Cx<double>* b, double* dst) {
-    column_dots_kernel<<<count, kThreads, 0, st>>>(a, b, n, dst);
+    column_dots_kernel<<<count, kDotThreads, 0, st>>>(a, b, n, dst);
     SDFT_LAUNCH("column_dots_kernel");
   };
 
@@ -205,15 +204,15 @@ void jacobi_davidson_corrections(DeviceOperator& op, CorrectionBuffers& buf, con
   for (int step = 0; step < steps; ++step) {
     double* rz_old = rz[step & 1];
     double* rz_new = rz[(step + 1) & 1];
-    op.apply_pair(p, count, hp, sp, Precision::Mixed);
-    shift_kernel<<<grid, kThreads, 0, st>>>(hp, sp, n, theta);
-    SDFT_LAUNCH("shift_kernel");
+    op.apply_shifted(p, count, theta, hp, Precision::Mixed);  // (H - theta S) p
     project_left(hp);
     dots(p, hp, pq);
-    cg_step_kernel<<<grid, kThreads, 0, st>>>(t, res, p, hp, n, rz_old, pq);
+    const bool last = step + 1 == steps;
+    cg_step_kernel<<<grid, kThreads, 0, st>>>(t, res, p, hp, n, rz_old, pq, op.device_kinetic(), energy,
+                                              last ? nullptr : z);
     SDFT_LAUNCH("cg_step_kernel");
-    if (step + 1 == steps) break;
-    precondition();
+    if (last) break;
+    project_right(z);
     dots(res, z, rz_new);
     cg_direction_kernel<<<grid, kThreads, 0, st>>>(p, z, n, rz_new, rz_old);
     SDFT_LAUNCH("cg_direction_kernel");

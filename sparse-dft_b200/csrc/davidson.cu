@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
+#include <limits>
 #include <numeric>
 #include <string>
 
@@ -32,6 +33,14 @@ void check_solver(cusolverStatus_t status, const char* what) {
 void check_blas(cublasStatus_t status, const char* what) {
   if (status != CUBLAS_STATUS_SUCCESS)
     throw CudaError(std::string("cuBLAS error ") + std::to_string(static_cast<int>(status)) + " in " + what);
+}
+// The reference's 0/1 environment switches (src/pw_core.cpp:598-603).
+bool boolean_control(const char* name, bool fallback) {
+  const char* flag = std::getenv(name);
+  if (!flag) return fallback;
+  const std::string value(flag);
+  if (value != "0" && value != "1") throw InvalidArgument(std::string(name) + " must be 0 or 1");
+  return value == "1";
 }
 double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -370,6 +379,189 @@ void DavidsonSolver::certify() {
   SDFT_CUDA(cudaMemcpyAsync(w_, values, sizeof(double) * roots_, cudaMemcpyDeviceToDevice, st));
 }
 
+double DavidsonSolver::max_residual() const {
+  return residual_norms_.empty() ? 0.0 : *std::max_element(residual_norms_.begin(), residual_norms_.end());
+}
+
+// Normalises `trial` in the S metric with a fresh FP64 pair, re-applies the
+// pair to the normalised block, certifies it, and keeps it in place of X only
+// when it is S-orthonormal within 1e-12 (and S-orthogonal to completed bands)
+// and its fresh maximum residual meets the tolerance or is below 0.999 of
+// old_max (src/strict_residual_polish.hpp:97-115, 169-195).
+bool DavidsonSolver::commit_trial(Cx<double>* trial, Cx<double>* th, Cx<double>* ts, Cx<double>* errors,
+                                  double old_max) {
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  apply_pair(trial, roots_, th, ts, true);
+  metric_norms(trial, ts, n_, n_, roots_, dsmall_, st);
+  for (double m : download(dsmall_, roots_))
+    if (!std::isfinite(m) || !(m > 0)) return false;
+  scale_columns(trial, n_, n_, roots_, dsmall_, true, st);
+  apply_pair(trial, roots_, th, ts, true);
+  double* values = dsmall_ + roots_;
+  double* metrics = dsmall_ + 2 * roots_;
+  double* norms = dsmall_ + 3 * roots_;
+  rayleigh_certificate(trial, th, ts, n_, n_, roots_, values, metrics, errors, norms, st);
+  const auto energies = download(values, roots_);
+  const auto fresh = download(norms, roots_);
+  double new_max = 0.0;
+  for (std::size_t i = 0; i < fresh.size(); ++i) {
+    if (!std::isfinite(fresh[i]) || !std::isfinite(energies[i])) return false;
+    new_max = std::max(new_max, fresh[i]);
+  }
+  Cx<double>* gram = as<Cx<double>>(gram_, static_cast<std::size_t>(kmax_) * kmax_ * 4);
+  zgemm(ctx.blas, Op::C, Op::N, roots_, roots_, n_, trial, n_, ts, n_, gram, roots_, false);
+  const double deviation = identity_deviation(gram, roots_, eigen_, st);
+  if (!std::isfinite(deviation) || deviation > 1e-12) return false;
+  if (excluded_count_) {
+    std::vector<Cx<double>> overlap(static_cast<std::size_t>(excluded_count_) * roots_);
+    zgemm(ctx.blas, Op::C, Op::N, excluded_count_, roots_, n_, excluded_s_, n_, trial, n_, gram, excluded_count_,
+          false);
+    SDFT_CUDA(cudaMemcpyAsync(overlap.data(), gram, sizeof(Cx<double>) * overlap.size(), cudaMemcpyDeviceToHost, st));
+    ctx.synchronize();
+    for (const auto& v : overlap)
+      if (!(std::hypot(v.re, v.im) <= 1e-12)) return false;
+  }
+  if (!(new_max <= tolerance_ || new_max < 0.999 * old_max)) return false;
+  const std::size_t block = static_cast<std::size_t>(n_) * roots_;
+  SDFT_CUDA(cudaMemcpyAsync(x_, trial, sizeof(Cx<double>) * block, cudaMemcpyDeviceToDevice, st));
+  SDFT_CUDA(cudaMemcpyAsync(sx_, ts, sizeof(Cx<double>) * block, cudaMemcpyDeviceToDevice, st));
+  SDFT_CUDA(cudaMemcpyAsync(hx_, th, sizeof(Cx<double>) * block, cudaMemcpyDeviceToDevice, st));
+  SDFT_CUDA(cudaMemcpyAsync(r_, errors, sizeof(Cx<double>) * block, cudaMemcpyDeviceToDevice, st));
+  SDFT_CUDA(cudaMemcpyAsync(w_, values, sizeof(double) * roots_, cudaMemcpyDeviceToDevice, st));
+  values_ = energies;
+  residual_norms_ = fresh;
+  return true;
+}
+
+// src/strict_residual_polish.hpp:70-116: the generalized Ritz problem of the
+// original pair inside span(X) (compensated inner products), solved by the
+// device Rayleigh-Ritz; it repairs rotations among the requested roots that a
+// tangent step, orthogonal to all of them, cannot.
+bool DavidsonSolver::root_manifold_step() {
+  const double old_max = max_residual();
+  if (old_max <= tolerance_) return false;
+  ++stats_.manifold_steps;
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  const std::size_t block = static_cast<std::size_t>(n_) * roots_;
+  Cx<double>* base = as<Cx<double>>(b_.polish, 6 * block);
+  Cx<double>* trial = base;
+  Cx<double>* th = base + block;
+  Cx<double>* ts = base + 2 * block;
+  Cx<double>* hx = base + 3 * block;
+  Cx<double>* sx = base + 4 * block;
+  apply_pair(x_, roots_, hx, sx, true);
+  const std::size_t rr = static_cast<std::size_t>(roots_) * roots_;
+  Cx<double>* small = as<Cx<double>>(b_.polish_small, 4 * rr);
+  compensated_inner_matrix(x_, hx, n_, n_, roots_, roots_, small, roots_, st);
+  compensated_inner_matrix(x_, sx, n_, n_, roots_, roots_, small + rr, roots_, st);
+  hermitian_part(small, roots_, small + 2 * rr, roots_, roots_, st);
+  hermitian_part(small + rr, roots_, small + 3 * rr, roots_, roots_, st);
+  double* values = as<double>(b_.polish_values, roots_);
+  generalized_lowest(ctx.blas, ctx.solver, small + 2 * rr, small + 3 * rr, roots_, roots_, values, small + 2 * rr,
+                     eigen_, rr_mode(), st);
+  zgemm(ctx.blas, Op::N, Op::N, n_, roots_, roots_, x_, n_, small + 2 * rr, roots_, trial, n_, false);
+  const bool accepted = commit_trial(trial, th, ts, hx, old_max);
+  if (accepted) ++stats_.manifold_accepted;
+  return accepted;
+}
+
+// src/strict_residual_polish.hpp:118-197: per root, the step alpha = -g/c
+// along the preconditioned residual d (S-orthogonalised twice against the
+// completed bands and X), g = Re<d, r>, c = Re<d, H d> - e Re<d, S d>, taken
+// only when alpha > 0 and alpha |d| <= 1e-4, with x + alpha d formed by fma.
+bool DavidsonSolver::tangent_polish_step() {
+  const double old_max = max_residual();
+  if (old_max <= tolerance_) return false;
+  ++stats_.polish_steps;
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  const std::size_t block = static_cast<std::size_t>(n_) * roots_;
+  Cx<double>* base = as<Cx<double>>(b_.polish, 6 * block);
+  Cx<double>* trial = base;
+  Cx<double>* th = base + block;
+  Cx<double>* ts = base + 2 * block;
+  Cx<double>* d = base + 3 * block;
+  Cx<double>* dh = base + 4 * block;
+  Cx<double>* ds = base + 5 * block;
+  kinetic_precondition(r_, x_, n_, n_, roots_, op_.device_kinetic(), d, n_, st);  // -P r
+  Cx<double>* coef = as<Cx<double>>(b_.polish_small, 4 * static_cast<std::size_t>(roots_) * roots_);
+  for (int pass = 0; pass < 2; ++pass) {
+    if (excluded_count_) remove_excluded(d, roots_);
+    zgemm(ctx.blas, Op::C, Op::N, roots_, roots_, n_, sx_, n_, d, n_, coef, roots_, false);
+    zgemm(ctx.blas, Op::N, Op::N, n_, roots_, roots_, x_, n_, coef, roots_, d, n_, true, -1.0);
+  }
+  apply_pair(d, roots_, dh, ds, true);
+  metric_norms(d, r_, n_, n_, roots_, dsmall_, st);
+  metric_norms(d, dh, n_, n_, roots_, dsmall_ + roots_, st);
+  metric_norms(d, ds, n_, n_, roots_, dsmall_ + 2 * roots_, st);
+  column_norms(d, n_, n_, roots_, dsmall_ + 3 * roots_, st);
+  const auto scalars = download(dsmall_, 4 * roots_);
+  std::vector<double> alpha(roots_, 0.0);
+  bool moved = false;
+  for (int root = 0; root < roots_; ++root) {
+    if (residual_norms_[root] <= 0.5 * tolerance_) continue;
+    const double gradient = scalars[root];
+    const double curvature = scalars[roots_ + root] - values_[root] * scalars[2 * roots_ + root];
+    if (!(curvature > 0.0) || !std::isfinite(curvature) || !std::isfinite(gradient)) continue;
+    const double a = -gradient / curvature;
+    if (!(a > 0.0) || !std::isfinite(a) || a * scalars[3 * roots_ + root] > 1e-4) continue;
+    alpha[root] = a;
+    moved = true;
+  }
+  if (!moved) return false;
+  double* dalpha = as<double>(b_.polish_values, roots_);
+  SDFT_CUDA(cudaMemcpyAsync(dalpha, alpha.data(), sizeof(double) * roots_, cudaMemcpyHostToDevice, st));
+  fma_columns(dalpha, d, x_, n_, n_, roots_, trial, st);
+  const bool accepted = commit_trial(trial, th, ts, d, old_max);
+  if (accepted) ++stats_.polish_accepted;
+  return accepted;
+}
+
+void DavidsonSolver::preserve_search_subspace() {
+  auto& ctx = op_.context();
+  const cudaStream_t st = ctx.stream;
+  const bool at_capacity = size_ + roots_ > capacity_;
+  const int keep = at_capacity ? std::min(size_, 2 * roots_) : size_;
+  Cx<double>* retained = hv_;  // the images are recomputed for the new basis
+  copy_block(x_, n_, retained, n_, n_, roots_, st);
+  if (keep > roots_) {
+    Cx<double>* rest = retained + static_cast<long long>(roots_) * n_;
+    if (at_capacity) {
+      const Cx<double>* rotation = static_cast<const Cx<double>*>(rr_a_.ptr);
+      gemm(Op::N, n_, keep - roots_, size_, v_, n_, rotation + static_cast<long long>(roots_) * size_, size_, rest,
+           n_, false, 1.0, true);
+    } else {
+      // Complement of X in the basis: V Q2, Q2 the columns of the full Q of
+      // the QR factorisation of V^H S X beyond the first roots.
+      auto* q = as<Cx<double>>(rr_b_, static_cast<std::size_t>(size_) * size_);
+      gemm(Op::C, size_, roots_, n_, v_, n_, sx_, n_, q, size_, false, 1.0, true);
+      auto* tau = as<cuDoubleComplex>(small_, static_cast<std::size_t>(std::max(kmax_, roots_)) * 2);
+      int lwork = 0, lwork2 = 0;
+      auto* qz = reinterpret_cast<cuDoubleComplex*>(q);
+      check_solver(cusolverDnZgeqrf_bufferSize(ctx.solver, size_, roots_, qz, size_, &lwork), "zgeqrf_bufferSize");
+      check_solver(cusolverDnZungqr_bufferSize(ctx.solver, size_, size_, roots_, qz, size_, tau, &lwork2),
+                   "zungqr_bufferSize");
+      const int work_size = std::max({1, lwork, lwork2});
+      auto* work = as<cuDoubleComplex>(rr_work_, static_cast<std::size_t>(work_size));
+      int* info = as<int>(info_, 4);
+      check_solver(cusolverDnZgeqrf(ctx.solver, size_, roots_, qz, size_, tau, work, work_size, info), "zgeqrf");
+      check_solver(cusolverDnZungqr(ctx.solver, size_, size_, roots_, qz, size_, tau, work, work_size, info),
+                   "zungqr");
+      int host_info = 0;
+      SDFT_CUDA(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+      ctx.synchronize();
+      if (host_info) throw std::runtime_error("corrected Davidson search subspace factorisation failed");
+      gemm(Op::N, n_, size_ - roots_, size_, v_, n_, q + static_cast<long long>(roots_) * size_, size_, rest, n_,
+           false, 1.0, true);
+    }
+  }
+  size_ = computed_h_ = projected_size_ = 0;
+  for (int first = 0; first < keep; first += kmax_)
+    append_block(retained + static_cast<long long>(first) * n_, std::min(kmax_, keep - first));
+}
+
 void DavidsonSolver::refresh_images() {
   apply_pair(v_, size_, hv_, sv_, true);
   computed_h_ = size_;
@@ -412,6 +604,12 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
   }
   incremental_ = o.tolerance >= 1e-12;
   strict_projection_ = false;
+  // The reference's strict-refinement switches (src/pw_core.cpp:611-612),
+  // off for band-group local solves with an explicit capacity (:1273).
+  polish_enabled_ = boolean_control("SDFT_FRESH_RESIDUAL_POLISH", true) && o.capacity <= 0;
+  manifold_enabled_ = boolean_control("SDFT_STRICT_ROOT_MANIFOLD", true);
+  polish_attempts_ = manifold_attempts_ = 0;
+  strict_entry_ = std::numeric_limits<double>::infinity();
   size_ = computed_h_ = projected_size_ = 0;
   residual_history_.clear();
   const std::size_t nc = static_cast<std::size_t>(n_) * capacity_;
@@ -598,9 +796,55 @@ void DavidsonSolver::solve(const DavidsonOptions& o, const Cx<double>* initial) 
         continue;
       }
     }
+    // Strict FP64 refinements once Davidson stalls at the FP64 floor
+    // (src/pw_core.cpp:1273-1336); every step counts against the iteration budget.
+    // The Jacobi-Davidson-steered mixed form converges faster through its own
+    // corrections than through tangent steps, so it refines only once two
+    // successive FP64 iterations fail to halve the residual.
+    bool strict_polished = false;
+    const std::size_t hist = residual_history_.size();
+    const bool fp64_stalled = hist >= 3 && residual_history_[hist - 1] > 0.5 * residual_history_[hist - 2] &&
+                              residual_history_[hist - 2] > 0.5 * residual_history_[hist - 3];
+    if (polish_enabled_ && exact_mode_ && !converged && tolerance_ <= 1e-12 && max_res <= 1e-10 &&
+        (correction_steps_ == 0 || fp64_stalled) && max_res < 0.5 * strict_entry_ &&
+        (polish_attempts_ < 16 || (manifold_enabled_ && manifold_attempts_ < 4))) {
+      auto all_converged = [&]() {
+        return std::all_of(residual_norms_.begin(), residual_norms_.end(), [&](double r) { return r <= tolerance_; });
+      };
+      if (!fresh) {
+        certify();
+        fresh = true;
+        converged = all_converged();
+      }
+      strict_entry_ = max_residual();
+      if (manifold_enabled_ && !converged && manifold_attempts_ < 4 && iteration + 1 < o.max_iterations) {
+        ++manifold_attempts_;
+        ++iteration;
+        stats_.iterations = iteration + 1;
+        strict_polished |= root_manifold_step();
+        converged = all_converged();
+      }
+      for (; !converged && polish_attempts_ < 16 && iteration + 1 < o.max_iterations; ++polish_attempts_) {
+        ++iteration;
+        stats_.iterations = iteration + 1;
+        const bool improved = tangent_polish_step();
+        strict_polished |= improved;
+        if (!improved) {
+          ++polish_attempts_;
+          break;
+        }
+        converged = all_converged();
+      }
+      max_res = max_residual();
+      phase("strict_refinement");
+    }
     if (converged) {
       certified = fresh;
       if (certified) break;
+    }
+    if (strict_polished && iteration + 1 < o.max_iterations) {
+      preserve_search_subspace();
+      phase("preserve");
     }
     // Thick restart (src/pw_core.cpp:1357-1383).
     if (size_ + roots_ > capacity_) {

@@ -36,6 +36,8 @@ struct DavidsonStats {
   int rayleigh_ritz = 0, restarts = 0, fp64_refreshes = 0, certifications = 0, handoff_iteration = -1;
   int block_rank_fallbacks = 0;
   long long correction_columns = 0;
+  // Strict FP64 refinements (tangent polish and root-manifold steps), tried / accepted.
+  int polish_steps = 0, polish_accepted = 0, manifold_steps = 0, manifold_accepted = 0;
   double seconds = 0.0, rr_seconds = 0.0;
 };
 
@@ -83,6 +85,19 @@ class DavidsonSolver {
   void remove_excluded(Cx<double>* vectors, int cols);
   void rayleigh_ritz();
   void certify();
+  // Strict FP64 refinements of a certified block that Davidson no longer
+  // improves (src/strict_residual_polish.hpp:70-197): a generalized Ritz
+  // problem inside span(X) and a per-root tangent line search along the
+  // projected, preconditioned residual. Each replaces X only with a fresh,
+  // improved FP64 certificate and S-orthonormality within 1e-12.
+  bool root_manifold_step();
+  bool tangent_polish_step();
+  // Keeps the polished X and the rest of the search space (its S-orthogonal
+  // complement in the basis, or the guard Ritz vectors at capacity) as the
+  // new basis (src/pw_core.cpp:1337-1356).
+  void preserve_search_subspace();
+  bool commit_trial(Cx<double>* trial, Cx<double>* th, Cx<double>* ts, Cx<double>* errors, double old_max);
+  double max_residual() const;
   void refresh_images();
   std::vector<double> download(const double* device, int count);
 
@@ -94,6 +109,9 @@ class DavidsonSolver {
   Cx<double>* excluded_s_ = nullptr;      // their S images
   int excluded_count_ = 0;
   bool exact_mode_ = true, incremental_ = true, strict_projection_ = false;
+  bool polish_enabled_ = true, manifold_enabled_ = true;
+  int polish_attempts_ = 0, manifold_attempts_ = 0;
+  double strict_entry_ = 0.0;
   double tolerance_ = 1e-10;
   DavidsonBuffers& b_;
   Scratch &basis_, &hbasis_, &sbasis_, &cached_h_, &cached_s_, &rr_a_, &rr_b_, &rr_w_, &rr_work_, &info_;

@@ -149,6 +149,36 @@ __global__ void metric_norms_kernel(const Cx<double>* __restrict__ x, const Cx<d
   if (threadIdx.x == 0) out[blockIdx.x] = v;
 }
 
+// out(i, j) = sum_k conj(a(k, i)) b(k, j) with compensated sums of the
+// reference's terms (re: a.re b.re + a.im b.im; im: a.re b.im - a.im b.re).
+__global__ void compensated_inner_matrix_kernel(const Cx<double>* __restrict__ a, const Cx<double>* __restrict__ b,
+                                                long long ld, int rows, Cx<double>* __restrict__ out, long long ldo) {
+  __shared__ Neumaier shared[kReduceThreads];
+  const long long ia = blockIdx.x * ld, jb = blockIdx.y * ld;
+  Neumaier re, im;
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+    const Cx<double> u = a[ia + i], v = b[jb + i];
+    re.add(__dmul_rn(u.re, v.re));
+    re.add(__dmul_rn(u.im, v.im));
+    im.add(__dmul_rn(u.re, v.im));
+    im.add(-__dmul_rn(u.im, v.re));
+  }
+  const double r = block_reduce_compensated(re, shared).value();
+  const double m = block_reduce_compensated(im, shared).value();
+  if (threadIdx.x == 0) out[blockIdx.x + blockIdx.y * ldo] = Cx<double>{r, m};
+}
+
+// out(:, c) = fma(alpha[c], d(:, c), x(:, c)) componentwise.
+__global__ void fma_columns_kernel(const double* __restrict__ alpha, const Cx<double>* __restrict__ d,
+                                   const Cx<double>* __restrict__ x, long long ld, int rows, Cx<double>* __restrict__ out) {
+  const double a = alpha[blockIdx.y];
+  const long long base = blockIdx.y * ld;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const Cx<double> dv = d[base + i], xv = x[base + i];
+    out[base + i] = Cx<double>{__fma_rn(a, dv.re, xv.re), __fma_rn(a, dv.im, xv.im)};
+  }
+}
+
 __global__ void scale_columns_kernel(Cx<double>* __restrict__ x, long long ld, int rows, const double* __restrict__ scale,
                                      bool reciprocal_sqrt) {
   const double s = reciprocal_sqrt ? 1.0 / sqrt(scale[blockIdx.y]) : scale[blockIdx.y];
@@ -290,6 +320,46 @@ void metric_norms(const Cx<double>* x, const Cx<double>* sx, long long ld, int r
   if (cols <= 0) return;
   metric_norms_kernel<<<cols, kReduceThreads, 0, stream>>>(x, sx, ld, rows, out);
   SDFT_LAUNCH("metric_norms_kernel");
+}
+
+__global__ void adjoint_block_kernel(const Cx<double>* __restrict__ src, long long lds, int rows, int cols,
+                                     Cx<double>* __restrict__ dst, long long ldd) {
+  __shared__ Cx<double> tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int i = i0 + threadIdx.x, j = j0 + dy;
+    if (i < rows && j < cols) tile[dy][threadIdx.x] = src[i + static_cast<long long>(j) * lds];
+  }
+  __syncthreads();
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int j = j0 + threadIdx.x, i = i0 + dy;
+    if (i < rows && j < cols) {
+      const Cx<double> v = tile[threadIdx.x][dy];
+      dst[j + static_cast<long long>(i) * ldd] = Cx<double>{v.re, -v.im};
+    }
+  }
+}
+
+void adjoint_block(const Cx<double>* src, long long lds, int rows, int cols, Cx<double>* dst, long long ldd,
+                   cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return;
+  const dim3 grid(static_cast<unsigned>(ceil_div(rows, 32)), static_cast<unsigned>(ceil_div(cols, 32)));
+  adjoint_block_kernel<<<grid, dim3(32, 8), 0, stream>>>(src, lds, rows, cols, dst, ldd);
+  SDFT_LAUNCH("adjoint_block_kernel");
+}
+
+void compensated_inner_matrix(const Cx<double>* a, const Cx<double>* b, long long ld, int rows, int cols_a,
+                              int cols_b, Cx<double>* out, long long ldo, cudaStream_t stream) {
+  if (cols_a <= 0 || cols_b <= 0) return;
+  compensated_inner_matrix_kernel<<<dim3(cols_a, cols_b), kReduceThreads, 0, stream>>>(a, b, ld, rows, out, ldo);
+  SDFT_LAUNCH("compensated_inner_matrix_kernel");
+}
+
+void fma_columns(const double* alpha, const Cx<double>* d, const Cx<double>* x, long long ld, int rows, int cols,
+                 Cx<double>* out, cudaStream_t stream) {
+  if (cols <= 0 || rows <= 0) return;
+  fma_columns_kernel<<<column_grid(rows, cols), 256, 0, stream>>>(alpha, d, x, ld, rows, out);
+  SDFT_LAUNCH("fma_columns_kernel");
 }
 
 void scale_columns(Cx<double>* x, long long ld, int rows, int cols, const double* scale, bool reciprocal_sqrt,

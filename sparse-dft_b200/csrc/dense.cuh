@@ -30,6 +30,20 @@ void rayleigh_certificate(const Cx<double>* x, const Cx<double>* hx, const Cx<do
 void metric_norms(const Cx<double>* x, const Cx<double>* sx, long long ld, int rows, int cols, double* out,
                   cudaStream_t stream);
 
+// out(i, j) = x_i^H y_j for columns i < cols_a of a and j < cols_b of b, with
+// the compensated complex inner product of the strict refinements
+// (src/strict_residual_polish.hpp:33-44).
+void compensated_inner_matrix(const Cx<double>* a, const Cx<double>* b, long long ld, int rows, int cols_a,
+                              int cols_b, Cx<double>* out, long long ldo, cudaStream_t stream);
+
+// dst (cols x rows, ldd) = src^H for src (rows x cols, lds).
+void adjoint_block(const Cx<double>* src, long long lds, int rows, int cols, Cx<double>* dst, long long ldd,
+                   cudaStream_t stream);
+
+// out(:, c) = fma(alpha[c], d(:, c), x(:, c)) per real component (alpha on the device).
+void fma_columns(const double* alpha, const Cx<double>* d, const Cx<double>* x, long long ld, int rows, int cols,
+                 Cx<double>* out, cudaStream_t stream);
+
 // x(:,c) *= scale[c]  (scale is a device array).
 void scale_columns(Cx<double>* x, long long ld, int rows, int cols, const double* scale, bool reciprocal_sqrt,
                    cudaStream_t stream);

@@ -42,7 +42,14 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxCpc = 10;
-constexpr int kRowsPerThread = 5;  // rows per thread held in registers: m <= 1280
+// The tridiagonalisation runs one CTA of kTridiagThreads per SM; each thread
+// holds kRowsPerThread rows of the reflector and rank-2 vectors in registers
+// (m <= kRowsPerThread * kTridiagThreads). 512 threads with 3 rows each
+// measured slower than 256 with 5 (12.1 vs 9.9 ms at m = 1280): the step's
+// CTA barriers and reductions grow with the warp count.
+constexpr int kTridiagThreads = 256;
+constexpr int kTridiagWarps = kTridiagThreads / 32;
+constexpr int kRowsPerThread = 5;  // m <= 1280
 constexpr int kReflectorBlock = 64;
 constexpr int kInvitThreads = 4;
 constexpr int kMaxShares = 5;  // CTA shares per lane: grid <= 160
@@ -144,35 +151,35 @@ __device__ __forceinline__ Reflector make_reflector(Cx<double> alpha, double xno
   return h;
 }
 
-// Rows r = tid + kThreads k of the reflector and rank-2 vectors live in
+// Rows r = tid + kTridiagThreads k of the reflector and rank-2 vectors live in
 // registers; own columns c = cta + G s in shared memory. Step j+1's reflector
 // is formed before step j's rank-2 update, so the update of each own column
 // and its product with the next reflector share one pass. Per step: one CTA
 // barrier for the next column's norm, one for the column products, and the
 // grid barrier.
-__global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs t) {
+__global__ void __launch_bounds__(kTridiagThreads, 1) tridiagonalize_kernel(TridiagArgs t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int R = kRowsPerThread;
   const int m = t.m, G = t.grid, cpc = t.cpc, cta = blockIdx.x, tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   Cx<double>* cols = reinterpret_cast<Cx<double>*>(smem_raw);
-  Cx<double>* red = cols + static_cast<long long>(cpc) * m;  // kWarps x kMaxCpc column-product partials
-  Cx<double>* colv = red + kWarps * kMaxCpc;                  // 2 x kMaxCpc: v at own columns, by step parity
+  Cx<double>* red = cols + static_cast<long long>(cpc) * m;  // kTridiagWarps x kMaxCpc column-product partials
+  Cx<double>* colv = red + kTridiagWarps * kMaxCpc;                  // 2 x kMaxCpc: v at own columns, by step parity
   Cx<double>* colw = colv + 2 * kMaxCpc;                      // kMaxCpc: w at own columns
   Cx<double>* pick = colw + kMaxCpc;                          // alpha (row jc+1), diagonal (row jc)
-  double* nrm = reinterpret_cast<double*>(pick + 2);          // kWarps norm partials
+  double* nrm = reinterpret_cast<double*>(pick + 2);          // kTridiagWarps norm partials
   __shared__ int ok;
 
   int slot_of_row[R];
 #pragma unroll
   for (int k = 0; k < R; ++k) {
-    const int r = tid + k * kThreads;
+    const int r = tid + k * kTridiagThreads;
     slot_of_row[k] = (r < m && r >= cta && (r - cta) % G == 0) ? (r - cta) / G : -1;
   }
   for (int s = 0; s < cpc; ++s) {
     const int c = cta + s * G;
     if (c < m)
-      for (int r = tid; r < m; r += kThreads) cols[static_cast<long long>(s) * m + r] = t.a[r + static_cast<long long>(c) * m];
+      for (int r = tid; r < m; r += kTridiagThreads) cols[static_cast<long long>(s) * m + r] = t.a[r + static_cast<long long>(c) * m];
   }
 
   Cx<double> v[R], w[R], vn[R], col[R];
@@ -185,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     double part = 0.0;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const int r = tid + k * kThreads;
+      const int r = tid + k * kTridiagThreads;
       if (r < m && r >= jc + 2) part += col[k].re * col[k].re + col[k].im * col[k].im;
       if (r == jc + 1) pick[0] = col[k];
       if (r == jc) pick[1] = col[k];
@@ -196,7 +203,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     __syncthreads();
     double xnorm2 = 0.0;
 #pragma unroll
-    for (int q = 0; q < kWarps; ++q) xnorm2 += nrm[q];
+    for (int q = 0; q < kTridiagWarps; ++q) xnorm2 += nrm[q];
     const Reflector h = make_reflector(pick[0], xnorm2);
     if (cta == 0 && tid == 0) {
       t.d[jc] = pick[1].re;
@@ -206,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     Cx<double>* cv = colv + (jc & 1) * kMaxCpc;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const int r = tid + k * kThreads;
+      const int r = tid + k * kTridiagThreads;
       Cx<double> vr{0.0, 0.0};
       if (r == jc + 1) vr = Cx<double>{1.0, 0.0};
       else if (r > jc + 1 && r < m && !h.trivial) vr = cmulz(col[k], h.scale);
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
       const int c = cta + lane * G;
       if (lane < cpc && c > jc && c < m) {
         Cx<double> s{0.0, 0.0};
-        for (int q = 0; q < kWarps; ++q) s = cadd(s, red[q * kMaxCpc + lane]);
+        for (int q = 0; q < kTridiagWarps; ++q) s = cadd(s, red[q * kMaxCpc + lane]);
         const Cx<double> p = cmulz(h.tau, s);
         t.pbuf[static_cast<long long>(jc & 1) * m + c] = p;
         dot = cdot1(p, colv[(jc & 1) * kMaxCpc + lane]);
@@ -254,14 +261,14 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     if (jc + 1 < m && (jc + 1) % G == cta) {
       const long long slot = (jc + 1) / G;
       Cx<double>* dst = t.colbuf + static_cast<long long>((jc + 1) & 1) * m;
-      for (int r = jc + 1 + tid; r < m; r += kThreads) dst[r] = cols[slot * m + r];
+      for (int r = jc + 1 + tid; r < m; r += kTridiagThreads) dst[r] = cols[slot * m + r];
     }
   };
 
   // Step 0: reflector of column 0, p_0 over own columns, column 1 published.
 #pragma unroll
   for (int k = 0; k < R; ++k) {
-    const int r = tid + k * kThreads;
+    const int r = tid + k * kTridiagThreads;
     col[k] = r < m ? t.a[r] : Cx<double>{0.0, 0.0};
   }
   __syncthreads();  // own columns in shared memory
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
       const Cx<double>* a = cols + static_cast<long long>(q) * m;
 #pragma unroll
       for (int k = 0; k < R; ++k) {
-        const int r = tid + k * kThreads;
+        const int r = tid + k * kTridiagThreads;
         if (r >= 1 && r < m) acc[q] = cadd(acc[q], cdot1(a[r], v[k]));
       }
     }
@@ -298,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     double2 pq[R], cq[R], shares[kMaxShares];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const int r = tid + k * kThreads;
+      const int r = tid + k * kTridiagThreads;
       const bool row = r > j && r < m;
       pq[k] = (row && !cur.trivial) ? __ldcg(pb + r) : zero2;
       cq[k] = (row && !last) ? __ldcg(cb + r) : zero2;
@@ -324,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
     // w = p + alpha v on own rows; w at own columns for the update; w[j+1] (v[j+1] = 1).
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const int r = tid + k * kThreads;
+      const int r = tid + k * kTridiagThreads;
       w[k] = (r > j && r < m && !cur.trivial) ? cadd(Cx<double>{pq[k].x, pq[k].y}, cmulz(alpha, v[k]))
                                                : Cx<double>{0.0, 0.0};
       col[k] = Cx<double>{cq[k].x, cq[k].y};
@@ -337,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
       const Cx<double> hw = cconj(head_w);
 #pragma unroll
       for (int k = 0; k < R; ++k) {
-        const int r = tid + k * kThreads;
+        const int r = tid + k * kTridiagThreads;
         if (r > j && r < m) col[k] = csub(col[k], cadd(cmulz(v[k], hw), w[k]));
       }
       next = reflect(j + 1);
@@ -357,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, 1) tridiagonalize_kernel(TridiagArgs
       const bool dot_column = !last && c > j + 1;
 #pragma unroll
       for (int k = 0; k < R; ++k) {
-        const int r = tid + k * kThreads;
+        const int r = tid + k * kTridiagThreads;
         if (r > j && r < m) {
           Cx<double> x = a[r];
           if (!cur.trivial) {
@@ -747,8 +754,8 @@ int sm_count() {
 }
 
 std::size_t tridiag_smem(int m, int cpc) {
-  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc) * m + kWarps * kMaxCpc + 3 * kMaxCpc + 2) +
-         sizeof(double) * kWarps;
+  return sizeof(Cx<double>) * (static_cast<std::size_t>(cpc) * m + kTridiagWarps * kMaxCpc + 3 * kMaxCpc + 2) +
+         sizeof(double) * kTridiagWarps;
 }
 
 constexpr std::size_t kSmemLimit = 227 * 1024;
@@ -809,7 +816,7 @@ int hermitian_eigen_max_order() {
   for (int m = 2; m <= 4096; ++m) {
     const int grid = std::min({g, m, 32 * kMaxShares});
     const int cpc = (m + grid - 1) / grid;
-    if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit || m > kRowsPerThread * kThreads ||
+    if (cpc > kMaxCpc || tridiag_smem(m, cpc) > kSmemLimit || m > kRowsPerThread * kTridiagThreads ||
         invit_smem(m) > kSmemLimit)
       break;
     best = m;
@@ -844,7 +851,7 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
 
   allow_dynamic_smem(tridiagonalize_kernel, smem);
   int per_sm = 0;
-  SDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tridiagonalize_kernel, kThreads, smem));
+  SDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tridiagonalize_kernel, kTridiagThreads, smem));
   if (per_sm < 1) throw InvalidArgument("tridiagonalization kernel cannot be resident");
   // SDFT_B200_TRACE: device times of the stages, printed after the final synchronisation.
   static const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
@@ -856,7 +863,7 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   };
   mark(0);
   TridiagArgs t{a, m, grid, cpc, d, e, tau, reflectors, colbuf, pbuf, dotbuf, arrive, error_word};
-  cooperative_launch(reinterpret_cast<void*>(tridiagonalize_kernel), grid, kThreads, t, smem, stream);
+  cooperative_launch(reinterpret_cast<void*>(tridiagonalize_kernel), grid, kTridiagThreads, t, smem, stream);
   mark(1);
 
   const int warps_per_block = 4;
@@ -868,12 +875,16 @@ void hermitian_lowest(cublasHandle_t blas, Cx<double>* a, int m, int wanted, dou
   mark(2);
 
   const int blocks = static_cast<int>(ceil_div(m - 1, kReflectorBlock));
+  // The complex arrays after the real eigenvectors start on a 16-byte
+  // boundary: wanted * m doubles are rounded up to an even count (an odd
+  // product left them 8-byte aligned, which cuBLAS refuses for complex data).
+  const std::size_t zt_doubles = (static_cast<std::size_t>(wanted) * mm + 1) & ~static_cast<std::size_t>(1);
   const std::size_t vbytes =
-      sizeof(double) * static_cast<std::size_t>(wanted) * mm +
+      sizeof(double) * zt_doubles +
       sizeof(Cx<double>) * (2 * static_cast<std::size_t>(blocks) + 2 * static_cast<std::size_t>(wanted)) *
           kReflectorBlock * kReflectorBlock;
   auto* zt = static_cast<double*>(ws.vectors.reserve(vbytes));
-  auto* tfac = reinterpret_cast<Cx<double>*>(zt + static_cast<std::size_t>(wanted) * mm);
+  auto* tfac = reinterpret_cast<Cx<double>*>(zt + zt_doubles);
   Cx<double>* grams = tfac + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
   Cx<double>* wtmp = grams + static_cast<std::size_t>(blocks) * kReflectorBlock * kReflectorBlock;
   Cx<double>* utmp = wtmp + static_cast<std::size_t>(wanted) * kReflectorBlock;

@@ -67,6 +67,52 @@ __global__ void block_product_kernel(const int* __restrict__ offsets, const long
   out[static_cast<long long>(column) * ldo + first + local] = Cx<double>{re.value(), im.value()};
 }
 
+// out(:, c) = (M_a - shift[c] N_a) P(:, c) per atom block: both products with
+// the compensated sums of block_product_kernel, combined once.
+__global__ void shifted_block_product_kernel(const int* __restrict__ offsets, const long long* __restrict__ storage,
+                                             const Cx<double>* __restrict__ m_blocks,
+                                             const Cx<double>* __restrict__ n_blocks, const double* __restrict__ shift,
+                                             const Cx<double>* __restrict__ p, long long ldp, int columns,
+                                             Cx<double>* __restrict__ out, long long ldo) {
+  const int atom = blockIdx.x;
+  const int first = offsets[atom], rows = offsets[atom + 1] - first;
+  const Cx<double>* m = m_blocks + storage[atom];
+  const Cx<double>* nb = n_blocks + storage[atom];
+  const int per_block = blockDim.x / rows;
+  if (per_block == 0) return;
+  const int local = threadIdx.x % rows;
+  const int column = blockIdx.y * per_block + threadIdx.x / rows;
+  if (threadIdx.x >= per_block * rows || column >= columns) return;
+  CompensatedSum mre, mim, nre, nim;
+  const Cx<double>* pc = p + static_cast<long long>(column) * ldp + first;
+  for (int j = 0; j < rows; ++j) {
+    const Cx<double> a = m[local + static_cast<long long>(j) * rows], b = nb[local + static_cast<long long>(j) * rows];
+    const Cx<double> right = pc[j];
+    mre.product(a.re, right.re);
+    mre.product(-a.im, right.im);
+    mim.product(a.re, right.im);
+    mim.product(a.im, right.re);
+    nre.product(b.re, right.re);
+    nre.product(-b.im, right.im);
+    nim.product(b.re, right.im);
+    nim.product(b.im, right.re);
+  }
+  const double s = shift[column];
+  out[static_cast<long long>(column) * ldo + first + local] =
+      Cx<double>{__fma_rn(-s, nre.value(), mre.value()), __fma_rn(-s, nim.value(), mim.value())};
+}
+
+// y(:, c) -= shift[c] * scale * x(:, c).
+__global__ void shifted_axpy_kernel(const Cx<double>* __restrict__ x, long long ldx, Cx<double>* __restrict__ y,
+                                    long long ldy, int n, const double* __restrict__ shift, double scale) {
+  const int c = blockIdx.y;
+  const double a = shift[c] * scale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Cx<double> v = x[i + c * ldx], w = y[i + c * ldy];
+    y[i + c * ldy] = Cx<double>{__fma_rn(-a, v.re, w.re), __fma_rn(-a, v.im, w.im)};
+  }
+}
+
 __global__ void scale_copy_kernel(const Cx<double>* __restrict__ x, long long ldx, Cx<double>* __restrict__ y,
                                   long long ldy, int n, int columns, double alpha) {
   const long long total = static_cast<long long>(n) * columns;
@@ -113,6 +159,28 @@ void block_product(int atoms, const int* offsets, const long long* storage, int 
   // Blocks smaller than max_block still map per_block(their size) >= per_block(max) columns per CTA.
   block_product_kernel<<<grid, threads, 0, stream>>>(offsets, storage, blocks, p, ldp, columns, out, ldo);
   SDFT_LAUNCH("block_product_kernel");
+}
+
+void shifted_block_product(int atoms, const int* offsets, const long long* storage, int max_block,
+                           const Cx<double>* m_blocks, const Cx<double>* n_blocks, const double* shift,
+                           const Cx<double>* p, long long ldp, int columns, Cx<double>* out, long long ldo,
+                           cudaStream_t stream) {
+  if (atoms <= 0 || columns <= 0) return;
+  if (max_block < 1 || max_block > 256) throw InvalidArgument("PAW block size out of range");
+  const int threads = 256;
+  const int per_block = threads / max_block;
+  const dim3 grid(atoms, static_cast<unsigned>(ceil_div(columns, per_block)));
+  shifted_block_product_kernel<<<grid, threads, 0, stream>>>(offsets, storage, m_blocks, n_blocks, shift, p, ldp,
+                                                            columns, out, ldo);
+  SDFT_LAUNCH("shifted_block_product_kernel");
+}
+
+void shifted_axpy(const Cx<double>* x, long long ldx, Cx<double>* y, long long ldy, int n, int columns,
+                  const double* shift, double scale, cudaStream_t stream) {
+  if (n <= 0 || columns <= 0) return;
+  const dim3 grid(static_cast<unsigned>(std::min<long long>(ceil_div(n, 256), 64)), static_cast<unsigned>(columns));
+  shifted_axpy_kernel<<<grid, 256, 0, stream>>>(x, ldx, y, ldy, n, shift, scale);
+  SDFT_LAUNCH("shifted_axpy_kernel");
 }
 
 void scale_copy(const Cx<double>* x, long long ldx, Cx<double>* y, long long ldy, int n, int columns, double alpha,

@@ -30,6 +30,17 @@ void block_product(int atoms, const int* offsets, const long long* storage, int 
                    const Cx<double>* p, long long ldp, int columns, Cx<double>* out, long long ldo,
                    cudaStream_t stream);
 
+// out(:, c) = (M_a - shift[c] N_a) P(:, c) per atom block (shift on the
+// device), both products compensated as in block_product.
+void shifted_block_product(int atoms, const int* offsets, const long long* storage, int max_block,
+                           const Cx<double>* m_blocks, const Cx<double>* n_blocks, const double* shift,
+                           const Cx<double>* p, long long ldp, int columns, Cx<double>* out, long long ldo,
+                           cudaStream_t stream);
+
+// y(:, c) -= shift[c] * scale * x(:, c) (shift on the device).
+void shifted_axpy(const Cx<double>* x, long long ldx, Cx<double>* y, long long ldy, int n, int columns,
+                  const double* shift, double scale, cudaStream_t stream);
+
 // y = alpha * x (columns of length n, leading dims ldx/ldy).
 void scale_copy(const Cx<double>* x, long long ldx, Cx<double>* y, long long ldy, int n, int columns, double alpha,
                 cudaStream_t stream);

@@ -180,13 +180,13 @@ void DavidsonBuffers::release() {
                      &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
                      &eigen.solver_work, &xs, &sxs, &hxs, &res, &block, &metric, &original, &projections, &gram,
                      &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb,
-                     &excluded})
+                     &excluded, &polish, &polish_small, &polish_values})
     s->release();
   corrections.release();
 }
 
 void CorrectionBuffers::release() {
-  for (Scratch* s : {&res, &z, &p, &hp, &sp, &xh, &sxh, &xl, &sxl, &coefficients, &scalars, &index}) s->release();
+  for (Scratch* s : {&res, &z, &p, &hp, &xh, &sxh, &xl, &sxl, &coefficients, &scalars, &index}) s->release();
 }
 
 GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
@@ -759,6 +759,22 @@ void DeviceOperator::apply_overlap(const Cx<double>* x, int columns, Cx<double>*
     auto* p = static_cast<Cx<double>*>(ctx_.projections.reserve(sizeof(Cx<double>) * static_cast<std::size_t>(np_) * columns));
     project(x, columns, p, precision);
     paw_add(p, columns, true, y, precision);
+  }
+}
+
+void DeviceOperator::apply_shifted(const Cx<double>* x, int columns, const double* shift, Cx<double>* y,
+                                   Precision precision) {
+  if (columns <= 0 || !x || !y || !shift || x == y) throw InvalidArgument("invalid shifted plane-wave buffers");
+  local_part(x, columns, y, precision);
+  shifted_axpy(x, npw_, y, npw_, npw_, columns, shift, 1.0 + regularization_, ctx_.stream);
+  if (np_) {
+    const std::size_t pc = static_cast<std::size_t>(np_) * columns;
+    auto* p = static_cast<Cx<double>*>(ctx_.projections.reserve(sizeof(Cx<double>) * pc));
+    auto* dp = static_cast<Cx<double>*>(ctx_.onsite.reserve(sizeof(Cx<double>) * pc));
+    project(x, columns, p, precision);
+    shifted_block_product(atoms_, block_offsets_, block_storage_, max_block_, d_, q_, shift, p, np_, columns, dp,
+                          np_, ctx_.stream);
+    backproject(dp, columns, y, precision);
   }
 }
 

@@ -36,6 +36,25 @@ struct AcceleratorCache {
   }
 };
 
+// Left operands the caller promises immutable for an identity token
+// (src/compute_backend.hpp:32-41): the FP64 matrix and, once a mixed
+// product needs it, its tensor-core packing stay on the device; dynamic
+// right operands are uploaded anew on every call. Four entries, least
+// recently used replaced.
+struct ImmutableLeft {
+  std::uint64_t identity = 0;
+  int aop = 0;
+  std::size_t rows = 0, cols = 0;  // stored A (rows x cols, leading dimension rows)
+  Scratch fp64;
+  PackedA packed;
+  unsigned long long used = 0;
+  ~ImmutableLeft() { release(packed); }
+};
+struct ImmutableCache {
+  ImmutableLeft entries[4];
+  unsigned long long clock = 0;
+};
+
 // Density-side device state: the sphere plan of the last band-density call
 // (reused while the density grid and the plane-wave keys repeat) and its slabs.
 struct DensityCache {
@@ -55,7 +74,7 @@ struct DensityCache {
 // context reuse the allocations.
 // Device state of the Jacobi-Davidson corrections (correction.cu).
 struct CorrectionBuffers {
-  Scratch res, z, p, hp, sp;   // n x count blocks (the corrections themselves go to the caller's block)
+  Scratch res, z, p, hp;       // n x count blocks (the corrections themselves go to the caller's block)
   Scratch xh, sxh, xl, sxl;    // packed X^H, (SX)^H (rows) and X, SX (left factors)
   Scratch coefficients;        // roots x count projections
   Scratch scalars;             // per column: theta, kinetic energy, two (res, z) slots, (p, q)
@@ -70,6 +89,9 @@ struct DavidsonBuffers {
   Scratch pack_vc, pack_vn, pack_hn, pack_sn, pack_hb, pack_sb;
   Scratch excluded;  // S images and projections of a band-group solve's completed bands
   CorrectionBuffers corrections;
+  Scratch polish;         // strict refinements: direction, trial and their images (n x roots each)
+  Scratch polish_small;   // their roots x roots matrices
+  Scratch polish_values;  // their per-root scalars
   void release();
 };
 
@@ -82,6 +104,7 @@ struct Context {
   Scratch slab32, slab64, staging_in, staging_out, staging_aux, projections, onsite;
   TensorCoreWorkspace tc;
   AcceleratorCache accel;
+  ImmutableCache immutable;
   DensityCache density;
   EigenWorkspace eigen;
   DavidsonBuffers davidson;
@@ -196,6 +219,10 @@ class DeviceOperator {
   void apply_hamiltonian(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
   void apply_overlap(const Cx<double>* x, int columns, Cx<double>* y, Precision precision);
   void apply_pair(const Cx<double>* x, int columns, Cx<double>* hy, Cx<double>* sy, Precision precision);
+  // y(:, c) = (H~ - shift[c] S~) x(:, c), shift on the device: the local part,
+  // minus shift (1+reg) x, plus B^H (D - shift Q) B x -- one projection and one
+  // back-projection for both operators.
+  void apply_shifted(const Cx<double>* x, int columns, const double* shift, Cx<double>* y, Precision precision);
   // Local part only: y = T x + V(r) term.
   void apply_local(const Cx<double>* x, int columns, Cx<double>* y, Precision precision) {
     local_part(x, columns, y, precision);

@@ -18,6 +18,9 @@
 #include <mutex>
 #include <string>
 
+#include <map>
+#include <tuple>
+#include <vector>
 #include "umma_gemm.cuh"
 
 namespace sdft_b200 {
@@ -513,15 +516,11 @@ void pack_b(const Cx<double>* src, long long ldb, int k, int n, Split split, std
   SDFT_LAUNCH("pack_b_kernel");
 }
 
-void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n,
-                       long long kexp, Cx<double>* c, long long ldc, bool add, double alpha, Scratch& workspace,
-                       cudaStream_t stream) {
-  if (m <= 0 || n <= 0 || kexp <= 0) return;
-  if (kexp % BK != 0) throw InvalidArgument("expanded K must be a multiple of 64");
-  const int n2 = 2 * n;
-  const int k_blocks = static_cast<int>(kexp / BK);
-  // Column tile width: the one of 128 / 160 / 256 that pads the 2n real
-  // columns least (the larger on ties).
+namespace {
+
+// Column tile width of the cost model: the one of 128 / 160 / 256 that pads
+// the 2n real columns least (the larger on ties).
+int model_width(int n2) {
   int bn = 256;
   long long padded = ceil_div(n2, 256) * 256LL;
   for (int w : {160, 128}) {
@@ -531,17 +530,22 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
       bn = w;
     }
   }
+  return bn;
+}
+
+int max_splits_for(int k_blocks) { return static_cast<int>(std::min<long long>(128, std::max(1, k_blocks / 8))); }
+
+// Split-K count of the cost model for width bn: one CTA per SM is resident
+// (the ring takes ~200 KB), so the time goes as waves x K blocks per CTA, plus
+// the FP32 partials that a split writes and the reduction reads, counted in K
+// blocks' worth of operand traffic spread over the SMs; the smallest split on
+// ties, at least 8 K blocks per split.
+int model_splits(int m, int n2, int k_blocks, int bn) {
   const long long tiles = static_cast<long long>(ceil_div(m, BM)) * static_cast<long long>(ceil_div(n2, bn));
-  // Split-K count: one CTA per SM is resident (the ring takes ~200 KB), so the
-  // time goes as waves x K blocks per CTA, plus the FP32 partials that a split
-  // writes and the reduction reads, counted in K blocks' worth of operand
-  // traffic spread over the SMs; the smallest split on ties, at least 8 K
-  // blocks per split.
   const double kblock_bytes = static_cast<double>(BM + bn) * BK * 2;
-  const long long max_splits = std::min<long long>(128, std::max(1, k_blocks / 8));
   double best_cost = -1;
   int splits = 1;
-  for (long long s = 1; s <= max_splits; ++s) {
+  for (long long s = 1; s <= max_splits_for(k_blocks); ++s) {
     const long long waves = (tiles * s + 147) / 148;
     const double partial = s > 1 ? 2.0 * 4.0 * static_cast<double>(m) * n2 * s / (148.0 * kblock_bytes) : 0.0;
     const double cost = static_cast<double>(waves * ((k_blocks + s - 1) / s)) + partial;
@@ -550,6 +554,15 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
       splits = static_cast<int>(s);
     }
   }
+  return splits;
+}
+
+// One product with the given tile width and split count.
+void run_config(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n,
+                long long kexp, Cx<double>* c, long long ldc, bool add, double alpha, int bn, int splits,
+                Scratch& workspace, cudaStream_t stream) {
+  const int n2 = 2 * n;
+  const int k_blocks = static_cast<int>(kexp / BK);
   const int kpb = static_cast<int>(ceil_div(k_blocks, splits));
   splits = static_cast<int>(ceil_div(k_blocks, kpb));
   EpilogueArgs ep{m, n2, nullptr, c, ldc, alpha, add ? 1 : 0};
@@ -564,6 +577,118 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
         m, n, splits, ep.partial, c, ldc, add, alpha);
     SDFT_LAUNCH("reduce_splits_kernel");
   }
+}
+
+// Tile autotuner. Shapes are grouped into classes (row tiles of 128, real
+// column count rounded up to 32, K blocks exactly); the first product of a
+// class times every candidate -- the three column widths, each with the cost
+// model's split count, half and twice it, and no split -- on the caller's
+// stream into a scratch output (CUDA events, one untimed run first) and keeps
+// the fastest for the class, for the life of the process. Later products of
+// the class, on any stream or thread, use that choice, so a given process
+// computes every later product of a class with the same tiles and the same
+// summation order. SDFT_B200_GEMM_AUTOTUNE=0 uses the cost model alone.
+struct ShapeClass {
+  int row_tiles, column_units, k_blocks;
+  bool operator<(const ShapeClass& o) const {
+    return std::tie(row_tiles, column_units, k_blocks) < std::tie(o.row_tiles, o.column_units, o.k_blocks);
+  }
+};
+struct TileChoice {
+  int bn, splits;
+  float ms;
+};
+std::mutex g_tune_mutex;
+std::map<ShapeClass, TileChoice> g_tuned;
+
+bool autotune_enabled() {
+  static const bool enabled = [] {
+    const char* v = std::getenv("SDFT_B200_GEMM_AUTOTUNE");
+    if (!v || std::string(v) == "1") return true;
+    if (std::string(v) == "0") return false;
+    throw InvalidArgument("SDFT_B200_GEMM_AUTOTUNE must be 0 or 1");
+  }();
+  return enabled;
+}
+
+TileChoice tuned_choice(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n,
+                        long long kexp, Scratch& workspace, cudaStream_t stream) {
+  const int n2 = 2 * n;
+  const int k_blocks = static_cast<int>(kexp / BK);
+  const ShapeClass key{static_cast<int>(ceil_div(m, BM)), static_cast<int>(ceil_div(n2, 32)), k_blocks};
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto found = g_tuned.find(key);
+  if (found != g_tuned.end()) return found->second;
+  std::vector<std::pair<int, int>> candidates;
+  for (int bn : {128, 160, 256}) {
+    const int s = model_splits(m, n2, k_blocks, bn);
+    for (int split : {1, s, std::max(1, s / 2), std::min(max_splits_for(k_blocks), 2 * s)})
+      if (std::find(candidates.begin(), candidates.end(), std::make_pair(bn, split)) == candidates.end())
+        candidates.emplace_back(bn, split);
+  }
+  static thread_local Scratch output, partials;
+  auto* c = static_cast<Cx<double>*>(output.reserve(sizeof(Cx<double>) * static_cast<std::size_t>(m) * n));
+  cudaEvent_t start = nullptr, stop = nullptr;
+  SDFT_CUDA(cudaEventCreate(&start));
+  SDFT_CUDA(cudaEventCreate(&stop));
+  TileChoice best{model_width(n2), 0, -1.0f};
+  best.splits = model_splits(m, n2, k_blocks, best.bn);
+  try {
+    for (const auto& [bn, splits] : candidates) {
+      run_config(a, lda, b, ldb, m, n, kexp, c, m, false, 1.0, bn, splits, partials, stream);
+      SDFT_CUDA(cudaEventRecord(start, stream));
+      run_config(a, lda, b, ldb, m, n, kexp, c, m, false, 1.0, bn, splits, partials, stream);
+      SDFT_CUDA(cudaEventRecord(stop, stream));
+      SDFT_CUDA(cudaEventSynchronize(stop));
+      float ms = 0;
+      SDFT_CUDA(cudaEventElapsedTime(&ms, start, stop));
+      if (best.ms < 0 || ms < best.ms) best = TileChoice{bn, splits, ms};
+    }
+  } catch (...) {
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    throw;
+  }
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  g_tuned.emplace(key, best);
+  return best;
+}
+
+}  // namespace
+
+void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_t* b, long long ldb, int m, int n,
+                       long long kexp, Cx<double>* c, long long ldc, bool add, double alpha, Scratch& workspace,
+                       cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || kexp <= 0) return;
+  if (kexp % BK != 0) throw InvalidArgument("expanded K must be a multiple of 64");
+  int bn, splits;
+  if (autotune_enabled()) {
+    const TileChoice choice = tuned_choice(a, lda, b, ldb, m, n, kexp, workspace, stream);
+    bn = choice.bn;
+    splits = choice.splits;
+  } else {
+    bn = model_width(2 * n);
+    splits = model_splits(m, 2 * n, static_cast<int>(kexp / BK), bn);
+  }
+  run_config(a, lda, b, ldb, m, n, kexp, c, ldc, add, alpha, bn, splits, workspace, stream);
+}
+
+std::size_t gemm_tuned_classes(std::size_t capacity, int* rows) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  std::size_t i = 0;
+  for (const auto& [key, choice] : g_tuned) {
+    if (i < capacity && rows) {
+      int* r = rows + 5 * i;
+      r[0] = key.row_tiles * BM;
+      r[1] = key.column_units * 32;
+      r[2] = key.k_blocks;
+      r[3] = choice.bn;
+      r[4] = choice.splits;
+    }
+    ++i;
+  }
+  return g_tuned.size();
 }
 
 Split search_split() {

@@ -54,6 +54,12 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
                        long long kexp, Cx<double>* c, long long ldc, bool add, double alpha, Scratch& workspace,
                        cudaStream_t stream);
 
+// The tile autotuner's table so far: per shape class (rows rounded up to
+// 128, real columns rounded up to 32, K blocks of 64) the chosen column tile
+// width and split-K count, five ints per class into rows[0..5*capacity).
+// Returns the number of classes.
+std::size_t gemm_tuned_classes(std::size_t capacity, int* rows);
+
 // True when the running device supports the tcgen05 path (sm_100).
 bool umma_available();
 
@@ -68,6 +74,7 @@ struct PackedA {
 
 struct TensorCoreWorkspace {
   Scratch a, b, partial;
+  Scratch adjoint;  // a right operand formed as B^H for the tensor-core path
 };
 
 // Search-precision split (SDFT_B200_SPLIT=x3|x6, default x6), read once.

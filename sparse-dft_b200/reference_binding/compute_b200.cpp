@@ -17,23 +17,14 @@
 #include <stdexcept>
 #include <string>
 
+#include "b200_solver.hpp"
 #include "compute_backend.hpp"
 #include "sdft_b200.h"
 
 namespace sdft {
 namespace {
 
-void check(sdft_b200_status status) {
-  if (status == SDFT_B200_OK) return;
-  char message[1024];
-  sdft_b200_last_error(message, sizeof(message));
-  switch (status) {
-    case SDFT_B200_INVALID_ARGUMENT: throw std::invalid_argument(message);
-    case SDFT_B200_OVERFLOW: throw std::overflow_error(message);
-    case SDFT_B200_CUDA_ERROR: throw std::runtime_error(std::string("CUDA: ") + message);
-    default: throw std::runtime_error(message);
-  }
-}
+void check(sdft_b200_status status) { b200::throw_on_error(status); }
 
 int search_precision() {
   const char* value = std::getenv("SDFT_B200_ACCELERATOR_PRECISION");
@@ -41,6 +32,8 @@ int search_precision() {
   if (std::string(value) == "mixed") return SDFT_B200_PRECISION_MIXED;
   throw std::invalid_argument("SDFT_B200_ACCELERATOR_PRECISION must be fp64 or mixed");
 }
+
+int op(MatrixOp o) { return o == MatrixOp::Adjoint ? SDFT_B200_OP_ADJOINT : SDFT_B200_OP_NORMAL; }
 
 class B200Accelerator final : public Accelerator {
  public:
@@ -54,12 +47,31 @@ class B200Accelerator final : public Accelerator {
 
   void gemm(MatrixOp ao, MatrixOp bo, std::size_t m, std::size_t n, std::size_t k, const Complex64* a,
             std::size_t lda, const Complex64* b, std::size_t ldb, Complex64* c, std::size_t ldc, bool add) override {
-    // The tensor-core path takes a normal right operand; an adjoint one runs in FP64.
-    const int precision = bo == MatrixOp::Normal ? precision_ : SDFT_B200_PRECISION_FP64;
-    check(sdft_b200_complex_gemm(context_, ao == MatrixOp::Adjoint ? SDFT_B200_OP_ADJOINT : SDFT_B200_OP_NORMAL,
-                                 bo == MatrixOp::Adjoint ? SDFT_B200_OP_ADJOINT : SDFT_B200_OP_NORMAL, m, n, k,
-                                 reinterpret_cast<const double*>(a), lda, reinterpret_cast<const double*>(b), ldb,
-                                 reinterpret_cast<double*>(c), ldc, precision, add ? 1 : 0, SDFT_B200_MEMORY_HOST));
+    check(sdft_b200_complex_gemm(context_, op(ao), op(bo), m, n, k, reinterpret_cast<const double*>(a), lda,
+                                 reinterpret_cast<const double*>(b), ldb, reinterpret_cast<double*>(c), ldc,
+                                 precision_, add ? 1 : 0, SDFT_B200_MEMORY_HOST));
+  }
+
+  // The left operand stays on the device for its identity (and, in the mixed
+  // form, its tensor-core packing); only B and C cross the bus.
+  void gemm_immutable_left(std::uint64_t identity, MatrixOp ao, std::size_t m, std::size_t n, std::size_t k,
+                           const Complex64* a, std::size_t lda, const Complex64* b, std::size_t ldb, Complex64* c,
+                           std::size_t ldc, bool add) override {
+    check(sdft_b200_complex_gemm_immutable_left(context_, identity, op(ao), m, n, k, reinterpret_cast<const double*>(a),
+                                                lda, reinterpret_cast<const double*>(b), ldb,
+                                                reinterpret_cast<double*>(c), ldc, precision_, add ? 1 : 0,
+                                                SDFT_B200_MEMORY_HOST));
+  }
+
+  // One upload of the shared right operand for the three products.
+  void gemm_triple_right(std::size_t m, std::size_t n, std::size_t k, const std::array<const Complex64*, 3>& a,
+                         std::size_t lda, const Complex64* b, std::size_t ldb, const std::array<Complex64*, 3>& c,
+                         std::size_t ldc) override {
+    const double* left[3] = {reinterpret_cast<const double*>(a[0]), reinterpret_cast<const double*>(a[1]),
+                             reinterpret_cast<const double*>(a[2])};
+    double* out[3] = {reinterpret_cast<double*>(c[0]), reinterpret_cast<double*>(c[1]), reinterpret_cast<double*>(c[2])};
+    check(sdft_b200_complex_gemm_triple_right(context_, m, n, k, left, lda, reinterpret_cast<const double*>(b), ldb,
+                                              out, ldc, precision_, SDFT_B200_MEMORY_HOST));
   }
 
   void local_hamiltonian(const std::array<int, 3>& shape, const std::vector<std::size_t>& indices,

@@ -122,7 +122,9 @@ class DavidsonStats(ctypes.Structure):
                 ("s_columns_search", ctypes.c_size_t), ("s_columns_fp64", ctypes.c_size_t),
                 ("rayleigh_ritz_calls", ctypes.c_int), ("restarts", ctypes.c_int), ("fp64_refreshes", ctypes.c_int),
                 ("certifications", ctypes.c_int), ("handoff_iteration", ctypes.c_int),
-                ("block_rank_fallbacks", ctypes.c_int), ("correction_columns", ctypes.c_size_t)]
+                ("block_rank_fallbacks", ctypes.c_int), ("correction_columns", ctypes.c_size_t),
+                ("polish_steps", ctypes.c_int), ("polish_accepted", ctypes.c_int), ("manifold_steps", ctypes.c_int),
+                ("manifold_accepted", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -169,6 +171,11 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_paw_pair", [P, ctypes.c_uint64, SZ, SZ, SZ, P, P, P, P, P, P, ctypes.c_int, ctypes.c_uint64])
     fn("sdft_b200_complex_gemm", [P, ctypes.c_int, ctypes.c_int, SZ, SZ, SZ, P, SZ, P, SZ, P, SZ, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_complex_gemm_immutable_left", [P, ctypes.c_uint64, ctypes.c_int, SZ, SZ, SZ, P, SZ, P, SZ, P, SZ,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_complex_gemm_triple_right", [P, SZ, SZ, SZ, ctypes.POINTER(P), SZ, P, SZ, ctypes.POINTER(P), SZ,
+                                               ctypes.c_int, ctypes.c_int])
+    fn("sdft_b200_gemm_tuned_classes", [SZ, I32, SZP])
     fn("sdft_b200_operator_arrays", [P, U64, D, D, D, D])
     fn("sdft_b200_apply", [P, ctypes.c_int, P, SZ, P, ctypes.c_int, ctypes.c_int])
     fn("sdft_b200_apply_pair", [P, P, SZ, P, P, ctypes.c_int, ctypes.c_int])
@@ -185,6 +192,17 @@ def _declare(lib: ctypes.CDLL) -> None:
                                  ctypes.POINTER(SolveTiming)])
     fn("sdft_b200_server_memory", [P, U64, U64, U64])
     fn("sdft_b200_solve_footprint", [SZ, I32, SZ, SZ, ctypes.c_int, U64])
+
+
+def gemm_tuned_classes() -> list:
+    """The tensor-core GEMM autotuner's table: (rows, real columns, K blocks,
+    tile width, split-K count) per shape class, rows and columns rounded up."""
+    lib = library()
+    count = ctypes.c_size_t()
+    check(lib.sdft_b200_gemm_tuned_classes(0, None, ctypes.byref(count)))
+    table = np.zeros((max(count.value, 1), 5), dtype=np.int32)
+    check(lib.sdft_b200_gemm_tuned_classes(table.shape[0], table.ctypes.data_as(I32), ctypes.byref(count)))
+    return [tuple(int(v) for v in row) for row in table[:min(count.value, table.shape[0])]]
 
 
 def last_error() -> str:

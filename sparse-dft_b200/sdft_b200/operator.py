@@ -352,6 +352,47 @@ def complex_gemm(context: Context, a, b, adjoint_a: bool = False, precision="fp6
     return out
 
 
+def complex_gemm_immutable_left(context: Context, identity: int, a, b, adjoint_a: bool = False, precision="fp64",
+                                c=None):
+    """C = op(A) B (+ c when given) with A cached on the device for `identity`
+    (the reference's complex_gemm_immutable_left; host arrays)."""
+    lib = C.library()
+    a = np.asfortranarray(a, dtype=np.complex128)
+    b = np.asfortranarray(b, dtype=np.complex128)
+    m = a.shape[1] if adjoint_a else a.shape[0]
+    k = a.shape[0] if adjoint_a else a.shape[1]
+    if b.shape[0] != k:
+        raise ValueError("inner dimensions differ")
+    n = b.shape[1]
+    add = c is not None
+    out = np.asfortranarray(c, dtype=np.complex128).copy(order="F") if add else np.zeros((m, n), np.complex128, order="F")
+    C.check(lib.sdft_b200_complex_gemm_immutable_left(
+        context.handle, identity, 1 if adjoint_a else 0, m, n, k, ctypes.c_void_p(a.ctypes.data), a.shape[0],
+        ctypes.c_void_p(b.ctypes.data), b.shape[0], ctypes.c_void_p(out.ctypes.data), m, _precision(precision),
+        int(add), C.HOST))
+    return out
+
+
+def complex_gemm_triple_right(context: Context, lefts, b, precision="fp64"):
+    """[A_0 B, A_1 B, A_2 B] for three m x k left operands sharing B (the
+    reference's complex_gemm_triple_right; host arrays)."""
+    lib = C.library()
+    lefts = [np.asfortranarray(x, dtype=np.complex128) for x in lefts]
+    if len(lefts) != 3 or any(x.shape != lefts[0].shape for x in lefts):
+        raise ValueError("three left operands of one shape")
+    b = np.asfortranarray(b, dtype=np.complex128)
+    m, k = lefts[0].shape
+    if b.shape[0] != k:
+        raise ValueError("inner dimensions differ")
+    n = b.shape[1]
+    outs = [np.zeros((m, n), np.complex128, order="F") for _ in range(3)]
+    a_ptrs = (ctypes.c_void_p * 3)(*[x.ctypes.data for x in lefts])
+    c_ptrs = (ctypes.c_void_p * 3)(*[x.ctypes.data for x in outs])
+    C.check(lib.sdft_b200_complex_gemm_triple_right(context.handle, m, n, k, a_ptrs, m, ctypes.c_void_p(b.ctypes.data),
+                                                    k, c_ptrs, m, _precision(precision), C.HOST))
+    return outs
+
+
 def rayleigh_ritz(context: Context, h, s, requested: int = 0):
     """Lowest `requested` (0 = all) solutions of H y = e S y for n x n Hermitian
     H and S (lower triangles referenced), the reference's rayleigh_ritz. Returns

@@ -16,7 +16,10 @@ evaluate_density_functionals / evaluate_collinear_density_functionals
 (functional_*.npz, collinear_*.npz, on synthetic.functional_case /
 collinear_case). Single groups: --kpoints, --snapshots, --projection,
 --functional, --collinear, --si64-apply (si64_apply.npz: the
-headline pencil's operator arrays and a 160-column H~x/S~x probe).
+headline pencil's operator arrays and a 160-column H~x/S~x probe), --polish
+(strict_polish.npz: solves at tolerance 1e-13 that end in the reference's
+strict polish), --gaas64 [k ...] (gaas64_k*.npz: the 64-atom GaAs cell at
+Ecut 18 Ha, 192 bands, two k-points of the 3x3x3 mesh; long).
 """
 from __future__ import annotations
 
@@ -268,6 +271,76 @@ def si64_apply_fixture(lib):
     print("si64_apply npw", inputs.npw, "grid", snap["shape"])
 
 
+POLISH_CASES = (("tiny", 1), ("tiny", 3), ("si8", 2026))
+POLISH_TOLERANCE = 1e-13
+
+
+def polish_case(name, seed):
+    """One reference solve at POLISH_TOLERANCE with SDFT_TRACE_STRICT_POLISH=1
+    (run in a child process so that its stderr trace can be counted)."""
+    import json
+    import os
+    import subprocess
+    code = (f"import sys, json; sys.path[:0] = [{str(ROOT)!r}, {str(ROOT / 'sparse-dft_b200')!r}]\n"
+            "from oracle import ref_oracle\nfrom sdft_b200 import synthetic\nimport numpy as np\n"
+            f"x = synthetic.{name}(seed={seed})\n"
+            f"r = ref_oracle.ReferenceOperator(ref_oracle.ReferenceLibrary(), x).davidson(x.roots, 256, {POLISH_TOLERANCE})\n"
+            "print(json.dumps({'eigenvalues': list(map(float, r['eigenvalues'])), 'iterations': r['iterations'],"
+            " 'converged': r['converged'], 'max_residual': float(np.max(r['residuals']))}))\n")
+    env = dict(os.environ, SDFT_TRACE_STRICT_POLISH="1")
+    run = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+    result = json.loads(run.stdout.strip().splitlines()[-1])
+    result["polish_steps"] = sum(1 for line in run.stderr.splitlines() if line.startswith("strict_polish "))
+    return result
+
+
+def polish_fixtures():
+    """The reference's solves at tolerance 1e-13, where its strict tangent
+    polish (src/strict_residual_polish.hpp:118-197, driven from
+    src/pw_core.cpp:1273-1336) takes the last steps: eigenvalues, iterations
+    and the number of polish steps its trace reports."""
+    fields = {"tolerance": np.array(POLISH_TOLERANCE)}
+    for name, seed in POLISH_CASES:
+        r = polish_case(name, seed)
+        key = f"{name}_{seed}"
+        fields[f"{key}_eigenvalues"] = np.array(r["eigenvalues"])
+        fields[f"{key}_iterations"] = np.array(r["iterations"])
+        fields[f"{key}_polish_steps"] = np.array(r["polish_steps"])
+        print("polish", key, {k: r[k] for k in ("iterations", "converged", "max_residual", "polish_steps")})
+    np.savez_compressed(HERE / "strict_polish.npz", **fields)
+
+
+GAAS64_KPOINTS = (26, 5)
+
+
+def gaas64_fixture(lib, index):
+    """Config-2 cell (GaAs 2x2x2, a = 21.36 bohr, 64 atoms, Ecut 18 Ha, 192
+    bands) at k-point `index` of the 3x3x3 mesh: the reference's Davidson
+    eigenvalues at 1e-12, its index map and kinetic energies in full, and for
+    a seeded 16-column probe the norms and probe-vector inner products of its
+    H~x and S~x."""
+    inputs = synthetic.gaas_kpoint(index)
+    op = ref_oracle.ReferenceOperator(lib, inputs)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = pathlib.Path(tmp) / "op.pwop"
+        op.save_snapshot(path, inputs.roots, inputs.max_iterations, inputs.tolerance)
+        snap = read_pwo3(path)
+    x = probe_block(inputs.npw, 16, 11)
+    u = probe_block(inputs.npw, 1, 12)[:, 0]
+    hx, sx = op.apply(x, overlap=False, exact=True), op.apply(x, overlap=True, exact=True)
+    t = time.time()
+    result = op.davidson(inputs.roots, inputs.max_iterations, inputs.tolerance)
+    np.savez_compressed(
+        HERE / f"gaas64_k{index}.npz", kpoint=np.array(inputs.kpoint), shape=np.array(snap["shape"]),
+        indices=snap["indices"].astype(np.uint32), kinetic=snap["kinetic"], probe_seed=np.array(11),
+        checksum_seed=np.array(12), hx_norms=np.linalg.norm(hx, axis=0), sx_norms=np.linalg.norm(sx, axis=0),
+        hx_dots=u.conj() @ hx, sx_dots=u.conj() @ sx, eigenvalues=result["eigenvalues"],
+        residuals=result["residuals"], converged=np.array(result["converged"]),
+        iterations=np.array(result["iterations"]), seconds=np.array(time.time() - t))
+    print(f"gaas64_k{index} npw", inputs.npw, "grid", snap["shape"], "iterations", result["iterations"],
+          "converged", result["converged"], "seconds", round(time.time() - t, 1))
+
+
 def kpoint_fixtures(lib):
     """Reference operator and solve of the 8-atom GaAs cell at two k-points of
     the 3x3x3 Monkhorst-Pack mesh (complex, off-Gamma pencils, two species)."""
@@ -284,6 +357,8 @@ def main():
     parser.add_argument("--functional", action="store_true", help="only the Hartree + XC functional fixtures")
     parser.add_argument("--collinear", action="store_true", help="only the collinear spin functional fixtures")
     parser.add_argument("--si64-apply", action="store_true", help="only the Si64 operator and 160-column apply fixture")
+    parser.add_argument("--polish", action="store_true", help="only the strict-polish solves at tolerance 1e-13")
+    parser.add_argument("--gaas64", type=int, nargs="*", help="only the config-2 GaAs64 k-point solves (long)")
     args = parser.parse_args()
     lib = ref_oracle.ReferenceLibrary()
     if args.kpoints:
@@ -303,6 +378,13 @@ def main():
         return
     if args.si64_apply:
         si64_apply_fixture(lib)
+        return
+    if args.polish:
+        polish_fixtures()
+        return
+    if args.gaas64 is not None:
+        for index in args.gaas64 or GAAS64_KPOINTS:
+            gaas64_fixture(lib, index)
         return
     operator_fixture(lib, synthetic.tiny(), "tiny")
     operator_fixture(lib, synthetic.si8(), "si8", solve=True)

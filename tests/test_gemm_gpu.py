@@ -67,3 +67,87 @@ def test_host_gemm_on_submatrix_leaves_other_rows(context, add):
     assert np.array_equal(full[:offset], expected[:offset])
     assert np.array_equal(full[offset + m:], expected[offset + m:])
     assert relative_error(full[offset:offset + m], expected[offset:offset + m]) < 1e-14
+
+
+@pytest.mark.parametrize("adjoint", [False, True])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 2e-5)])
+def test_immutable_left_is_cached_per_identity(context, adjoint, precision, tol):
+    """The reference's complex_gemm_immutable_left contract
+    (src/compute_backend.hpp:32-41): the left operand is read once per
+    identity; a new identity picks up new contents of the same host array."""
+    from sdft_b200.operator import complex_gemm_immutable_left
+    rng = np.random.default_rng(17 + adjoint)
+    a = np.asfortranarray(random(rng, (300, 120) if adjoint else (120, 300)))
+    original = a.copy()
+    op_a = (lambda x: x.conj().T) if adjoint else (lambda x: x)
+    identity = 900 + 2 * adjoint + (precision == "mixed") * 10
+    for call in range(3):
+        b = random(rng, (300, 7 + call))
+        out = complex_gemm_immutable_left(context, identity, a, b, adjoint_a=adjoint, precision=precision)
+        assert relative_error(out, op_a(original) @ b) < tol
+        a[:] = random(rng, a.shape)  # same identity: the cached operand stays the original one
+    out = complex_gemm_immutable_left(context, identity + 1, a, b, adjoint_a=adjoint, precision=precision)
+    assert relative_error(out, op_a(a) @ b) < tol
+    if precision == "fp64":
+        plain = complex_gemm(context, a, b, adjoint_a=adjoint, precision="fp64")
+        assert np.array_equal(out, plain)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 2e-5)])
+def test_triple_right_equals_three_products(context, precision, tol):
+    from sdft_b200.operator import complex_gemm_triple_right
+    rng = np.random.default_rng(23)
+    lefts = [random(rng, (2000, 96)) for _ in range(3)]
+    b = random(rng, (96, 40))
+    outs = complex_gemm_triple_right(context, lefts, b, precision=precision)
+    for a, out in zip(lefts, outs):
+        assert relative_error(out, a @ b) < tol
+        assert np.array_equal(out, complex_gemm(context, a, b, precision=precision))
+
+
+def test_triple_right_rejects_aliased_outputs(context):
+    import ctypes
+    from sdft_b200 import _capi as C
+    rng = np.random.default_rng(2)
+    a = [np.asfortranarray(random(rng, (10, 4))) for _ in range(3)]
+    b = np.asfortranarray(random(rng, (4, 3)))
+    out = np.zeros((10, 3), np.complex128, order="F")
+    lib = C.library()
+    a_ptrs = (ctypes.c_void_p * 3)(*[x.ctypes.data for x in a])
+    same = (ctypes.c_void_p * 3)(*([out.ctypes.data] * 3))
+    assert lib.sdft_b200_complex_gemm_triple_right(context.handle, 10, 3, 4, a_ptrs, 10, ctypes.c_void_p(b.ctypes.data),
+                                                   4, same, 10, C.FP64, C.HOST) == C.INVALID_ARGUMENT
+    into_b = (ctypes.c_void_p * 3)(b.ctypes.data, out.ctypes.data, a[0].ctypes.data)
+    assert lib.sdft_b200_complex_gemm_triple_right(context.handle, 4, 3, 4, a_ptrs, 10, ctypes.c_void_p(b.ctypes.data),
+                                                   4, into_b, 4, C.FP64, C.HOST) == C.INVALID_ARGUMENT
+
+
+def test_mixed_gemm_with_adjoint_right_operand(context):
+    """The tensor-core path forms B^H on the device for an adjoint right operand."""
+    import ctypes
+    from sdft_b200 import _capi as C
+    rng = np.random.default_rng(4)
+    a = np.asfortranarray(random(rng, (64, 200)))
+    b = np.asfortranarray(random(rng, (48, 200)))  # op(B) = B^H is 200 x 48
+    out = np.zeros((64, 48), np.complex128, order="F")
+    C.check(C.library().sdft_b200_complex_gemm(context.handle, 0, 1, 64, 48, 200, ctypes.c_void_p(a.ctypes.data), 64,
+                                               ctypes.c_void_p(b.ctypes.data), 48, ctypes.c_void_p(out.ctypes.data), 64,
+                                               C.MIXED, 0, C.HOST))
+    assert relative_error(out, a @ b.conj().T) < 2e-5
+
+
+def test_autotuner_records_each_shape_class_once(context):
+    """The tile autotuner keeps one (width, split) choice per shape class, and a
+    repeated product of that class gives the same bits."""
+    from sdft_b200 import _capi as C
+    rng = np.random.default_rng(31)
+    a, b = random(rng, (200, 3000)), random(rng, (3000, 24))
+    first = complex_gemm(context, a, b, precision="mixed")
+    table = C.gemm_tuned_classes()
+    assert table, "no tuned shape class recorded"
+    for rows, cols, kblocks, width, splits in table:
+        assert rows % 128 == 0 and cols % 32 == 0 and kblocks > 0
+        assert width in (128, 160, 256) and 1 <= splits <= 128
+    again = complex_gemm(context, a, b, precision="mixed")
+    assert np.array_equal(first, again)
+    assert len(C.gemm_tuned_classes()) == len(table)

@@ -39,8 +39,11 @@ def check(context, h, s, requested, eig_tol=1e-11, res_tol=1e-11):
     assert np.max(np.abs(gram - np.eye(count))) < 1e-11
 
 
-@pytest.mark.parametrize("n,requested", [(2, 0), (37, 10), (320, 0), (800, 320)])
+@pytest.mark.parametrize("n,requested", [(2, 0), (37, 10), (320, 0), (800, 320), (7, 3), (9, 0), (31, 15), (65, 0),
+                                         (129, 0)])
 def test_identity_overlap(context, n, requested):
+    """Odd orders with an odd number of wanted pairs included: the workspace
+    keeps its complex arrays 16-byte aligned whatever m * wanted is."""
     rng = np.random.Generator(np.random.PCG64(n))
     h, s = pencil(n, rng)
     check(context, h, s, requested)
