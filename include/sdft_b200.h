@@ -55,7 +55,8 @@ SDFT_B200_API unsigned long long sdft_b200_kernel_launches(void);
 
 /* The tensor-core GEMM tile autotuner's table so far (process-wide): per
  * shape class five values -- rows rounded up to 128, real columns (twice the
- * complex columns) rounded up to 32, K blocks of 64, the chosen column tile
+ * complex columns) rounded up to 32, K blocks of 64 rounded up to a geometric
+ * grid of ratio 2^(1/8), the chosen column tile
  * width and split-K count -- into rows[0 .. 5*capacity). *count receives the
  * number of classes. The first product of a class times each candidate
  * (three tile widths x split counts around the cost model's) on its stream

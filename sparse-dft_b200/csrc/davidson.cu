@@ -340,7 +340,13 @@ void DavidsonSolver::rayleigh_ritz() {
   // Traced runs drain the queue first so that the time is the Rayleigh-Ritz step's alone.
   static const bool trace = std::getenv("SDFT_B200_TRACE") != nullptr;
   if (trace) SDFT_CUDA(cudaStreamSynchronize(st));
-  const double t0 = now();
+  // Device time of the step, from events on the solver's stream (a host clock
+  // would also count the work still queued ahead of it).
+  if (!rr_events_[0]) {
+    SDFT_CUDA(cudaEventCreate(&rr_events_[0]));
+    SDFT_CUDA(cudaEventCreate(&rr_events_[1]));
+  }
+  SDFT_CUDA(cudaEventRecord(rr_events_[0], st));
   const int m = size_;
   auto* a = as<Cx<double>>(rr_a_, static_cast<std::size_t>(capacity_) * capacity_);
   auto* b = as<Cx<double>>(rr_b_, static_cast<std::size_t>(capacity_) * capacity_);
@@ -354,9 +360,17 @@ void DavidsonSolver::rayleigh_ritz() {
   // 4e-3. The FP64 phase stays tight.
   generalized_lowest(ctx.blas, ctx.solver, a, b, m, std::min(m, 2 * roots_), w_, a, eigen_, rr_mode(), st,
                      exact_mode_ ? 5e-5 : 4e-3, exact_mode_ ? 1e-8 : 1e-4);
+  SDFT_CUDA(cudaEventRecord(rr_events_[1], st));
   values_ = download(w_, std::min(m, roots_));
   ++stats_.rayleigh_ritz;
-  stats_.rr_seconds += now() - t0;
+  float ms = 0.0f;
+  SDFT_CUDA(cudaEventElapsedTime(&ms, rr_events_[0], rr_events_[1]));
+  stats_.rr_seconds += 1e-3 * ms;
+}
+
+DavidsonSolver::~DavidsonSolver() {
+  for (cudaEvent_t& e : rr_events_)
+    if (e) cudaEventDestroy(e);
 }
 
 // Fresh FP64 certificate of the Ritz block (src/pw_core.cpp:1125-1149).

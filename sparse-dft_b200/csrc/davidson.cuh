@@ -38,7 +38,7 @@ struct DavidsonStats {
   long long correction_columns = 0;
   // Strict FP64 refinements (tangent polish and root-manifold steps), tried / accepted.
   int polish_steps = 0, polish_accepted = 0, manifold_steps = 0, manifold_accepted = 0;
-  double seconds = 0.0, rr_seconds = 0.0;
+  double seconds = 0.0, rr_seconds = 0.0;  // rr_seconds: device time of the Rayleigh-Ritz steps
 };
 
 class DavidsonSolver {
@@ -53,6 +53,9 @@ class DavidsonSolver {
         gram_(b_.gram), small_(b_.small), order_(b_.order), select_(b_.select), pack_vc_(b_.pack_vc),
         pack_vn_(b_.pack_vn), pack_hn_(b_.pack_hn), pack_sn_(b_.pack_sn), pack_hb_(b_.pack_hb),
         pack_sb_(b_.pack_sb) {}
+  ~DavidsonSolver();
+  DavidsonSolver(const DavidsonSolver&) = delete;
+  DavidsonSolver& operator=(const DavidsonSolver&) = delete;
   // initial: device n x roots (column-major) warm vectors, or null for a cold start.
   void solve(const DavidsonOptions& options, const Cx<double>* initial);
 
@@ -135,6 +138,7 @@ class DavidsonSolver {
   double* dsmall_ = nullptr;  // per-column device scalars (norms, metric, values)
   std::vector<double> values_, residual_norms_;
   std::vector<double> residual_history_;
+  cudaEvent_t rr_events_[2] = {nullptr, nullptr};  // Rayleigh-Ritz step start / end on the solver's stream
 };
 
 }  // namespace sdft_b200

@@ -14,6 +14,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <mutex>
 #include <string>
@@ -580,9 +581,11 @@ void run_config(const std::uint16_t* a, long long lda, const std::uint16_t* b, l
 }
 
 // Tile autotuner. Shapes are grouped into classes (row tiles of 128, real
-// column count rounded up to 32, K blocks exactly); the first product of a
-// class times every candidate -- the three column widths, each with the cost
-// model's split count, half and twice it, and no split -- on the caller's
+// column count rounded up to 32, K blocks rounded up to a geometric grid of
+// ratio 2^(1/8), so that operators whose plane-wave counts differ by a few
+// per cent share their classes); the first product of a class times every
+// candidate -- the three column widths, each with the cost model's split
+// count and twice it, and no split -- on the caller's
 // stream into a scratch output (CUDA events, one untimed run first) and keeps
 // the fastest for the class, for the life of the process. Later products of
 // the class, on any stream or thread, use that choice, so a given process
@@ -615,14 +618,16 @@ TileChoice tuned_choice(const std::uint16_t* a, long long lda, const std::uint16
                         long long kexp, Scratch& workspace, cudaStream_t stream) {
   const int n2 = 2 * n;
   const int k_blocks = static_cast<int>(kexp / BK);
-  const ShapeClass key{static_cast<int>(ceil_div(m, BM)), static_cast<int>(ceil_div(n2, 32)), k_blocks};
+  int k_class = 1;
+  for (int j = 1; k_class < k_blocks; ++j) k_class = static_cast<int>(std::ceil(std::exp2(j / 8.0)));
+  const ShapeClass key{static_cast<int>(ceil_div(m, BM)), static_cast<int>(ceil_div(n2, 32)), k_class};
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   auto found = g_tuned.find(key);
   if (found != g_tuned.end()) return found->second;
   std::vector<std::pair<int, int>> candidates;
   for (int bn : {128, 160, 256}) {
     const int s = model_splits(m, n2, k_blocks, bn);
-    for (int split : {1, s, std::max(1, s / 2), std::min(max_splits_for(k_blocks), 2 * s)})
+    for (int split : {1, s, std::min(max_splits_for(k_blocks), 2 * s)})
       if (std::find(candidates.begin(), candidates.end(), std::make_pair(bn, split)) == candidates.end())
         candidates.emplace_back(bn, split);
   }

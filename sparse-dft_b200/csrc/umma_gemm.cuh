@@ -55,7 +55,8 @@ void umma_complex_gemm(const std::uint16_t* a, long long lda, const std::uint16_
                        cudaStream_t stream);
 
 // The tile autotuner's table so far: per shape class (rows rounded up to
-// 128, real columns rounded up to 32, K blocks of 64) the chosen column tile
+// 128, real columns rounded up to 32, K blocks of 64 rounded up to a geometric
+// grid of ratio 2^(1/8)) the chosen column tile
 // width and split-K count, five ints per class into rows[0..5*capacity).
 // Returns the number of classes.
 std::size_t gemm_tuned_classes(std::size_t capacity, int* rows);

@@ -231,24 +231,35 @@ def _block_diag(blocks: np.ndarray) -> np.ndarray:
     return out
 
 
-def overlap_minimum(amplitudes: np.ndarray, q_blocks: np.ndarray, regularization: float) -> float:
-    """lambda_min of S~ on the projector span, as src/plane_wave_operator.cpp:702-717 evaluates it."""
+def _gram_root(amplitudes: np.ndarray) -> np.ndarray:
+    """(B B^H)^(1/2) with the Gram eigenvalues clamped at 0."""
     gram = amplitudes @ amplitudes.conj().T
     w, v = np.linalg.eigh(0.5 * (gram + gram.conj().T))
-    root = (v * np.sqrt(np.maximum(w, 0.0))) @ v.conj().T
+    return (v * np.sqrt(np.maximum(w, 0.0))) @ v.conj().T
+
+
+def _root_minimum(root: np.ndarray, q_blocks: np.ndarray, regularization: float) -> float:
     qfull = _block_diag(q_blocks)
-    small = (1.0 + regularization) * np.eye(gram.shape[0]) + root @ qfull @ root
+    small = (1.0 + regularization) * np.eye(root.shape[0]) + root @ qfull @ root
     lam = np.linalg.eigvalsh(0.5 * (small + small.conj().T))
     return float(min(1.0 + regularization, lam.min()))
 
 
+def overlap_minimum(amplitudes: np.ndarray, q_blocks: np.ndarray, regularization: float) -> float:
+    """lambda_min of S~ on the projector span, as src/plane_wave_operator.cpp:702-717 evaluates it."""
+    return _root_minimum(_gram_root(amplitudes), q_blocks, regularization)
+
+
 def _scale_q(amplitudes, q_raw, regularization, floor=0.3):
-    if overlap_minimum(amplitudes, q_raw, regularization) >= floor:
+    # The Gram root depends on B alone: formed once, not per bisection step
+    # (each step's arithmetic is unchanged).
+    root = _gram_root(amplitudes)
+    if _root_minimum(root, q_raw, regularization) >= floor:
         return 1.0
     lo, hi = 0.0, 1.0
     for _ in range(60):
         mid = 0.5 * (lo + hi)
-        if overlap_minimum(amplitudes, mid * q_raw, regularization) >= floor:
+        if _root_minimum(root, mid * q_raw, regularization) >= floor:
             lo = mid
         else:
             hi = mid
