@@ -455,9 +455,11 @@ def density_side(ctx, inputs, stream, peak):
     occ = np.full(bands, 2.0)
     out = {"bands": bands, "band_density": {}}
     grid16 = None
+    densities = {}
     for factor in (4.0, 8.0, 16.0):
         support = synthetic.density_support(inputs, factor)
-        ms, _ = timed(lambda: density.band_density(ctx, inputs.hkl, psi, occ, inputs.volume, support))
+        ms, values = timed(lambda: density.band_density(ctx, inputs.hkl, psi, occ, inputs.volume, support))
+        densities[factor] = (support, values.cpu().numpy())
         span = [int(2 * max(np.abs(support[:, a]).max(), inputs.hkl[:, a].max() - min(inputs.hkl[:, a].min(), 0)) + 1)
                 for a in range(3)]
         n = [fast_length(max(3, v)) for v in span]
@@ -467,6 +469,16 @@ def density_side(ctx, inputs, stream, peak):
         gbs = algorithmic / (ms * 1e-3) / 1e9
         out["band_density"][f"f{int(factor)}"] = {"grid": n, "support": int(support.shape[0]), "ms": ms,
                                                   "achieved_gbs": gbs, "frac_of_hbm": gbs / peak}
+    # Error of the f = 4 and f = 8 densities against the f = 16 one on their
+    # keys (all of which the f = 16 support holds), relative to max |n_16(G)|.
+    support16, values16 = densities[16.0]
+    where16 = {tuple(key): i for i, key in enumerate(support16.tolist())}
+    scale16 = float(np.max(np.abs(values16)))
+    for factor in (4.0, 8.0):
+        support, values = densities[factor]
+        index = np.array([where16[tuple(key)] for key in support.tolist()])
+        out["band_density"][f"f{int(factor)}"]["max_error_vs_f16"] = float(
+            np.max(np.abs(values - values16[index])) / scale16)
     # Compensation charge on the f = 16 support.
     aug = synthetic.augmentation()
     rows = int(np.sum(2 * aug["channel_l"] + 1))
@@ -655,7 +667,8 @@ def cpu_baseline(inputs):
 
 def run_case(args):
     """A few launches of one kernel family on the bench workload, for profiling
-    captures (no timing, no JSON): local, pair, project, density, pbe."""
+    captures (no JSON): local, pair, project, density, pbe, compensation (the
+    last prints each call's CUDA-event time)."""
     import numpy as np
     import torch
     from sdft_b200 import density, synthetic
@@ -687,6 +700,25 @@ def run_case(args):
         n = np.exp(np.linspace(-20, 1, cols * 65536))
         for _ in range(args.repeat):
             density.pbe_points(ctx, n, 0.3 * n)
+    elif args.case == "compensation":
+        aug = synthetic.augmentation()
+        rows = int(np.sum(2 * aug["channel_l"] + 1))
+        atoms = inputs.positions.shape[0]
+        onsite = density.onsite_density(ctx, synthetic.projected_amplitudes(atoms, rows, cols), rows,
+                                        np.full(cols, 2.0))
+        keys = synthetic.density_support(inputs, args.factor)
+        charge = density.CompensationCharge(ctx, inputs.lattice, inputs.positions, keys, aug,
+                                            synthetic.lm_transform(aug))
+        rho = torch.from_numpy(onsite).cuda()
+        for _ in range(args.repeat):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            charge.density(rho)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            print(f"compensation keys {keys.shape[0]} atoms {atoms}: {e0.elapsed_time(e1):.3f} ms")
+        charge.close()
     ctx.close()
     print("case", args.case, "done")
 
@@ -702,7 +734,7 @@ def main():
     parser.add_argument("--no-serving", action="store_true", help="skip the serving-stream sample")
     parser.add_argument("--no-kpoints", action="store_true", help="skip the GaAs64 k-point batch")
     parser.add_argument("--all-kpoints", action="store_true", help="all 27 k-points of the GaAs64 batch (default: 4)")
-    parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe"],
+    parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe", "compensation"],
                         help="run a few launches of one kernel family for a profiler capture and exit")
     parser.add_argument("--columns", type=int, default=32, help="columns (bands) for --case")
     parser.add_argument("--repeat", type=int, default=2, help="repetitions for --case")

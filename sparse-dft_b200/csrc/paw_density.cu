@@ -158,25 +158,37 @@ __global__ void multipoles_kernel(const Cx<double>* __restrict__ rho, const Cx<d
   moments[id] = sum;
 }
 
+// e^{-i G.tau_a} for the integer key (h, k, l): G.tau = 2 pi (h f1 + k f2 +
+// l f3) for G on the reciprocal lattice and fractional coordinates f, so the
+// phase is sincospi of -2 (h f1 + k f2 + l f3), an argument formed without
+// the 2 pi scaling and reduced exactly by sincospi.
+__device__ __forceinline__ Cx<double> atom_phase(const double* __restrict__ fractional, int a, int h, int k, int l) {
+  const double x = __dadd_rn(__dadd_rn(__dmul_rn(static_cast<double>(h), __ldg(fractional + 3 * a)),
+                                       __dmul_rn(static_cast<double>(k), __ldg(fractional + 3 * a + 1))),
+                             __dmul_rn(static_cast<double>(l), __ldg(fractional + 3 * a + 2)));
+  double s, c;
+  sincospi(-2.0 * x, &s, &c);
+  return Cx<double>{c, s};
+}
+
 template <int LMS>
-__global__ void compensation_kernel(const double* __restrict__ q, const double* __restrict__ form, std::size_t count,
-                                    const double* __restrict__ positions, const Cx<double>* __restrict__ moments,
+__global__ void compensation_kernel(const int* __restrict__ keys, const double* __restrict__ form, std::size_t count,
+                                    const double* __restrict__ fractional, const Cx<double>* __restrict__ moments,
                                     int atoms, int lms_runtime, double volume, Cx<double>* __restrict__ out) {
   const int lms = LMS > 0 ? LMS : lms_runtime;
   for (std::size_t g = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; g < count;
        g += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
-    const double qx = q[3 * g], qy = q[3 * g + 1], qz = q[3 * g + 2];
+    const int h = keys[3 * g], k = keys[3 * g + 1], l = keys[3 * g + 2];
     double f[LMS > 0 ? LMS : 1];
     if (LMS > 0) {
 #pragma unroll
       for (int lm = 0; lm < (LMS > 0 ? LMS : 1); ++lm) f[lm] = form[static_cast<std::size_t>(lm) * count + g];
     }
+    // Atoms in order; F.M_a by fused multiply-adds, one division by the
+    // volume per G (within the 1e-12 relative bar of the reference's
+    // per-atom division).
     Cx<double> sum{0.0, 0.0};
     for (int a = 0; a < atoms; ++a) {
-      const double theta = dot3(qx, qy, qz, __ldg(positions + 3 * a), __ldg(positions + 3 * a + 1),
-                                __ldg(positions + 3 * a + 2));
-      double s, c;
-      sincos(-theta, &s, &c);
       Cx<double> value{0.0, 0.0};
       const Cx<double>* m = moments + static_cast<std::size_t>(a) * lms;
       int lm = 0;
@@ -186,15 +198,14 @@ __global__ void compensation_kernel(const double* __restrict__ q, const double* 
           const double fv = LMS > 0 ? f[lm] : form[static_cast<std::size_t>(lm) * count + g];
           const Cx<double> mv = m[lm];
           // (fv, 0) or (0, fv) times the moment.
-          const Cx<double> term = imaginary ? Cx<double>{-__dmul_rn(fv, mv.im), __dmul_rn(fv, mv.re)}
-                                            : Cx<double>{__dmul_rn(fv, mv.re), __dmul_rn(fv, mv.im)};
-          value = {__dadd_rn(value.re, term.re), __dadd_rn(value.im, term.im)};
+          if (imaginary) value = {fma(-fv, mv.im, value.re), fma(fv, mv.re, value.im)};
+          else value = {fma(fv, mv.re, value.re), fma(fv, mv.im, value.im)};
         }
       }
-      const Cx<double> phased = mul_rn(Cx<double>{c, s}, value);
-      sum = {__dadd_rn(sum.re, __ddiv_rn(phased.re, volume)), __dadd_rn(sum.im, __ddiv_rn(phased.im, volume))};
+      const Cx<double> p = atom_phase(fractional, a, h, k, l);
+      sum = {fma(p.re, value.re, fma(-p.im, value.im, sum.re)), fma(p.re, value.im, fma(p.im, value.re, sum.im))};
     }
-    out[g] = sum;
+    out[g] = Cx<double>{sum.re / volume, sum.im / volume};
   }
 }
 
@@ -205,13 +216,13 @@ constexpr int kProjectThreads = 256;
 
 template <int LMS>
 __global__ void __launch_bounds__(kProjectThreads) project_partials_kernel(
-    const double* __restrict__ q, const double* __restrict__ form, std::size_t count,
-    const double* __restrict__ positions, int atoms, const int* __restrict__ opposite,
-    const Cx<double>* __restrict__ potential, Cx<double>* __restrict__ partials) {
+    const int* __restrict__ keys, const double* __restrict__ form, std::size_t count,
+    const double* __restrict__ fractional,
+    int atoms, const int* __restrict__ opposite, const Cx<double>* __restrict__ potential,
+    Cx<double>* __restrict__ partials) {
   __shared__ Cx<double> red[kProjectThreads / 32][LMS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int a = 0; a < atoms; ++a) {
-    const double tx = __ldg(positions + 3 * a), ty = __ldg(positions + 3 * a + 1), tz = __ldg(positions + 3 * a + 2);
     Cx<double> acc[LMS];
 #pragma unroll
     for (int lm = 0; lm < LMS; ++lm) acc[lm] = Cx<double>{0.0, 0.0};
@@ -219,10 +230,7 @@ __global__ void __launch_bounds__(kProjectThreads) project_partials_kernel(
          g += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
       const int o = opposite[g];
       if (o < 0) continue;
-      const double theta = dot3(q[3 * g], q[3 * g + 1], q[3 * g + 2], tx, ty, tz);
-      double sn, cs;
-      sincos(-theta, &sn, &cs);
-      const Cx<double> w = mul_rn(potential[o], Cx<double>{cs, sn});
+      const Cx<double> w = mul_rn(potential[o], atom_phase(fractional, a, keys[3 * g], keys[3 * g + 1], keys[3 * g + 2]));
       int lm = 0;
 #pragma unroll
       for (int L = 0; L * L < LMS; ++L) {
@@ -392,16 +400,11 @@ CompensationCharge::CompensationCharge(Context& ctx, const CompensationInput& in
     if (found.second) radii.push_back(radius);
     shell[g] = found.first->second;
   }
-  std::vector<double> positions(3 * atoms_);
-  for (std::size_t i = 0; i < atoms_; ++i) {
-    const V3 p = combine(a, in.fractional[3 * i], in.fractional[3 * i + 1], in.fractional[3 * i + 2]);
-    positions[3 * i] = p.x;
-    positions[3 * i + 1] = p.y;
-    positions[3 * i + 2] = p.z;
-  }
-
+  for (std::size_t i = 0; i < 3 * atoms_; ++i)
+    if (!std::isfinite(in.fractional[i])) throw InvalidArgument("nonfinite PAW compensation position");
   q_ = upload(q.data(), q.size());
-  positions_ = upload(positions.data(), positions.size());
+  keys_ = upload(in.keys, 3 * count_);
+  fractional_ = upload(in.fractional, 3 * atoms_);
   transform_ = upload(reinterpret_cast<const Cx<double>*>(in.transform), static_cast<std::size_t>(lms_) * dim_ * dim_);
   SDFT_CUDA(cudaMalloc(&form_, sizeof(double) * lms_ * count_));
   SDFT_CUDA(cudaMalloc(&moments_, sizeof(Cx<double>) * lms_ * atoms_));
@@ -444,7 +447,8 @@ CompensationCharge::CompensationCharge(Context& ctx, const CompensationInput& in
 }
 
 CompensationCharge::~CompensationCharge() {
-  for (void* p : {static_cast<void*>(q_), static_cast<void*>(positions_), static_cast<void*>(form_),
+  for (void* p : {static_cast<void*>(q_), static_cast<void*>(keys_), static_cast<void*>(fractional_),
+                  static_cast<void*>(form_),
                   static_cast<void*>(transform_), static_cast<void*>(moments_), static_cast<void*>(flags_),
                   static_cast<void*>(opposite_), static_cast<void*>(partials_), static_cast<void*>(responses_)})
     if (p) cudaFree(p);
@@ -460,8 +464,8 @@ void CompensationCharge::project(const Cx<double>* potential, Cx<double>* out) {
   }
 #define SDFT_PROJECT_CASE(N)                                                                                     \
   case N:                                                                                                        \
-    project_partials_kernel<N><<<blocks, kProjectThreads, 0, ctx_.stream>>>(q_, form_, count_, positions_, atoms, \
-                                                                          opposite_, potential, partials_);     \
+    project_partials_kernel<N><<<blocks, kProjectThreads, 0, ctx_.stream>>>(keys_, form_, count_, fractional_, \
+                                                                          atoms, opposite_, potential, partials_); \
     break;
   switch (lms_) {
     SDFT_PROJECT_CASE(1)
@@ -494,8 +498,8 @@ void CompensationCharge::density(const Cx<double>* onsite, Cx<double>* out) {
   const unsigned blocks = static_cast<unsigned>(std::min<std::size_t>(ceil_div(count_, 128), 148ULL * 32));
 #define SDFT_COMPENSATION_CASE(N)                                                                                \
   case N:                                                                                                        \
-    compensation_kernel<N><<<blocks, 128, 0, ctx_.stream>>>(q_, form_, count_, positions_, moments_, atoms, lms_, \
-                                                            volume_, out);                                      \
+    compensation_kernel<N><<<blocks, 128, 0, ctx_.stream>>>(keys_, form_, count_, fractional_, moments_, atoms, \
+                                                            lms_, volume_, out);                                \
     break;
   switch (lms_) {
     SDFT_COMPENSATION_CASE(1)
@@ -503,8 +507,8 @@ void CompensationCharge::density(const Cx<double>* onsite, Cx<double>* out) {
     SDFT_COMPENSATION_CASE(9)
     SDFT_COMPENSATION_CASE(16)
     default:
-      compensation_kernel<0><<<blocks, 128, 0, ctx_.stream>>>(q_, form_, count_, positions_, moments_, atoms, lms_,
-                                                              volume_, out);
+      compensation_kernel<0><<<blocks, 128, 0, ctx_.stream>>>(keys_, form_, count_, fractional_, moments_, atoms,
+                                                              lms_, volume_, out);
   }
 #undef SDFT_COMPENSATION_CASE
   SDFT_LAUNCH("compensation_kernel");

@@ -33,8 +33,8 @@ struct CompensationInput {
 };
 
 // Device-resident compensation geometry shared by all atoms: reciprocal
-// vectors, compact form factors F_LM(G) (signed real; i times it for odd L),
-// cartesian positions and the (L,M) transform. density() evaluates
+// vectors, integer keys, compact form factors F_LM(G) (signed real; i times
+// it for odd L), fractional positions and the (L,M) transform. density() evaluates
 // rho^(G) = sum_a exp(-i G.tau_a)/Omega sum_LM F_LM(G) M_a,LM with
 // M_a = transform . rho_a, in atom order per G.
 class CompensationCharge {
@@ -66,7 +66,8 @@ class CompensationCharge {
   int lms_ = 0, max_l_ = 0;
   double volume_ = 0;
   double* q_ = nullptr;          // count x 3 cartesian G, 1/bohr
-  double* positions_ = nullptr;  // atoms x 3 cartesian, bohr
+  int* keys_ = nullptr;          // count x 3 integer keys
+  double* fractional_ = nullptr; // atoms x 3 fractional positions
   double* form_ = nullptr;       // lms x count
   Cx<double>* transform_ = nullptr;
   Cx<double>* moments_ = nullptr;  // atoms x lms
