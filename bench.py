@@ -667,8 +667,8 @@ def cpu_baseline(inputs):
 
 def run_case(args):
     """A few launches of one kernel family on the bench workload, for profiling
-    captures (no JSON): local, pair, project, density, pbe, compensation (the
-    last prints each call's CUDA-event time)."""
+    captures (no JSON): local, pair, project, density, pbe, compensation;
+    local, pair, project and compensation print each call's CUDA-event time."""
     import numpy as np
     import torch
     from sdft_b200 import density, synthetic
@@ -682,13 +682,18 @@ def run_case(args):
         op = PlaneWaveOperator(ctx, inputs)
         x = torch.randn(cols, op.npw, dtype=torch.complex128, device="cuda").T
         for _ in range(args.repeat):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             if args.case == "local":
                 op.local_apply(x, precision=args.precision)
             elif args.case == "pair":
                 op.apply_pair(x, precision=args.precision)
             else:
                 op.project(x, precision=args.precision)
-        torch.cuda.synchronize()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            print(f"{args.case} {args.precision} {cols} columns: {e0.elapsed_time(e1):.3f} ms")
         op.close()
     elif args.case == "density":
         support = synthetic.density_support(inputs, args.factor)

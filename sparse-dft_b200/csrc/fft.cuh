@@ -638,6 +638,97 @@ __device__ Cx<T>* fft_lines_pp_general(Cx<T>* src, Cx<T>* dst, int count, int li
   return src;
 }
 
+// ---- register-resident lines -----------------------------------------------
+// One thread transforms one line of compile-time length N held in its
+// registers: the Stockham stages of fft_lines_fixed unrolled over the whole
+// line, so every element index and twiddle offset is a constant and the
+// line never touches shared memory. The twiddles are read through `tw`,
+// which callers point at a kernel-parameter table (RegTwiddles), so each
+// twiddle is a constant-bank operand rather than a load.
+template <typename T, int N>
+struct RegTwiddles {
+  Cx<T> w[N];  // w[m] = exp(-2 pi i m / N)
+};
+
+template <typename T, bool INV, int N, int S = 0>
+__device__ __forceinline__ void fft_line_registers(Cx<T> (&v)[N], const Cx<T>* tw) {
+  static_assert(fixed_stage_count(N) > 0, "line length must be 2/3/5/7-smooth");
+  if constexpr (S < fixed_stage_count(N)) {
+    constexpr int R = fixed_radix(N, S), NS = fixed_ns(N, S), M = N / R, TWSTRIDE = N / (NS * R);
+    Cx<T> out[N];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int jq = j / NS, jk = j - jq * NS;
+      Cx<T> b[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        Cx<T> x = v[j + r * M];
+        if (r > 0 && jk > 0) x = cmul(x, twiddle<T, INV>(tw, r * jk * TWSTRIDE));
+        b[r] = x;
+      }
+      radix_dft<T, R, INV>(b, tw, M);
+#pragma unroll
+      for (int r = 0; r < R; ++r) out[jq * NS * R + jk + r * NS] = b[r];
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) v[e] = out[e];
+    fft_line_registers<T, INV, N, S + 1>(v, tw);
+  }
+}
+
+// ---- lines split over a lane pair --------------------------------------------
+// A line of even length N held by lanes l and l ^ kPairXor of one warp, N/2
+// values each. The radix-2 step of the transform is one exchange through
+// warp shuffles; the halves then run independent length-N/2 transforms in
+// registers (fft_line_registers). Lanes 0-15 hold the lower halves, 16-31
+// the upper ones. Every lane of the warp must call these (shuffles).
+//
+//   fft_pair_dif: input in natural halves (lower x[j], upper x[j + N/2]),
+//                 output interleaved (lower X[2m], upper X[2m + 1]);
+//   fft_pair_dit: input interleaved, output in natural halves.
+constexpr int kPairXor = 16;
+
+// lower: v_j <- other_j + v_j; upper: v_j <- other_j - v_j.
+template <typename T, int H>
+__device__ __forceinline__ void pair_combine(Cx<T> (&v)[H], bool upper) {
+  const T sign = upper ? T(-1) : T(1);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const T ore = __shfl_xor_sync(0xffffffffu, v[j].re, kPairXor);
+    const T oim = __shfl_xor_sync(0xffffffffu, v[j].im, kPairXor);
+    v[j] = Cx<T>{fma(sign, v[j].re, ore), fma(sign, v[j].im, oim)};
+  }
+}
+
+// upper: v_j <- v_j W^j with W = exp(-+2 pi i / N) (sign of the transform); lower unchanged.
+template <typename T, bool INV, int H>
+__device__ __forceinline__ void pair_twiddle(Cx<T> (&v)[H], bool upper, const Cx<T>* tw_n) {
+#pragma unroll
+  for (int j = 1; j < H; ++j) {
+    const Cx<T> w = twiddle<T, INV>(tw_n, j);
+    v[j] = cmul(v[j], Cx<T>{upper ? w.re : T(1), upper ? w.im : T(0)});
+  }
+}
+
+// tw_n: the length-N table; tw_half: the length-N/2 table (tw_half[m] = tw_n[2m]).
+template <typename T, bool INV, int N>
+__device__ __forceinline__ void fft_pair_dif(Cx<T> (&v)[N / 2], bool upper, const Cx<T>* tw_n,
+                                             const Cx<T>* tw_half) {
+  static_assert(N % 2 == 0, "pair-split lines have even length");
+  pair_combine<T, N / 2>(v, upper);
+  pair_twiddle<T, INV, N / 2>(v, upper, tw_n);
+  fft_line_registers<T, INV, N / 2>(v, tw_half);
+}
+
+template <typename T, bool INV, int N>
+__device__ __forceinline__ void fft_pair_dit(Cx<T> (&v)[N / 2], bool upper, const Cx<T>* tw_n,
+                                             const Cx<T>* tw_half) {
+  static_assert(N % 2 == 0, "pair-split lines have even length");
+  fft_line_registers<T, INV, N / 2>(v, tw_half);
+  pair_twiddle<T, INV, N / 2>(v, upper, tw_n);
+  pair_combine<T, N / 2>(v, upper);
+}
+
 // Host-side twiddle tables, w[m] = exp(-2 pi i m / n), one per (n, precision).
 template <typename T>
 const Cx<T>* device_twiddles(int n);

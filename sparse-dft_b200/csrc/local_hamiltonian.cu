@@ -18,6 +18,7 @@
 #include <cstring>
 #include <limits>
 #include <set>
+#include <type_traits>
 
 #include "local_hamiltonian.cuh"
 
@@ -182,6 +183,175 @@ __global__ void __launch_bounds__(kThreads, plane_blocks<T>()) pencil_fixed_kern
   }
 }
 
+// FP32 pencil pass with one thread per (i1, i2) line: the line's n0 values
+// live in registers through both transforms (fft_line_registers), so no
+// transform stage touches shared memory. The kernel is persistent: CTA k
+// walks a contiguous range of units (block of 128 lines, column), column
+// fastest. While a unit's transforms run, cp.async stages the next unit's
+// slab rows into the other half of a double buffer, and V(r) of the line
+// block is staged once per block (it is the same for every column), so no
+// global load sits between the transforms. Thread t copies, reads and writes
+// only line t of each staged row, so the pass needs no CTA barrier. The
+// twiddles and the row -> slot map are kernel parameters.
+constexpr int kRegisterPencilThreads = 128;
+
+template <int N0>
+struct PencilRegisterArgs {
+  RegTwiddles<float, N0> tw;
+  int slot_of_row[N0];  // slab slot of grid row i0, or -1 (row outside the sphere's span)
+};
+
+template <int BYTES>
+__device__ __forceinline__ void copy_async(void* smem, const void* gmem) {
+  const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Waits until at most one committed group of this thread is still pending.
+__device__ __forceinline__ void copy_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int N0>
+__global__ void __launch_bounds__(kRegisterPencilThreads) pencil_registers_kernel(
+    Cx<float>* __restrict__ slab, long long n12, int slots, int columns, long long units,
+    const float* __restrict__ potential, const __grid_constant__ PencilRegisterArgs<N0> p) {
+  constexpr int TL = kRegisterPencilThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<float>* staged = reinterpret_cast<Cx<float>*>(smem_raw);     // [2][slots][TL]
+  float* staged_v = reinterpret_cast<float*>(staged + 2 * slots * TL);  // [N0][TL]
+  const int t = threadIdx.x;
+  const long long begin = units * blockIdx.x / gridDim.x, end = units * (blockIdx.x + 1) / gridDim.x;
+  auto stage_slab = [&](long long u) {
+    const long long kl0 = (u / columns) * TL;
+    const int c = static_cast<int>(u % columns);
+    if (kl0 + t < n12) {
+      const Cx<float>* src = slab + static_cast<long long>(c) * slots * n12 + kl0 + t;
+      Cx<float>* dst = staged + (u & 1) * slots * TL + t;
+      for (int s = 0; s < slots; ++s) copy_async<8>(dst + s * TL, src + s * n12);
+    }
+  };
+  if (begin < end) stage_slab(begin);
+  copy_async_commit();
+  long long block = -1;
+  for (long long u = begin; u < end; ++u) {
+    const long long b = u / columns;
+    const long long kl = b * TL + t;
+    const bool live = kl < n12;
+    if (b != block) {  // V(r) of the new line block
+      block = b;
+      if (live)
+        for (int i = 0; i < N0; ++i) copy_async<4>(staged_v + i * TL + t, potential + i * n12 + kl);
+      copy_async_commit();
+    }
+    if (u + 1 < end) stage_slab(u + 1);
+    copy_async_commit();
+    copy_async_wait_all_but_one();  // unit u's slab rows and the block's V(r) have landed
+    const Cx<float>* mine = staged + (u & 1) * slots * TL + t;
+    Cx<float> v[N0];
+#pragma unroll
+    for (int i = 0; i < N0; ++i) {
+      const int s = p.slot_of_row[i];
+      v[i] = s >= 0 ? mine[s * TL] : Cx<float>{0.0f, 0.0f};
+    }
+    fft_line_registers<float, true, N0>(v, p.tw.w);
+#pragma unroll
+    for (int i = 0; i < N0; ++i) v[i] = cscale(v[i], staged_v[i * TL + t]);
+    fft_line_registers<float, false, N0>(v, p.tw.w);
+    if (live) {
+      Cx<float>* out = slab + static_cast<long long>(u % columns) * slots * n12 + kl;
+#pragma unroll
+      for (int i = 0; i < N0; ++i) {
+        const int s = p.slot_of_row[i];
+        if (s >= 0) out[s * n12] = v[i];
+      }
+    }
+  }
+}
+
+// The same persistent pencil pass with pair-split lines (fft_pair_dif /
+// fft_pair_dit) for even n0: lane pair (l, l ^ 16) of warp w holds line
+// 16 w + (l & 15), the lower lane grid rows [0, n0/2), the upper one
+// [n0/2, n0); V(r) multiplies the interleaved spectrum (lower rows 2m,
+// upper 2m + 1). Half the registers of the one-thread form, so twice the
+// resident warps. Each lane stages, reads and writes only its own rows of
+// its own line: no CTA barrier.
+constexpr int kPairPencilThreads = 128;
+constexpr int kPairPencilLines = kPairPencilThreads / 2;
+constexpr int kPairPencilBlocks = 2;  // resident CTAs per SM: up to 255 registers a thread, no spills
+// Longest line the one-thread pencil holds in registers without spilling;
+// longer (even) lines take the pair form.
+constexpr int kRegisterPencilMax = 72;
+
+template <int N0>
+struct PencilPairArgs {
+  RegTwiddles<float, N0> tw;
+  RegTwiddles<float, N0 / 2> tw_half;
+  int slot_of_row[N0];  // slab slot of grid row i0, or -1
+};
+
+template <int N0>
+__global__ void __launch_bounds__(kPairPencilThreads, kPairPencilBlocks) pencil_pair_kernel(
+    Cx<float>* __restrict__ slab, long long n12, int slots, int columns, long long units,
+    const float* __restrict__ potential, const __grid_constant__ PencilPairArgs<N0> p) {
+  constexpr int H = N0 / 2, TL = kPairPencilLines;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<float>* staged = reinterpret_cast<Cx<float>*>(smem_raw);           // [2][slots][TL]
+  float* staged_v = reinterpret_cast<float*>(staged + 2 * slots * TL);  // [N0][TL]
+  const int lane = threadIdx.x & (kWarp - 1);
+  const bool upper = lane >= kPairXor;
+  const int t = (threadIdx.x >> 5) * kPairXor + (lane & (kPairXor - 1));
+  const int h = upper ? H : 0, odd = upper ? 1 : 0;
+  const long long begin = units * blockIdx.x / gridDim.x, end = units * (blockIdx.x + 1) / gridDim.x;
+  auto stage_slab = [&](long long u) {
+    const long long kl0 = (u / columns) * TL;
+    const int c = static_cast<int>(u % columns);
+    if (kl0 + t < n12) {
+      const Cx<float>* src = slab + static_cast<long long>(c) * slots * n12 + kl0 + t;
+      Cx<float>* dst = staged + (u & 1) * slots * TL + t;
+      for (int j = 0; j < H; ++j) {
+        const int s = p.slot_of_row[j + h];
+        if (s >= 0) copy_async<8>(dst + s * TL, src + s * n12);
+      }
+    }
+  };
+  if (begin < end) stage_slab(begin);
+  copy_async_commit();
+  long long block = -1;
+  for (long long u = begin; u < end; ++u) {
+    const long long b = u / columns;
+    const long long kl = b * TL + t;
+    const bool live = kl < n12;
+    if (b != block) {  // V(r) rows 2m + odd of the new line block
+      block = b;
+      if (live)
+        for (int m = 0; m < H; ++m)
+          copy_async<4>(staged_v + (2 * m + odd) * TL + t, potential + (2 * m + odd) * n12 + kl);
+      copy_async_commit();
+    }
+    if (u + 1 < end) stage_slab(u + 1);
+    copy_async_commit();
+    copy_async_wait_all_but_one();
+    const Cx<float>* mine = staged + (u & 1) * slots * TL + t;
+    Cx<float> v[H];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const int s = upper ? p.slot_of_row[j + H] : p.slot_of_row[j];
+      v[j] = s >= 0 ? mine[s * TL] : Cx<float>{0.0f, 0.0f};
+    }
+    fft_pair_dif<float, true, N0>(v, upper, p.tw.w, p.tw_half.w);
+#pragma unroll
+    for (int m = 0; m < H; ++m) v[m] = cscale(v[m], staged_v[(2 * m + odd) * TL + t]);
+    fft_pair_dit<float, false, N0>(v, upper, p.tw.w, p.tw_half.w);
+    if (live) {
+      Cx<float>* out = slab + static_cast<long long>(u % columns) * slots * n12 + kl;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const int s = upper ? p.slot_of_row[k + H] : p.slot_of_row[k];
+        if (s >= 0) out[s * n12] = v[k];
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) plane_out_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
                                                              const Cx<double>* __restrict__ x, long long ldx,
@@ -277,6 +447,16 @@ template <typename Kernel>
 void allow_smem(Kernel kernel, std::size_t bytes) {
   if (bytes > kMaxDynamicSmem) throw InvalidArgument("FFT tile does not fit in shared memory");
   allow_dynamic_smem(kernel, bytes);
+}
+
+// CTAs of `kernel` resident on the whole device at once (persistent grids).
+template <typename Kernel>
+long long resident_ctas(Kernel kernel, int threads, std::size_t smem) {
+  int per_sm = 0, device = 0, sms = 0;
+  SDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  SDFT_CUDA(cudaGetDevice(&device));
+  SDFT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  return static_cast<long long>(std::max(per_sm, 1)) * sms;
 }
 
 // plane_in_kernel for compile-time axis lengths N1 = N2 = N, one plane
@@ -378,6 +558,219 @@ __global__ void __launch_bounds__(kThreads, plane_blocks<T>()) plane_out_fixed_k
   }
 }
 
+// FP32 plane passes with pair-split lines (fft_pair_dif / fft_pair_dit):
+// one CTA per (slot, column) plane, lane pair (l, l ^ 16) of warp w on line
+// 16 w + (l & 15). The i1 transform runs on the i2 columns, the i2 transform
+// on the active i1 rows (row krow[line]); shared memory holds the plane once,
+// for the transpose between the two directions and the sphere scatter /
+// gather. Rows outside the active i1 set are zero in the column transform's
+// input (plane_in) and never transformed along i2 (plane_out).
+constexpr int kPointBatch = 8;
+
+template <int N>
+struct PlanePairArgs {
+  RegTwiddles<float, N> tw;
+  RegTwiddles<float, N / 2> tw_half;
+  int row_active[N];  // 1 where grid row i1 holds sphere points in some slot
+};
+
+template <int N>
+constexpr int plane_pair_threads() {
+  return (N + 15) / 16 * kWarp;
+}
+
+template <int N>
+__global__ void __launch_bounds__(plane_pair_threads<N>()) plane_in_pair_kernel(
+    const Cx<double>* __restrict__ x, long long ldx, LocalArgs<float> a, Cx<float>* __restrict__ slab,
+    const __grid_constant__ PlanePairArgs<N> p) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<float>* plane = reinterpret_cast<Cx<float>*>(smem_raw);  // [N][np]
+  const int np = a.n2p, s = blockIdx.x, c = blockIdx.y, tid = threadIdx.x;
+  const int lane = tid & (kWarp - 1);
+  const bool upper = lane >= kPairXor;
+  const int line = (tid >> 5) * kPairXor + (lane & (kPairXor - 1));
+  const int h = upper ? H : 0;
+  for (int i = tid; i < a.krows * N; i += blockDim.x) {
+    const int r = i / N, i2 = i - r * N;
+    plane[__ldg(a.krow + r) * np + i2] = Cx<float>{0.0f, 0.0f};
+  }
+  __syncthreads();
+  // Sphere points in rounds of kPointBatch per thread, every load of a round in flight together.
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  const int p_begin = a.point_offset[s], points = a.point_offset[s + 1] - p_begin;
+  for (int first = tid; first < points; first += kPointBatch * blockDim.x) {
+    int dst[kPointBatch], g[kPointBatch];
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u) {
+      const int i = first + u * blockDim.x;
+      dst[u] = -1;
+      if (i < points) {
+        dst[u] = __ldg(a.point_smem + p_begin + i);
+        g[u] = __ldg(a.point_g + p_begin + i);
+      }
+    }
+    Cx<double> value[kPointBatch];
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u)
+      if (dst[u] >= 0) value[u] = xc[g[u]];
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u)
+      if (dst[u] >= 0) plane[dst[u]] = cconvert<float>(value[u]);
+  }
+  __syncthreads();
+  Cx<float> v[H];
+  {  // i2 along active row krow[line]: natural halves in, interleaved out
+    const bool live = line < a.krows;
+    Cx<float>* row = plane + (live ? __ldg(a.krow + line) : 0) * np;
+#pragma unroll
+    for (int j = 0; j < H; ++j) v[j] = live ? row[j + h] : Cx<float>{0.0f, 0.0f};
+    fft_pair_dif<float, true, N>(v, upper, p.tw.w, p.tw_half.w);
+    if (live) {
+#pragma unroll
+      for (int m = 0; m < H; ++m) row[2 * m + (upper ? 1 : 0)] = v[m];
+    }
+  }
+  __syncthreads();
+  {  // i1 along column i2 = line, straight to the slab rows 2m + upper
+    const bool live = line < N;
+    const int col = live ? line : 0;  // lanes past the last column read column 0 and store nothing
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const int active = upper ? p.row_active[j + H] : p.row_active[j];
+      v[j] = live && active ? plane[(j + h) * np + col] : Cx<float>{0.0f, 0.0f};
+    }
+    fft_pair_dif<float, true, N>(v, upper, p.tw.w, p.tw_half.w);
+    if (live) {
+      Cx<float>* out = slab + (static_cast<long long>(c) * a.slots + s) * (N * N) + col + (upper ? N : 0);
+#pragma unroll
+      for (int m = 0; m < H; ++m) out[2 * m * N] = v[m];
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(plane_pair_threads<N>()) plane_out_pair_kernel(
+    const Cx<float>* __restrict__ slab, LocalArgs<float> a, const Cx<double>* __restrict__ x, long long ldx,
+    const double* __restrict__ kinetic, double count, Cx<double>* __restrict__ y, long long ldy,
+    const __grid_constant__ PlanePairArgs<N> p) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<float>* plane = reinterpret_cast<Cx<float>*>(smem_raw);  // [N][np]
+  const int np = a.n2p, s = blockIdx.x, c = blockIdx.y, tid = threadIdx.x;
+  const int lane = tid & (kWarp - 1);
+  const bool upper = lane >= kPairXor;
+  const int line = (tid >> 5) * kPairXor + (lane & (kPairXor - 1));
+  const int h = upper ? H : 0;
+  Cx<float> v[H];
+  {  // i1 along column i2 = line: slab rows 2m + upper in, natural halves out
+    const bool live = line < N;
+    const int col = live ? line : 0;  // lanes past the last column read column 0 and store nothing
+    const Cx<float>* in = slab + (static_cast<long long>(c) * a.slots + s) * (N * N) + col + (upper ? N : 0);
+#pragma unroll
+    for (int m = 0; m < H; ++m) v[m] = live ? in[2 * m * N] : Cx<float>{0.0f, 0.0f};
+    fft_pair_dit<float, false, N>(v, upper, p.tw.w, p.tw_half.w);
+    if (live) {
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const int active = upper ? p.row_active[k + H] : p.row_active[k];
+        if (active) plane[(k + h) * np + col] = v[k];
+      }
+    }
+  }
+  __syncthreads();
+  {  // i2 along active row krow[line]: interleaved in, natural halves out
+    const bool live = line < a.krows;
+    Cx<float>* row = plane + (live ? __ldg(a.krow + line) : 0) * np;
+#pragma unroll
+    for (int m = 0; m < H; ++m) v[m] = live ? row[2 * m + (upper ? 1 : 0)] : Cx<float>{0.0f, 0.0f};
+    fft_pair_dit<float, false, N>(v, upper, p.tw.w, p.tw_half.w);
+    if (live) {
+#pragma unroll
+      for (int k = 0; k < H; ++k) row[k + h] = v[k];
+    }
+  }
+  __syncthreads();
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
+  const int p_begin = a.point_offset[s], points = a.point_offset[s + 1] - p_begin;
+  for (int first = tid; first < points; first += kPointBatch * blockDim.x) {
+    int g[kPointBatch], at[kPointBatch];
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u) {
+      const int i = first + u * blockDim.x;
+      g[u] = -1;
+      if (i < points) {
+        g[u] = __ldg(a.point_g + p_begin + i);
+        at[u] = __ldg(a.point_smem + p_begin + i);
+      }
+    }
+    Cx<double> in_g[kPointBatch];
+    double t[kPointBatch];
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u)
+      if (g[u] >= 0) {
+        in_g[u] = xc[g[u]];
+        t[u] = __ldg(kinetic + g[u]);
+      }
+#pragma unroll
+    for (int u = 0; u < kPointBatch; ++u)
+      if (g[u] >= 0) {
+        const Cx<double> value = cconvert<double>(plane[at[u]]);
+        yc[g[u]] = Cx<double>{t[u] * in_g[u].re + value.re / count, t[u] * in_g[u].im + value.im / count};
+      }
+  }
+}
+
+// FP32 plane passes with the pair kernels for square planes of the even
+// lengths they are compiled for; false otherwise.
+template <typename T>
+bool launch_planes_pair(const SpherePlan& plan, const LocalArgs<T>& a, bool inward, int columns,
+                        const Cx<double>* x, long long ldx, Cx<T>* slab, const double* kinetic, double count,
+                        Cx<double>* y, long long ldy, cudaStream_t stream) {
+  if constexpr (!std::is_same_v<T, float>) {
+    return false;
+  } else {
+    if (a.n1 != a.n2) return false;
+    auto go = [&](auto length) {
+      constexpr int N = decltype(length)::value;
+      PlanePairArgs<N> p;
+      for (int i = 0; i < N; ++i) p.tw.w[i] = plan.twiddles_host[1][i];
+      for (int i = 0; i < N / 2; ++i) p.tw_half.w[i] = plan.twiddles_host[1][2 * i];
+      for (int i = 0; i < N; ++i) p.row_active[i] = 0;
+      for (int r : plan.krow_host) p.row_active[r] = 1;
+      const std::size_t smem = sizeof(Cx<float>) * N * static_cast<std::size_t>(a.n2p);
+      const dim3 grid(a.slots, columns);
+      constexpr int threads = plane_pair_threads<N>();
+      if (inward) {
+        allow_smem(plane_in_pair_kernel<N>, smem);
+        plane_in_pair_kernel<N><<<grid, threads, smem, stream>>>(x, ldx, a, slab, p);
+        SDFT_LAUNCH("plane_in_pair_kernel");
+      } else {
+        allow_smem(plane_out_pair_kernel<N>, smem);
+        plane_out_pair_kernel<N><<<grid, threads, smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy, p);
+        SDFT_LAUNCH("plane_out_pair_kernel");
+      }
+      return true;
+    };
+    switch (a.n1) {
+      case 40: return go(std::integral_constant<int, 40>{});
+      case 42: return go(std::integral_constant<int, 42>{});
+      case 48: return go(std::integral_constant<int, 48>{});
+      case 54: return go(std::integral_constant<int, 54>{});
+      case 56: return go(std::integral_constant<int, 56>{});
+      case 60: return go(std::integral_constant<int, 60>{});
+      case 70: return go(std::integral_constant<int, 70>{});
+      case 72: return go(std::integral_constant<int, 72>{});
+      case 80: return go(std::integral_constant<int, 80>{});
+      case 84: return go(std::integral_constant<int, 84>{});
+      case 90: return go(std::integral_constant<int, 90>{});
+      case 96: return go(std::integral_constant<int, 96>{});
+      default: return false;
+    }
+  }
+}
+
 // Plane passes with the compile-time kernels for square planes of the common
 // lengths; false when the plane has another shape.
 template <typename T>
@@ -421,6 +814,74 @@ bool launch_planes_fixed(const LocalArgs<T>& a, bool inward, int columns, const 
     default: return false;
   }
 #undef SDFT_PLANES
+}
+
+// FP32 pencil pass with the register kernel where n0 has one; false otherwise.
+template <typename T>
+bool launch_pencil_registers(const SpherePlan& plan, int columns, const T* potential, Cx<T>* slab,
+                             cudaStream_t stream) {
+  if constexpr (!std::is_same_v<T, float>) {
+    return false;
+  } else {
+    const long long n12 = static_cast<long long>(plan.n[1]) * plan.n[2];
+    const long long units = static_cast<long long>(ceil_div(static_cast<std::size_t>(n12), kRegisterPencilThreads)) *
+                            columns;
+    auto go = [&](auto length) {
+      constexpr int N0 = decltype(length)::value;
+      if constexpr (N0 > kRegisterPencilMax) {
+        const long long pair_units =
+            static_cast<long long>(ceil_div(static_cast<std::size_t>(n12), kPairPencilLines)) * columns;
+        PencilPairArgs<N0> p;
+        for (int i = 0; i < N0; ++i) {
+          p.tw.w[i] = plan.twiddles_host[0][i];
+          p.slot_of_row[i] = plan.slot_of_row_host[i];
+        }
+        for (int i = 0; i < N0 / 2; ++i) p.tw_half.w[i] = plan.twiddles_host[0][2 * i];
+        const std::size_t smem =
+            sizeof(Cx<float>) * 2 * plan.slots * kPairPencilLines + sizeof(float) * N0 * kPairPencilLines;
+        allow_smem(pencil_pair_kernel<N0>, smem);
+        const long long grid =
+            std::min<long long>(pair_units, resident_ctas(pencil_pair_kernel<N0>, kPairPencilThreads, smem));
+        pencil_pair_kernel<N0><<<static_cast<unsigned>(grid), kPairPencilThreads, smem, stream>>>(
+            slab, n12, plan.slots, columns, pair_units, potential, p);
+        SDFT_LAUNCH("pencil_pair_kernel");
+      } else {
+        PencilRegisterArgs<N0> p;
+        for (int i = 0; i < N0; ++i) {
+          p.tw.w[i] = plan.twiddles_host[0][i];
+          p.slot_of_row[i] = plan.slot_of_row_host[i];
+        }
+        const std::size_t smem =
+            sizeof(Cx<float>) * 2 * plan.slots * kRegisterPencilThreads + sizeof(float) * N0 * kRegisterPencilThreads;
+        allow_smem(pencil_registers_kernel<N0>, smem);
+        const long long grid =
+            std::min<long long>(units, resident_ctas(pencil_registers_kernel<N0>, kRegisterPencilThreads, smem));
+        pencil_registers_kernel<N0><<<static_cast<unsigned>(grid), kRegisterPencilThreads, smem, stream>>>(
+            slab, n12, plan.slots, columns, units, potential, p);
+        SDFT_LAUNCH("pencil_registers_kernel");
+      }
+      return true;
+    };
+    switch (plan.n[0]) {
+      case 35: return go(std::integral_constant<int, 35>{});
+      case 40: return go(std::integral_constant<int, 40>{});
+      case 42: return go(std::integral_constant<int, 42>{});
+      case 45: return go(std::integral_constant<int, 45>{});
+      case 48: return go(std::integral_constant<int, 48>{});
+      case 49: return go(std::integral_constant<int, 49>{});
+      case 54: return go(std::integral_constant<int, 54>{});
+      case 56: return go(std::integral_constant<int, 56>{});
+      case 60: return go(std::integral_constant<int, 60>{});
+      case 63: return go(std::integral_constant<int, 63>{});
+      case 70: return go(std::integral_constant<int, 70>{});
+      case 72: return go(std::integral_constant<int, 72>{});
+      case 80: return go(std::integral_constant<int, 80>{});
+      case 84: return go(std::integral_constant<int, 84>{});
+      case 90: return go(std::integral_constant<int, 90>{});
+      case 96: return go(std::integral_constant<int, 96>{});
+      default: return false;
+    }
+  }
 }
 
 // Pencil pass with the compile-time kernel for the common axis lengths.
@@ -481,24 +942,27 @@ LocalArgs<T> make_args(const SpherePlan& plan) {
 // The three passes: plane_in, pencil (V(r) multiply) and plane_out, each
 // with its compile-time kernel where the lengths have one.
 template <typename T>
-void run_local_passes(const LocalArgs<T>& a, double count, const Cx<double>* x, long long ldx, int columns,
+void run_local_passes(const SpherePlan& plan, const LocalArgs<T>& a, double count, const Cx<double>* x, long long ldx, int columns,
                       const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
                       cudaStream_t stream) {
   const std::size_t plane_smem = sizeof(Cx<T>) * (a.n1 + a.n2 + 2 * static_cast<std::size_t>(a.n1) * a.n2p);
   const std::size_t pencil_smem = sizeof(Cx<T>) * (a.n0 + 2 * static_cast<std::size_t>(a.n0) * (kPencilLines + 1));
   const dim3 planes(a.slots, columns);
-  if (!launch_planes_fixed<T>(a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
+  if (!launch_planes_pair<T>(plan, a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream) &&
+      !launch_planes_fixed<T>(a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
     allow_smem(plane_in_kernel<T>, plane_smem);
     plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
     SDFT_LAUNCH("plane_in_kernel");
   }
-  if (!launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
+  if (!launch_pencil_registers<T>(plan, columns, potential, slab, stream) &&
+      !launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
     const dim3 pencils(static_cast<unsigned>(ceil_div(static_cast<std::size_t>(a.n12), kPencilLines)), columns);
     allow_smem(pencil_kernel<T>, pencil_smem);
     pencil_kernel<T><<<pencils, kThreads, pencil_smem, stream>>>(slab, a, potential);
     SDFT_LAUNCH("pencil_kernel");
   }
-  if (!launch_planes_fixed<T>(a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
+  if (!launch_planes_pair<T>(plan, a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream) &&
+      !launch_planes_fixed<T>(a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
     allow_smem(plane_out_kernel<T>, plane_smem);
     plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
     SDFT_LAUNCH("plane_out_kernel");
@@ -510,7 +974,8 @@ void local_hamiltonian_impl(const SpherePlan& plan, const Cx<double>* x, long lo
                             const T* potential, const double* kinetic, Cx<double>* y, long long ldy, Cx<T>* slab,
                             cudaStream_t stream) {
   const LocalArgs<T> a = make_args<T>(plan);
-  run_local_passes<T>(a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
+  run_local_passes<T>(plan, a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab,
+                      stream);
 }
 
 template <typename T, bool INV, int TL, bool GENERAL>
@@ -586,6 +1051,12 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
   std::vector<int> h_slot_row(rows0.begin(), rows0.end());
   slots = static_cast<int>(h_slot_row.size());
   for (int s = 0; s < slots; ++s) slot_of_row[h_slot_row[s]] = s;
+  slot_of_row_host = slot_of_row;
+  krow_host.assign(rows1.begin(), rows1.end());
+  for (int a = 0; a < 3; ++a) {
+    twiddles_host[a].resize(n[a]);
+    host_twiddles<float>(n[a], twiddles_host[a].data());
+  }
   std::vector<int> h_krow(rows1.begin(), rows1.end());
   krows = static_cast<int>(h_krow.size());
   std::vector<int> h_offset(slots + 1, 0);
@@ -674,7 +1145,8 @@ void local_hamiltonian_preset(const SpherePlan& plan, const Cx<double>* x, long 
   a.tw0 = twiddle[0];
   a.tw1 = twiddle[1];
   a.tw2 = twiddle[2];
-  run_local_passes<T>(a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab, stream);
+  run_local_passes<T>(plan, a, static_cast<double>(plan.count), x, ldx, columns, potential, kinetic, y, ldy, slab,
+                      stream);
 }
 
 template void local_hamiltonian_preset<float>(const SpherePlan&, const Cx<double>*, long long, int, const float*,

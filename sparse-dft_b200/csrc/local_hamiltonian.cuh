@@ -25,6 +25,9 @@ struct SpherePlan {
   int* point_compact = nullptr; // [npw] k*n2 + i2, k = position of i1 in krow
   int* krow = nullptr;          // [krows]
   LinePlan line[3];
+  std::vector<int> slot_of_row_host;       // [n0] slot of grid row i0, or -1
+  std::vector<int> krow_host;              // [krows] the active i1 rows
+  std::vector<Cx<float>> twiddles_host[3]; // [n[a]] FP32 twiddles, passed as kernel parameters
 
   void build(const int shape[3], const std::vector<std::uint64_t>& indices);
   void release();
