@@ -419,7 +419,7 @@ def fused_local_roofline(op, inputs, stream):
     # DRAM bytes (read + write) of plane_in + pencil + plane_out for one
     # 160-column launch, from one ncu capture of `bench.py --case local
     # --columns 160` (profiles/fused_local_h_si64_160cols.md).
-    traffic = 951_051_520 if cols == 160 and (n0, n1, n2) == (70, 70, 70) else None
+    traffic = 956_765_952 if cols == 160 and (n0, n1, n2) == (70, 70, 70) else None
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": "fused local H~psi (plane_in + pencil + plane_out), FP32, 160 columns",
             "ms_per_launch": ms, "algorithmic_bytes": algorithmic,
