@@ -308,7 +308,8 @@ def run_b200(args):
 
     serving_rows = None
     if rank == 0 and world == 1 and not args.no_serving:
-        serving_rows = serving_stream(local)
+        serving_rows = serving_stream(local, requests=args.serving_requests,
+                                      forms=("mixed",) if args.serving_mixed_only else ("mixed", "fp64"))
 
     kpoint_rows = None
     if rank == 0 and world == 1 and not args.no_kpoints:
@@ -523,31 +524,56 @@ def density_side(ctx, inputs, stream, peak):
     return out
 
 
-def serving_stream(device, requests=24, slots=4, rate_hz=8.0, cap=150e9, seed=4242):
-    """A sample of the seeded serving stream through the solve server: Poisson
-    arrivals (rate_hz) of requests with 2-16 atoms, Ecut 10-15 Ha, 1-2
-    k-points (one solve per k-point), admitted by device footprint under cap
-    with `slots` concurrent solves; the same stream in the mixed and the FP64
-    plain form. Latency = finish - submit of a request's last k-point."""
-    import numpy as np
+def _serving_request(index, seed):
+    """One request of the seeded serving stream (run in a spawned host process)."""
     from sdft_b200 import synthetic
+    return synthetic.serving_request(index, seed=seed)
+
+
+def serving_stream(device, requests=16, slots=4, rate_hz=1.0, cap=150e9, seed=4242, forms=("mixed", "fp64"),
+                   generators=8):
+    """A sample of the seeded serving stream through the solve server: the
+    first `requests` requests of the config-4 stream (cubic cells of 2-128
+    atoms drawn log-uniformly, Ecut U(10, 25) Ha, bands 1.25x occupied within
+    [8, 320], 1-8 k-points, one solve per k-point), Poisson arrivals at
+    rate_hz, admitted by device footprint under `cap` with `slots` concurrent
+    solves; the same stream in each form. `generators` spawned host processes
+    build the requests ahead of their arrival; a request submitted after its
+    arrival time because its inputs were not ready yet counts as
+    generation-paced (its latency is measured from its submission).
+    Latency = finish of a request's last k-point - submission of its first."""
+    import concurrent.futures
+    import multiprocessing
+    import numpy as np
     from sdft_b200.serving import SolveServer
 
-    stream = [synthetic.serving_request(i, seed=seed, atoms=(2, 16), ecut_ha=(10.0, 15.0), kpoints=(1, 2))
-              for i in range(requests)]
     arrivals = np.cumsum(np.random.Generator(np.random.PCG64(seed)).exponential(1.0 / rate_hz, size=requests))
+    context = multiprocessing.get_context("spawn")
 
     def run(precision):
-        with SolveServer(device, cap, slots) as server:
-            t0 = time.perf_counter()
-            tickets = []
-            for when, ops in zip(arrivals, stream):
-                delay = when - (time.perf_counter() - t0)
+        with concurrent.futures.ProcessPoolExecutor(max_workers=generators, mp_context=context) as pool, \
+                SolveServer(device, cap, slots) as server:
+            pending = [pool.submit(_serving_request, i, seed) for i in range(min(requests, 2 * generators))]
+            tickets, paced, atoms, kpoints = [], 0, [], []
+            t0 = None
+            for i in range(requests):
+                ops = pending[i].result()
+                pending[i] = None
+                if len(pending) < requests:
+                    pending.append(pool.submit(_serving_request, len(pending), seed))
+                if t0 is None:
+                    t0 = time.perf_counter() - arrivals[0]
+                delay = arrivals[i] - (time.perf_counter() - t0)
                 if delay > 0:
                     time.sleep(delay)
+                else:
+                    paced += 1
+                atoms.append(int(ops[0].positions.shape[0]))
+                kpoints.append(len(ops))
                 tickets.append([server.submit(x, precision=precision) for x in ops])
+                del ops
             results = [[server.wait(t) for t in group] for group in tickets]
-            makespan = time.perf_counter() - t0
+            makespan = time.perf_counter() - t0 - arrivals[0]
             memory = server.memory()
         latency = [1e3 * (max(r["timing"]["finished"] for r in group) - min(r["timing"]["submitted"] for r in group))
                    for group in results]
@@ -563,11 +589,15 @@ def serving_stream(device, requests=24, slots=4, rate_hz=8.0, cap=150e9, seed=42
                 "certified_pairs_per_s": pairs / makespan, "certified_pairs": pairs,
                 "solves": len(flat), "all_converged": all(r["converged"] for r in flat),
                 "makespan_s": makespan, "peak_concurrent_solves": peak_depth,
-                "peak_budget_gb": memory["peak"] / 1e9}
+                "peak_budget_gb": memory["peak"] / 1e9, "generation_paced_requests": paced,
+                "atoms_range": [min(atoms), max(atoms)], "kpoints_total": int(sum(kpoints))}
 
-    return {"requests": requests, "slots": slots, "arrival_rate_hz": rate_hz, "memory_cap_gb": cap / 1e9,
-            "sample": "seeded stream, 2-16 atoms, Ecut 10-15 Ha, 1-2 k-points, bands 1.25x occupied (min 8)",
-            "mixed": run("mixed"), "fp64_plain": run("fp64")}
+    out = {"requests": requests, "slots": slots, "arrival_rate_hz": rate_hz, "memory_cap_gb": cap / 1e9,
+           "sample": f"the first {requests} requests of the seeded config-4 stream: 2-128 atoms (log-uniform), "
+                     "Ecut U(10, 25) Ha, 1-8 k-points, bands 1.25x occupied in [8, 320]"}
+    for form in forms:
+        out["mixed" if form == "mixed" else "fp64_plain"] = run(form)
+    return out
 
 
 KPOINT_SAMPLE = (26, 5, 13, 0)
@@ -738,6 +768,10 @@ def main():
     parser.add_argument("--no-density", action="store_true", help="skip the density-side measurements")
     parser.add_argument("--no-serving", action="store_true", help="skip the serving-stream sample")
     parser.add_argument("--no-kpoints", action="store_true", help="skip the GaAs64 k-point batch")
+    parser.add_argument("--serving-requests", type=int, default=16,
+                        help="requests of the serving-stream sample (the stream has 2000)")
+    parser.add_argument("--serving-mixed-only", action="store_true",
+                        help="run the serving sample in the mixed form only")
     parser.add_argument("--all-kpoints", action="store_true", help="all 27 k-points of the GaAs64 batch (default: 4)")
     parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe", "compensation"],
                         help="run a few launches of one kernel family for a profiler capture and exit")

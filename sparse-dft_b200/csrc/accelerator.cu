@@ -44,7 +44,7 @@ void accelerator_local_hamiltonian(Context& ctx, const int shape[3], const std::
     std::vector<std::uint64_t> idx(indices, indices + npw);
     for (auto i : idx)
       if (i >= count) throw InvalidArgument("accelerated FFT plane-wave index out of range");
-    cache.plan.build(shape, idx);
+    cache.plan.build(shape, idx, st);
     double* v64 = as<double>(cache.v64, count);
     float* v32 = as<float>(cache.v32, count);
     SDFT_CUDA(cudaMemcpyAsync(v64, potential, sizeof(double) * count, cudaMemcpyHostToDevice, st));

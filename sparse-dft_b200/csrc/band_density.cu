@@ -275,7 +275,7 @@ void band_density(Context& ctx, const std::int32_t* hkl, std::size_t npw, const 
   if (std::memcmp(cache.shape, shape, sizeof(shape)) != 0 || cache.indices != indices) {
     std::unordered_set<std::uint64_t> seen(indices.begin(), indices.end());
     if (seen.size() != indices.size()) throw InvalidArgument("duplicate plane-wave key in density basis");
-    cache.plan.build(shape, indices);
+    cache.plan.build(shape, indices, ctx.stream);
     std::memcpy(cache.shape, shape, sizeof(shape));
     cache.indices = std::move(indices);
   }

@@ -38,6 +38,16 @@ unsigned long long launch_count();
 #define SDFT_CUDA(call) ::sdft_b200::check_cuda((call), #call)
 #define SDFT_LAUNCH(what) (::sdft_b200::count_launch(), ::sdft_b200::check_cuda(cudaGetLastError(), what))
 
+// Stream-ordered device memory from the library's pool on the current device
+// (device_memory.cu): neither call synchronises the device. The memory is
+// valid for work ordered after the allocation on `stream` (or after the
+// stream has been synchronised); a freed block returns to the pool and is
+// kept there for the next allocation. trim_pool() hands the pool's unused
+// memory back to the device.
+void* stream_alloc(std::size_t bytes, cudaStream_t stream);
+void stream_free(void* ptr, cudaStream_t stream);
+void trim_pool();
+
 // Largest dynamic shared memory a kernel here may take (B200 opt-in limit).
 constexpr std::size_t kMaxDynamicSmem = 227 * 1024;
 

@@ -7,15 +7,19 @@ namespace sdft_b200 {
 
 void* Scratch::reserve(std::size_t need) {
   if (need <= bytes) return ptr;
-  release();
   const std::size_t grown = std::max(need, bytes + bytes / 4);
-  SDFT_CUDA(cudaMalloc(&ptr, grown));
+  release();
+  if (stream) ptr = stream_alloc(grown, stream);
+  else SDFT_CUDA(cudaMalloc(&ptr, grown));
   bytes = grown;
   return ptr;
 }
 
 void Scratch::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    if (stream) stream_free(ptr, stream);
+    else cudaFree(ptr);
+  }
   ptr = nullptr;
   bytes = 0;
 }

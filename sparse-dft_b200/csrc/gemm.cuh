@@ -9,9 +9,14 @@ namespace sdft_b200 {
 enum class Op { N, C };  // C = conjugate transpose (the reference's MatrixOp::Adjoint)
 
 // Grow-only device scratch owned by a context.
+// Grow-only device buffer. With `stream` set (by the owning context) its
+// memory is stream-ordered pool memory on that stream (stream_alloc), so
+// growing or releasing it never synchronises the device; without, plain
+// cudaMalloc / cudaFree.
 struct Scratch {
   void* ptr = nullptr;
   std::size_t bytes = 0;
+  cudaStream_t stream = nullptr;
   void* reserve(std::size_t need);
   void release();
   ~Scratch() { release(); }

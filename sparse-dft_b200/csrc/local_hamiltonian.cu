@@ -1027,8 +1027,9 @@ void fft3d_impl(Cx<T>* grid, const int n[3], int batch, cudaStream_t stream) {
 
 }  // namespace
 
-void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& indices) {
+void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& indices, cudaStream_t on) {
   release();
+  stream = on;
   for (int a = 0; a < 3; ++a) {
     if (shape[a] < 1 || !fft_length_supported(shape[a]))
       throw InvalidArgument("grid axis length must be a 2/3/5/7-smooth integer in [1,512]");
@@ -1075,9 +1076,11 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
     h_smem[p] = i1 * n2p + i2;
     h_compact[p] = kpos[i1] * n[2] + i2;
   }
-  auto upload = [](int*& dst, const std::vector<int>& src) {
-    SDFT_CUDA(cudaMalloc(&dst, sizeof(int) * std::max<std::size_t>(1, src.size())));
-    SDFT_CUDA(cudaMemcpy(dst, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice));
+  // Pageable host sources: each copy has staged its source when the call returns.
+  auto upload = [&](int*& dst, const std::vector<int>& src) {
+    dst = static_cast<int*>(stream_alloc(sizeof(int) * std::max<std::size_t>(1, src.size()), stream));
+    if (!src.empty())
+      SDFT_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, stream));
   };
   upload(slot_row, h_slot_row);
   upload(point_offset, h_offset);
@@ -1089,7 +1092,7 @@ void SpherePlan::build(const int shape[3], const std::vector<std::uint64_t>& ind
 
 void SpherePlan::release() {
   for (int** p : {&slot_row, &point_offset, &point_g, &point_smem, &point_compact, &krow}) {
-    if (*p) cudaFree(*p);
+    stream_free(*p, stream);
     *p = nullptr;
   }
 }

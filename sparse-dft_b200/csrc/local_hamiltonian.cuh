@@ -29,7 +29,10 @@ struct SpherePlan {
   std::vector<int> krow_host;              // [krows] the active i1 rows
   std::vector<Cx<float>> twiddles_host[3]; // [n[a]] FP32 twiddles, passed as kernel parameters
 
-  void build(const int shape[3], const std::vector<std::uint64_t>& indices);
+  cudaStream_t stream = nullptr;  // the device arrays are stream-ordered pool memory on it
+
+  // Device arrays are allocated and uploaded on `stream` (stream-ordered).
+  void build(const int shape[3], const std::vector<std::uint64_t>& indices, cudaStream_t stream);
   void release();
   std::size_t slab_elements(std::size_t columns) const {
     return static_cast<std::size_t>(slots) * n[1] * n[2] * columns;

@@ -148,6 +148,8 @@ Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
     SDFT_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     owns_stream = true;
   }
+  for (Scratch* buffer : working_buffers()) buffer->stream = stream;
+  for (Scratch* buffer : cache_buffers()) buffer->stream = stream;
   check_blas(cublasCreate(&blas), "cublasCreate");
   check_blas(cublasSetStream(blas, stream), "cublasSetStream");
   check_blas(cublasSetMathMode(blas, CUBLAS_DEFAULT_MATH), "cublasSetMathMode");  // true FP64, no TF32
@@ -156,37 +158,56 @@ Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
 }
 
 Context::~Context() {
+  // Everything stream-ordered on this stream is released before the stream goes.
+  cudaStreamSynchronize(stream);
+  for (Scratch* buffer : working_buffers()) buffer->release();
+  for (Scratch* buffer : cache_buffers()) buffer->release();
+  accel.plan.release();
+  density.plan.release();
+  release(accel.b_packed);
+  release(accel.bh_packed);
+  for (ImmutableLeft& entry : immutable.entries) release(entry.packed);
   if (solver) cusolverDnDestroy(solver);
   if (blas) cublasDestroy(blas);
-  for (Scratch* s : {&slab32, &slab64, &staging_in, &staging_out, &staging_aux, &projections, &onsite, &tc.a, &tc.b,
-                     &tc.partial})
-    s->release();
   if (owns_stream && stream) cudaStreamDestroy(stream);
 }
 
 void Context::synchronize() const { SDFT_CUDA(cudaStreamSynchronize(stream)); }
 
-void Context::release_scratch() {
+std::vector<Scratch*> Context::working_buffers() {
+  std::vector<Scratch*> all = {&slab32, &slab64, &staging_in, &staging_out, &staging_aux, &projections, &onsite,
+                               &tc.a, &tc.b, &tc.partial, &tc.adjoint};
+  for (EigenWorkspace* w : {&eigen, &davidson.eigen})
+    for (Scratch* s : {&w->tridiagonal, &w->vectors, &w->scalar, &w->product, &w->product2, &w->solver_work})
+      all.push_back(s);
+  DavidsonBuffers& d = davidson;
+  for (Scratch* s : {&d.basis, &d.hbasis, &d.sbasis, &d.cached_h, &d.cached_s, &d.rr_a, &d.rr_b, &d.rr_w,
+                     &d.rr_work, &d.info, &d.xs, &d.sxs, &d.hxs, &d.res, &d.block, &d.metric, &d.original,
+                     &d.projections, &d.gram, &d.small, &d.order, &d.select, &d.pack_vc, &d.pack_vn, &d.pack_hn,
+                     &d.pack_sn, &d.pack_hb, &d.pack_sb, &d.excluded, &d.polish, &d.polish_small,
+                     &d.polish_values})
+    all.push_back(s);
+  CorrectionBuffers& c = davidson.corrections;
+  for (Scratch* s : {&c.res, &c.z, &c.p, &c.hp, &c.xh, &c.sxh, &c.xl, &c.sxl, &c.coefficients, &c.scalars, &c.index})
+    all.push_back(s);
+  return all;
+}
+
+std::vector<Scratch*> Context::cache_buffers() {
+  std::vector<Scratch*> all = {&accel.v64, &accel.v32, &accel.kinetic, &accel.b, &accel.d, &accel.q,
+                               &density.rows, &density.planes, &density.grid, &density.meta};
+  for (ImmutableLeft& entry : immutable.entries) all.push_back(&entry.fp64);
+  return all;
+}
+
+void Context::recycle_scratch() {
   synchronize();
-  for (Scratch* s : {&slab32, &slab64, &staging_in, &staging_out, &staging_aux, &projections, &onsite, &tc.a, &tc.b,
-                     &tc.partial, &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
-                     &eigen.solver_work})
-    s->release();
-  davidson.release();
+  for (Scratch* buffer : working_buffers()) buffer->release();
 }
 
-void DavidsonBuffers::release() {
-  for (Scratch* s : {&basis, &hbasis, &sbasis, &cached_h, &cached_s, &rr_a, &rr_b, &rr_w, &rr_work, &info,
-                     &eigen.tridiagonal, &eigen.vectors, &eigen.scalar, &eigen.product, &eigen.product2,
-                     &eigen.solver_work, &xs, &sxs, &hxs, &res, &block, &metric, &original, &projections, &gram,
-                     &small, &order, &select, &pack_vc, &pack_vn, &pack_hn, &pack_sn, &pack_hb, &pack_sb,
-                     &excluded, &polish, &polish_small, &polish_values})
-    s->release();
-  corrections.release();
-}
-
-void CorrectionBuffers::release() {
-  for (Scratch* s : {&res, &z, &p, &hp, &xh, &sxh, &xl, &sxl, &coefficients, &scalars, &index}) s->release();
+void Context::release_scratch() {
+  recycle_scratch();
+  trim_pool();
 }
 
 GVectorList enumerate_g_vectors(const double reciprocal[9], double cutoff_ev, const double kpoint[3],
@@ -306,18 +327,17 @@ LocalPotential local_potential(Context& ctx, const int span[3], std::size_t pote
     if (!retained) continue;
     grid[index(k[0], k[1], k[2])] = Cx<double>{potential[2 * i], potential[2 * i + 1]};
   }
-  Cx<double>* dgrid = nullptr;
-  SDFT_CUDA(cudaMalloc(&dgrid, sizeof(Cx<double>) * count));
+  Cx<double>* dgrid = static_cast<Cx<double>*>(stream_alloc(sizeof(Cx<double>) * count, ctx.stream));
   try {
     SDFT_CUDA(cudaMemcpyAsync(dgrid, grid.data(), sizeof(Cx<double>) * count, cudaMemcpyHostToDevice, ctx.stream));
     fft3d<double>(dgrid, out.shape, 1, true, ctx.stream);
     SDFT_CUDA(cudaMemcpyAsync(grid.data(), dgrid, sizeof(Cx<double>) * count, cudaMemcpyDeviceToHost, ctx.stream));
     SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
   } catch (...) {
-    cudaFree(dgrid);
+    stream_free(dgrid, ctx.stream);
     throw;
   }
-  cudaFree(dgrid);
+  stream_free(dgrid, ctx.stream);
   out.real.resize(count);
   for (std::size_t i = 0; i < count; ++i) {
     if (std::abs(grid[i].im) > 1e-9 * std::max(1., std::abs(grid[i].re)))
@@ -451,17 +471,15 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     // Re(b_g^H Q b_g) are summed on the device in the host order (atoms, rows,
     // columns) with unfused products.
     const std::size_t entries = static_cast<std::size_t>(np_) * npw_;
-    Cx<double>* raw = nullptr;
-    SDFT_CUDA(cudaMalloc(&raw, sizeof(Cx<double>) * entries));
-    SDFT_CUDA(cudaMemcpy(raw, in.amplitudes, sizeof(Cx<double>) * entries, cudaMemcpyHostToDevice));
-    SDFT_CUDA(cudaMalloc(&b_, sizeof(Cx<double>) * entries));
-    double* diag = nullptr;
-    unsigned int* flag = nullptr;
-    SDFT_CUDA(cudaMalloc(&diag, sizeof(double) * 2 * npw_ + 16));
-    flag = reinterpret_cast<unsigned int*>(diag + 2 * npw_);
-    SDFT_CUDA(cudaMemcpy(diag, h_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice));
-    SDFT_CUDA(cudaMemcpy(diag + npw_, s_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice));
-    SDFT_CUDA(cudaMemset(flag, 0, sizeof(unsigned int)));
+    const cudaStream_t st = ctx.stream;
+    Cx<double>* raw = static_cast<Cx<double>*>(stream_alloc(sizeof(Cx<double>) * entries, st));
+    SDFT_CUDA(cudaMemcpyAsync(raw, in.amplitudes, sizeof(Cx<double>) * entries, cudaMemcpyHostToDevice, st));
+    b_ = static_cast<Cx<double>*>(stream_alloc(sizeof(Cx<double>) * entries, st));
+    double* diag = static_cast<double*>(stream_alloc(sizeof(double) * 2 * npw_ + 16, st));
+    unsigned int* flag = reinterpret_cast<unsigned int*>(diag + 2 * npw_);
+    SDFT_CUDA(cudaMemcpyAsync(diag, h_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice, st));
+    SDFT_CUDA(cudaMemcpyAsync(diag + npw_, s_diag_.data(), sizeof(double) * npw_, cudaMemcpyHostToDevice, st));
+    SDFT_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), st));
     paw_prepare(raw, np_, npw_, atoms_, block_offsets_, block_storage_, d_, q_, b_, diag, diag + npw_, flag,
                 ctx.stream);
     unsigned int bad = 0;
@@ -470,8 +488,8 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
     SDFT_CUDA(cudaMemcpyAsync(s_diag_.data(), diag + npw_, sizeof(double) * npw_, cudaMemcpyDeviceToHost,
                               ctx.stream));
     SDFT_CUDA(cudaStreamSynchronize(ctx.stream));
-    cudaFree(raw);
-    cudaFree(diag);
+    stream_free(raw, st);
+    stream_free(diag, st);
     if (bad) throw InvalidArgument("nonfinite PAW projector/D/Q data");
     const Split split = search_split();
     pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
@@ -481,26 +499,29 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorInput& in) : ctx_(ctx
 }
 
 namespace {
+// Stream-ordered pool memory on `stream`; a pageable host source has been
+// staged when the copy call returns, so it may go out of scope.
 template <typename T>
-void upload_array(T*& dst, const std::vector<T>& src) {
-  SDFT_CUDA(cudaMalloc(reinterpret_cast<void**>(&dst), sizeof(T) * std::max<std::size_t>(1, src.size())));
-  if (!src.empty()) SDFT_CUDA(cudaMemcpy(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+void upload_array(T*& dst, const std::vector<T>& src, cudaStream_t stream) {
+  dst = static_cast<T*>(stream_alloc(sizeof(T) * std::max<std::size_t>(1, src.size()), stream));
+  if (!src.empty())
+    SDFT_CUDA(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, stream));
 }
 }  // namespace
 
 void DeviceOperator::upload_common(const int shape[3], const std::vector<Cx<double>>& d_blocks,
                                    const std::vector<Cx<double>>& q_blocks, const std::vector<int>& offsets,
                                    const std::vector<long long>& storage) {
-  plan_.build(shape, h_indices_);
-  upload_array(kinetic_, h_kinetic_);
-  upload_array(v64_, h_local_real_);
+  plan_.build(shape, h_indices_, ctx_.stream);
+  upload_array(kinetic_, h_kinetic_, ctx_.stream);
+  upload_array(v64_, h_local_real_, ctx_.stream);
   std::vector<float> v32(h_local_real_.begin(), h_local_real_.end());
-  upload_array(v32_, v32);
+  upload_array(v32_, v32, ctx_.stream);
   if (np_) {
-    upload_array(d_, d_blocks);
-    upload_array(q_, q_blocks);
-    upload_array(block_offsets_, offsets);
-    upload_array(block_storage_, storage);
+    upload_array(d_, d_blocks, ctx_.stream);
+    upload_array(q_, q_blocks, ctx_.stream);
+    upload_array(block_offsets_, offsets, ctx_.stream);
+    upload_array(block_storage_, storage, ctx_.stream);
   }
 }
 
@@ -536,7 +557,7 @@ DeviceOperator::DeviceOperator(Context& ctx, const OperatorSnapshot& snap) : ctx
   np_ = static_cast<int>(total);
   upload_common(snap.shape, snap.d, snap.q, offsets, storage);
   if (np_) {
-    upload_array(b_, snap.all_b);
+    upload_array(b_, snap.all_b, ctx_.stream);
     const Split split = search_split();
     pack_persistent(Op::N, b_, np_, np_, npw_, split, b_packed_, ctx.stream);
     pack_persistent(Op::C, b_, np_, npw_, np_, split, bh_packed_, ctx.stream);
@@ -698,7 +719,7 @@ DeviceOperator::~DeviceOperator() {
   for (void* p : {static_cast<void*>(kinetic_), static_cast<void*>(v64_), static_cast<void*>(v32_),
                   static_cast<void*>(b_), static_cast<void*>(d_), static_cast<void*>(q_),
                   static_cast<void*>(block_offsets_), static_cast<void*>(block_storage_)})
-    if (p) cudaFree(p);
+    stream_free(p, ctx_.stream);
 }
 
 std::size_t DeviceOperator::device_bytes() const {

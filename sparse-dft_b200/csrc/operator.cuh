@@ -79,7 +79,6 @@ struct CorrectionBuffers {
   Scratch coefficients;        // roots x count projections
   Scratch scalars;             // per column: theta, kinetic energy, two (res, z) slots, (p, q)
   Scratch index;               // selected roots
-  void release();
 };
 
 struct DavidsonBuffers {
@@ -92,7 +91,6 @@ struct DavidsonBuffers {
   Scratch polish;         // strict refinements: direction, trial and their images (n x roots each)
   Scratch polish_small;   // their roots x roots matrices
   Scratch polish_values;  // their per-root scalars
-  void release();
 };
 
 struct Context {
@@ -113,7 +111,15 @@ struct Context {
   Context(const Context&) = delete;
   Context& operator=(const Context&) = delete;
   void synchronize() const;
-  // Frees every scratch buffer (they grow again on demand).
+  // The grow-only working buffers (slabs, staging, Davidson and eigensolver
+  // state) and the identity-keyed caches; every one is stream-ordered pool
+  // memory on this context's stream.
+  std::vector<Scratch*> working_buffers();
+  std::vector<Scratch*> cache_buffers();
+  // Returns every working buffer to the library's pool, which keeps the
+  // memory for the next allocation (no device-wide synchronisation).
+  void recycle_scratch();
+  // recycle_scratch, then hands the pool's unused memory back to the device.
   void release_scratch();
 };
 

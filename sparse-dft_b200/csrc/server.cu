@@ -244,11 +244,11 @@ void SolveServer::worker(int slot) {
           }
           ctx->synchronize();
         }
-        ctx->release_scratch();
+        ctx->recycle_scratch();
       } catch (...) {
         result.status = status_of(std::current_exception(), result.error);
         try {
-          ctx->release_scratch();
+          ctx->recycle_scratch();
         } catch (...) {
         }
       }

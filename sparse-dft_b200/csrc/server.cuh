@@ -5,6 +5,10 @@
 // running. Every worker owns a context (stream, cuBLAS and cuSOLVER handles,
 // scratch), so admitted solves overlap on the device; a solve's result does
 // not depend on what else runs (same kernels, same inputs, own buffers).
+// A request's operator and working buffers are stream-ordered allocations
+// from the library's memory pool on the worker's stream: they return to the
+// pool when the request ends and serve the next request's allocations, so
+// no request start or end synchronises the device.
 #pragma once
 #include <chrono>
 #include <condition_variable>

@@ -713,12 +713,14 @@ void pack_persistent(Op aop, const Cx<double>* a, long long lda, int rows, int k
   out.rows = rows;
   out.k = k;
   out.split = split;
-  SDFT_CUDA(cudaMalloc(&out.data, sizeof(std::uint16_t) * static_cast<std::size_t>(out.ld) * rows));
+  out.stream = stream;
+  out.data = static_cast<std::uint16_t*>(
+      stream_alloc(sizeof(std::uint16_t) * static_cast<std::size_t>(out.ld) * rows, stream));
   pack_a(aop, a, lda, rows, k, split, out.data, out.ld, stream);
 }
 
 void release(PackedA& packed) {
-  if (packed.data) cudaFree(packed.data);
+  stream_free(packed.data, packed.stream);
   packed = PackedA{};
 }
 

@@ -71,6 +71,7 @@ struct PackedA {
   int rows = 0;
   int k = 0;
   Split split = Split::BF16x3;
+  cudaStream_t stream = nullptr;  // data is stream-ordered pool memory on this stream
 };
 
 struct TensorCoreWorkspace {

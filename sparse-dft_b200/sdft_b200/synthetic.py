@@ -199,9 +199,13 @@ def local_potential(lattice, reciprocal, positions, depths, ecut_ha, noise, nois
     noise_values = noise * (draws[:, 0] + 1j * draws[:, 1]) / math.sqrt(2.0)
     noise_values[zero] = noise * draws[zero, 0]
     values = values + np.where(positive | zero, noise_values, 0.0)
-    index = {tuple(key): i for i, key in enumerate(hkl.tolist())}
     negative = np.nonzero(~(positive | zero))[0]
-    partner = np.array([index[(-hkl[i, 0], -hkl[i, 1], -hkl[i, 2])] for i in negative], dtype=np.int64)
+    if np.array_equal(hkl[::-1], -hkl):
+        # A key set closed under G -> -G in lexicographic order lists -G at the mirrored position.
+        partner = hkl.shape[0] - 1 - negative
+    else:
+        index = {tuple(key): i for i, key in enumerate(hkl.tolist())}
+        partner = np.array([index[(-hkl[i, 0], -hkl[i, 1], -hkl[i, 2])] for i in negative], dtype=np.int64)
     values[negative] = np.conj(values[partner])
     values[zero] = values[zero].real
     return hkl.astype(np.int32), values.astype(np.complex128)
@@ -250,6 +254,17 @@ def overlap_minimum(amplitudes: np.ndarray, q_blocks: np.ndarray, regularization
     return _root_minimum(_gram_root(amplitudes), q_blocks, regularization)
 
 
+def _scale_q_linear(amplitudes, q_raw, regularization, floor=0.3):
+    """The scale of _scale_q in closed form: lambda_min((1+reg) I + s R Q R)
+    is (1+reg) + s mu for the lowest eigenvalue mu of R Q R, so one
+    eigenvalue solve gives the largest s <= 1 that keeps it at the floor."""
+    root = _gram_root(amplitudes)
+    rqr = root @ _block_diag(q_raw) @ root
+    mu = float(np.linalg.eigvalsh(0.5 * (rqr + rqr.conj().T)).min())
+    top = 1.0 + regularization
+    return 1.0 if top + mu >= floor else (floor - top) / mu
+
+
 def _scale_q(amplitudes, q_raw, regularization, floor=0.3):
     # The Gram root depends on B alone: formed once, not per bisection step
     # (each step's arithmetic is unchanged).
@@ -269,9 +284,14 @@ def _scale_q(amplitudes, q_raw, regularization, floor=0.3):
 def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, depths=(-2.0, -2.0),
                    kpoint=(0.0, 0.0, 0.0), seed: int = 2026, noise: float = 0.05, noise_cut: float = 4.0,
                    width: float = 1.0, tolerance: float = 1e-12, max_iterations: int = 256,
-                   regularization: float = 1e-12, sites=None) -> OperatorInputs:
+                   regularization: float = 1e-12, sites=None, potential=None,
+                   q_scaling: str = "bisection") -> OperatorInputs:
     """One synthetic H~/S~ pencil on an a*reps cubic zincblende/diamond supercell
-    (or on the given (fractional positions, species) sites of an a*reps cube)."""
+    (or on the given (fractional positions, species) sites of an a*reps cube).
+    potential: the (v_hkl, v_values) this call would draw (same cell, seed and
+    noise arguments), reused instead of recomputed; q_scaling: "bisection"
+    (the fixtures' inputs) or "linear" (_scale_q_linear, the same floor in
+    one eigenvalue solve)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     cell = a * reps
     lattice = np.eye(3) * cell
@@ -281,8 +301,12 @@ def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, d
                                                                         np.asarray(sites[1], dtype=np.int64))
     atom_depths = np.array([depths[s] for s in species], dtype=np.float64)
     hkl, cart, kinetic = enumerate_g_vectors(reciprocal, ecut_ha * HARTREE_TO_EV, kpoint)
-    v_hkl, v_values = local_potential(lattice, reciprocal, positions, atom_depths, ecut_ha, noise, noise_cut,
-                                      width, rng)
+    if potential is None:
+        v_hkl, v_values = local_potential(lattice, reciprocal, positions, atom_depths, ecut_ha, noise, noise_cut,
+                                          width, rng)
+    else:
+        v_hkl, v_values = potential
+        rng.standard_normal((v_hkl.shape[0], 2))  # the noise draws local_potential takes, so d and Q repeat
     kcart = np.asarray(kpoint, dtype=np.float64) @ reciprocal
     amplitudes = projector_amplitudes(cart, kcart, positions, lattice, volume)
     atoms = positions.shape[0]
@@ -290,7 +314,8 @@ def build_operator(name: str, a: float, reps: int, ecut_ha: float, roots: int, d
     d = 0.5 * (d + np.transpose(d, (0, 2, 1)))
     q_raw = rng.uniform(-0.5, 0.5, size=(atoms, 8, 8))
     q_raw = 0.5 * (q_raw + np.transpose(q_raw, (0, 2, 1)))
-    scale = _scale_q(amplitudes, q_raw.astype(np.complex128), regularization)
+    scale = (_scale_q_linear if q_scaling == "linear" else _scale_q)(amplitudes, q_raw.astype(np.complex128),
+                                                                     regularization)
     return OperatorInputs(name=name, lattice=lattice, reciprocal=reciprocal, volume=volume, positions=positions,
                           species=species, kpoint=np.asarray(kpoint, dtype=np.float64), ecut_ha=ecut_ha, hkl=hkl,
                           cartesian=cart, kinetic_ev=kinetic, v_hkl=v_hkl, v_values=v_values,
@@ -384,7 +409,8 @@ def serving_request(index: int, seed: int = 4242, atoms=(2, 128), ecut_ha=(10.0,
     """One request of the seeded serving stream: a cubic cell with a
     log-uniform atom count (random sites, two species), Ecut uniform in the
     range, bands = 1.25 x the occupied count (2 per atom) within [8, 320], and
-    1..8 k-points; returns one OperatorInputs per k-point."""
+    1..8 k-points; returns one OperatorInputs per k-point (Q scaled in
+    closed form, V(G) drawn once per cell)."""
     rng = np.random.Generator(np.random.PCG64([seed, index]))
     count = int(round(math.exp(rng.uniform(math.log(atoms[0]), math.log(atoms[1])))))
     a = (count * SI_VOLUME_PER_ATOM) ** (1.0 / 3.0)
@@ -396,8 +422,10 @@ def serving_request(index: int, seed: int = 4242, atoms=(2, 128), ecut_ha=(10.0,
     out = []
     for j in range(nk):
         kpoint = tuple(float(v) for v in rng.uniform(-0.5, 0.5, size=3)) if j else (0.0, 0.0, 0.0)
+        potential = (out[0].v_hkl, out[0].v_values) if out else None  # V(G) is the cell's, not the k-point's
         out.append(build_operator(f"request{index}_k{j}", a, 1, ecut, bands, depths=(-2.2, -1.8), kpoint=kpoint,
-                                  seed=seed * 1000 + index, sites=(positions, species)))
+                                  seed=seed * 1000 + index, sites=(positions, species), potential=potential,
+                                  q_scaling="linear"))
     return out
 
 

@@ -7,8 +7,9 @@ each precision, no change in free device memory across calls after the
 first (set-up) call, a clear rejection of a block beyond the array (the
 largest accepted block is exactly the column limit the rejection names),
 calls for two operators with different grids interleaved on one stream (each
-rewrites the shared tables), and the rejection of host pointers before any
-launch."""
+rewrites the shared tables), the rejection of host pointers before any
+launch, and a call captured into a CUDA graph after the set-up call, replayed
+on new inputs, equal to the regular entry point."""
 import numpy as np
 import pytest
 
@@ -145,3 +146,33 @@ def test_noalloc_rejects_host_pointers_before_launch(si8_operator):
     assert status == _capi.INVALID_ARGUMENT
     assert _capi.library().sdft_b200_kernel_launches() == launches
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_noalloc_call_replays_from_a_cuda_graph(precision):
+    import torch
+    from sdft_b200 import synthetic
+    from sdft_b200.operator import Context, PlaneWaveOperator
+    stream = torch.cuda.Stream()
+    ctx = Context(0, stream.cuda_stream)
+    op = PlaneWaveOperator(ctx, synthetic.si8())
+    try:
+        x = _device_block(op.npw, 6, 31)
+        y = torch.empty((6, op.npw), dtype=torch.complex128, device="cuda").T
+        op.local_apply_noalloc(x, y, precision=precision)  # set-up call, outside the capture
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream, capture_error_mode="thread_local"):
+            op.local_apply_noalloc(x, y, precision=precision)
+        x.copy_(_device_block(op.npw, 6, 32))  # new inputs in the captured buffer
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        regular = op.local_apply(x, out=torch.empty((6, op.npw), dtype=torch.complex128, device="cuda").T,
+                                 precision=precision)
+        ctx.synchronize()
+        assert torch.equal(y, regular)
+        del graph
+    finally:
+        op.close()
+        ctx.close()
