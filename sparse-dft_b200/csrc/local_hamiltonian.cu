@@ -939,6 +939,91 @@ LocalArgs<T> make_args(const SpherePlan& plan) {
   return a;
 }
 
+// Plane passes through the slab in global memory, for planes whose two
+// shared-memory buffers do not fit (FP64 beyond ~118 points per axis, FP32
+// beyond ~167, or lengths without a compiled plane kernel whose two buffers
+// exceed the limit): scatter the sphere points into zeroed slab planes, then
+// the i2 transform of every row of every plane (tiled rows kernel) and the
+// i1 transform of every plane (strided kernel); plane_out runs the forward
+// transforms in the opposite order and gathers. Rows without sphere points
+// are transformed too (zeros): this path trades work for shared memory.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) slab_scatter_kernel(const Cx<double>* __restrict__ x, long long ldx,
+                                                                LocalArgs<T> a, Cx<T>* __restrict__ slab) {
+  const int s = blockIdx.x, c = blockIdx.y;
+  Cx<T>* plane = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
+  for (long long i = threadIdx.x; i < a.n12; i += blockDim.x) plane[i] = Cx<T>{0, 0};
+  __syncthreads();  // the zeros are in place before any point lands
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  for (int p = a.point_offset[s] + threadIdx.x; p < a.point_offset[s + 1]; p += blockDim.x) {
+    const int at = a.point_smem[p], i1 = at / a.n2p, i2 = at - i1 * a.n2p;
+    plane[static_cast<long long>(i1) * a.n2 + i2] = cconvert<T>(xc[a.point_g[p]]);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) slab_gather_kernel(const Cx<T>* __restrict__ slab, LocalArgs<T> a,
+                                                               const Cx<double>* __restrict__ x, long long ldx,
+                                                               const double* __restrict__ kinetic, double count,
+                                                               Cx<double>* __restrict__ y, long long ldy) {
+  const int s = blockIdx.x, c = blockIdx.y;
+  const Cx<T>* plane = slab + (static_cast<long long>(c) * a.slots + s) * a.n12;
+  const Cx<double>* xc = x + static_cast<long long>(c) * ldx;
+  Cx<double>* yc = y + static_cast<long long>(c) * ldy;
+  for (int p = a.point_offset[s] + threadIdx.x; p < a.point_offset[s + 1]; p += blockDim.x) {
+    const int g = a.point_g[p], at = a.point_smem[p], i1 = at / a.n2p, i2 = at - i1 * a.n2p;
+    const Cx<double> v = cconvert<double>(plane[static_cast<long long>(i1) * a.n2 + i2]);
+    const Cx<double> in_g = xc[g];
+    const double t = kinetic[g];
+    yc[g] = Cx<double>{t * in_g.re + v.re / count, t * in_g.im + v.im / count};
+  }
+}
+
+// Rows of the slab planes along i2 (contiguous), tiles of the widest TR in
+// {32, 16, 8} that fits.
+template <typename T, bool INV>
+void slab_rows(const LocalArgs<T>& a, int columns, Cx<T>* slab, cudaStream_t stream) {
+  const int np = a.n2 | 1;
+  const long long rows = static_cast<long long>(columns) * a.slots * a.n1;
+  auto go = [&](auto tile) {
+    constexpr int TR = decltype(tile)::value;
+    const std::size_t smem = sizeof(Cx<T>) * (a.n2 + 2 * static_cast<std::size_t>(TR) * np);
+    if (smem > kMaxDynamicSmem) return false;
+    allow_smem(fft_rows_kernel<T, INV, TR, false>, smem);
+    fft_rows_kernel<T, INV, TR, false><<<static_cast<unsigned>(ceil_div(rows, TR)), kThreads, smem, stream>>>(
+        slab, a.n2, np, rows, a.p2, a.tw2);
+    SDFT_LAUNCH("fft_rows_kernel slab planes");
+    return true;
+  };
+  if (!go(std::integral_constant<int, 32>{}) && !go(std::integral_constant<int, 16>{}) &&
+      !go(std::integral_constant<int, 8>{}))
+    throw InvalidArgument("FFT tile does not fit in shared memory");
+}
+
+// Columns of the slab planes along i1 (stride n2), TL lines per tile.
+template <typename T, bool INV>
+void slab_columns(const LocalArgs<T>& a, int columns, Cx<T>* slab, cudaStream_t stream) {
+  const long long planes = static_cast<long long>(columns) * a.slots;
+  auto go = [&](auto tile) {
+    constexpr int TL = decltype(tile)::value;
+    const std::size_t smem = sizeof(Cx<T>) * (a.n1 + 2 * static_cast<std::size_t>(a.n1) * (TL + 1));
+    if (smem > kMaxDynamicSmem) return false;
+    allow_smem(fft_strided_kernel<T, INV, TL, false>, smem);
+    // One plane per blockIdx.y, in launches of at most 65535 planes.
+    for (long long first = 0; first < planes; first += 65535) {
+      const dim3 blocks(static_cast<unsigned>(ceil_div(a.n2, TL)),
+                        static_cast<unsigned>(std::min<long long>(65535, planes - first)));
+      fft_strided_kernel<T, INV, TL, false><<<blocks, kThreads, smem, stream>>>(slab + first * a.n12, a.n1, a.n2,
+                                                                               a.n2, a.n12, a.p1, a.tw1);
+      SDFT_LAUNCH("fft_strided_kernel slab planes");
+    }
+    return true;
+  };
+  if (!go(std::integral_constant<int, 32>{}) && !go(std::integral_constant<int, 16>{}) &&
+      !go(std::integral_constant<int, 8>{}))
+    throw InvalidArgument("FFT tile does not fit in shared memory");
+}
+
 // The three passes: plane_in, pencil (V(r) multiply) and plane_out, each
 // with its compile-time kernel where the lengths have one.
 template <typename T>
@@ -948,11 +1033,19 @@ void run_local_passes(const SpherePlan& plan, const LocalArgs<T>& a, double coun
   const std::size_t plane_smem = sizeof(Cx<T>) * (a.n1 + a.n2 + 2 * static_cast<std::size_t>(a.n1) * a.n2p);
   const std::size_t pencil_smem = sizeof(Cx<T>) * (a.n0 + 2 * static_cast<std::size_t>(a.n0) * (kPencilLines + 1));
   const dim3 planes(a.slots, columns);
+  const bool planes_fit = plane_smem <= kMaxDynamicSmem;
   if (!launch_planes_pair<T>(plan, a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream) &&
       !launch_planes_fixed<T>(a, true, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
-    allow_smem(plane_in_kernel<T>, plane_smem);
-    plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
-    SDFT_LAUNCH("plane_in_kernel");
+    if (planes_fit) {
+      allow_smem(plane_in_kernel<T>, plane_smem);
+      plane_in_kernel<T><<<planes, kThreads, plane_smem, stream>>>(x, ldx, a, slab);
+      SDFT_LAUNCH("plane_in_kernel");
+    } else {
+      slab_scatter_kernel<T><<<planes, kThreads, 0, stream>>>(x, ldx, a, slab);
+      SDFT_LAUNCH("slab_scatter_kernel");
+      slab_rows<T, true>(a, columns, slab, stream);
+      slab_columns<T, true>(a, columns, slab, stream);
+    }
   }
   if (!launch_pencil_registers<T>(plan, columns, potential, slab, stream) &&
       !launch_pencil_fixed<T>(a, columns, potential, slab, stream)) {
@@ -963,9 +1056,16 @@ void run_local_passes(const SpherePlan& plan, const LocalArgs<T>& a, double coun
   }
   if (!launch_planes_pair<T>(plan, a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream) &&
       !launch_planes_fixed<T>(a, false, columns, x, ldx, slab, kinetic, count, y, ldy, stream)) {
-    allow_smem(plane_out_kernel<T>, plane_smem);
-    plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
-    SDFT_LAUNCH("plane_out_kernel");
+    if (planes_fit) {
+      allow_smem(plane_out_kernel<T>, plane_smem);
+      plane_out_kernel<T><<<planes, kThreads, plane_smem, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
+      SDFT_LAUNCH("plane_out_kernel");
+    } else {
+      slab_columns<T, false>(a, columns, slab, stream);
+      slab_rows<T, false>(a, columns, slab, stream);
+      slab_gather_kernel<T><<<planes, kThreads, 0, stream>>>(slab, a, x, ldx, kinetic, count, y, ldy);
+      SDFT_LAUNCH("slab_gather_kernel");
+    }
   }
 }
 

@@ -250,31 +250,33 @@ __global__ void __launch_bounds__(kThreads, 1)
 // the splits summed in order with two interleaved accumulators.
 __global__ void reduce_splits_kernel(int m, int n, int splits, const Cx<float>* __restrict__ partial,
                                      Cx<double>* __restrict__ c, long long ldc, bool add, double alpha) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   const long long total = static_cast<long long>(m) * n;
-  const Cx<float>* p = partial + static_cast<long long>(j) * m + i;
-  double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
-  int s = 0;
-  for (; s + 1 < splits; s += 2) {
-    const Cx<float> a = p[s * total], b = p[(s + 1) * total];
-    re0 += a.re;
-    im0 += a.im;
-    re1 += b.re;
-    im1 += b.im;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const Cx<float>* p = partial + static_cast<long long>(j) * m + i;
+    double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+    int s = 0;
+    for (; s + 1 < splits; s += 2) {
+      const Cx<float> a = p[s * total], b = p[(s + 1) * total];
+      re0 += a.re;
+      im0 += a.im;
+      re1 += b.re;
+      im1 += b.im;
+    }
+    if (s < splits) {
+      const Cx<float> a = p[s * total];
+      re0 += a.re;
+      im0 += a.im;
+    }
+    double re = (re0 + re1) * alpha, im = (im0 + im1) * alpha;
+    Cx<double>& out = c[i + static_cast<long long>(j) * ldc];
+    if (add) {
+      re += out.re;
+      im += out.im;
+    }
+    out = Cx<double>{re, im};
   }
-  if (s < splits) {
-    const Cx<float> a = p[s * total];
-    re0 += a.re;
-    im0 += a.im;
-  }
-  double re = (re0 + re1) * alpha, im = (im0 + im1) * alpha;
-  Cx<double>& out = c[i + static_cast<long long>(j) * ldc];
-  if (add) {
-    re += out.re;
-    im += out.im;
-  }
-  out = Cx<double>{re, im};
 }
 
 // ---- packing (FP64 complex -> BF16 split terms) ---------------------------
@@ -332,18 +334,20 @@ template <int P, bool CONJ_T>
 __global__ void pack_a_direct_kernel(const Cx<double>* __restrict__ src, long long lds, int rows, int k,
                                      std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
   // CONJ_T: A[i,k] = conj(src[k + i*lds]) (k contiguous in the source).
-  const int i = blockIdx.y;
-  const Cx<double>* in = src + static_cast<long long>(i) * lds;
-  std::uint16_t* row = out + static_cast<long long>(i) * ldo;
-  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
-    Cx<double> v = in[kk];
-    if (CONJ_T) v.im = -v.im;
-    write_a<P>(row + static_cast<long long>(kk) * 2 * P, v);
+  // Rows i = blockIdx.y, blockIdx.y + gridDim.y, ... (any row count).
+  for (int i = blockIdx.y; i < rows; i += gridDim.y) {
+    const Cx<double>* in = src + static_cast<long long>(i) * lds;
+    std::uint16_t* row = out + static_cast<long long>(i) * ldo;
+    for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
+      Cx<double> v = in[kk];
+      if (CONJ_T) v.im = -v.im;
+      write_a<P>(row + static_cast<long long>(kk) * 2 * P, v);
+    }
+    // zero padding [2Pk, kexp) of the row
+    for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
+         q += static_cast<long long>(gridDim.x) * blockDim.x)
+      row[q] = 0;
   }
-  // zero padding [2Pk, kexp) of the row
-  for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
-       q += static_cast<long long>(gridDim.x) * blockDim.x)
-    row[q] = 0;
 }
 
 // A[i,k] = src[i + k*lds] (rows contiguous): 32x32 shared-memory transpose.
@@ -373,35 +377,40 @@ __global__ void zero_pad_kernel(std::uint16_t* __restrict__ out, long long ldo, 
     out[(idx / pad) * ldo + from + idx % pad] = 0;
 }
 
-// One source column j per blockIdx.y (two expanded rows); threads stride over k.
+// Source columns j = blockIdx.y, blockIdx.y + gridDim.y, ... (two expanded
+// rows each); threads stride over k.
 template <int P>
 __global__ void pack_b_kernel(const Cx<double>* __restrict__ src, long long ldb, int k, int n,
                               std::uint16_t* __restrict__ out, long long ldo, long long kexp) {
-  const int j = blockIdx.y;
-  const Cx<double>* in = src + static_cast<long long>(j) * ldb;
-  std::uint16_t* row0 = out + (2LL * j) * ldo;
-  std::uint16_t* row1 = row0 + ldo;
-  for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
-    const Cx<double> v = in[kk];
-    std::uint16_t re[3], im[3];
-    split3(v.re, re);
-    split3(v.im, im);
-    std::uint32_t p0[P], p1[P];
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const Cx<double>* in = src + static_cast<long long>(j) * ldb;
+    std::uint16_t* row0 = out + (2LL * j) * ldo;
+    std::uint16_t* row1 = row0 + ldo;
+    for (int kk = blockIdx.x * blockDim.x + threadIdx.x; kk < k; kk += gridDim.x * blockDim.x) {
+      const Cx<double> v = in[kk];
+      std::uint16_t re[3], im[3];
+      split3(v.re, re);
+      split3(v.im, im);
+      std::uint32_t p0[P], p1[P];
 #pragma unroll
-    for (int p = 0; p < P; ++p) {
-      const int t = term_b(p);
-      p0[p] = pair(re[t], im[t] ^ 0x8000u);  // [Re, -Im] (sign flip is exact)
-      p1[p] = pair(im[t], re[t]);            // [Im, Re]
+      for (int p = 0; p < P; ++p) {
+        const int t = term_b(p);
+        p0[p] = pair(re[t], im[t] ^ 0x8000u);  // [Re, -Im] (sign flip is exact)
+        p1[p] = pair(im[t], re[t]);            // [Im, Re]
+      }
+      store_pairs<P>(row0 + static_cast<long long>(kk) * 2 * P, p0);
+      store_pairs<P>(row1 + static_cast<long long>(kk) * 2 * P, p1);
     }
-    store_pairs<P>(row0 + static_cast<long long>(kk) * 2 * P, p0);
-    store_pairs<P>(row1 + static_cast<long long>(kk) * 2 * P, p1);
-  }
-  for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
-       q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    row0[q] = 0;
-    row1[q] = 0;
+    for (long long q = 2LL * P * k + blockIdx.x * blockDim.x + threadIdx.x; q < kexp;
+         q += static_cast<long long>(gridDim.x) * blockDim.x) {
+      row0[q] = 0;
+      row1[q] = 0;
+    }
   }
 }
+
+// Largest gridDim.y; kernels that put rows or columns on y stride past it.
+constexpr int kMaxGridY = 65535;
 
 // Blocks along a row of `length` entries when `rows` rows run side by side:
 // enough CTAs in total for ~16 per SM, at least one per row.
@@ -472,8 +481,8 @@ void pack_a(Op aop, const Cx<double>* src, long long lds, int rows, int k, Split
             long long ldo, cudaStream_t stream) {
   const long long kexp = expanded_k(k, split);
   if (aop == Op::C) {
-    if (rows > 65535) throw InvalidArgument("packed operand has more than 65535 rows");
-    const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), rows), rows);
+    const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), rows),
+                    static_cast<unsigned>(std::min(rows, kMaxGridY)));
     if (split == Split::BF16x3)
       pack_a_direct_kernel<3, true><<<grid, 256, 0, stream>>>(src, lds, rows, k, out, ldo, kexp);
     else
@@ -510,8 +519,8 @@ void pack_a_columns(const Cx<double>* src, long long lds, int rows, int first, i
 void pack_b(const Cx<double>* src, long long ldb, int k, int n, Split split, std::uint16_t* out, long long ldo,
             cudaStream_t stream) {
   const long long kexp = expanded_k(k, split);
-  if (n > 65535) throw InvalidArgument("packed operand has more than 65535 columns");
-  const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), n), n);
+  const dim3 grid(row_blocks(std::max<long long>(k, kexp - 2LL * split_terms(split) * k), n),
+                  static_cast<unsigned>(std::min(n, kMaxGridY)));
   if (split == Split::BF16x3) pack_b_kernel<3><<<grid, 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
   else pack_b_kernel<6><<<grid, 256, 0, stream>>>(src, ldb, k, n, out, ldo, kexp);
   SDFT_LAUNCH("pack_b_kernel");
@@ -573,8 +582,8 @@ void run_config(const std::uint16_t* a, long long lda, const std::uint16_t* b, l
   else if (bn == 160) launch<160>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   else launch<128>(a, lda, b, ldb, m, n2, kexp, ep, splits, k_blocks, kpb, stream);
   if (splits > 1) {
-    if (n > 65535) throw InvalidArgument("split-K reduction has more than 65535 columns");
-    reduce_splits_kernel<<<dim3(static_cast<unsigned>(ceil_div(m, 256)), static_cast<unsigned>(n)), 256, 0, stream>>>(
+    reduce_splits_kernel<<<dim3(static_cast<unsigned>(ceil_div(m, 256)), static_cast<unsigned>(std::min(n, kMaxGridY))),
+                           256, 0, stream>>>(
         m, n, splits, ep.partial, c, ldc, add, alpha);
     SDFT_LAUNCH("reduce_splits_kernel");
   }
