@@ -309,7 +309,8 @@ def run_b200(args):
     serving_rows = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving_rows = serving_stream(local, requests=args.serving_requests,
-                                      forms=("mixed",) if args.serving_mixed_only else ("mixed", "fp64"))
+                                      forms=("mixed",) if args.serving_mixed_only else ("mixed", "fp64"),
+                                      log=args.serving_log)
 
     kpoint_rows = None
     if rank == 0 and world == 1 and not args.no_kpoints:
@@ -531,7 +532,7 @@ def _serving_request(index, seed):
 
 
 def serving_stream(device, requests=8, slots=4, rate_hz=1.0, cap=150e9, seed=4242, forms=("mixed", "fp64"),
-                   generators=8):
+                   generators=8, log=None):
     """A sample of the seeded serving stream through the solve server: the
     first `requests` requests of the config-4 stream (cubic cells of 2-128
     atoms drawn log-uniformly, Ecut U(10, 25) Ha, bands 1.25x occupied within
@@ -542,7 +543,9 @@ def serving_stream(device, requests=8, slots=4, rate_hz=1.0, cap=150e9, seed=424
     first 2 x `generators` are built); a request submitted after its
     arrival time because its inputs were not ready yet counts as
     generation-paced (its latency is measured from its submission).
-    Latency = finish of a request's last k-point - submission of its first."""
+    Latency = finish of a request's last k-point - submission of its first.
+    log: a path that receives one JSON line per request as its last k-point
+    finishes (a long sample leaves its partial results there)."""
     import concurrent.futures
     import multiprocessing
     import numpy as np
@@ -574,7 +577,18 @@ def serving_stream(device, requests=8, slots=4, rate_hz=1.0, cap=150e9, seed=424
                 kpoints.append(len(ops))
                 tickets.append([server.submit(x, precision=precision) for x in ops])
                 del ops
-            results = [[server.wait(t) for t in group] for group in tickets]
+            results = []
+            for i, group in enumerate(tickets):
+                results.append([server.wait(t) for t in group])
+                if log:
+                    with open(log, "a") as f:
+                        done = results[-1]
+                        f.write(json.dumps({"form": precision, "request": i, "atoms": atoms[i],
+                                            "kpoints": kpoints[i],
+                                            "latency_ms": 1e3 * (max(r["timing"]["finished"] for r in done) -
+                                                                 min(r["timing"]["submitted"] for r in done)),
+                                            "certified": int(sum(np.sum(r["residuals"] <= TOLERANCE) for r in done)),
+                                            "converged": all(r["converged"] for r in done)}) + "\n")
             makespan = time.perf_counter() - t0 - arrivals[0]
             memory = server.memory()
         latency = [1e3 * (max(r["timing"]["finished"] for r in group) - min(r["timing"]["submitted"] for r in group))
@@ -774,6 +788,7 @@ def main():
                         help="requests of the serving-stream sample (the stream has 2000)")
     parser.add_argument("--serving-mixed-only", action="store_true",
                         help="run the serving sample in the mixed form only")
+    parser.add_argument("--serving-log", help="file that receives one JSON line per finished serving request")
     parser.add_argument("--all-kpoints", action="store_true", help="all 27 k-points of the GaAs64 batch (default: 4)")
     parser.add_argument("--case", choices=["local", "pair", "project", "density", "pbe", "compensation"],
                         help="run a few launches of one kernel family for a profiler capture and exit")
