@@ -578,9 +578,16 @@ template <int N>
 constexpr int plane_pair_threads() {
   return (N + 15) / 16 * kWarp;
 }
+// Resident CTAs per SM the pair plane kernels are compiled for: four up to
+// 80 points (at most 96-128 registers a thread, no spills), two above (the
+// 192-thread CTAs of 84-96 points would spill at a four-CTA bound).
+template <int N>
+constexpr int plane_pair_blocks() {
+  return N <= 80 ? 4 : 2;
+}
 
 template <int N>
-__global__ void __launch_bounds__(plane_pair_threads<N>()) plane_in_pair_kernel(
+__global__ void __launch_bounds__(plane_pair_threads<N>(), plane_pair_blocks<N>()) plane_in_pair_kernel(
     const Cx<double>* __restrict__ x, long long ldx, LocalArgs<float> a, Cx<float>* __restrict__ slab,
     const __grid_constant__ PlanePairArgs<N> p) {
   constexpr int H = N / 2;
@@ -650,7 +657,7 @@ __global__ void __launch_bounds__(plane_pair_threads<N>()) plane_in_pair_kernel(
 }
 
 template <int N>
-__global__ void __launch_bounds__(plane_pair_threads<N>()) plane_out_pair_kernel(
+__global__ void __launch_bounds__(plane_pair_threads<N>(), plane_pair_blocks<N>()) plane_out_pair_kernel(
     const Cx<float>* __restrict__ slab, LocalArgs<float> a, const Cx<double>* __restrict__ x, long long ldx,
     const double* __restrict__ kinetic, double count, Cx<double>* __restrict__ y, long long ldy,
     const __grid_constant__ PlanePairArgs<N> p) {

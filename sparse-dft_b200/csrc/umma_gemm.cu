@@ -708,8 +708,8 @@ std::size_t gemm_tuned_classes(std::size_t capacity, int* rows) {
 Split search_split() {
   static const Split split = [] {
     const char* v = std::getenv("SDFT_B200_SPLIT");
-    if (!v || std::string(v) == "x6") return Split::BF16x6;
-    if (std::string(v) == "x3") return Split::BF16x3;
+    if (!v || std::string(v) == "x3") return Split::BF16x3;
+    if (std::string(v) == "x6") return Split::BF16x6;
     throw InvalidArgument("SDFT_B200_SPLIT must be x3 or x6");
   }();
   return split;

@@ -79,7 +79,8 @@ struct TensorCoreWorkspace {
   Scratch adjoint;  // a right operand formed as B^H for the tensor-core path
 };
 
-// Search-precision split (SDFT_B200_SPLIT=x3|x6, default x6), read once.
+// Search-precision split (SDFT_B200_SPLIT=x3|x6, default x3: on the Si64
+// pencil its mixed-apply error is that of the FP32 FFTs, 5e-7), read once.
 Split search_split();
 
 // Packs op(A) (rows x k) into a new device buffer owned by `out`.
