@@ -68,7 +68,18 @@ SDFT_B200_API sdft_b200_status sdft_b200_gemm_tuned_classes(size_t capacity, int
  * private non-blocking stream is created) or a cudaStream_t to share.
  * Replaces: make_cuda_accelerator() / class Accelerator, src/compute_backend.hpp:64-91. */
 SDFT_B200_API sdft_b200_status sdft_b200_context_create(int device, void* stream, sdft_b200_context** out);
+/* Destroying a context releases its buffers and hands the library's unused
+ * pooled device memory back to the device. */
 SDFT_B200_API sdft_b200_status sdft_b200_context_destroy(sdft_b200_context* context);
+/* Device memory of operators, plans and working buffers is stream-ordered
+ * memory from one library pool per device; freed blocks stay in the pool for
+ * the next allocation (creating and destroying operators then never
+ * synchronises the device). This call waits for the context's stream, frees
+ * its working buffers (they grow again on demand) and hands every unused
+ * block of the pool back to the device, for callers that want the memory for
+ * another allocator. Live operators and other contexts keep theirs.
+ * No reference counterpart (the reference's accelerator frees on destruction). */
+SDFT_B200_API sdft_b200_status sdft_b200_context_release_memory(sdft_b200_context* context);
 SDFT_B200_API sdft_b200_status sdft_b200_context_synchronize(sdft_b200_context* context);
 
 /* Plane-wave sphere 1/2|G+k|^2 <= cutoff_ev, sorted by (kinetic, h, k, l);

@@ -224,6 +224,14 @@ sdft_b200_status sdft_b200_context_destroy(sdft_b200_context* context) {
   return guarded([&] { delete context; });
 }
 
+sdft_b200_status sdft_b200_context_release_memory(sdft_b200_context* context) {
+  return guarded([&] {
+    require(context != nullptr, "null context");
+    SDFT_CUDA(cudaSetDevice(context->impl->device));
+    context->impl->release_scratch();
+  });
+}
+
 sdft_b200_status sdft_b200_context_synchronize(sdft_b200_context* context) {
   return guarded([&] {
     require(context != nullptr, "null context");

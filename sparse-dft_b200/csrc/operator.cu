@@ -167,6 +167,15 @@ Context::~Context() {
   release(accel.b_packed);
   release(accel.bh_packed);
   for (ImmutableLeft& entry : immutable.entries) release(entry.packed);
+  // The frees above are stream-ordered: once they have run, the pool's
+  // unused memory goes back to the device (a torn-down context leaves
+  // nothing reserved beyond what other live objects hold).
+  if (cudaStreamSynchronize(stream) == cudaSuccess && cudaSetDevice(device) == cudaSuccess) {
+    try {
+      trim_pool();
+    } catch (...) {
+    }
+  }
   if (solver) cusolverDnDestroy(solver);
   if (blas) cublasDestroy(blas);
   if (owns_stream && stream) cudaStreamDestroy(stream);
@@ -207,6 +216,7 @@ void Context::recycle_scratch() {
 
 void Context::release_scratch() {
   recycle_scratch();
+  synchronize();  // the stream-ordered frees have run: their blocks are unused
   trim_pool();
 }
 

@@ -142,6 +142,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     fn("sdft_b200_context_create", [ctypes.c_int, P, ctypes.POINTER(P)])
     fn("sdft_b200_context_destroy", [P])
     fn("sdft_b200_context_synchronize", [P])
+    fn("sdft_b200_context_release_memory", [P])
     fn("sdft_b200_enumerate_g_vectors", [D, ctypes.c_double, D, ctypes.c_double, I32, D, D, SZ, SZP])
     fn("sdft_b200_operator_create", [P, SZ, I32, D, SZ, I32, D, SZ, U64, D, D, D, ctypes.c_double, ctypes.c_double,
                                      ctypes.POINTER(P)])

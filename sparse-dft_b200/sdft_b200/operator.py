@@ -43,6 +43,11 @@ class Context:
     def synchronize(self) -> None:
         C.check(self._lib.sdft_b200_context_synchronize(self.handle))
 
+    def release_memory(self) -> None:
+        """Frees this context's working buffers and hands the library pool's
+        unused device memory back to the device (sdft_b200_context_release_memory)."""
+        C.check(self._lib.sdft_b200_context_release_memory(self.handle))
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self._lib.sdft_b200_context_destroy(self.handle)

@@ -120,3 +120,33 @@ def test_construction_rejects_invalid_inputs(context):
     with pytest.raises(C.InvalidArgument, match="nonfinite"):
         PlaneWaveOperator(context, nan)
     PlaneWaveOperator(context, base)  # the context stays usable after rejected inputs
+
+
+def test_release_memory_hands_pooled_memory_back():
+    """Operator arrays and working buffers are stream-ordered pool memory:
+    after the operator closes they stay reserved in the library's pool (the
+    next operator reuses them without synchronising the device), and
+    Context.release_memory hands them back to the device."""
+    import torch
+    from sdft_b200 import synthetic
+    from sdft_b200.operator import Context
+    ctx = Context(0)
+    op = PlaneWaveOperator(ctx, synthetic.si8())
+    columns = 2000
+    x = torch.from_numpy(np.ascontiguousarray(probe_block(op.npw, columns, 11).T)).cuda().T
+    y = torch.empty((columns, op.npw), dtype=torch.complex128, device="cuda").T
+    op.local_apply(x, out=y, precision="fp64")  # cuBLAS and other lazy set-up happen here
+    ctx.release_memory()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    op.local_apply(x, out=y, precision="fp64")  # the FP64 slab: slots x n1 x n2 x 2000 x 16 B
+    ctx.synchronize()
+    op.close()
+    held = free_before - torch.cuda.mem_get_info()[0]
+    ctx.release_memory()
+    returned = torch.cuda.mem_get_info()[0] - (free_before - held)
+    try:
+        assert held > 256 * 2**20  # the slab stayed in the pool after close
+        assert returned >= held - 64 * 2**20
+    finally:
+        ctx.close()
